@@ -1,0 +1,665 @@
+// esr_device.cuh -- device numerics and kernels of the explicit FVM solve.
+//
+// Every formula restates the EulerSR JAX solver (citations are paths inside
+// the EulerSR checkout) with its evaluation order, so float32/float64 results
+// track the reference's rounding; the data layout and the kernel split are
+// this project's own:
+//
+//   state      W[item], item = seg.off + cell * B + slot  (one float4/double4
+//              per cell and case, cases of one mesh innermost so a warp of a
+//              batched mesh walks 32 cases of the same cell: every geometry
+//              load is a broadcast and every branch on boundary type uniform)
+//   geometry   per mesh, structure of arrays geo[field * stride + cell]
+//   K1 recon   cell + 3 neighbour primitives, LSQ gradient, Venkatakrishnan
+//              limiter, the 3 MUSCL face states of the cell -> FV[k][item]
+//   K2 flux    per cell: the 3 face fluxes (HLLC or Rusanov) from its own
+//              face states and its neighbours' face states on the shared
+//              faces, sum / area, sponge, Runge-Kutta stage update. Each cell
+//              owns its residual (no atomics); the sum order is fixed.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "esr_layout.h"
+
+namespace esr {
+
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { using type = double4; };
+template <typename T> using V4 = typename Vec4<T>::type;
+
+template <typename T> __host__ __device__ inline V4<T> mk4(T a, T b, T c, T d) {
+  V4<T> r; r.x = a; r.y = b; r.z = c; r.w = d; return r;
+}
+
+template <typename T>
+struct Seg {                 // one mesh and its B case slots
+  int n_cells;
+  int B;                     // case slots on this mesh
+  int case0;                 // global slot index of slot 0
+  int geo_stride;
+  long long off;             // first item of this segment in the state arrays
+  const int4* nbr;           // x,y,z neighbour cell (-1 boundary), w packed slot info
+  const T* geo;              // G_COUNT * geo_stride
+  const int* wall_cell;      // force faces: owner cell
+  const T* wall_nx;          // owner's outward unit normal
+  const T* wall_ny;
+  const T* wall_ds;          // face length
+  int n_wall;
+  int pad;
+};
+
+template <typename T>
+struct Consts {
+  T gamma, gm1;              // run gamma and gamma - 1 rounded from double
+  T gm1_14;                  // 1.4 - 1 (wall ghost and forces use gamma 1.4)
+  T half, eps_lim, venk_eps; // 0.5, limiter threshold, Venkatakrishnan 1e-7
+  T ss_eps, den_eps;         // HLLC 1e-6 wave-speed split, 1e-12 denominator guard
+  T sub_rho, sub_u, sub_v;   // subsonic inlet primitives
+};
+
+template <typename T>
+struct Cases {               // per global slot
+  const T* dt;
+  const V4<T>* inlet;        // conserved inlet state
+  const T* strength;         // sponge strength (|U_inf| + a_inf) / width
+  const int* active;
+  const int* step;           // steps done at the start of the current chunk
+  const int* nmax;
+};
+
+// ----------------------------------------------------------- conversions
+// helper.py:37-46 getPrimitive (M = 1)
+template <typename T>
+__device__ __forceinline__ void prim(const V4<T>& W, T gm1, T half, T P[4]) {
+  T r = W.x;
+  T u = W.y / r;
+  T v = W.z / r;
+  P[0] = r; P[1] = u; P[2] = v;
+  P[3] = (W.w - half * r * (u * u + v * v)) * gm1;
+}
+// helper.py:25-35 getConserved (M = 1)
+template <typename T>
+__device__ __forceinline__ V4<T> cons(const T P[4], T gm1, T half) {
+  T r = P[0], u = P[1], v = P[2];
+  return mk4<T>(r, r * u, r * v, P[3] / gm1 + half * r * (u * u + v * v));
+}
+
+// helper.py:196-204 slip wall ghost (gamma 1.4, background value 0)
+template <typename T>
+__device__ __forceinline__ V4<T> wall_ghost(const V4<T>& Wc, T nx, T ny, const Consts<T>& k) {
+  T P[4];
+  prim<T>(Wc, k.gm1_14, k.half, P);
+  T vn = P[1] * nx + P[2] * ny;
+  T Q[4] = {P[0], P[1] - T(2) * vn * nx, P[2] - T(2) * vn * ny, P[3]};
+  return cons<T>(Q, k.gm1_14, k.half);
+}
+// helper.py:179-194 subsonic inlet ghost: rho,u,v imposed, p from the cell (gamma 1.4)
+template <typename T>
+__device__ __forceinline__ V4<T> subsonic_ghost(const V4<T>& Wc, const Consts<T>& k) {
+  T P[4];
+  prim<T>(Wc, k.gm1_14, k.half, P);
+  T Q[4] = {k.sub_rho, k.sub_u, k.sub_v, P[3]};
+  return cons<T>(Q, k.gm1_14, k.half);
+}
+// helper.py:233-256 BC_state for one boundary slot (conserved ghost)
+template <typename T>
+__device__ __forceinline__ V4<T> ghost_cons(int kind, const V4<T>& Wc, T nx, T ny, const V4<T>& inlet,
+                                            const Consts<T>& k) {
+  if (kind == K_WALL) return wall_ghost<T>(Wc, nx, ny, k);
+  if (kind == K_INLET) return inlet;
+  if (kind == K_SUBSONIC) return subsonic_ghost<T>(Wc, k);
+  return Wc;  // outlet
+}
+
+// euler_solver.py:36-39 Venkatakrishnan with K = 0
+template <typename T>
+__device__ __forceinline__ T venkat(T a, T b, T eps) {
+  return (a * a + T(2) * a * b) / (a * a + T(2) * b * b + a * b + eps);
+}
+
+// ------------------------------------------------------------------ fluxes
+// euler_solver.py:376-420 getFlux with the HLLC dissipation of :273-374;
+// returns Fc - (Fc - F_HLLC) exactly as the reference assembles it.
+template <typename T>
+__device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
+                                     T nx, T ny, const Consts<T>& k, T F[4]) {
+  const T rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
+  const T rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
+  const T unL = uL * nx + vL * ny;
+  const T unR = uR * nx + vR * ny;
+  const T tx = -ny, ty = nx;
+  const T utL = uL * tx + vL * ty;
+  const T utR = uR * tx + vR * ty;
+  const T aL = sqrt(fabs(k.gamma * pL / rL));
+  const T aR = sqrt(fabs(k.gamma * pR / rR));
+  T SL = fmin(unL - aL, unR - aR);
+  T SR = fmax(unL + aL, unR + aR);
+  if (SL == SR) SL = SL - k.ss_eps;
+  if (SL == SR) SR = SR + k.ss_eps;
+  const T EL = WL.w, ER = WR.w;
+  const T FL0 = rL * unL, FL1 = rL * uL * unL + pL * nx, FL2 = rL * vL * unL + pL * ny, FL3 = (EL + pL) * unL;
+  const T FR0 = rR * unR, FR1 = rR * uR * unR + pR * nx, FR2 = rR * vR * unR + pR * ny, FR3 = (ER + pR) * unR;
+  const T Fc0 = k.half * (FL0 + FR0), Fc1 = k.half * (FL1 + FR1);
+  const T Fc2 = k.half * (FL2 + FR2), Fc3 = k.half * (FL3 + FR3);
+  T den = rL * (SL - unL) - rR * (SR - unR);
+  if (den == T(0)) den = k.den_eps;
+  const T Ss = (pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR)) / den;
+  const T PsL = pL + rL * (SL - unL) * (Ss - unL);
+  const T PsR = pR + rR * (SR - unR) * (Ss - unR);
+  const T Ps = k.half * (PsL + PsR);
+  // jnp.where cascade of :369-371; the star state is built once for the side it needs
+  const bool c1 = SL >= T(0);
+  const bool c2 = (SL <= T(0)) && (Ss >= T(0));
+  const bool c3 = (Ss <= T(0)) && (SR >= T(0));
+  const bool left = c1 || c2;
+  const T rK = left ? rL : rR, unK = left ? unL : unR, SK = left ? SL : SR;
+  const T EK = left ? EL : ER, pK = left ? pL : pR, utK = left ? utL : utR;
+  const T rs = rK * (SK - unK) / (SK - Ss);
+  const T Us0 = rs, Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
+  const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) / (SK - Ss);
+  T H0, H1, H2, H3;
+  if (c1) { H0 = FL0; H1 = FL1; H2 = FL2; H3 = FL3; }
+  else if (c2) { H0 = FL0 + SL * (Us0 - WL.x); H1 = FL1 + SL * (Us1 - WL.y); H2 = FL2 + SL * (Us2 - WL.z); H3 = FL3 + SL * (Us3 - WL.w); }
+  else if (c3) { H0 = FR0 + SR * (Us0 - WR.x); H1 = FR1 + SR * (Us1 - WR.y); H2 = FR2 + SR * (Us2 - WR.z); H3 = FR3 + SR * (Us3 - WR.w); }
+  else { H0 = FR0; H1 = FR1; H2 = FR2; H3 = FR3; }
+  F[0] = Fc0 - (Fc0 - H0); F[1] = Fc1 - (Fc1 - H1);
+  F[2] = Fc2 - (Fc2 - H2); F[3] = Fc3 - (Fc3 - H3);
+}
+
+// euler_solver.py:203-240 Rusanov (plain branch) inside getFlux
+template <typename T>
+__device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
+                                        T nx, T ny, const Consts<T>& k, T F[4]) {
+  const T unL = PL[1] * nx + PL[2] * ny;
+  const T unR = PR[1] * nx + PR[2] * ny;
+  const T FL0 = PL[0] * unL, FL1 = PL[0] * PL[1] * unL + PL[3] * nx, FL2 = PL[0] * PL[2] * unL + PL[3] * ny, FL3 = (WL.w + PL[3]) * unL;
+  const T FR0 = PR[0] * unR, FR1 = PR[0] * PR[1] * unR + PR[3] * nx, FR2 = PR[0] * PR[2] * unR + PR[3] * ny, FR3 = (WR.w + PR[3]) * unR;
+  const T CL = sqrt(fabs(k.gamma * PL[3] / PL[0])) + fabs(unL);
+  const T CR = sqrt(fabs(k.gamma * PR[3] / PR[0])) + fabs(unR);
+  const T C = fmax(CR, CL);
+  F[0] = k.half * (FL0 + FR0) - k.half * C * (WR.x - WL.x);
+  F[1] = k.half * (FL1 + FR1) - k.half * C * (WR.y - WL.y);
+  F[2] = k.half * (FL2 + FR2) - k.half * C * (WR.z - WL.z);
+  F[3] = k.half * (FL3 + FR3) - k.half * C * (WR.w - WL.w);
+}
+
+template <typename T>
+__device__ __forceinline__ T geo(const Seg<T>& s, int f, int c) { return __ldg(s.geo + (size_t)f * s.geo_stride + c); }
+
+// --------------------------------------------------------------- K1 recon
+// euler_solver.py:106-122 build_reconstruction for MUSCL: BC ghosts, LSQ
+// gradient (helper.py:136-153), limiter (euler_solver.py:45-67) and the cell's
+// own MUSCL face states (euler_solver.py:69-98). Writes FV[k][item] (primitive).
+// With LOCALDT it also writes the per-cell CFL time step of the state.
+// MUSCL=false only computes the local dt (constant reconstruction needs no face states).
+template <typename T, bool MUSCL, bool LOCALDT>
+__global__ void __launch_bounds__(256) k_recon(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
+                                               const V4<T>* __restrict__ W, V4<T>* __restrict__ FV,
+                                               long long total, Cases<T> cs, Consts<T> kc, int pos,
+                                               T* __restrict__ dt_local) {
+  const int2 bt = blk[blockIdx.x];
+  const Seg<T> s = segs[bt.x];
+  const int item = bt.y + threadIdx.x;
+  if (item >= s.n_cells * s.B) return;
+  const int c = item / s.B;
+  const int b = item - c * s.B;
+  const int g = s.case0 + b;
+  if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
+  const long long gi = s.off + item;
+  const V4<T> Wc = W[gi];
+  T Pc[4];
+  prim<T>(Wc, kc.gm1, kc.half, Pc);
+  if (LOCALDT) {
+    const T cel = sqrt(fabs(kc.gamma * Pc[3] / Pc[0]));
+    T lam = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T un = Pc[1] * geo(s, G_N0X + 2 * k, c) + Pc[2] * geo(s, G_N0Y + 2 * k, c);
+      const T term = (cel + fabs(un)) * geo(s, G_S0 + k, c);
+      lam = (k == 0) ? term : lam + term;
+    }
+    dt_local[gi] = geo(s, G_AREA, c) / lam * cs.dt[g];   // cs.dt holds the case CFL in local mode
+  }
+  if (!MUSCL) return;
+  const int4 nb = __ldg(s.nbr + c);
+  const int nbk[3] = {nb.x, nb.y, nb.z};
+  T Pk[3][4];
+  const V4<T> inlet = cs.inlet[g];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int kind = slot_kind(nb.w, k);
+    V4<T> Wk;
+    if (kind == K_INTERIOR) Wk = W[s.off + (long long)nbk[k] * s.B + b];
+    else Wk = ghost_cons<T>(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc);
+    prim<T>(Wk, kc.gm1, kc.half, Pk[k]);
+  }
+  T gx[4], gy[4];
+  const T c0x = geo(s, G_C0X, c), c0y = geo(s, G_C0Y, c), c1x = geo(s, G_C1X, c), c1y = geo(s, G_C1Y, c);
+  const T c2x = geo(s, G_C2X, c), c2y = geo(s, G_C2Y, c);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
+    gx[v] = c0x * d0 + c1x * d1 + c2x * d2;
+    gy[v] = c0y * d0 + c1y * d1 + c2y * d2;
+  }
+  const T fx[3] = {geo(s, G_F0X, c), geo(s, G_F1X, c), geo(s, G_F2X, c)};
+  const T fy[3] = {geo(s, G_F0Y, c), geo(s, G_F1Y, c), geo(s, G_F2Y, c)};
+  T phi[4], D[3][4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const T mn = fmin(fmin(Pc[v], Pk[0][v]), fmin(Pk[1][v], Pk[2][v]));
+    const T mx = fmax(fmax(Pc[v], Pk[0][v]), fmax(Pk[1][v], Pk[2][v]));
+    // min over the three faces only: the Venkatakrishnan value can exceed 1
+    T ph = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T d = fx[k] * gx[v] + fy[k] * gy[v];
+      D[k][v] = d;
+      T p = T(1);
+      if (d > kc.eps_lim) p = venkat<T>(mx - Pc[v], d, kc.venk_eps);
+      else if (d < -kc.eps_lim) p = venkat<T>(mn - Pc[v], d, kc.venk_eps);
+      ph = (k == 0) ? p : fmin(ph, p);
+    }
+    phi[v] = ph;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int kind = slot_kind(nb.w, k);
+    V4<T> o;
+    if (kind == K_INTERIOR)
+      o = mk4<T>(Pc[0] + phi[0] * D[k][0], Pc[1] + phi[1] * D[k][1], Pc[2] + phi[2] * D[k][2], Pc[3] + phi[3] * D[k][3]);
+    else
+      o = mk4<T>(Pc[0], Pc[1], Pc[2], Pc[3]);
+    FV[(long long)k * total + gi] = o;
+  }
+}
+
+// ----------------------------------------------------------------- K2 flux
+enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
+
+// euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
+// then the stage update of :630-653.
+template <typename T, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
+__global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
+                                              const V4<T>* __restrict__ Win, const V4<T>* __restrict__ Wbase,
+                                              V4<T>* __restrict__ Wout, const V4<T>* __restrict__ FV,
+                                              long long total, Cases<T> cs, Consts<T> kc, int pos,
+                                              const T* __restrict__ dt_local) {
+  const int2 bt = blk[blockIdx.x];
+  const Seg<T> s = segs[bt.x];
+  const int item = bt.y + threadIdx.x;
+  if (item >= s.n_cells * s.B) return;
+  const int c = item / s.B;
+  const int b = item - c * s.B;
+  const int g = s.case0 + b;
+  if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
+  const long long gi = s.off + item;
+  const V4<T> Wc = Win[gi];
+  const int4 nb = __ldg(s.nbr + c);
+  const int nbk[3] = {nb.x, nb.y, nb.z};
+  const V4<T> inlet = cs.inlet[g];
+  T acc[4];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int kind = slot_kind(nb.w, k);
+    const T nx = geo(s, G_N0X + 2 * k, c), ny = geo(s, G_N0Y + 2 * k, c);
+    V4<T> WL, WR;
+    T PL[4], PR[4];
+    if (MUSCL) {
+      const V4<T> fl = FV[(long long)k * total + gi];
+      T qL[4] = {fl.x, fl.y, fl.z, fl.w};
+      T qR[4];
+      if (kind == K_INTERIOR) {
+        const V4<T> fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)nbk[k] * s.B + b];
+        qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
+      } else {
+        prim<T>(ghost_cons<T>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+      }
+      WL = cons<T>(qL, kc.gm1, kc.half);
+      WR = cons<T>(qR, kc.gm1, kc.half);
+    } else {
+      WL = Wc;
+      WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T>(kind, Wc, nx, ny, inlet, kc);
+    }
+    prim<T>(WL, kc.gm1, kc.half, PL);
+    prim<T>(WR, kc.gm1, kc.half, PR);
+    T F[4];
+    if (FLUX == 0) hllc<T>(WL, PL, WR, PR, nx, ny, kc, F);
+    else rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
+    const T sk = geo(s, G_S0 + k, c);
+    if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
+    else { acc[0] = acc[0] + sk * F[0]; acc[1] = acc[1] + sk * F[1]; acc[2] = acc[2] + sk * F[2]; acc[3] = acc[3] + sk * F[3]; }
+  }
+  const T area = geo(s, G_AREA, c);
+  const T sig = cs.strength[g] * geo(s, G_BLEND3, c);
+  const T R0 = acc[0] / area - sig * (inlet.x - Wc.x);
+  const T R1 = acc[1] / area - sig * (inlet.y - Wc.y);
+  const T R2 = acc[2] / area - sig * (inlet.z - Wc.z);
+  const T R3 = acc[3] / area - sig * (inlet.w - Wc.w);
+  const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+  V4<T> o;
+  if (STAGE == ST_FIRST) {
+    o = mk4<T>(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
+  } else if (STAGE == ST_SRK2_SECOND) {
+    const V4<T> W0 = Wbase[gi];
+    o = mk4<T>(kc.half * (W0.x + Wc.x - dt * R0), kc.half * (W0.y + Wc.y - dt * R1),
+               kc.half * (W0.z + Wc.z - dt * R2), kc.half * (W0.w + Wc.w - dt * R3));
+  } else {
+    const V4<T> W0 = Wbase[gi];
+    o = mk4<T>(kc.half * (W0.x - dt * R0 + Wc.x), kc.half * (W0.y - dt * R1 + Wc.y),
+               kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
+  }
+  Wout[gi] = o;
+}
+
+// copy a stage result back into the state for live slots (explicit Euler)
+template <typename T>
+__global__ void k_commit(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk, const V4<T>* __restrict__ src,
+                         V4<T>* __restrict__ dst, Cases<T> cs, int pos) {
+  const int2 bt = blk[blockIdx.x];
+  const Seg<T> s = segs[bt.x];
+  const int item = bt.y + threadIdx.x;
+  if (item >= s.n_cells * s.B) return;
+  const int c = item / s.B;
+  const int g = s.case0 + (item - c * s.B);
+  if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
+  dst[s.off + item] = src[s.off + item];
+}
+
+// ------------------------------------------------------ per-case reductions
+enum RedOp { RED_NORM = 0, RED_DTMIN = 1, RED_ENTROPY = 2, RED_DIFF = 3 };
+
+struct CaseMap {             // global slot -> (segment, slot)
+  const int* seg;
+  const int* slot;
+};
+
+// Block (chunk, case) reduces a fixed cell range of one case; partials are
+// combined in a fixed order by the consumer, so results are bitwise
+// reproducible. RED_NORM: sum |W - Wref|^2, sum |Wref|^2 and Wref <- W
+// (euler/main.py:150-152); RED_DTMIN: min_i area/sum_k (c+|u.n|) s
+// (helper.py:8-18); RED_ENTROPY: sum rho log(p/rho^g) area/(g-1)
+// (helper.py:48-55,312-315); RED_DIFF: sum |A - B|^2, sum |B|^2 (probe).
+template <typename T, int OP>
+__global__ void __launch_bounds__(256) k_case_reduce(const Seg<T>* __restrict__ segs, CaseMap cm,
+                                                     const V4<T>* __restrict__ W, V4<T>* __restrict__ Wref,
+                                                     const int* __restrict__ due, int chunk_cells,
+                                                     double2* __restrict__ partial, int n_chunks, Consts<T> kc) {
+  const int g = blockIdx.y;
+  const int chunk = blockIdx.x;
+  if (due != nullptr && !due[g]) return;
+  const int si = cm.seg[g];
+  const Seg<T> s = segs[si];
+  const int b = cm.slot[g];
+  const int c0 = chunk * chunk_cells;
+  const int c1 = min(s.n_cells, c0 + chunk_cells);
+  double a0 = (OP == RED_DTMIN) ? 1e300 : 0.0, a1 = 0.0;
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const long long gi = s.off + (long long)c * s.B + b;
+    const V4<T> w = W[gi];
+    if (OP == RED_NORM || OP == RED_DIFF) {
+      const V4<T> r = Wref[gi];
+      const double d0 = (double)w.x - (double)r.x, d1 = (double)w.y - (double)r.y;
+      const double d2 = (double)w.z - (double)r.z, d3 = (double)w.w - (double)r.w;
+      a0 += d0 * d0 + d1 * d1 + d2 * d2 + d3 * d3;
+      a1 += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z + (double)r.w * r.w;
+      if (OP == RED_NORM) Wref[gi] = w;
+    } else if (OP == RED_DTMIN) {
+      T P[4];
+      prim<T>(w, kc.gm1, kc.half, P);
+      const T cel = sqrt(fabs(kc.gamma * P[3] / P[0]));
+      T lam = T(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const T un = P[1] * geo(s, G_N0X + 2 * k, c) + P[2] * geo(s, G_N0Y + 2 * k, c);
+        const T term = (cel + fabs(un)) * geo(s, G_S0 + k, c);
+        lam = (k == 0) ? term : lam + term;
+      }
+      const T d = geo(s, G_AREA, c) / lam;
+      a0 = fmin(a0, (double)d);
+    } else {  // entropy
+      const T r = w.x, u = w.y / r, v = w.z / r;
+      const T p = (w.w - kc.half * r * (u * u + v * v)) * kc.gm1;
+      const T sv = log(p / pow(r, kc.gamma));
+      a0 += (double)(r * sv * geo(s, G_AREA, c) / kc.gm1);
+    }
+  }
+  // fixed-shape block reduction
+  __shared__ double sh0[256], sh1[256];
+  sh0[threadIdx.x] = a0;
+  sh1[threadIdx.x] = a1;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      if (OP == RED_DTMIN) sh0[threadIdx.x] = fmin(sh0[threadIdx.x], sh0[threadIdx.x + w]);
+      else { sh0[threadIdx.x] += sh0[threadIdx.x + w]; sh1[threadIdx.x] += sh1[threadIdx.x + w]; }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[(size_t)g * n_chunks + chunk] = make_double2(sh0[0], sh1[0]);
+}
+
+// ---------------------------------------------------------- case bookkeeping
+struct CaseCtl {             // mutable per-slot control words (device)
+  int* active;
+  int* step;
+  int* nmax;
+  int* ref_step;
+  int* streak;
+  int* streak_start;
+  int* stopping_step;
+  int* status;
+  int* due;
+  double* last_rel;
+  long long* t_start;        // globaltimer at the case start (ns)
+  long long* t_end;
+};
+
+// Which slots need a stop-rule check after `pos` steps of the chunk.
+__global__ void k_mark_due(CaseCtl cc, int n_slots, int pos, int check_every) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots) return;
+  int d = 0;
+  if (cc.active[g]) {
+    const int done = min(cc.step[g] + pos, cc.nmax[g]);
+    d = (done > cc.ref_step[g]) && ((done % check_every) == 0 || done >= cc.nmax[g]);
+  }
+  cc.due[g] = d;
+}
+
+__device__ __forceinline__ long long globaltimer() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// euler/main.py:147-158: rel, streak, confirmation and the stopping step.
+// STOP_RULE 0: rel = ||dW|| / (block * (||Wref|| + 1e-16)); 1: density-residual RMS
+__global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* __restrict__ partial, int n_chunks,
+                        const int* __restrict__ ncells, double threshold, int patience, int stop_rule) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !cc.due[g]) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = 0; i < n_chunks; ++i) {
+    const double2 p = partial[(size_t)g * n_chunks + i];
+    s0 += p.x;
+    s1 += p.y;
+  }
+  const int done = min(cc.step[g] + pos, cc.nmax[g]);
+  const int block = max(1, done - cc.ref_step[g]);
+  double rel;
+  if (stop_rule == 0) rel = sqrt(s0) / ((double)block * (sqrt(s1) + 1e-16));
+  else rel = sqrt(s0 / (double)ncells[g]);
+  cc.last_rel[g] = rel;
+  const bool finite = isfinite(s0) && isfinite(s1);
+  const bool under = rel <= threshold;
+  const int streak = cc.streak[g];
+  const int nstreak = under ? streak + 1 : 0;
+  if (under && streak == 0) cc.streak_start[g] = done;
+  cc.streak[g] = nstreak;
+  cc.ref_step[g] = done;
+  int st = 0;
+  if (!finite) st = 4;
+  else if (nstreak >= patience) st = 2;
+  else if (done >= cc.nmax[g]) st = 3;
+  if (st) {
+    cc.status[g] = st;
+    cc.stopping_step[g] = (st == 2) ? cc.streak_start[g] : cc.nmax[g];
+    cc.step[g] = done;
+    cc.active[g] = 0;
+    cc.t_end[g] = globaltimer();
+  }
+}
+
+// chunk end without checks: every live slot advanced `len` steps
+__global__ void k_advance(CaseCtl cc, int n_slots, int len, int stop_at_nmax) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !cc.active[g]) return;
+  const int done = min(cc.step[g] + len, cc.nmax[g]);
+  cc.step[g] = done;
+  if (stop_at_nmax && done >= cc.nmax[g] && cc.status[g] == 1) {
+    cc.status[g] = 3;
+    cc.stopping_step[g] = cc.nmax[g];
+    cc.active[g] = 0;
+    cc.t_end[g] = globaltimer();
+  }
+}
+
+// dt of freshly (re)filled slots from the RED_DTMIN partials: dt = CFL * min,
+// N = int(tf / dt) + 1 in the state precision (euler/main.py:121-122)
+template <typename T>
+__global__ void k_dt_finish(const int* __restrict__ fill, int n_slots, const double2* __restrict__ partial,
+                            int n_chunks, const double* __restrict__ cfl, const double* __restrict__ tf,
+                            const long long* __restrict__ max_steps, T* __restrict__ dt, CaseCtl cc, int local_mode) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !fill[g]) return;
+  double m = 1e300;
+  for (int i = 0; i < n_chunks; ++i) m = fmin(m, partial[(size_t)g * n_chunks + i].x);
+  const T d = (T)m * (T)cfl[g];
+  long long n;
+  if (local_mode) {
+    dt[g] = (T)cfl[g];
+    n = max_steps[g] > 0 ? max_steps[g] : (long long)((T)tf[g] / d) + 1;
+  } else {
+    dt[g] = d;
+    n = (long long)((T)tf[g] / d) + 1;
+  }
+  if (max_steps[g] > 0 && n > max_steps[g]) n = max_steps[g];
+  if (!(n >= 1)) n = 1;
+  if (n > 2000000000LL) n = 2000000000LL;
+  cc.nmax[g] = (int)n;
+  cc.t_start[g] = globaltimer();
+}
+
+// pressure force coefficients of every live-or-finished slot
+// (helper.py:366-415): sum_w p(cell_w) n_w ds_w / (q_inf L_ref), p at gamma 1.4
+template <typename T>
+__global__ void k_forces(const Seg<T>* __restrict__ segs, CaseMap cm, const V4<T>* __restrict__ W,
+                         const double* __restrict__ qref, double* __restrict__ out, Consts<T> kc) {
+  const int g = blockIdx.x;
+  const Seg<T> s = segs[cm.seg[g]];
+  const int b = cm.slot[g];
+  double ax = 0.0, ay = 0.0;
+  for (int i = threadIdx.x; i < s.n_wall; i += blockDim.x) {
+    const int c = s.wall_cell[i];
+    T P[4];
+    prim<T>(W[s.off + (long long)c * s.B + b], kc.gm1_14, kc.half, P);
+    ax += (double)(P[3] * s.wall_nx[i] * s.wall_ds[i]);
+    ay += (double)(P[3] * s.wall_ny[i] * s.wall_ds[i]);
+  }
+  __shared__ double sx[256], sy[256];
+  sx[threadIdx.x] = ax;
+  sy[threadIdx.x] = ay;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { sx[threadIdx.x] += sx[threadIdx.x + w]; sy[threadIdx.x] += sy[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * g] = sx[0] / qref[g];
+    out[2 * g + 1] = sy[0] / qref[g];
+  }
+}
+
+// ----------------------------------------------------------- state movers
+// host-order float64 rows -> device precision, cell c of the caller's order
+// goes to renumbered cell inv[c]
+template <typename T>
+__global__ void k_scatter_state(const double* __restrict__ src, const int* __restrict__ inv, int n_cells,
+                                V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, long long off, int B, int b) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const double* r = src + 4 * (size_t)c;
+  const V4<T> w = mk4<T>((T)r[0], (T)r[1], (T)r[2], (T)r[3]);
+  const long long gi = off + (long long)inv[c] * B + b;
+  W[gi] = w;
+  if (Wref) Wref[gi] = w;
+}
+
+template <typename T>
+__global__ void k_gather_state(const V4<T>* __restrict__ W, const int* __restrict__ inv, int n_cells,
+                               long long off, int B, int b, double* __restrict__ dst) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const V4<T> w = W[off + (long long)inv[c] * B + b];
+  double* r = dst + 4 * (size_t)c;
+  r[0] = (double)w.x; r[1] = (double)w.y; r[2] = (double)w.z; r[3] = (double)w.w;
+}
+
+// freestream fill of a slot: W = Wref = inlet
+template <typename T>
+__global__ void k_fill_freestream(V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, int n_cells, long long off, int B,
+                                  int b, V4<T> w) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const long long gi = off + (long long)c * B + b;
+  W[gi] = w;
+  Wref[gi] = w;
+}
+
+// state in the device precision, caller cell order <-> solver order
+template <typename T>
+__global__ void k_copy_in_device(const V4<T>* __restrict__ src, const int* __restrict__ inv, int n_cells,
+                                 V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, long long off, int B, int b) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const long long gi = off + (long long)inv[c] * B + b;
+  W[gi] = src[c];
+  if (Wref) Wref[gi] = src[c];
+}
+
+template <typename T>
+__global__ void k_copy_out_device(const V4<T>* __restrict__ W, const int* __restrict__ inv, int n_cells,
+                                  long long off, int B, int b, V4<T>* __restrict__ dst) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  dst[c] = W[off + (long long)inv[c] * B + b];
+}
+
+// ------------------------------------------------------------------- IDW
+// eval/core.py:135-142 with utils/metrics.py:9-14: weights from float64
+// distances, float32 weighted sum over the k neighbours in order.
+__global__ void k_idw(const float* __restrict__ src, int n_vars, const int* __restrict__ idx,
+                      const float* __restrict__ dist, int n_dst, int k, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_dst) return;
+  double wsum = 0.0;
+  double w[16];
+  for (int j = 0; j < k; ++j) {
+    const double d = (double)dist[(size_t)i * k + j];
+    w[j] = 1.0 / (d * d + 1e-12);
+    wsum += w[j];
+  }
+  for (int v = 0; v < n_vars; ++v) {
+    float acc = 0.0f;
+    for (int j = 0; j < k; ++j) {
+      const float wf = (float)(w[j] / wsum);
+      acc += wf * src[(size_t)idx[(size_t)i * k + j] * n_vars + v];
+    }
+    out[(size_t)i * n_vars + v] = acc;
+  }
+}
+
+}  // namespace esr

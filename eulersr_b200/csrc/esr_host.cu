@@ -1,0 +1,979 @@
+// esr_host.cu -- solver runtime and the C ABI (include/eulersr.h).
+//
+// A solver owns every case slot of every mesh it was created with. One step
+// of all live slots is one launch per kernel (K1 recon, K2 flux, per stage);
+// the launch grid walks a block table whose entries point into per-mesh
+// segments, so meshes of different sizes (the ragged batch) share launches.
+// Steps are issued in chunks captured once as CUDA graphs; stop-rule checks
+// (norm reduction + bookkeeping) sit inside the chunk graph at multiples of
+// check_every, so a run needs no host round trip until the host polls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "esr_device.cuh"
+#include "esr_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define ESR_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) {                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? ESR_ERR_OOM : ESR_ERR_CUDA,                \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+    }                                                                                          \
+  } while (0)
+
+#define ESR_TRY(expr)            \
+  do {                           \
+    int r_ = (expr);             \
+    if (r_ != ESR_OK) return r_; \
+  } while (0)
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  int alloc(size_t count) {
+    if (p) { cudaFree(p); p = nullptr; }
+    n = count;
+    if (count == 0) return ESR_OK;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) { p = nullptr; return fail(ESR_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
+    return ESR_OK;
+  }
+};
+
+constexpr int kChunkMax = 64;       // steps per captured chunk (upper bound)
+constexpr int kReduceThreads = 256;
+constexpr int kReduceCells = 2048;  // cells per reduction block
+
+}  // namespace
+
+using namespace esr;
+
+// ------------------------------------------------------------------ solver
+struct SolverBase {
+  virtual ~SolverBase() = default;
+  int64_t launches = 0;
+};
+
+template <typename T>
+struct SolverT : SolverBase {
+  using V = V4<T>;
+  esr_params P{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int block = 128;
+
+  struct MeshDev {
+    const HostMesh* hm;
+    DevBuf<T> geo;
+    DevBuf<int4> nbr;
+    DevBuf<int> wall_cell;
+    DevBuf<T> wall_nx, wall_ny, wall_ds;
+    DevBuf<int> inv;  // caller cell -> solver cell
+    int B = 0, case0 = 0;
+    long long off = 0;
+  };
+  std::vector<std::unique_ptr<MeshDev>> meshes;
+  int n_slots = 0;
+  long long total = 0;   // items (cells x slots) over all meshes
+  int n_chunks = 0;      // reduction chunks per case (max over meshes)
+
+  DevBuf<Seg<T>> d_segs;
+  DevBuf<int2> d_blk;
+  int n_blk = 0;
+  DevBuf<int> d_case_seg, d_case_slot, d_ncells;
+
+  DevBuf<V> W, Wa, Wref, FV;
+  DevBuf<T> dt_local, res;
+  DevBuf<T> dt, strength;
+  DevBuf<V> inlet;
+  DevBuf<double> cfl, tf, qref, forces;
+  DevBuf<long long> max_steps, t_start, t_end;
+  DevBuf<int> active, step, nmax, nmax_inf, ref_step, streak, streak_start, stopping, status, due, fill;
+  DevBuf<double> last_rel;
+  DevBuf<double2> partial;
+  DevBuf<double> stage_rows;  // host rows staging for set/get state
+
+  // host mirrors of per-slot case data
+  std::vector<esr_case> hcase;
+  std::vector<int> hcase_index;
+  Consts<T> kc{};
+
+  // graphs
+  cudaGraphExec_t g_run = nullptr;   // chunk with stop-rule checks
+  int g_run_len = 0;
+  cudaGraphExec_t g_plain = nullptr; // chunk without checks
+  int g_plain_len = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+
+  ~SolverT() override {
+    if (g_run) cudaGraphExecDestroy(g_run);
+    if (g_plain) cudaGraphExecDestroy(g_plain);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  Cases<T> cases(bool ignore_nmax = false) {
+    Cases<T> c;
+    c.dt = dt.p; c.inlet = inlet.p; c.strength = strength.p; c.active = active.p; c.step = step.p;
+    c.nmax = ignore_nmax ? nmax_inf.p : nmax.p;
+    return c;
+  }
+  CaseCtl ctl() {
+    CaseCtl c;
+    c.active = active.p; c.step = step.p; c.nmax = nmax.p; c.ref_step = ref_step.p; c.streak = streak.p;
+    c.streak_start = streak_start.p; c.stopping_step = stopping.p; c.status = status.p; c.due = due.p;
+    c.last_rel = last_rel.p; c.t_start = t_start.p; c.t_end = t_end.p;
+    return c;
+  }
+  CaseMap cmap() { return CaseMap{d_case_seg.p, d_case_slot.p}; }
+
+  int init(const esr_mesh* const* ms, const int32_t* slots, int nm, const esr_params* p) {
+    P = *p;
+    device = p->device;
+    ESR_CUDA(cudaSetDevice(device));
+    ESR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    ESR_CUDA(cudaEventCreate(&ev0));
+    ESR_CUDA(cudaEventCreate(&ev1));
+    const double g = p->gamma;
+    kc.gamma = (T)g;
+    kc.gm1 = (T)(g - 1.0);
+    kc.gm1_14 = (T)(1.4 - 1.0);
+    kc.half = (T)0.5;
+    kc.eps_lim = sizeof(T) == 8 ? (T)1e-12 : (T)1e-7;
+    kc.venk_eps = (T)1e-7;
+    kc.ss_eps = (T)1e-6;
+    kc.den_eps = (T)1e-12;
+    // layout
+    long long off = 0;
+    int case0 = 0;
+    int max_cells = 0;
+    for (int m = 0; m < nm; ++m) {
+      auto md = std::make_unique<MeshDev>();
+      md->hm = &ms[m]->hm;
+      md->B = slots[m];
+      md->case0 = case0;
+      md->off = off;
+      off += (long long)md->hm->n_cells * md->B;
+      case0 += md->B;
+      max_cells = std::max(max_cells, md->hm->n_cells);
+      meshes.push_back(std::move(md));
+    }
+    n_slots = case0;
+    total = off;
+    if (n_slots <= 0 || total <= 0) return fail(ESR_ERR_ARG, "solver: no case slots");
+    if (total > (long long)INT_MAX * 4) return fail(ESR_ERR_ARG, "solver: too many cells x slots");
+    n_chunks = (max_cells + kReduceCells - 1) / kReduceCells;
+    const auto& hm0 = *meshes[0]->hm;
+    kc.sub_rho = (T)hm0.inlet_subsonic[0];
+    kc.sub_u = (T)hm0.inlet_subsonic[1];
+    kc.sub_v = (T)hm0.inlet_subsonic[2];
+    // block size: enough blocks to cover the SMs twice when possible
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    block = p->block_size > 0 ? p->block_size : 0;
+    if (block == 0) {
+      block = 256;
+      while (block > 64 && (total + block - 1) / block < 2 * sms) block /= 2;
+    }
+    if (block != 64 && block != 128 && block != 256) return fail(ESR_ERR_ARG, "solver: block_size must be 64, 128 or 256");
+    // upload meshes
+    std::vector<Seg<T>> hsegs;
+    std::vector<int2> hblk;
+    std::vector<int> hseg_of(n_slots), hslot_of(n_slots), hnc(n_slots);
+    for (int m = 0; m < nm; ++m) {
+      MeshDev& md = *meshes[m];
+      const HostMesh& hm = *md.hm;
+      const int N = hm.n_cells;
+      std::vector<T> g(hm.geo.size());
+      for (size_t i = 0; i < g.size(); ++i) g[i] = (T)hm.geo[i];
+      ESR_TRY(md.geo.alloc(g.size()));
+      ESR_CUDA(cudaMemcpy(md.geo.p, g.data(), g.size() * sizeof(T), cudaMemcpyHostToDevice));
+      ESR_TRY(md.nbr.alloc(N));
+      ESR_CUDA(cudaMemcpy(md.nbr.p, hm.nbr.data(), (size_t)N * sizeof(int4), cudaMemcpyHostToDevice));
+      const int nw = (int)hm.wall_cell.size();
+      std::vector<T> wx(nw), wy(nw), wd(nw);
+      for (int i = 0; i < nw; ++i) { wx[i] = (T)hm.wall_n[2 * i]; wy[i] = (T)hm.wall_n[2 * i + 1]; wd[i] = (T)hm.wall_ds[i]; }
+      ESR_TRY(md.wall_cell.alloc(std::max(nw, 1)));
+      ESR_TRY(md.wall_nx.alloc(std::max(nw, 1)));
+      ESR_TRY(md.wall_ny.alloc(std::max(nw, 1)));
+      ESR_TRY(md.wall_ds.alloc(std::max(nw, 1)));
+      if (nw) {
+        ESR_CUDA(cudaMemcpy(md.wall_cell.p, hm.wall_cell.data(), nw * sizeof(int), cudaMemcpyHostToDevice));
+        ESR_CUDA(cudaMemcpy(md.wall_nx.p, wx.data(), nw * sizeof(T), cudaMemcpyHostToDevice));
+        ESR_CUDA(cudaMemcpy(md.wall_ny.p, wy.data(), nw * sizeof(T), cudaMemcpyHostToDevice));
+        ESR_CUDA(cudaMemcpy(md.wall_ds.p, wd.data(), nw * sizeof(T), cudaMemcpyHostToDevice));
+      }
+      ESR_TRY(md.inv.alloc(N));
+      ESR_CUDA(cudaMemcpy(md.inv.p, hm.inv.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+      Seg<T> s{};
+      s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = N; s.off = md.off;
+      s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
+      s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
+      hsegs.push_back(s);
+      const long long items = (long long)N * md.B;
+      for (long long b0 = 0; b0 < items; b0 += block) hblk.push_back(make_int2(m, (int)b0));
+      for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
+    }
+    n_blk = (int)hblk.size();
+    ESR_TRY(d_segs.alloc(hsegs.size()));
+    ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
+    ESR_TRY(d_blk.alloc(hblk.size()));
+    ESR_CUDA(cudaMemcpy(d_blk.p, hblk.data(), hblk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESR_TRY(d_case_seg.alloc(n_slots));
+    ESR_TRY(d_case_slot.alloc(n_slots));
+    ESR_TRY(d_ncells.alloc(n_slots));
+    ESR_CUDA(cudaMemcpy(d_case_seg.p, hseg_of.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice));
+    ESR_CUDA(cudaMemcpy(d_case_slot.p, hslot_of.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice));
+    ESR_CUDA(cudaMemcpy(d_ncells.p, hnc.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice));
+    // state
+    ESR_TRY(W.alloc(total));
+    ESR_TRY(Wa.alloc(total));
+    ESR_TRY(Wref.alloc(total));
+    if (P.reconstruction == ESR_RECON_MUSCL) ESR_TRY(FV.alloc(3 * total));
+    if (P.dt_mode == ESR_DT_LOCAL) ESR_TRY(dt_local.alloc(total));
+    if (P.stop_rule == ESR_STOP_DENSITY_L2) ESR_TRY(res.alloc(total));
+    ESR_CUDA(cudaMemsetAsync(W.p, 0, total * sizeof(V), stream));
+    ESR_CUDA(cudaMemsetAsync(Wa.p, 0, total * sizeof(V), stream));
+    ESR_CUDA(cudaMemsetAsync(Wref.p, 0, total * sizeof(V), stream));
+    // per-slot arrays
+    ESR_TRY(dt.alloc(n_slots)); ESR_TRY(strength.alloc(n_slots)); ESR_TRY(inlet.alloc(n_slots));
+    ESR_TRY(cfl.alloc(n_slots)); ESR_TRY(tf.alloc(n_slots)); ESR_TRY(qref.alloc(n_slots));
+    ESR_TRY(forces.alloc(2 * n_slots)); ESR_TRY(max_steps.alloc(n_slots));
+    ESR_TRY(t_start.alloc(n_slots)); ESR_TRY(t_end.alloc(n_slots));
+    for (DevBuf<int>* b : {&active, &step, &nmax, &nmax_inf, &ref_step, &streak, &streak_start, &stopping, &status, &due, &fill})
+      ESR_TRY(b->alloc(n_slots));
+    ESR_TRY(last_rel.alloc(n_slots));
+    ESR_TRY(partial.alloc((size_t)n_slots * n_chunks));
+    for (DevBuf<int>* b : {&active, &step, &nmax, &ref_step, &streak, &streak_start, &stopping, &status, &due, &fill})
+      ESR_CUDA(cudaMemsetAsync(b->p, 0, n_slots * sizeof(int), stream));
+    std::vector<int> inf(n_slots, INT_MAX);
+    ESR_CUDA(cudaMemcpy(nmax_inf.p, inf.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice));
+    ESR_CUDA(cudaMemsetAsync(dt.p, 0, n_slots * sizeof(T), stream));
+    ESR_CUDA(cudaMemsetAsync(strength.p, 0, n_slots * sizeof(T), stream));
+    ESR_CUDA(cudaMemsetAsync(inlet.p, 0, n_slots * sizeof(V), stream));
+    hcase.assign(n_slots, esr_case{});
+    hcase_index.assign(n_slots, -1);
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    return ESR_OK;
+  }
+
+  int mesh_of_slot(int slot, int& m, int& b) {
+    if (slot < 0 || slot >= n_slots) return fail(ESR_ERR_ARG, "slot out of range");
+    for (m = 0; m < (int)meshes.size(); ++m) {
+      if (slot < meshes[m]->case0 + meshes[m]->B) { b = slot - meshes[m]->case0; return ESR_OK; }
+    }
+    return fail(ESR_ERR_ARG, "slot out of range");
+  }
+
+  // ---------------------------------------------------------------- kernels
+  template <int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
+  void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
+    k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, win, wbase, wout, FV.p,
+                                                                        total, cs, kc, pos, dt_local.p);
+    ++launches;
+  }
+  template <int STAGE>
+  void flux_dispatch(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
+    const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
+    const bool local = P.dt_mode == ESR_DT_LOCAL;
+    const bool rus = P.flux == ESR_FLUX_RUSANOV;
+#define ESR_FLUX_CASE(F, M, L) if (rus == (F == 1) && muscl == M && local == L) { launch_flux<F, M, STAGE, L>(win, wbase, wout, cs, pos); return; }
+    ESR_FLUX_CASE(0, true, false) ESR_FLUX_CASE(0, true, true) ESR_FLUX_CASE(0, false, false) ESR_FLUX_CASE(0, false, true)
+    ESR_FLUX_CASE(1, true, false) ESR_FLUX_CASE(1, true, true) ESR_FLUX_CASE(1, false, false) ESR_FLUX_CASE(1, false, true)
+#undef ESR_FLUX_CASE
+  }
+  void recon(const V* w, const Cases<T>& cs, int pos, bool write_dt) {
+    if (P.reconstruction != ESR_RECON_MUSCL) {
+      if (write_dt) {  // constant reconstruction still needs the local dt
+        k_recon<T, false, true><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, nullptr, 0, cs, kc, pos, dt_local.p);
+        ++launches;
+      }
+      return;
+    }
+    if (write_dt) k_recon<T, true, true><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
+    else k_recon<T, true, false><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
+    ++launches;
+  }
+  // one time step of every live slot, step index `pos` inside the chunk
+  void step_kernels(const Cases<T>& cs, int pos) {
+    const bool local = P.dt_mode == ESR_DT_LOCAL;
+    switch (P.time_scheme) {
+      case ESR_TIME_EE:
+        recon(W.p, cs, pos, local);
+        flux_dispatch<ST_FIRST>(W.p, nullptr, Wa.p, cs, pos);
+        k_commit<T><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, Wa.p, W.p, cs, pos);
+        ++launches;
+        break;
+      case ESR_TIME_RK2:
+        recon(W.p, cs, pos, local);
+        flux_dispatch<ST_FIRST>(W.p, nullptr, Wa.p, cs, pos);
+        recon(Wa.p, cs, pos, false);
+        flux_dispatch<ST_RK2_SECOND>(Wa.p, W.p, W.p, cs, pos);
+        break;
+      default:  // SRK2
+        recon(W.p, cs, pos, local);
+        flux_dispatch<ST_FIRST>(W.p, nullptr, Wa.p, cs, pos);
+        recon(Wa.p, cs, pos, false);
+        flux_dispatch<ST_SRK2_SECOND>(Wa.p, W.p, W.p, cs, pos);
+        break;
+    }
+  }
+  void check_point(int pos) {
+    const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    k_mark_due<<<nb, tb, 0, stream>>>(ctl(), n_slots, pos, std::max(1, P.check_every));
+    dim3 grid(n_chunks, n_slots);
+    k_case_reduce<T, RED_NORM><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, Wref.p, due.p, kReduceCells,
+                                                                    partial.p, n_chunks, kc);
+    k_check<<<nb, tb, 0, stream>>>(ctl(), n_slots, pos, partial.p, n_chunks, d_ncells.p, P.threshold,
+                                   std::max(1, P.patience), 0);
+    launches += 3;
+  }
+  void issue_run_chunk(int len) {
+    const Cases<T> cs = cases(false);
+    const int ce = std::max(1, P.check_every);
+    for (int i = 0; i < len; ++i) {
+      step_kernels(cs, i);
+      if ((i + 1) % ce == 0 || i + 1 == len) check_point(i + 1);
+    }
+    const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    k_advance<<<nb, tb, 0, stream>>>(ctl(), n_slots, len, 1);
+    ++launches;
+  }
+  void issue_plain_chunk(int len) {
+    const Cases<T> cs = cases(true);
+    for (int i = 0; i < len; ++i) step_kernels(cs, i);
+    const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    k_advance<<<nb, tb, 0, stream>>>(ctl(), n_slots, len, 0);
+    ++launches;
+  }
+  int run_chunk_len() const {
+    const int ce = std::max(1, P.check_every);
+    if (ce <= kChunkMax) return ce * std::max(1, kChunkMax / ce);
+    for (int l = kChunkMax; l >= 1; --l)
+      if (ce % l == 0) return l;
+    return 1;
+  }
+  int capture(bool run, int len, cudaGraphExec_t* out) {
+    cudaGraph_t graph = nullptr;
+    ESR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = launches;
+    if (run) issue_run_chunk(len); else issue_plain_chunk(len);
+    launches = before;  // counted again when the graph is launched
+    ESR_CUDA(cudaStreamEndCapture(stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return ESR_OK;
+  }
+  int64_t chunk_launches(bool run, int len) {
+    const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
+    const bool local = P.dt_mode == ESR_DT_LOCAL;
+    int per_step;
+    if (P.time_scheme == ESR_TIME_EE) per_step = 2 + ((muscl || local) ? 1 : 0);
+    else per_step = 2 + (muscl ? 2 : (local ? 1 : 0));
+    int64_t n = (int64_t)per_step * len + 1;
+    if (run) {
+      const int ce = std::max(1, P.check_every);
+      int cps = 0;
+      for (int i = 0; i < len; ++i) if ((i + 1) % ce == 0 || i + 1 == len) ++cps;
+      n += 3LL * cps;
+    }
+    return n;
+  }
+  int launch_run_chunk() {
+    const int len = run_chunk_len();
+    if (P.use_graphs) {
+      if (!g_run || g_run_len != len) {
+        if (g_run) cudaGraphExecDestroy(g_run);
+        g_run = nullptr;
+        ESR_TRY(capture(true, len, &g_run));
+        g_run_len = len;
+      }
+      ESR_CUDA(cudaGraphLaunch(g_run, stream));
+      launches += chunk_launches(true, len);
+    } else {
+      issue_run_chunk(len);
+    }
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+
+  // ------------------------------------------------------------- case setup
+  int set_case(int slot, const esr_case* c, const double* W_init, bool defer_dt = false) {
+    int m, b;
+    ESR_TRY(mesh_of_slot(slot, m, b));
+    if (!c) return fail(ESR_ERR_ARG, "set_case: null case");
+    if (!(c->tf > 0) && c->max_steps <= 0) return fail(ESR_ERR_ARG, "set_case: tf must be > 0");
+    if (!(c->cfl > 0)) return fail(ESR_ERR_ARG, "set_case: cfl must be > 0");
+    MeshDev& md = *meshes[m];
+    const HostMesh& hm = *md.hm;
+    const int N = hm.n_cells;
+    hcase[slot] = *c;
+    // per-slot constants: inlet, sponge strength (helper.py:279-285), force reference
+    const V in = mk4<T>((T)c->inlet[0], (T)c->inlet[1], (T)c->inlet[2], (T)c->inlet[3]);
+    const T r = in.x, u = in.y / r, v = in.z / r;
+    const T p = (in.w - kc.half * r * (u * u + v * v)) * kc.gm1;
+    const T U = std::sqrt(u * u + v * v);
+    const T a = std::sqrt(kc.gamma * p / r);
+    const T Ly = (T)hm.y_max - (T)hm.y_min;   // helper.py:271-277 in the state precision
+    const T wdt = (T)0.2 * Ly;
+    T str = (T)1.0 * (U + a) / wdt;
+    if (!(std::isfinite((double)str))) str = T(0);
+    const double cflv = c->cfl;
+    const double tfv = c->tf;
+    const long long ms = c->max_steps;
+    const double q = 0.5 * c->rho_inf * c->u_inf * c->u_inf * c->l_ref;
+    const double qv = q > 0 ? q : 1.0;
+    ESR_CUDA(cudaMemcpyAsync(inlet.p + slot, &in, sizeof(V), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(strength.p + slot, &str, sizeof(T), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(cfl.p + slot, &cflv, sizeof(double), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(tf.p + slot, &tfv, sizeof(double), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(max_steps.p + slot, &ms, sizeof(long long), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(qref.p + slot, &qv, sizeof(double), cudaMemcpyHostToDevice, stream));
+    const int tb = 256, nb = (N + tb - 1) / tb;
+    if (W_init) {
+      if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
+      ESR_CUDA(cudaMemcpyAsync(stage_rows.p, W_init, (size_t)4 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+      k_scatter_state<T><<<nb, tb, 0, stream>>>(stage_rows.p, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
+    } else {
+      k_fill_freestream<T><<<nb, tb, 0, stream>>>(W.p, Wref.p, N, md.off, md.B, b, in);
+    }
+    launches += 1;
+    return reset_slot(slot, defer_dt);
+  }
+  // counters to zero; dt and N from the slot's current state (now, or with the
+  // next flush_fills when deferred so many refills share one reduction)
+  std::vector<int> pending_fill;
+  int reset_slot(int slot, bool defer = false) {
+    const int one = 1, zero = 0;
+    for (DevBuf<int>* bfr : {&step, &ref_step, &streak, &streak_start, &stopping, &due})
+      ESR_CUDA(cudaMemcpyAsync(bfr->p + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(status.p + slot, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(active.p + slot, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    const double inf = INFINITY;
+    ESR_CUDA(cudaMemcpyAsync(last_rel.p + slot, &inf, sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (pending_fill.size() != (size_t)n_slots) pending_fill.assign(n_slots, 0);
+    pending_fill[slot] = 1;
+    return defer ? ESR_OK : flush_fills();
+  }
+  int flush_fills() {
+    if (pending_fill.size() != (size_t)n_slots) return ESR_OK;
+    bool any = false;
+    for (int v : pending_fill) any |= v != 0;
+    if (!any) return ESR_OK;
+    ESR_CUDA(cudaMemcpyAsync(fill.p, pending_fill.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_TRY(finish_fill());
+    ESR_CUDA(cudaStreamSynchronize(stream));  // pending_fill is reused as the copy source
+    std::fill(pending_fill.begin(), pending_fill.end(), 0);
+    return ESR_OK;
+  }
+  // dt + N for every slot flagged in `fill` (one reduction launch for all)
+  int finish_fill() {
+    dim3 grid(n_chunks, n_slots);
+    k_case_reduce<T, RED_DTMIN><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, fill.p, kReduceCells,
+                                                                     partial.p, n_chunks, kc);
+    const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    k_dt_finish<T><<<nb, tb, 0, stream>>>(fill.p, n_slots, partial.p, n_chunks, cfl.p, tf.p, max_steps.p, dt.p, ctl(),
+                                          P.dt_mode == ESR_DT_LOCAL);
+    launches += 2;
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int clear_slot(int slot) {
+    int m, b;
+    ESR_TRY(mesh_of_slot(slot, m, b));
+    const int zero = 0;
+    ESR_CUDA(cudaMemcpyAsync(active.p + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(status.p + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    hcase_index[slot] = -1;
+    return ESR_OK;
+  }
+  int set_state(int slot, const double* Wh, bool device_src) {
+    int m, b;
+    ESR_TRY(mesh_of_slot(slot, m, b));
+    MeshDev& md = *meshes[m];
+    const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
+    if (device_src) {
+      k_copy_in_device<T><<<nb, tb, 0, stream>>>((const V*)Wh, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
+    } else {
+      if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
+      ESR_CUDA(cudaMemcpyAsync(stage_rows.p, Wh, (size_t)4 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+      k_scatter_state<T><<<nb, tb, 0, stream>>>(stage_rows.p, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
+    }
+    ++launches;
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int get_state(int slot, double* Wh, bool device_dst) {
+    int m, b;
+    ESR_TRY(mesh_of_slot(slot, m, b));
+    MeshDev& md = *meshes[m];
+    const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
+    if (device_dst) {
+      k_copy_out_device<T><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, (V*)Wh);
+      ++launches;
+      ESR_CUDA(cudaGetLastError());
+      return ESR_OK;
+    }
+    if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
+    k_gather_state<T><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, stage_rows.p);
+    ++launches;
+    ESR_CUDA(cudaMemcpyAsync(Wh, stage_rows.p, (size_t)4 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    return ESR_OK;
+  }
+
+  // ----------------------------------------------------------------- runs
+  int step_n(int nsteps) {
+    if (nsteps < 0) return fail(ESR_ERR_ARG, "step: nsteps < 0");
+    ESR_CUDA(cudaEventRecord(ev0, stream));
+    int left = nsteps;
+    const int L = 32;
+    while (left > 0) {
+      const int len = std::min(left, L);
+      if (P.use_graphs && len == L) {
+        if (!g_plain || g_plain_len != L) {
+          if (g_plain) cudaGraphExecDestroy(g_plain);
+          g_plain = nullptr;
+          ESR_TRY(capture(false, L, &g_plain));
+          g_plain_len = L;
+        }
+        ESR_CUDA(cudaGraphLaunch(g_plain, stream));
+        launches += chunk_launches(false, L);
+      } else {
+        issue_plain_chunk(len);
+      }
+      left -= len;
+    }
+    ESR_CUDA(cudaEventRecord(ev1, stream));
+    ESR_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_ms = ms;
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int any_active(int& n_live, std::vector<int>* st = nullptr) {
+    std::vector<int> a(n_slots);
+    ESR_CUDA(cudaMemcpyAsync(a.data(), active.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (st) { st->resize(n_slots); ESR_CUDA(cudaMemcpyAsync(st->data(), status.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream)); }
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    n_live = 0;
+    for (int v : a) n_live += v != 0;
+    return ESR_OK;
+  }
+  int run_all(esr_result* res) {
+    ESR_CUDA(cudaEventRecord(ev0, stream));
+    int live = 0;
+    ESR_TRY(any_active(live));
+    int poll = 2;
+    while (live > 0) {
+      for (int i = 0; i < poll; ++i) ESR_TRY(launch_run_chunk());
+      ESR_TRY(any_active(live));
+      poll = std::min(poll * 2, 16);
+    }
+    ESR_CUDA(cudaEventRecord(ev1, stream));
+    ESR_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_ms = ms;
+    if (res) ESR_TRY(results(res));
+    return ESR_OK;
+  }
+  int compute_forces() {
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc);
+    ++launches;
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int results(esr_result* out) {
+    ESR_TRY(compute_forces());
+    std::vector<int> st(n_slots), stp(n_slots), nm(n_slots), sstep(n_slots);
+    std::vector<double> lr(n_slots), fo(2 * n_slots);
+    std::vector<T> d(n_slots);
+    std::vector<long long> ts(n_slots), te(n_slots);
+    ESR_CUDA(cudaMemcpyAsync(st.data(), status.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(stp.data(), step.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(nm.data(), nmax.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(sstep.data(), stopping.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(lr.data(), last_rel.p, n_slots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(fo.data(), forces.p, 2 * n_slots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(d.data(), dt.p, n_slots * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(ts.data(), t_start.p, n_slots * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(te.data(), t_end.p, n_slots * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    for (int g = 0; g < n_slots; ++g) {
+      esr_result& r = out[g];
+      r.status = st[g];
+      r.converged = st[g] == ESR_CASE_CONVERGED;
+      r.stopping_step = (st[g] == ESR_CASE_CONVERGED || st[g] == ESR_CASE_MAXSTEP || st[g] == ESR_CASE_NONFINITE) ? sstep[g] : nm[g];
+      r.steps = stp[g];
+      r.n_max = nm[g];
+      r.case_index = hcase_index[g];
+      r.dt = P.dt_mode == ESR_DT_LOCAL ? 0.0 : (double)d[g];
+      r.last_rel = lr[g];
+      r.cd = fo[2 * g];
+      r.cl = fo[2 * g + 1];
+      r.solve_time_s = (te[g] > ts[g] && st[g] >= ESR_CASE_CONVERGED) ? (double)(te[g] - ts[g]) * 1e-9 : 0.0;
+    }
+    return ESR_OK;
+  }
+  int residual_probe(double* rel) {
+    // one step of every running slot from the current state without keeping it
+    // (euler/main.py:228-230): ||W_probe - W|| / (||W|| + 1e-16)
+    DevBuf<V> save;
+    ESR_TRY(save.alloc(total));
+    ESR_CUDA(cudaMemcpyAsync(save.p, W.p, total * sizeof(V), cudaMemcpyDeviceToDevice, stream));
+    std::vector<int> act(n_slots), st(n_slots);
+    ESR_CUDA(cudaMemcpyAsync(act.data(), active.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(st.data(), status.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int> on(n_slots);
+    for (int g = 0; g < n_slots; ++g) on[g] = st[g] != ESR_CASE_EMPTY;
+    ESR_CUDA(cudaMemcpyAsync(active.p, on.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    step_kernels(cases(true), 0);
+    ESR_CUDA(cudaMemcpyAsync(due.p, on.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    dim3 grid(n_chunks, n_slots);
+    k_case_reduce<T, RED_DIFF><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, save.p, due.p, kReduceCells,
+                                                                    partial.p, n_chunks, kc);
+    ++launches;
+    std::vector<double2> pt((size_t)n_slots * n_chunks);
+    ESR_CUDA(cudaMemcpyAsync(pt.data(), partial.p, pt.size() * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(W.p, save.p, total * sizeof(V), cudaMemcpyDeviceToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(active.p, act.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    for (int g = 0; g < n_slots; ++g) {
+      double s0 = 0, s1 = 0;
+      for (int i = 0; i < n_chunks; ++i) { s0 += pt[(size_t)g * n_chunks + i].x; s1 += pt[(size_t)g * n_chunks + i].y; }
+      rel[g] = on[g] ? std::sqrt(s0) / (std::sqrt(s1) + 1e-16) : 0.0;
+    }
+    return ESR_OK;
+  }
+  int entropy(double* S) {
+    std::vector<int> on(n_slots, 1);
+    ESR_CUDA(cudaMemcpyAsync(due.p, on.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    dim3 grid(n_chunks, n_slots);
+    k_case_reduce<T, RED_ENTROPY><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, due.p, kReduceCells,
+                                                                       partial.p, n_chunks, kc);
+    ++launches;
+    std::vector<double2> pt((size_t)n_slots * n_chunks);
+    ESR_CUDA(cudaMemcpyAsync(pt.data(), partial.p, pt.size() * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    for (int g = 0; g < n_slots; ++g) {
+      double s0 = 0;
+      for (int i = 0; i < n_chunks; ++i) s0 += pt[(size_t)g * n_chunks + i].x;
+      S[g] = s0;
+    }
+    return ESR_OK;
+  }
+  int dts(double* out) {
+    std::vector<T> d(n_slots);
+    ESR_CUDA(cudaMemcpyAsync(d.data(), dt.p, n_slots * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    for (int g = 0; g < n_slots; ++g) out[g] = (double)d[g];
+    return ESR_OK;
+  }
+
+  // ------------------------------------------- batch with retire / refill
+  int batch(const esr_case* cs, int n, const double* const* init, double* const* finals, esr_result* out) {
+    for (int i = 0; i < n; ++i) {
+      if (cs[i].mesh < 0 || cs[i].mesh >= (int)meshes.size()) return fail(ESR_ERR_ARG, "batch: case mesh out of range");
+      out[i] = esr_result{};
+      out[i].case_index = i;
+    }
+    // per-mesh queues
+    std::vector<std::vector<int>> queue(meshes.size());
+    for (int i = n - 1; i >= 0; --i) queue[cs[i].mesh].push_back(i);
+    for (int g = 0; g < n_slots; ++g) ESR_TRY(clear_slot(g));
+    ESR_CUDA(cudaEventRecord(ev0, stream));
+    auto refill = [&](int g) -> int {
+      int m, b;
+      ESR_TRY(mesh_of_slot(g, m, b));
+      if (queue[m].empty()) return ESR_OK;
+      const int i = queue[m].back();
+      queue[m].pop_back();
+      ESR_TRY(set_case(g, &cs[i], init ? init[i] : nullptr, true));
+      hcase_index[g] = i;
+      return ESR_OK;
+    };
+    for (int g = 0; g < n_slots; ++g) ESR_TRY(refill(g));
+    ESR_TRY(flush_fills());
+    std::vector<esr_result> slot_res(n_slots);
+    int remaining = n;
+    int poll = 2;
+    while (remaining > 0) {
+      for (int i = 0; i < poll; ++i) ESR_TRY(launch_run_chunk());
+      int live = 0;
+      std::vector<int> st;
+      ESR_TRY(any_active(live, &st));
+      bool harvest = false;
+      for (int g = 0; g < n_slots; ++g) if (hcase_index[g] >= 0 && st[g] >= ESR_CASE_CONVERGED) harvest = true;
+      if (harvest) {
+        ESR_TRY(results(slot_res.data()));
+        for (int g = 0; g < n_slots; ++g) {
+          if (hcase_index[g] < 0 || st[g] < ESR_CASE_CONVERGED) continue;
+          const int i = hcase_index[g];
+          out[i] = slot_res[g];
+          out[i].case_index = i;
+          if (finals && finals[i]) ESR_TRY(get_state(g, finals[i], false));
+          hcase_index[g] = -1;
+          --remaining;
+          ESR_TRY(refill(g));
+        }
+        ESR_TRY(flush_fills());
+        poll = 2;
+      } else {
+        poll = std::min(poll * 2, 16);
+      }
+      if (live == 0 && remaining > 0) {
+        bool any_filled = false;
+        for (int g = 0; g < n_slots; ++g) any_filled |= hcase_index[g] >= 0;
+        if (!any_filled) return fail(ESR_ERR_STATE, "batch: queue stalled");
+      }
+    }
+    ESR_CUDA(cudaEventRecord(ev1, stream));
+    ESR_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_ms = ms;
+    return ESR_OK;
+  }
+};
+
+struct esr_solver {
+  std::unique_ptr<SolverBase> impl;
+  int precision = 0;
+};
+
+// ------------------------------------------------------------------- C ABI
+#define ESR_GUARD_BEGIN try {
+#define ESR_GUARD_END                                                   \
+  }                                                                     \
+  catch (const std::exception& e) { return fail(ESR_ERR_STATE, e.what()); } \
+  catch (...) { return fail(ESR_ERR_STATE, "unknown C++ exception"); }
+
+template <typename F>
+static int dispatch(esr_solver* s, F&& f) {
+  if (!s || !s->impl) return fail(ESR_ERR_ARG, "null solver");
+  if (s->precision == ESR_PREC_F64) return f(*static_cast<SolverT<double>*>(s->impl.get()));
+  return f(*static_cast<SolverT<float>*>(s->impl.get()));
+}
+
+extern "C" {
+
+int32_t esr_api_version(void) { return ESR_API_VERSION; }
+const char* esr_last_error(void) { return g_last_error.c_str(); }
+
+int esr_mesh_create(const esr_mesh_desc* desc, esr_mesh** out) {
+  ESR_GUARD_BEGIN
+  if (!desc || !out) return fail(ESR_ERR_ARG, "mesh_create: null argument");
+  auto m = std::make_unique<esr_mesh>();
+  std::string err;
+  int rc = esr::prepare_mesh(*desc, m->hm, err);
+  if (rc != ESR_OK) return fail(rc, err);
+  *out = m.release();
+  return ESR_OK;
+  ESR_GUARD_END
+}
+
+int esr_mesh_destroy(esr_mesh* mesh) {
+  delete mesh;
+  return ESR_OK;
+}
+
+int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info) {
+  if (!mesh || !info) return fail(ESR_ERR_ARG, "mesh_get_info: null argument");
+  const HostMesh& hm = mesh->hm;
+  info->n_cells = hm.n_cells;
+  info->n_faces = hm.n_faces;
+  info->n_wall_faces = (int)hm.wall_cell.size();
+  info->n_boundary_slots = hm.n_boundary_slots;
+  info->y_min = hm.y_min;
+  info->y_max = hm.y_max;
+  info->device_bytes_f32 = (int64_t)hm.n_cells * (G_COUNT * 4 + 16);
+  info->device_bytes_f64 = (int64_t)hm.n_cells * (G_COUNT * 8 + 16);
+  return ESR_OK;
+}
+
+int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm) {
+  if (!mesh || !perm) return fail(ESR_ERR_ARG, "mesh_get_permutation: null argument");
+  std::memcpy(perm, mesh->hm.perm.data(), mesh->hm.perm.size() * sizeof(int32_t));
+  return ESR_OK;
+}
+
+int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_mesh, int32_t n_meshes,
+                      const esr_params* params, esr_solver** out) {
+  ESR_GUARD_BEGIN
+  if (!meshes || !slots_per_mesh || n_meshes <= 0 || !params || !out) return fail(ESR_ERR_ARG, "solver_create: null argument");
+  for (int m = 0; m < n_meshes; ++m) {
+    if (!meshes[m]) return fail(ESR_ERR_ARG, "solver_create: null mesh");
+    if (slots_per_mesh[m] <= 0) return fail(ESR_ERR_ARG, "solver_create: slots_per_mesh must be > 0");
+  }
+  const esr_params& p = *params;
+  if (p.precision != ESR_PREC_F32 && p.precision != ESR_PREC_F64) return fail(ESR_ERR_ARG, "unknown precision");
+  if (p.flux != ESR_FLUX_HLLC && p.flux != ESR_FLUX_RUSANOV) return fail(ESR_ERR_ARG, "Unknown flux type");
+  if (p.reconstruction != ESR_RECON_MUSCL && p.reconstruction != ESR_RECON_CONSTANT) return fail(ESR_ERR_ARG, "Unknown reconstruction scheme");
+  if (p.time_scheme < ESR_TIME_SRK2 || p.time_scheme > ESR_TIME_RK2) return fail(ESR_ERR_ARG, "unknown time scheme");
+  if (p.dt_mode != ESR_DT_GLOBAL && p.dt_mode != ESR_DT_LOCAL) return fail(ESR_ERR_ARG, "unknown dt mode");
+  if (p.stop_rule != ESR_STOP_REFERENCE) return fail(ESR_ERR_ARG, "stop rule not supported by this build");
+  if (!(p.gamma > 1.0)) return fail(ESR_ERR_ARG, "gamma must be > 1");
+  auto s = std::make_unique<esr_solver>();
+  s->precision = p.precision;
+  int rc;
+  if (p.precision == ESR_PREC_F64) {
+    auto impl = std::make_unique<SolverT<double>>();
+    rc = impl->init(meshes, slots_per_mesh, n_meshes, &p);
+    s->impl = std::move(impl);
+  } else {
+    auto impl = std::make_unique<SolverT<float>>();
+    rc = impl->init(meshes, slots_per_mesh, n_meshes, &p);
+    s->impl = std::move(impl);
+  }
+  if (rc != ESR_OK) return rc;
+  *out = s.release();
+  return ESR_OK;
+  ESR_GUARD_END
+}
+
+int esr_solver_destroy(esr_solver* solver) {
+  delete solver;
+  return ESR_OK;
+}
+
+int esr_solver_num_slots(const esr_solver* solver, int32_t* n) {
+  if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
+  return dispatch(const_cast<esr_solver*>(solver), [&](auto& s) { *n = s.n_slots; return ESR_OK; });
+}
+
+int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) {
+    int rc = s.set_case(slot, c, W_init);
+    if (rc == ESR_OK) s.hcase_index[slot] = slot;
+    return rc;
+  });
+  ESR_GUARD_END
+}
+int esr_clear_slot(esr_solver* solver, int32_t slot) {
+  return dispatch(solver, [&](auto& s) { return s.clear_slot(slot); });
+}
+int esr_set_state(esr_solver* solver, int32_t slot, const double* W) {
+  if (!W) return fail(ESR_ERR_ARG, "set_state: null state");
+  return dispatch(solver, [&](auto& s) {
+    int rc = s.set_state(slot, W, false);
+    return rc != ESR_OK ? rc : s.reset_slot(slot);
+  });
+}
+int esr_get_state(esr_solver* solver, int32_t slot, double* W) {
+  if (!W) return fail(ESR_ERR_ARG, "get_state: null output");
+  return dispatch(solver, [&](auto& s) { return s.get_state(slot, W, false); });
+}
+int esr_set_state_device(esr_solver* solver, int32_t slot, const void* d_W) {
+  if (!d_W) return fail(ESR_ERR_ARG, "set_state_device: null state");
+  return dispatch(solver, [&](auto& s) {
+    int rc = s.set_state(slot, (const double*)d_W, true);
+    return rc != ESR_OK ? rc : s.reset_slot(slot);
+  });
+}
+int esr_get_state_device(esr_solver* solver, int32_t slot, void* d_W) {
+  if (!d_W) return fail(ESR_ERR_ARG, "get_state_device: null output");
+  return dispatch(solver, [&](auto& s) { return s.get_state(slot, (double*)d_W, true); });
+}
+int esr_compute_dt(esr_solver* solver, double* dt_per_slot) {
+  if (!dt_per_slot) return fail(ESR_ERR_ARG, "compute_dt: null output");
+  return dispatch(solver, [&](auto& s) { return s.dts(dt_per_slot); });
+}
+int esr_step(esr_solver* solver, int32_t nsteps) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.step_n(nsteps); });
+  ESR_GUARD_END
+}
+int esr_run(esr_solver* solver, esr_result* results) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.run_all(results); });
+  ESR_GUARD_END
+}
+int esr_get_results(esr_solver* solver, esr_result* results) {
+  if (!results) return fail(ESR_ERR_ARG, "get_results: null output");
+  return dispatch(solver, [&](auto& s) { return s.results(results); });
+}
+int esr_residual_probe(esr_solver* solver, double* rel) {
+  if (!rel) return fail(ESR_ERR_ARG, "residual_probe: null output");
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.residual_probe(rel); });
+  ESR_GUARD_END
+}
+int esr_forces(esr_solver* solver, double* cd, double* cl) {
+  if (!cd || !cl) return fail(ESR_ERR_ARG, "forces: null output");
+  return dispatch(solver, [&](auto& s) {
+    int rc = s.compute_forces();
+    if (rc != ESR_OK) return rc;
+    std::vector<double> fo(2 * s.n_slots);
+    cudaError_t e = cudaMemcpyAsync(fo.data(), s.forces.p, fo.size() * sizeof(double), cudaMemcpyDeviceToHost, s.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+    if (e != cudaSuccess) return fail(ESR_ERR_CUDA, cudaGetErrorString(e));
+    for (int g = 0; g < s.n_slots; ++g) { cd[g] = fo[2 * g]; cl[g] = fo[2 * g + 1]; }
+    return ESR_OK;
+  });
+}
+int esr_entropy(esr_solver* solver, double* total) {
+  if (!total) return fail(ESR_ERR_ARG, "entropy: null output");
+  return dispatch(solver, [&](auto& s) { return s.entropy(total); });
+}
+int esr_synchronize(esr_solver* solver) {
+  return dispatch(solver, [&](auto& s) {
+    cudaError_t e = cudaStreamSynchronize(s.stream);
+    return e == cudaSuccess ? ESR_OK : fail(ESR_ERR_CUDA, cudaGetErrorString(e));
+  });
+}
+int esr_last_elapsed_ms(esr_solver* solver, double* ms) {
+  if (!ms) return fail(ESR_ERR_ARG, "null output");
+  return dispatch(solver, [&](auto& s) { *ms = s.last_ms; return ESR_OK; });
+}
+int esr_kernel_launches(const esr_solver* solver, int64_t* n) {
+  if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
+  *n = solver->impl->launches;
+  return ESR_OK;
+}
+int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases, const double* const* init_fields,
+                    double* const* final_states, esr_result* results) {
+  ESR_GUARD_BEGIN
+  if (!cases || n_cases < 0 || !results) return fail(ESR_ERR_ARG, "batch_solve: null argument");
+  return dispatch(solver, [&](auto& s) { return s.batch(cases, n_cases, init_fields, final_states, results); });
+  ESR_GUARD_END
+}
+
+int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars, const int32_t* d_idx, const float* d_dist,
+                  int32_t n_dst, int32_t k, float* d_out, void* stream) {
+  if (!d_src || !d_idx || !d_dist || !d_out || n_src <= 0 || n_vars <= 0 || n_dst < 0) return fail(ESR_ERR_ARG, "idw: bad argument");
+  if (k < 1 || k > 16) return fail(ESR_ERR_ARG, "idw: k must be in [1, 16]");
+  if (n_dst == 0) return ESR_OK;
+  const int tb = 128, nb = (n_dst + tb - 1) / tb;
+  esr::k_idw<<<nb, tb, 0, (cudaStream_t)stream>>>(d_src, n_vars, d_idx, d_dist, n_dst, k, d_out);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ESR_OK : fail(ESR_ERR_CUDA, cudaGetErrorString(e));
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// esr_internal.h -- declarations shared by the host runtime files.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/eulersr.h"
+#include "esr_layout.h"
+
+namespace esr {
+
+struct HostMesh {
+  int n_cells = 0, n_faces = 0, n_boundary_slots = 0;
+  double y_min = 0, y_max = 0;
+  std::vector<int> perm;          // new -> old
+  std::vector<int> inv;           // old -> new
+  std::vector<double> geo;        // G_COUNT x n_cells, renumbered
+  std::vector<int> nbr;           // 4 x n_cells (x,y,z neighbours, w packed)
+  std::vector<int> wall_cell;     // renumbered owner cell of each force face
+  std::vector<double> wall_n;     // (nx, ny) per force face
+  std::vector<double> wall_ds;    // face length per force face
+  double inlet_subsonic[4] = {1.0, 1.0, 0.0, 1.0};
+};
+
+int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err);
+std::vector<int> rcm_order(int n, const std::vector<int>& nbr);
+
+}  // namespace esr
+
+struct esr_mesh {
+  esr::HostMesh hm;
+};

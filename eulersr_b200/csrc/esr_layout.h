@@ -1,0 +1,30 @@
+// esr_layout.h -- data-layout constants shared by host and device code.
+#pragma once
+
+namespace esr {
+
+// per-cell geometry fields, stored structure-of-arrays: geo[field * stride + cell]
+enum GeoField {
+  G_C0X, G_C0Y, G_C1X, G_C1Y, G_C2X, G_C2Y,   // LSQ: grad = sum_k c_k (P_k - P_c)
+  G_F0X, G_F0Y, G_F1X, G_F1Y, G_F2X, G_F2Y,   // face midpoint - barycentre
+  G_N0X, G_N0Y, G_N1X, G_N1Y, G_N2X, G_N2Y,   // outward unit normals
+  G_S0, G_S1, G_S2,                           // face lengths
+  G_AREA, G_BLEND3,                           // cell area, sponge blend^3
+  G_COUNT
+};
+
+// slot kinds (face markers of euler/jax_fvm/src/mesh.py:47-52)
+enum SlotKind { K_INTERIOR = 0, K_WALL = 2, K_INLET = 3, K_OUTLET = 4, K_SUBSONIC = 5 };
+
+// neighbour word w: per edge slot k, bits 6k..6k+2 kind, 6k+3..6k+4 the
+// neighbour's slot of the shared face
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int slot_kind(int packed, int k) { return (packed >> (6 * k)) & 7; }
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int slot_opp(int packed, int k) { return (packed >> (6 * k + 3)) & 3; }
+
+}  // namespace esr

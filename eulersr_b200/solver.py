@@ -1,0 +1,297 @@
+"""Python face of the native solver: meshes, solver handles, cases.
+
+Every numerical step runs in ``libeulersr.so`` on the GPU; this module only
+marshals arrays. There is no CPU path: if the library or a CUDA device is
+missing, the constructors raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _ffi as F
+from .mesh import Mesh
+
+
+# ------------------------------------------------------------------ cases
+def freestream(mach: float, aoa_deg: float = 0.0, gamma: float = 1.4, rho_inf: float = 1.0, p_inf: float = 1.0,
+               dtype=np.float64):
+    """Conserved freestream state (euler/main.py:28-41): primitive
+    (rho, M c cos a, M c sin a, p) converted in ``dtype``."""
+    c_inf = (gamma * p_inf / rho_inf) ** 0.5
+    a = math.radians(aoa_deg)
+    prim = np.asarray([rho_inf, mach * c_inf * np.cos(a), mach * c_inf * np.sin(a), p_inf], dtype=dtype)
+    t = prim.dtype.type
+    rho, u, v, p = prim
+    E = p / ((t(gamma) - 1) * t(1.0) ** 2) + t(0.5) * rho * (u ** 2 + v ** 2)
+    return np.asarray([rho, rho * u, rho * v, E], dtype=dtype)
+
+
+def clamp_cfl(mach: float, cfl: float) -> float:
+    """Transonic CFL clamp of euler/main.py:117-120."""
+    return 0.45 if (0.6 < mach < 1.1 and cfl > 0.45) else cfl
+
+
+@dataclass
+class FlowCase:
+    """One (Mach, alpha) run on mesh index ``mesh`` of a solver."""
+    mach: float
+    aoa_deg: float = 0.0
+    mesh: int = 0
+    cfl: float = 0.6
+    tf: float = 4.0
+    max_steps: int = 0
+    gamma: float = 1.4
+    rho_inf: float = 1.0
+    p_inf: float = 1.0
+    l_ref: float = 1.0
+    clamp: bool = True
+    dtype: type = np.float64
+
+    def to_c(self) -> F.Case:
+        c = F.Case()
+        c.mesh = int(self.mesh)
+        c.mach = float(self.mach)
+        c.aoa_deg = float(self.aoa_deg)
+        c.cfl = float(clamp_cfl(self.mach, self.cfl) if self.clamp else self.cfl)
+        c.tf = float(self.tf)
+        c.max_steps = int(self.max_steps)
+        inl = freestream(self.mach, self.aoa_deg, self.gamma, self.rho_inf, self.p_inf, self.dtype)
+        for i in range(4):
+            c.inlet[i] = float(inl[i])
+        c.rho_inf = float(self.rho_inf)
+        c.u_inf = float(self.mach * math.sqrt(self.gamma * self.p_inf / self.rho_inf))
+        c.l_ref = float(self.l_ref)
+        return c
+
+
+# ------------------------------------------------------------------- mesh
+class DeviceMesh:
+    """A mesh prepared by the native library (renumbered, geometry in float64)."""
+
+    def __init__(self, mesh: Mesh, renumber: bool = True, sponge: bool | None = None, sponge_width: float | None = None):
+        L = F.lib()
+        self.mesh = mesh
+        self._keep = dict(points=F.f64(mesh.points), tris=F.i32(mesh.tris), neighbors=F.i32(mesh.neighbors),
+                          faces=F.i32(mesh.faces), face_markers=F.i32(mesh.face_markers),
+                          face_connectivity=F.i32(mesh.face_connectivity), walls=F.i32(mesh.wall_markers()))
+        k = self._keep
+        d = F.MeshDesc()
+        d.n_points, d.n_cells, d.n_faces = len(k['points']), len(k['tris']), len(k['faces'])
+        d.points = F.ptr(k['points'], C.c_double)
+        d.tris = F.ptr(k['tris'], C.c_int32)
+        d.neighbors = F.ptr(k['neighbors'], C.c_int32)
+        d.faces = F.ptr(k['faces'], C.c_int32)
+        d.face_markers = F.ptr(k['face_markers'], C.c_int32)
+        d.face_connectivity = F.ptr(k['face_connectivity'], C.c_int32)
+        d.wall_markers = F.ptr(k['walls'], C.c_int32)
+        d.n_wall_markers = len(k['walls'])
+        d.force_marker = mesh.force_marker()
+        if sponge is None:
+            sponge = mesh.metadata.get('case') != 'bump'
+        d.sponge = int(bool(sponge))
+        d.sponge_width = float(sponge_width or 0.0)
+        sub = mesh.metadata.get('inlet_subsonic', [1.0, 1.0, 0.0, 1.0])
+        for i in range(4):
+            d.inlet_subsonic[i] = float(sub[i])
+        d.renumber = int(bool(renumber))
+        h = C.c_void_p()
+        F.check(L.esr_mesh_create(C.byref(d), C.byref(h)))
+        self.handle = h
+        info = F.MeshInfo()
+        F.check(L.esr_mesh_get_info(h, C.byref(info)))
+        self.info = info
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.info.n_cells)
+
+    def permutation(self) -> np.ndarray:
+        perm = np.empty(self.n_cells, dtype=np.int32)
+        F.check(F.lib().esr_mesh_get_permutation(self.handle, F.ptr(perm, C.c_int32)))
+        return perm
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            F.lib().esr_mesh_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------------- solver
+class Solver:
+    """All case slots of one or more meshes, advanced together on one GPU."""
+
+    def __init__(self, meshes, slots, precision='f32', flux='hllc', reconstruction='muscl', time_scheme='SRK2',
+                 dt_mode='global', stop_rule='reference', gamma=1.4, threshold=1e-6, check_every=25, patience=1,
+                 device=0, use_graphs=True, block_size=0):
+        L = F.lib()
+        if isinstance(meshes, (DeviceMesh, Mesh)):
+            meshes = [meshes]
+        self.meshes = [m if isinstance(m, DeviceMesh) else DeviceMesh(m) for m in meshes]
+        slots = [int(slots)] * len(self.meshes) if np.isscalar(slots) else [int(s) for s in slots]
+        if len(slots) != len(self.meshes):
+            raise ValueError("one slot count per mesh")
+        p = F.Params()
+        p.precision = F.PREC[str(precision).lower()]
+        try:
+            p.flux = F.FLUX[str(flux).lower()]
+        except KeyError:
+            raise ValueError(f"Unknown flux type '{flux}'.") from None
+        try:
+            p.reconstruction = F.RECON[str(reconstruction).lower()]
+        except KeyError:
+            raise ValueError(f"Unknown reconstruction scheme '{reconstruction}'. Expected 'constant' or 'muscl'.") from None
+        p.time_scheme = F.TIME[str(time_scheme).upper()]
+        p.dt_mode = F.DT_MODE[dt_mode]
+        p.stop_rule = F.STOP_RULE[stop_rule]
+        p.gamma = float(gamma)
+        p.threshold = float(threshold)
+        p.check_every = max(1, int(check_every))
+        p.patience = max(1, int(patience))
+        p.device = int(device)
+        p.use_graphs = int(bool(use_graphs))
+        p.block_size = int(block_size)
+        self.params = p
+        self.precision = 'f64' if p.precision == 1 else 'f32'
+        self.dtype = np.float64 if p.precision == 1 else np.float32
+        arr = (C.c_void_p * len(self.meshes))(*[m.handle for m in self.meshes])
+        sl = np.asarray(slots, dtype=np.int32)
+        h = C.c_void_p()
+        F.check(L.esr_solver_create(arr, F.ptr(sl, C.c_int32), len(self.meshes), C.byref(p), C.byref(h)))
+        self.handle = h
+        n = C.c_int32()
+        F.check(L.esr_solver_num_slots(h, C.byref(n)))
+        self.n_slots = int(n.value)
+        self.slots = slots
+        self.slot_mesh = np.repeat(np.arange(len(slots)), slots)
+
+    # ----------------------------------------------------------- state
+    def _n_cells(self, slot):
+        return self.meshes[int(self.slot_mesh[slot])].n_cells
+
+    def set_case(self, slot: int, case: FlowCase, W_init=None):
+        c = case.to_c()
+        if W_init is not None:
+            W = F.f64(W_init)
+            if W.shape != (self._n_cells(slot), 4):
+                raise ValueError(f"init field has shape {W.shape}, expected ({self._n_cells(slot)}, 4)")
+            F.check(F.lib().esr_set_case(self.handle, slot, C.byref(c), F.ptr(W, C.c_double)))
+        else:
+            F.check(F.lib().esr_set_case(self.handle, slot, C.byref(c), None))
+
+    def set_state(self, slot: int, W):
+        W = F.f64(W)
+        if W.shape != (self._n_cells(slot), 4):
+            raise ValueError("state shape mismatch")
+        F.check(F.lib().esr_set_state(self.handle, slot, F.ptr(W, C.c_double)))
+
+    def get_state(self, slot: int = 0) -> np.ndarray:
+        out = np.empty((self._n_cells(slot), 4), dtype=np.float64)
+        F.check(F.lib().esr_get_state(self.handle, slot, F.ptr(out, C.c_double)))
+        return out
+
+    def set_state_device(self, slot: int, ptr: int):
+        F.check(F.lib().esr_set_state_device(self.handle, slot, C.c_void_p(ptr)))
+
+    def get_state_device(self, slot: int, ptr: int):
+        F.check(F.lib().esr_get_state_device(self.handle, slot, C.c_void_p(ptr)))
+
+    def clear_slot(self, slot: int):
+        F.check(F.lib().esr_clear_slot(self.handle, slot))
+
+    # ------------------------------------------------------------ runs
+    def dt(self) -> np.ndarray:
+        out = np.empty(self.n_slots)
+        F.check(F.lib().esr_compute_dt(self.handle, F.ptr(out, C.c_double)))
+        return out
+
+    def step(self, nsteps: int = 1):
+        F.check(F.lib().esr_step(self.handle, int(nsteps)))
+
+    def run(self) -> list[dict]:
+        res = (F.Result * self.n_slots)()
+        F.check(F.lib().esr_run(self.handle, res))
+        return [r.as_dict() for r in res]
+
+    def results(self) -> list[dict]:
+        res = (F.Result * self.n_slots)()
+        F.check(F.lib().esr_get_results(self.handle, res))
+        return [r.as_dict() for r in res]
+
+    def residual_probe(self) -> np.ndarray:
+        out = np.empty(self.n_slots)
+        F.check(F.lib().esr_residual_probe(self.handle, F.ptr(out, C.c_double)))
+        return out
+
+    def forces(self):
+        cd = np.empty(self.n_slots)
+        cl = np.empty(self.n_slots)
+        F.check(F.lib().esr_forces(self.handle, F.ptr(cd, C.c_double), F.ptr(cl, C.c_double)))
+        return cd, cl
+
+    def entropy(self) -> np.ndarray:
+        out = np.empty(self.n_slots)
+        F.check(F.lib().esr_entropy(self.handle, F.ptr(out, C.c_double)))
+        return out
+
+    def synchronize(self):
+        F.check(F.lib().esr_synchronize(self.handle))
+
+    def elapsed_ms(self) -> float:
+        v = C.c_double()
+        F.check(F.lib().esr_last_elapsed_ms(self.handle, C.byref(v)))
+        return float(v.value)
+
+    def kernel_launches(self) -> int:
+        v = C.c_int64()
+        F.check(F.lib().esr_kernel_launches(self.handle, C.byref(v)))
+        return int(v.value)
+
+    def batch_solve(self, cases, init_fields=None, want_states=False):
+        """Solve every case through the slots with retire/refill; returns
+        (results, final states or None)."""
+        n = len(cases)
+        carr = (F.Case * n)(*[c.to_c() for c in cases])
+        res = (F.Result * n)()
+        keep = []
+        init_arr = None
+        if init_fields is not None:
+            init_arr = (F._f64p * n)()
+            for i, f in enumerate(init_fields):
+                if f is not None:
+                    a = F.f64(f)
+                    keep.append(a)
+                    init_arr[i] = F.ptr(a, C.c_double)
+        fin_arr = None
+        states = None
+        if want_states:
+            states = [np.empty((self.meshes[c.mesh].n_cells, 4)) for c in cases]
+            fin_arr = (F._f64p * n)(*[F.ptr(s, C.c_double) for s in states])
+        F.check(F.lib().esr_batch_solve(self.handle, carr, n, init_arr, fin_arr, res))
+        return [r.as_dict() for r in res], states
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            F.lib().esr_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,209 @@
+/*
+ * eulersr.h -- C ABI of the B200-native explicit finite-volume Euler solver.
+ *
+ * This is the boundary a host (Python through ctypes, or any FFI) binds to
+ * replace EulerSR's JAX solve path. Every entry point is extern "C", takes
+ * plain pointers and sizes, returns an int status (ESR_OK = 0) and never lets
+ * an exception cross the boundary; the text of the last error of the calling
+ * thread is returned by esr_last_error().
+ *
+ * Reference interfaces each call replaces (paths inside the EulerSR checkout):
+ *   esr_mesh_create      Mesh (euler/jax_fvm/src/mesh.py:28-150) + its geometry
+ *                        (mesh.py:223-260), loaded by euler/config.py:63-79
+ *   esr_solver_create    kwargs + scheme selection of euler/main.py:43-60
+ *   esr_set_case         euler/main.py:28-41 initialize(); the warm-start init
+ *                        field of eval/_fvm_solve_worker.py:97-105
+ *   esr_compute_dt       euler/jax_fvm/src/helper.py:8-18 get_dt (with the CFL
+ *                        clamp of euler/main.py:117-121)
+ *   esr_step             euler/jax_fvm/src/euler_solver.py:635-643
+ *                        time_step_RK2_SSP (and :630-653 EE/RK2)
+ *   esr_run              the lax.scan loop and stop rule of euler/main.py:141-216
+ *   esr_residual_probe   euler/main.py:228-230 and eval/_fvm_solve_worker.py:120-139
+ *   esr_forces           euler/jax_fvm/src/helper.py:366-415 (get_drag/lift_coefficient)
+ *   esr_entropy          euler/jax_fvm/src/helper.py:312-320 get_total_entropy
+ *   esr_batch_solve      the serial grid loop of slurm/run_euler_grid.py:94-104,
+ *                        run as one batch with retire/refill
+ *   esr_idw_apply        eval/core.py:135-142 predict_idw (weights utils/metrics.py:9-14)
+ *
+ * Threading: a solver handle owns one CUDA stream and must not be used from
+ * two threads at once. Handles of different solvers are independent.
+ */
+#ifndef EULERSR_H
+#define EULERSR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESR_API_VERSION 1
+
+/* status codes */
+#define ESR_OK             0
+#define ESR_ERR_ARG        1   /* invalid argument (ValueError in the reference) */
+#define ESR_ERR_CUDA       2   /* CUDA runtime error */
+#define ESR_ERR_NONFINITE  3   /* non-finite value met where a finite one is required */
+#define ESR_ERR_TIMEOUT    4   /* a bounded device wait gave up */
+#define ESR_ERR_OOM        5   /* device allocation failed */
+#define ESR_ERR_STATE      6   /* call not valid in the handle's current state */
+
+/* per-case status words (esr_result.status) */
+#define ESR_CASE_EMPTY      0
+#define ESR_CASE_RUNNING    1
+#define ESR_CASE_CONVERGED  2   /* stop rule met `patience` times in a row */
+#define ESR_CASE_MAXSTEP    3   /* reached N = int(tf/dt)+1 (or max_steps) unconverged */
+#define ESR_CASE_NONFINITE  4   /* NaN/Inf in the state norm: case retired */
+
+/* options */
+#define ESR_PREC_F32 0
+#define ESR_PREC_F64 1
+#define ESR_FLUX_HLLC 0
+#define ESR_FLUX_RUSANOV 1
+#define ESR_RECON_MUSCL 0
+#define ESR_RECON_CONSTANT 1
+#define ESR_TIME_SRK2 0
+#define ESR_TIME_EE 1
+#define ESR_TIME_RK2 2
+#define ESR_DT_GLOBAL 0        /* one dt per case from the initial field (reference) */
+#define ESR_DT_LOCAL 1         /* per-cell CFL dt recomputed every step */
+#define ESR_STOP_REFERENCE 0   /* ||W_n - W_ref||_F / (steps (||W_ref||_F + 1e-16)) */
+#define ESR_STOP_DENSITY_L2 1  /* RMS over cells of the density residual */
+
+/* Mesh description; all host arrays are owned by the caller and copied. */
+typedef struct esr_mesh_desc {
+    int32_t n_points;
+    int32_t n_cells;
+    int32_t n_faces;
+    const double*  points;            /* (n_points, 2) */
+    const int32_t* tris;              /* (n_cells, 3), counter-clockwise */
+    const int32_t* neighbors;         /* (n_cells, 3), cell across edge k (v_k, v_k+1), -1 = boundary */
+    const int32_t* faces;             /* (n_faces, 2) vertex ids */
+    const int32_t* face_markers;      /* (n_faces,) 0 interior, 2 wall, 3 inlet, 4 outlet, 5 subsonic inlet */
+    const int32_t* face_connectivity; /* (n_cells, 3) face id of edge k */
+    const int32_t* wall_markers;      /* markers treated as slip walls (NULL -> {2}) */
+    int32_t n_wall_markers;
+    int32_t force_marker;             /* marker of the faces the force coefficients integrate (2) */
+    int32_t sponge;                   /* 1: top/bottom sponge layer (all cases but 'bump') */
+    double sponge_width;              /* <= 0: 0.2 * (y_max - y_min) */
+    double inlet_subsonic[4];         /* rho, u, v, p of the subsonic inlet (marker 5) */
+    int32_t renumber;                 /* 1: reorder cells (reverse Cuthill-McKee) for locality */
+} esr_mesh_desc;
+
+typedef struct esr_mesh_info {
+    int32_t n_cells;
+    int32_t n_faces;
+    int32_t n_wall_faces;
+    int32_t n_boundary_slots;
+    double y_min, y_max;
+    int64_t device_bytes_f32;
+    int64_t device_bytes_f64;
+} esr_mesh_info;
+
+typedef struct esr_params {
+    int32_t precision;        /* ESR_PREC_* */
+    int32_t flux;             /* ESR_FLUX_* */
+    int32_t reconstruction;   /* ESR_RECON_* */
+    int32_t time_scheme;      /* ESR_TIME_* */
+    int32_t dt_mode;          /* ESR_DT_* */
+    int32_t stop_rule;        /* ESR_STOP_* */
+    double gamma;             /* ratio of specific heats of the run (1.4) */
+    double threshold;         /* stationarity threshold */
+    int32_t check_every;      /* steps between stop-rule checks (>= 1) */
+    int32_t patience;         /* consecutive checks under the threshold (>= 1) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t use_graphs;       /* 1: capture step chunks in CUDA graphs */
+    int32_t block_size;       /* threads per block for the cell kernels (0: autotuned) */
+    int32_t reserved;
+} esr_params;
+
+/* One (Mach, alpha) case. inlet = conserved freestream (euler/main.py:39). */
+typedef struct esr_case {
+    int32_t mesh;             /* index of the mesh the case runs on */
+    int32_t reserved;
+    double mach;
+    double aoa_deg;
+    double cfl;               /* already clamped by the caller or not: see esr_params */
+    double tf;                /* N = int(tf/dt) + 1 */
+    int64_t max_steps;        /* extra cap on N (0: none) */
+    double inlet[4];          /* conserved inlet state */
+    double rho_inf;           /* force reference density */
+    double u_inf;             /* force reference speed |U_inf| */
+    double l_ref;             /* force reference length (obstacle_length) */
+} esr_case;
+
+typedef struct esr_result {
+    int32_t status;           /* ESR_CASE_* */
+    int32_t converged;        /* 1 when the stop rule confirmed */
+    int32_t stopping_step;    /* first step of the confirming streak, else N */
+    int32_t steps;            /* steps actually advanced */
+    int32_t n_max;            /* N = int(tf/dt)+1 (capped by max_steps) */
+    int32_t case_index;       /* index into the submitted case list */
+    double dt;                /* global dt of the case (0 in local mode) */
+    double last_rel;          /* last stop-rule value */
+    double cd, cl;            /* body-axis pressure force coefficients at the end */
+    double solve_time_s;      /* device time from the case's start to its retirement */
+} esr_result;
+
+typedef struct esr_mesh esr_mesh;
+typedef struct esr_solver esr_solver;
+
+int32_t     esr_api_version(void);
+const char* esr_last_error(void);
+
+int esr_mesh_create(const esr_mesh_desc* desc, esr_mesh** out);
+int esr_mesh_destroy(esr_mesh* mesh);
+int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info);
+/* new-to-old cell permutation chosen by the renumbering (n_cells entries) */
+int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm);
+
+/* A solver holds `n_meshes` meshes and slots_per_mesh[m] concurrent case
+ * slots on mesh m; all slots advance together in one launch per kernel. */
+int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_mesh, int32_t n_meshes,
+                      const esr_params* params, esr_solver** out);
+int esr_solver_destroy(esr_solver* solver);
+int esr_solver_num_slots(const esr_solver* solver, int32_t* n_slots);
+/* Slot `slot` gets case `c`; W_init = (n_cells, 4) conserved state in the
+ * caller's cell order, or NULL for the freestream of c->inlet. Computes the
+ * case's dt (global mode) and resets its stop-rule counters. */
+int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init);
+int esr_clear_slot(esr_solver* solver, int32_t slot);
+int esr_set_state(esr_solver* solver, int32_t slot, const double* W);
+int esr_get_state(esr_solver* solver, int32_t slot, double* W);
+/* device-resident float32/float64 state of a slot in the caller's cell order */
+int esr_set_state_device(esr_solver* solver, int32_t slot, const void* d_W);
+int esr_get_state_device(esr_solver* solver, int32_t slot, void* d_W);
+int esr_compute_dt(esr_solver* solver, double* dt_per_slot);
+/* Advance every running slot by nsteps (no stop rule). */
+int esr_step(esr_solver* solver, int32_t nsteps);
+/* Run every running slot to its stop (stop rule, N, or non-finite). */
+int esr_run(esr_solver* solver, esr_result* results_per_slot);
+int esr_get_results(esr_solver* solver, esr_result* results_per_slot);
+int esr_residual_probe(esr_solver* solver, double* rel_per_slot);
+int esr_forces(esr_solver* solver, double* cd_per_slot, double* cl_per_slot);
+int esr_entropy(esr_solver* solver, double* total_per_slot);
+int esr_synchronize(esr_solver* solver);
+/* Device milliseconds of the solver's stream between the last two esr_run /
+ * esr_step / esr_batch_solve boundaries. */
+int esr_last_elapsed_ms(esr_solver* solver, double* ms);
+/* Number of kernel launches issued by the solver since creation. */
+int esr_kernel_launches(const esr_solver* solver, int64_t* n);
+
+/* Solve n_cases cases through the solver's slots: every slot retired by the
+ * stop rule is refilled in place with the next queued case. init_fields[i]
+ * is a (n_cells,4) conserved warm start or NULL; final_states[i] receives the
+ * final state when non-NULL. results has n_cases entries. */
+int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases,
+                    const double* const* init_fields, double* const* final_states,
+                    esr_result* results);
+
+/* IDW (k neighbours, weights 1/(d^2+1e-12) normalised) of a source field onto
+ * target points; all pointers are device pointers, float32, row-major. */
+int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars,
+                  const int32_t* d_idx, const float* d_dist, int32_t n_dst, int32_t k,
+                  float* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EULERSR_H */

@@ -1,0 +1,581 @@
+"""CPU oracle: a NumPy restatement of EulerSR's explicit FVM hot path.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the shipped package imports this module;
+only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of
+``bench.py`` use it, and only as the checker.
+
+Parity status: **unpinned** against the reference itself. The reference runs on
+JAX 0.4.38 (``pyproject.toml:14``), which is not installed here or on the GPU
+hosts, and the reference ships no tests, fixtures or golden vectors. This
+module therefore restates the reference source line by line (citations below
+are ``path:line`` inside the EulerSR checkout) and is pinned instead by
+known-answer properties (freestream preservation, HLLC consistency, LSQ
+exactness on linear fields) and by the analytic diamond shock-expansion theory
+(``oracle/theory.py``).
+
+All arithmetic is done in the dtype of the input arrays (float32 or float64),
+as the reference does under ``JAX_ENABLE_X64`` false / true. Quirks that are
+kept on purpose:
+
+* neighbour index -1 wraps to the last cell before boundary states overwrite
+  it (``euler_solver.py:108``);
+* the limiter min/max includes boundary ghost states (``euler_solver.py:46-47``);
+* the limiter threshold is 1e-7 in float32 and 1e-12 in float64, the
+  Venkatakrishnan denominator keeps a fixed 1e-7 (``euler_solver.py:38,55``);
+* MUSCL is first order on boundary faces (marker > 1) (``euler_solver.py:87-95``);
+* every interior face flux is evaluated once from each side
+  (``euler_solver.py:376-420`` over (N,3) face slots);
+* the wall ghost and the force coefficients use gamma=1.4 and M=1 whatever the
+  run's gamma (``helper.py:198-202,368``);
+* the global dt is computed once from the initial field (``euler/main.py:121``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+
+
+# ----------------------------------------------------------------------------
+# Mesh geometry (restates euler/jax_fvm/src/mesh.py:223-260)
+# ----------------------------------------------------------------------------
+
+@dataclass
+class OracleMesh:
+    """Minimal mesh record with the attributes the reference solver reads
+    (``mesh.py:131-150``): connectivity plus per-cell geometry."""
+
+    points: np.ndarray
+    tris: np.ndarray
+    neighbors: np.ndarray
+    faces: np.ndarray
+    face_markers: np.ndarray
+    face_connectivity: np.ndarray
+    face_connectivity_opposite: np.ndarray
+    barycenter: np.ndarray
+    area: np.ndarray
+    surface: np.ndarray
+    normals: np.ndarray
+    metadata: dict = field(default_factory=dict)
+
+
+def build_oracle_mesh(points, tris, neighbors, faces, face_markers, face_connectivity,
+                      dtype=np.float64, metadata: dict | None = None,
+                      face_connectivity_opposite=None) -> OracleMesh:
+    """Geometry in ``dtype`` exactly as ``mesh.py`` computes it.
+
+    barycenter = mean of the 3 vertices (``mesh.py:223-224``); normal k = (dy,-dx)/len
+    of edge v_k -> v_{k+1} (``mesh.py:226-230``); area = |1/2 cross| (``mesh.py:232-237``);
+    surface = face length (``mesh.py:239-240``). Without periodic faces
+    ``face_connectivity_opposite`` is the identity (``mesh.py:279-281``).
+    """
+    pts = np.asarray(points, dtype=dtype)
+    tris = np.asarray(tris, dtype=np.int64)
+    faces = np.asarray(faces, dtype=np.int64)
+    P = pts[tris]                                   # (N,3,2)
+    bary = np.mean(P, axis=-2)
+    diff = np.roll(P, -1, axis=-2) - P
+    norm = np.linalg.norm(diff, axis=-1)
+    normals = np.stack([diff[..., 1], -diff[..., 0]], -1) / norm[..., None]
+    area = np.abs(dtype(0.5) * ((P[..., 1, 1] - P[..., 0, 1]) * (P[..., 2, 0] - P[..., 0, 0])
+                                - (P[..., 1, 0] - P[..., 0, 0]) * (P[..., 2, 1] - P[..., 0, 1])))
+    surface = np.linalg.norm(pts[faces[:, 1]] - pts[faces[:, 0]], axis=1)
+    if face_connectivity_opposite is None:
+        face_connectivity_opposite = np.arange(faces.shape[0])
+    return OracleMesh(points=pts, tris=tris, neighbors=np.asarray(neighbors, dtype=np.int64),
+                      faces=faces, face_markers=np.asarray(face_markers, dtype=np.int64),
+                      face_connectivity=np.asarray(face_connectivity, dtype=np.int64),
+                      face_connectivity_opposite=np.asarray(face_connectivity_opposite, dtype=np.int64),
+                      barycenter=bary, area=area, surface=surface, normals=normals,
+                      metadata=dict(metadata or {}))
+
+
+# ----------------------------------------------------------------------------
+# State conversions (helper.py:25-46)
+# ----------------------------------------------------------------------------
+
+def get_conserved(P, gamma=1.4, M=1.0):
+    """helper.py:25-35."""
+    dt = P.dtype.type
+    rho, u, v, p = P[..., 0], P[..., 1], P[..., 2], P[..., 3]
+    E = p / ((dt(gamma) - 1) * dt(M) ** 2) + dt(0.5) * rho * (u ** 2 + v ** 2)
+    return np.stack([rho, rho * u, rho * v, E], axis=-1)
+
+
+def get_primitive(W, gamma=1.4, M=1.0):
+    """helper.py:37-46."""
+    dt = W.dtype.type
+    rho = W[..., 0]
+    u = W[..., 1] / rho
+    v = W[..., 2] / rho
+    p = (W[..., 3] - dt(0.5) * rho * (u ** 2 + v ** 2)) * dt(M) ** 2 * (dt(gamma) - 1)
+    return np.stack([rho, u, v, p], axis=-1)
+
+
+# ----------------------------------------------------------------------------
+# Time step (helper.py:8-18)
+# ----------------------------------------------------------------------------
+
+def get_dt(W, mesh: OracleMesh, CFL=0.5, gamma=1.4, M=1.0):
+    """Global CFL time step: CFL * min_i area_i / sum_k (c_i + |u_i.n_ik|) s_ik."""
+    dt = W.dtype.type
+    P = get_primitive(W, gamma, M)
+    c = np.sqrt(np.abs(dt(gamma) * P[..., 3] / P[..., 0])) / dt(M)
+    un = P[..., 1, None] * mesh.normals[..., 0] + P[..., 2, None] * mesh.normals[..., 1]
+    lam = c[..., None] + np.abs(un)
+    dt_cell = mesh.area / np.sum(lam * mesh.surface[mesh.face_connectivity], axis=-1)
+    return np.min(dt_cell) * dt(CFL)
+
+
+def get_local_dt(W, mesh: OracleMesh, CFL=0.5, gamma=1.4, M=1.0):
+    """Per-cell dt of the same formula (the local-time-step option)."""
+    dt = W.dtype.type
+    P = get_primitive(W, gamma, M)
+    c = np.sqrt(np.abs(dt(gamma) * P[..., 3] / P[..., 0])) / dt(M)
+    un = P[..., 1, None] * mesh.normals[..., 0] + P[..., 2, None] * mesh.normals[..., 1]
+    lam = c[..., None] + np.abs(un)
+    return mesh.area / np.sum(lam * mesh.surface[mesh.face_connectivity], axis=-1) * dt(CFL)
+
+
+# ----------------------------------------------------------------------------
+# Boundary states (helper.py:168-256)
+# ----------------------------------------------------------------------------
+
+def _face_marker_slots(mesh):
+    return mesh.face_markers[mesh.face_connectivity]          # (N,3)
+
+
+def bc_state(W_R, W_L, mesh: OracleMesh, inlet, wall_markers=None, inlet_subsonic=None):
+    """helper.py:233-256: walls (slip, gamma=1.4 fixed), inflow (3), outflow (4),
+    subsonic inlet (5), applied in that order on the (N,3,4) neighbour states."""
+    dt = W_L.dtype.type
+    mk = _face_marker_slots(mesh)
+    if wall_markers is None:
+        wall_markers = mesh.metadata.get('wall_markers', [2])
+    try:
+        wall_markers = tuple(int(m) for m in wall_markers)
+    except TypeError:
+        wall_markers = (int(wall_markers),)
+    # helper.py:196-204 slip wall, value = 0 background flow, default gamma=1.4
+    P_L = get_primitive(W_L)
+    vn = P_L[..., 1] * mesh.normals[..., 0] + P_L[..., 2] * mesh.normals[..., 1]
+    vb = P_L[..., 1:3] - dt(2) * vn[..., None] * mesh.normals
+    P_b = P_L.copy()
+    P_b[..., 1:3] = vb
+    W_wall = get_conserved(P_b)
+    for m in wall_markers:
+        W_R = np.where((mk == m)[..., None], W_wall, W_R)
+    # helper.py:173-177 inflow
+    W_R = np.where((mk == 3)[..., None], np.asarray(inlet, dtype=W_L.dtype), W_R)
+    # helper.py:168-171 outflow
+    W_R = np.where((mk == 4)[..., None], W_L, W_R)
+    # helper.py:179-194 subsonic inlet: rho,u,v from the mesh, p from the cell (gamma 1.4)
+    if np.any(mk == 5):
+        if inlet_subsonic is None:
+            inlet_subsonic = np.array([1.0, 1.0, 0.0, 1.0])
+        sub = np.asarray(inlet_subsonic, dtype=W_L.dtype)
+        P_s = get_primitive(W_L)
+        P_s[..., 0:3] = sub[0:3]
+        rho, u, v, p = P_s[..., 0], P_s[..., 1], P_s[..., 2], P_s[..., 3]
+        W_s = np.stack([rho, rho * u, rho * v, p / dt(1.4 - 1) + dt(0.5) * rho * (u ** 2 + v ** 2)], -1)
+        W_R = np.where((mk == 5)[..., None], W_s, W_R)
+    return W_R
+
+
+# ----------------------------------------------------------------------------
+# Reconstruction (helper.py:136-153, euler_solver.py:36-122)
+# ----------------------------------------------------------------------------
+
+def face_midpoints(mesh: OracleMesh):
+    """Face midpoints per cell slot, recomputed from the points as the
+    reference does on every call (``euler_solver.py:49``)."""
+    return np.mean(mesh.points[mesh.faces[mesh.face_connectivity]], axis=-2)   # (N,3,2)
+
+
+def lsq_gradient(P_L, P_R, mesh: OracleMesh):
+    """helper.py:136-153: weighted least squares, boundary faces use twice the
+    face-midpoint offset; one 2x2 LU solve per (cell, variable)."""
+    dt = P_L.dtype.type
+    dx = mesh.barycenter[mesh.neighbors] - mesh.barycenter[..., None, :]
+    repl = dt(2) * (face_midpoints(mesh) - mesh.barycenter[..., None, :])
+    dx = np.where((_face_marker_slots(mesh) > 0)[..., None], repl, dx)
+    dW = P_R - P_L
+    w = 1 / np.linalg.norm(dx, axis=-1) ** 2
+    A = np.einsum('ijk,ijl->ikl', w[..., None] * dx, dx)
+    b = np.einsum('ijk,ijl->ikl', w[..., None] * dW, dx)           # (N,4,2)
+    Ab = np.broadcast_to(A[:, None], (A.shape[0], b.shape[1], 2, 2))
+    return np.linalg.solve(Ab, b[..., None])[..., 0].astype(P_L.dtype)   # (N,4,2)
+
+
+def venkatakrishnan(a, b):
+    """euler_solver.py:36-39 with K=0 (omega = 0)."""
+    dt = a.dtype.type
+    return (a ** 2 + dt(2) * a * b) / (a ** 2 + dt(2) * b ** 2 + a * b + dt(1e-7))
+
+
+def limiter(P_L, P_R, grad, mesh: OracleMesh):
+    """euler_solver.py:45-67: min over the 3 faces of the Venkatakrishnan
+    function, with the cell + 3 neighbour/ghost states as the bounds."""
+    dt = P_L.dtype.type
+    Wm = np.min(np.concatenate([P_L, P_R], axis=-2), axis=-2)
+    WM = np.max(np.concatenate([P_L, P_R], axis=-2), axis=-2)
+    dxf = face_midpoints(mesh) - mesh.barycenter[..., None, :]
+    Delta = np.einsum('ijl,ikl->ijk', dxf, grad)
+    eps = dt(1e-12) if P_L.dtype == np.float64 else dt(1e-7)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        phi = np.ones_like(Delta)
+        phi = np.where(Delta > eps, venkatakrishnan(WM[..., None, :] - P_L, Delta), phi)
+        phi = np.where(Delta < -eps, venkatakrishnan(Wm[..., None, :] - P_L, Delta), phi)
+    return np.min(phi, axis=-2)
+
+
+def muscl(P_L, P_R, grad, mesh: OracleMesh):
+    """euler_solver.py:69-98."""
+    dt = P_L.dtype.type
+    phi = limiter(P_L, P_R, grad, mesh)
+    mid = face_midpoints(mesh)
+    dxf = mid - mesh.barycenter[..., None, :]
+    Delta = np.einsum('ijl,ikl->ijk', dxf, grad)
+    mid_n = np.mean(mesh.points[mesh.faces[mesh.face_connectivity_opposite[mesh.face_connectivity]]], axis=-2)
+    dxn = mid_n - mesh.barycenter[mesh.neighbors]
+    bnd = (_face_marker_slots(mesh) > 1)
+    dxn = np.where(bnd[..., None], -dxf, dxn)
+    Delta_n = np.einsum('ijl,ijkl->ijk', dxn, grad[mesh.neighbors])
+    phi_L = np.where(bnd[..., None], dt(0), np.repeat(phi[..., None, :], 3, axis=-2))
+    WL = P_L + phi_L * Delta
+    phi_R = np.where(bnd[..., None], dt(0), phi[mesh.neighbors])
+    WR = P_R + phi_R * Delta_n
+    return WL, WR
+
+
+def build_reconstruction(W, mesh: OracleMesh, gamma=1.4, M=1.0, inlet=None,
+                         reconstruction='muscl', wall_markers=None):
+    """euler_solver.py:106-122."""
+    W_L = np.repeat(W[..., None, :], 3, axis=-2)
+    W_R = W[mesh.neighbors]                      # -1 wraps to the last cell
+    W_R = bc_state(W_R, W_L, mesh, inlet, wall_markers)
+    rec = reconstruction.lower()
+    if rec in ('constant', 'first_order', 'none', 'godunov'):
+        return W_L, W_R
+    if rec in ('muscl', 'second_order', '2nd_order'):
+        P_L = get_primitive(W_L, gamma, M)
+        P_R = get_primitive(W_R, gamma, M)
+        grad = lsq_gradient(P_L, P_R, mesh)
+        P_L, P_R = muscl(P_L, P_R, grad, mesh)
+        return get_conserved(P_L, gamma, M), get_conserved(P_R, gamma, M)
+    raise ValueError(f"Unknown reconstruction scheme '{reconstruction}'. Expected 'constant' or 'muscl'.")
+
+
+# ----------------------------------------------------------------------------
+# Fluxes (euler_solver.py:141-143,203-240,273-420)
+# ----------------------------------------------------------------------------
+
+def hllc_dissipation(W_L, W_R, normals, gamma=1.4, M=1.0):
+    """euler_solver.py:273-374: returns central flux minus the HLLC flux."""
+    dt = W_L.dtype.type
+    g, Mm = dt(gamma), dt(M)
+    PL = get_primitive(W_L, gamma, M)
+    PR = get_primitive(W_R, gamma, M)
+    rL, uL, vL, pL = PL[..., 0], PL[..., 1], PL[..., 2], PL[..., 3]
+    rR, uR, vR, pR = PR[..., 0], PR[..., 1], PR[..., 2], PR[..., 3]
+    nx, ny = normals[..., 0], normals[..., 1]
+    unL = uL * nx + vL * ny
+    unR = uR * nx + vR * ny
+    tx, ty = -ny, nx
+    utL = uL * tx + vL * ty
+    utR = uR * tx + vR * ty
+    aL = np.sqrt(np.abs(g * pL / rL)) / Mm
+    aR = np.sqrt(np.abs(g * pR / rR)) / Mm
+    SL = np.minimum(unL - aL, unR - aR)
+    SR = np.maximum(unL + aL, unR + aR)
+    SL = np.where(SL == SR, SL - dt(1e-6), SL)
+    SR = np.where(SL == SR, SR + dt(1e-6), SR)
+    EL, ER = W_L[..., 3], W_R[..., 3]
+    FL = np.stack([rL * unL, rL * uL * unL + pL * nx / Mm ** 2, rL * vL * unL + pL * ny / Mm ** 2,
+                   (EL + pL / Mm ** 2) * unL], -1)
+    FR = np.stack([rR * unR, rR * uR * unR + pR * nx / Mm ** 2, rR * vR * unR + pR * ny / Mm ** 2,
+                   (ER + pR / Mm ** 2) * unR], -1)
+    Fc = dt(0.5) * (FL + FR)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        den = rL * (SL - unL) - rR * (SR - unR)
+        den = np.where(den == 0, dt(1e-12), den)
+        Ss = (pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR)) / den
+        PsL = pL + rL * (SL - unL) * (Ss - unL)
+        PsR = pR + rR * (SR - unR) * (Ss - unR)
+        Ps = dt(0.5) * (PsL + PsR)
+        rsL = rL * (SL - unL) / (SL - Ss)
+        UsL = np.stack([rsL, rsL * (Ss * nx + utL * tx), rsL * (Ss * ny + utL * ty),
+                        ((SL - unL) * EL - pL * unL + Ps * Ss) / (SL - Ss)], -1)
+        rsR = rR * (SR - unR) / (SR - Ss)
+        UsR = np.stack([rsR, rsR * (Ss * nx + utR * tx), rsR * (Ss * ny + utR * ty),
+                        ((SR - unR) * ER - pR * unR + Ps * Ss) / (SR - Ss)], -1)
+    SLb, SRb, Ssb = SL[..., None], SR[..., None], Ss[..., None]
+    F = np.where(SLb >= 0, FL,
+                 np.where((SLb <= 0) & (Ssb >= 0), FL + SLb * (UsL - W_L),
+                          np.where((Ssb <= 0) & (SRb >= 0), FR + SRb * (UsR - W_R), FR)))
+    return Fc - F
+
+
+def rusanov_dissipation(W_L, W_R, normals, gamma=1.4, M=1.0):
+    """euler_solver.py:203-240 (plain branch): 0.5 * C_max * (W_R - W_L)."""
+    dt = W_L.dtype.type
+    g, Mm = dt(gamma), dt(M)
+    PL = get_primitive(W_L, gamma, M)
+    PR = get_primitive(W_R, gamma, M)
+    nx, ny = normals[..., 0], normals[..., 1]
+    CL = np.sqrt(np.abs(g * PL[..., 3] / PL[..., 0])) / Mm + np.abs(PL[..., 1] * nx + PL[..., 2] * ny)
+    CR = np.sqrt(np.abs(g * PR[..., 3] / PR[..., 0])) / Mm + np.abs(PR[..., 1] * nx + PR[..., 2] * ny)
+    Cmax = np.maximum(CR, CL)
+    return dt(0.5) * Cmax[..., None] * (W_R - W_L)
+
+
+def get_flux(W_L, W_R, normals, surfaces, gamma=1.4, M=1.0, flux='hllc'):
+    """euler_solver.py:376-420 then apply_face_surfaces (:141-143)."""
+    dt = W_L.dtype.type
+    Mm = dt(M)
+    PL = get_primitive(W_L, gamma, M)
+    PR = get_primitive(W_R, gamma, M)
+    nx, ny = normals[..., 0], normals[..., 1]
+    unL = PL[..., 1] * nx + PL[..., 2] * ny
+    unR = PR[..., 1] * nx + PR[..., 2] * ny
+    inv_m2 = 1 / Mm ** 2
+    FL = [PL[..., 0] * unL, PL[..., 0] * PL[..., 1] * unL + inv_m2 * PL[..., 3] * nx,
+          PL[..., 0] * PL[..., 2] * unL + inv_m2 * PL[..., 3] * ny, (W_L[..., 3] + inv_m2 * PL[..., 3]) * unL]
+    FR = [PR[..., 0] * unR, PR[..., 0] * PR[..., 1] * unR + inv_m2 * PR[..., 3] * nx,
+          PR[..., 0] * PR[..., 2] * unR + inv_m2 * PR[..., 3] * ny, (W_R[..., 3] + inv_m2 * PR[..., 3]) * unR]
+    Fc = np.stack([dt(0.5) * (a + b) for a, b in zip(FL, FR)], -1)
+    f = flux.lower()
+    if f in ('hll', 'hllc'):
+        Fc = Fc - hllc_dissipation(W_L, W_R, normals, gamma, M)
+    elif f == 'rusanov':
+        Fc = Fc - rusanov_dissipation(W_L, W_R, normals, gamma, M)
+    else:
+        raise ValueError(f"Unknown flux type '{flux}'.")
+    return np.sum(surfaces[..., None] * Fc, axis=-2)
+
+
+# ----------------------------------------------------------------------------
+# Sponge and residual (helper.py:262-295, euler_solver.py:602-628)
+# ----------------------------------------------------------------------------
+
+def sponge_source(W, mesh: OracleMesh, inlet, gamma=1.4, M=1.0, width=None, strength=None):
+    """helper.py:262-295: cubic relaxation towards the inlet state in a band of
+    width 0.2*Ly along the bottom and top boundaries (none for 'bump')."""
+    dt = W.dtype.type
+    if mesh.metadata.get('case') == 'bump':
+        return np.zeros_like(W)
+    y_min = np.min(mesh.points[:, 1])
+    y_max = np.max(mesh.points[:, 1])
+    Ly = y_max - y_min
+    if width is None:
+        width = dt(0.2) * Ly
+    inlet = np.asarray(inlet, dtype=W.dtype)
+    Pinf = get_primitive(inlet, gamma, M)
+    U_inf = np.sqrt(Pinf[1] ** 2 + Pinf[2] ** 2)
+    a_inf = np.sqrt(dt(gamma) * Pinf[3] / Pinf[0]) / dt(M)
+    if strength is None:
+        strength = dt(1.0) * (U_inf + a_inf) / width
+    y = mesh.barycenter[..., 1]
+    dist = np.minimum(y - y_min, y_max - y)
+    blend = np.clip((width - dist) / width, dt(0), dt(1))
+    sigma = strength * blend ** 3
+    return sigma[..., None] * (inlet[None, :] - W)
+
+
+def residual(W, mesh: OracleMesh, inlet, gamma=1.4, M=1.0, reconstruction='muscl', flux='hllc',
+             wall_markers=None):
+    """euler_solver.py:602-628: dW/dt = -(sum_k F_k s_k)/area + sponge, returned
+    with the reference's sign convention (Flux/area - sponge)."""
+    W_L, W_R = build_reconstruction(W, mesh, gamma, M, inlet, reconstruction, wall_markers)
+    F = get_flux(W_L, W_R, mesh.normals, mesh.surface[mesh.face_connectivity], gamma, M, flux)
+    return F / mesh.area[..., None] - sponge_source(W, mesh, inlet, gamma, M)
+
+
+def time_step_srk2(W, mesh, dt, inlet, **kw):
+    """euler_solver.py:635-643 (strong-stability-preserving RK2)."""
+    h = W.dtype.type(0.5)
+    k1 = residual(W, mesh, inlet, **kw)
+    W1 = W - dt * k1
+    k2 = residual(W1, mesh, inlet, **kw)
+    return h * (W + W1 - dt * k2)
+
+
+def time_step_ee(W, mesh, dt, inlet, **kw):
+    """euler_solver.py:630-633."""
+    return W - dt * residual(W, mesh, inlet, **kw)
+
+
+def time_step_rk2(W, mesh, dt, inlet, **kw):
+    """euler_solver.py:645-653 (Heun)."""
+    h = W.dtype.type(0.5)
+    F1 = residual(W, mesh, inlet, **kw)
+    W1 = W - dt * F1
+    F2 = residual(W1, mesh, inlet, **kw)
+    Wn = W - dt * F2
+    return h * (Wn + W1)
+
+
+TIME_SCHEMES = {'SRK2': time_step_srk2, 'SSP_RK2': time_step_srk2, 'EE': time_step_ee, 'RK2': time_step_rk2}
+
+
+# ----------------------------------------------------------------------------
+# Initial state, forces, entropy (euler/main.py:28-41, helper.py:312-320,366-415)
+# ----------------------------------------------------------------------------
+
+AOA_CASES = ("diamond", "naca0012", "naca2412", "rae2822", "oneraD", "oa209", "diamond_tx",
+             "diamond_txy", "diamond_alpha10", "rae2822_txy", "diamond_sym", "naca23012",
+             "diamond_big", "cylinder")
+
+
+def initialize(n_cells, cfg, dtype=np.float64):
+    """euler/main.py:28-41: freestream primitive (rho, M c cos a, M c sin a, p)
+    to conserved; the angle of attack only applies to the AoA cases."""
+    rho_inf, p_inf, gamma, mach = cfg['rho_inf'], cfg['p_inf'], cfg['gamma'], cfg['Mach']
+    c_inf = (gamma * p_inf / rho_inf) ** 0.5
+    aoa = float(cfg.get('aoa', 0.0)) if str(cfg.get('case', '')).lower() in [c.lower() for c in AOA_CASES] else 0.0
+    a = math.radians(aoa)
+    prim0 = np.asarray([rho_inf, mach * c_inf * np.cos(a), mach * c_inf * np.sin(a), p_inf], dtype=dtype)
+    W = get_conserved(np.tile(prim0[None, :], (n_cells, 1)), gamma, 1.0)
+    inlet = get_conserved(prim0[None], gamma, 1.0)[0]
+    return W, inlet
+
+
+def wall_owner_data(mesh: OracleMesh, marker=2):
+    """Owner cell and local slot of every face with the force marker, found as
+    the reference finds them: the first cell listing the face (``helper.py:373-379``)."""
+    wall_faces = np.where(mesh.face_markers == marker)[0]
+    fc = mesh.face_connectivity
+    cells = np.array([int(np.argmax(np.any(fc == f, axis=1))) for f in wall_faces], dtype=np.int64)
+    slots = np.array([int(np.argmax(fc[c] == f)) for c, f in zip(cells, wall_faces)], dtype=np.int64)
+    return wall_faces, cells, slots
+
+
+def force_coefficients(W, mesh: OracleMesh, rho_inf, U_inf, L_ref, marker=None):
+    """helper.py:366-415: body-axis pressure force coefficients (cd uses nx,
+    cl uses ny), cell-centred pressure at gamma=1.4."""
+    if marker is None:
+        marker = int(mesh.metadata.get('force_marker', 2))
+    P = get_primitive(W)[:, 3]
+    faces, cells, slots = wall_owner_data(mesh, marker)
+    n = mesh.normals[cells, slots]
+    ds = mesh.surface[faces]
+    q = 0.5 * rho_inf * U_inf ** 2
+    cd = np.sum(P[cells] * n[:, 0] * ds) / (q * L_ref)
+    cl = np.sum(P[cells] * n[:, 1] * ds) / (q * L_ref)
+    return float(cd), float(cl)
+
+
+def total_entropy(W, mesh: OracleMesh, gamma=1.4):
+    """helper.py:48-55,312-315."""
+    dt = W.dtype.type
+    rho = W[..., 0]
+    u = W[..., 1] / rho
+    v = W[..., 2] / rho
+    p = (W[..., 3] - dt(0.5) * rho * (u ** 2 + v ** 2)) * (dt(gamma) - 1)
+    s = np.log(p / rho ** dt(gamma))
+    return np.sum(rho * s * mesh.area / (dt(gamma) - 1), axis=-1)
+
+
+# ----------------------------------------------------------------------------
+# The stepping loop with the stationarity rule (euler/main.py:116-230)
+# ----------------------------------------------------------------------------
+
+@dataclass
+class OracleRun:
+    W: np.ndarray
+    dt: float
+    n_max: int
+    converged: bool
+    stopping_step: int
+    steps_taken: int
+    last_rel: float
+    final_residual: float
+    rel_history: list
+
+
+def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None = None,
+        stop_rule: str = 'reference') -> OracleRun:
+    """euler/main.py:43-230 without the I/O.
+
+    CFL is clamped to 0.45 for 0.6 < M < 1.1 (``:117-120``); dt is computed once
+    (``:121``); N = int(tf/dt)+1 (``:122``). Every ``check_every`` steps and at
+    step N, rel = ||W - W_ref|| / (steps * (||W_ref|| + 1e-16)) (``:150-152``);
+    ``patience`` consecutive checks under the threshold stop the run and the
+    stopping step is the first step of that streak (``:153-158``). Stopped steps
+    keep W (``:146``). ``stop_rule='density_l2'`` replaces rel by the density
+    residual L2 ||rho_{n} - rho_{n-1}||/sqrt(N) / dt of the last step.
+    ``max_steps`` caps N for tests.
+    """
+    cfl = float(cfg['CFL'])
+    if 0.6 < cfg['Mach'] < 1.1 and cfl > 0.45:
+        cfl = 0.45
+    gamma = cfg['gamma']
+    kw = dict(gamma=gamma, M=1.0, reconstruction=cfg.get('reconstruction', 'MUSCL'),
+              flux=cfg.get('flux', 'HLLC'))
+    fn = TIME_SCHEMES[str(cfg.get('time_scheme', 'SRK2')).upper()]
+    dt = get_dt(W, mesh, CFL=cfl, gamma=gamma, M=1.0)
+    N = int(cfg['tf'] / dt) + 1
+    if max_steps is not None:
+        N = min(N, int(max_steps))
+    thr = float(cfg['stationarity_threshold'])
+    every = int(cfg['stationarity_check_every'])
+    patience = max(1, int(cfg.get('stationarity_patience', 1)))
+    W_ref = W
+    ref_step = 0
+    last_rel = math.inf
+    stop = False
+    stopping_step = N
+    streak = 0
+    streak_start = 0
+    hist = []
+    steps_taken = 0
+    for step in range(1, N + 1):
+        W_prev = W
+        if not stop:
+            W = fn(W, mesh, dt, inlet, **kw)
+            steps_taken = step
+        if step % every == 0 or step == N:
+            block = max(1, step - ref_step)
+            if stop_rule == 'density_l2':
+                rel = float(np.sqrt(np.mean((W[:, 0].astype(np.float64) - W_prev[:, 0]) ** 2)) / float(dt))
+            else:
+                rel = float(np.linalg.norm(W - W_ref) / (block * (np.linalg.norm(W_ref) + 1e-16)))
+            under = rel <= thr
+            new_streak = streak + 1 if under else 0
+            if under and streak == 0:
+                streak_start = step
+            confirmed = new_streak >= patience and not stop
+            if confirmed:
+                stop = True
+                stopping_step = streak_start
+            streak = new_streak
+            W_ref = W
+            ref_step = step
+            last_rel = rel
+            hist.append((step, rel))
+            if stop:
+                break
+    W_probe = fn(W, mesh, dt, inlet, **kw)
+    final_res = float(np.linalg.norm(W_probe - W) / (np.linalg.norm(W) + 1e-16))
+    return OracleRun(W=W, dt=float(dt), n_max=N, converged=stop, stopping_step=int(stopping_step),
+                     steps_taken=steps_taken, last_rel=last_rel, final_residual=final_res, rel_history=hist)
+
+
+# ----------------------------------------------------------------------------
+# IDW interpolation (eval/core.py:135-142, utils/metrics.py:9-14)
+# ----------------------------------------------------------------------------
+
+def idw_weights(dist, eps=1e-12):
+    """utils/metrics.py:9-14: w = 1/(d^2+eps), normalised per row (p=2)."""
+    d = np.asarray(dist, dtype=np.float64)
+    w = 1.0 / (d ** 2 + eps)
+    return w / w.sum(axis=1, keepdims=True)
+
+
+def idw_predict(lr_prim, idx, dist, k=6):
+    """eval/core.py:135-142: float32 weighted sum of the k nearest LR cells."""
+    idx_k = np.asarray(idx)[:, :k].astype(np.int64)
+    w = idw_weights(np.asarray(dist)[:, :k])
+    return (w[:, :, None].astype(np.float32) * np.asarray(lr_prim)[idx_k]).sum(axis=1)

@@ -1,0 +1,160 @@
+"""CUDA kernels vs the NumPy oracle on the same meshes and inputs.
+
+Tolerances: float64 kernels vs float64 oracle 1e-12 (field-scaled relative,
+after 100 SRK2 steps); float32 kernels vs float32 oracle 1e-5 after 100 steps;
+force coefficients 1e-4 relative in float32. A whole float64 run (hundreds
+of steps) is held to 1e-10. The float32 dt is held to 2e-6 relative: the oracle
+derives the geometry in float32 as the reference does, the library derives it in
+float64 and rounds once, so the minimum cell's area/perimeter term differs by
+a few ulp.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_mesh, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def _oracle_steps(mesh, dtype, mach, aoa, steps, cfl=0.6, flux='hllc', recon='muscl', scheme='SRK2'):
+    from oracle import euler_oracle as O
+    om = oracle_mesh(mesh, dtype)
+    cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa, case=mesh.metadata['case'])
+    W, inlet = O.initialize(mesh.n_cells, cfg, dtype)
+    c = 0.45 if (0.6 < mach < 1.1 and cfl > 0.45) else cfl
+    dt = O.get_dt(W, om, CFL=c)
+    fn = O.TIME_SCHEMES[scheme]
+    for _ in range(steps):
+        W = fn(W, om, dt, inlet, reconstruction=recon, flux=flux)
+    return W, dt, om, inlet
+
+
+def _gpu_steps(mesh, prec, mach, aoa, steps, cfl=0.6, flux='hllc', recon='muscl', scheme='SRK2', **kw):
+    from eulersr_b200.solver import Solver, FlowCase
+    dtype = np.float64 if prec == 'f64' else np.float32
+    s = Solver(mesh, 1, precision=prec, flux=flux, reconstruction=recon, time_scheme=scheme, **kw)
+    s.set_case(0, FlowCase(mach=mach, aoa_deg=aoa, cfl=cfl, tf=100.0, dtype=dtype, l_ref=1.0))
+    dt = s.dt()[0]
+    s.step(steps)
+    W = s.get_state(0)
+    return W, dt, s
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", TOL64), ("f32", TOL32)])
+def test_srk2_100_steps_diamond(diamond02, prec, tol):
+    dtype = np.float64 if prec == 'f64' else np.float32
+    Wo, dto, _, _ = _oracle_steps(diamond02, dtype, 2.5, 5.0, 100)
+    Wg, dtg, _ = _gpu_steps(diamond02, prec, 2.5, 5.0, 100)
+    dt_tol = 1e-14 if prec == 'f64' else 2e-6
+    assert abs(dtg - float(dto)) <= dt_tol * float(dto)
+    assert rel_err(Wg, Wo) <= tol, rel_err(Wg, Wo)
+
+
+def test_srk2_transonic_naca_f64(naca02):
+    Wo, dto, _, _ = _oracle_steps(naca02, np.float64, 0.8, 2.0, 60)
+    Wg, dtg, _ = _gpu_steps(naca02, 'f64', 0.8, 2.0, 60)
+    assert abs(dtg - dto) <= 1e-14 * dto
+    assert rel_err(Wg, Wo) <= TOL64
+
+
+@pytest.mark.parametrize("flux,recon,scheme", [("rusanov", "muscl", "SRK2"), ("hllc", "constant", "SRK2"),
+                                               ("hllc", "muscl", "EE"), ("hllc", "muscl", "RK2"),
+                                               ("rusanov", "constant", "EE")])
+def test_scheme_variants_f64(diamond02, flux, recon, scheme):
+    Wo, _, _, _ = _oracle_steps(diamond02, np.float64, 1.8, -3.0, 30, flux=flux, recon=recon, scheme=scheme)
+    Wg, _, _ = _gpu_steps(diamond02, 'f64', 1.8, -3.0, 30, flux=flux, recon=recon, scheme=scheme)
+    assert rel_err(Wg, Wo) <= TOL64
+
+
+def test_golden_fixture_f64(diamond02, golden):
+    g = np.load(golden / "oracle_diamond_h0.2_M2.5_a5_srk2x20.npz")
+    Wg, dtg, _ = _gpu_steps(diamond02, 'f64', 2.5, 5.0, int(g['steps']))
+    assert abs(dtg - float(g['dt'])) <= 1e-14 * float(g['dt'])
+    assert rel_err(Wg, g['W']) <= TOL64
+
+
+def test_forces_entropy_probe(diamond02):
+    from oracle import euler_oracle as O
+    Wo, dto, om, inlet = _oracle_steps(diamond02, np.float64, 2.0, 0.0, 50)
+    Wg, _, s = _gpu_steps(diamond02, 'f64', 2.0, 0.0, 50)
+    cd, cl = s.forces()
+    cdo, clo = O.force_coefficients(Wo, om, 1.0, 2.0 * np.sqrt(1.4), 1.0)
+    assert abs(cd[0] - cdo) <= 1e-10 * max(abs(cdo), 1e-3)
+    assert abs(cl[0] - clo) <= 1e-10 + 1e-10 * abs(clo)
+    S = s.entropy()[0]
+    So = O.total_entropy(Wo, om, 1.4)
+    assert abs(S - So) <= 1e-10 * max(1.0, abs(So))
+    rel = s.residual_probe()[0]
+    Wp = O.time_step_srk2(Wo, om, dto, inlet)
+    relo = np.linalg.norm(Wp - Wo) / (np.linalg.norm(Wo) + 1e-16)
+    assert abs(rel - relo) <= 1e-8 * relo
+    # the probe must not change the state
+    assert np.array_equal(s.get_state(0), Wg)
+
+
+def test_determinism_and_graphs(diamond02):
+    Wa, _, _ = _gpu_steps(diamond02, 'f32', 2.5, 5.0, 40, use_graphs=True)
+    Wb, _, _ = _gpu_steps(diamond02, 'f32', 2.5, 5.0, 40, use_graphs=True)
+    Wc, _, _ = _gpu_steps(diamond02, 'f32', 2.5, 5.0, 40, use_graphs=False)
+    assert np.array_equal(Wa, Wb)
+    assert np.array_equal(Wa, Wc)
+
+
+def test_renumbering_invariance(diamond02):
+    from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
+    out = []
+    for ren in (True, False):
+        s = Solver(DeviceMesh(diamond02, renumber=ren), 1, precision='f64')
+        s.set_case(0, FlowCase(mach=2.5, aoa_deg=5.0, cfl=0.6, tf=100.0))
+        s.step(30)
+        out.append(s.get_state(0))
+    assert np.array_equal(out[0], out[1])
+
+
+def test_stop_rule_matches_oracle_f64(diamond02):
+    """Full run with the reference stop rule: same stopping step, converged flag
+    and final field as the oracle's loop (euler/main.py:141-216)."""
+    from oracle import euler_oracle as O
+    from eulersr_b200.solver import Solver, FlowCase
+    cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=2.5, aoa=5.0, case='diamond', CFL=0.6, tf=6.0,
+               stationarity_threshold=1e-4, stationarity_check_every=25, stationarity_patience=2)
+    om = oracle_mesh(diamond02, np.float64)
+    W0, inlet = O.initialize(diamond02.n_cells, cfg, np.float64)
+    ro = O.run(W0, om, inlet, cfg)
+    s = Solver(diamond02, 1, precision='f64', threshold=1e-4, check_every=25, patience=2)
+    s.set_case(0, FlowCase(mach=2.5, aoa_deg=5.0, cfl=0.6, tf=6.0))
+    r = s.run()[0]
+    assert r['n_max'] == ro.n_max
+    assert bool(r['converged']) == ro.converged
+    assert r['stopping_step'] == ro.stopping_step
+    assert rel_err(s.get_state(0), ro.W) <= 1e-10
+
+
+def test_maxstep_cap(diamond02):
+    from eulersr_b200.solver import Solver, FlowCase
+    s = Solver(diamond02, 1, precision='f32', threshold=1e-30, check_every=7)
+    s.set_case(0, FlowCase(mach=2.5, aoa_deg=5.0, cfl=0.6, tf=0.05))
+    r = s.run()[0]
+    assert r['status'] == 3 and not r['converged']
+    assert r['steps'] == r['n_max'] == int(np.float32(0.05) / np.float32(r['dt'])) + 1
+
+
+def test_batch_equals_single(diamond02, naca02):
+    """A case solved inside a ragged two-mesh batch with retire/refill is
+    bitwise identical to the same case solved alone."""
+    from eulersr_b200.solver import Solver, FlowCase
+    cases = [FlowCase(mach=m, aoa_deg=a, mesh=i % 2, cfl=0.6, tf=0.4)
+             for i, (m, a) in enumerate([(2.5, 5.0), (1.5, -2.0), (3.0, 1.0), (0.9, 0.5), (2.0, 0.0)])]
+    s = Solver([diamond02, naca02], [2, 1], precision='f32', threshold=1e-5, check_every=10)
+    res, states = s.batch_solve(cases, want_states=True)
+    for i in (0, 3):
+        c = cases[i]
+        one = Solver([diamond02, naca02][c.mesh], 1, precision='f32', threshold=1e-5, check_every=10)
+        one.set_case(0, FlowCase(mach=c.mach, aoa_deg=c.aoa_deg, cfl=0.6, tf=0.4))
+        r1 = one.run()[0]
+        assert r1['stopping_step'] == res[i]['stopping_step']
+        assert r1['status'] == res[i]['status']
+        assert np.array_equal(one.get_state(0), states[i])
