@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Throughput of the batched explicit FVM solve on B200.
+
+Workload (one GPU): the batched plain method on NACA0012, HR mesh h=0.025
+(about 25k cells), 256 (Mach, alpha) cases drawn with default_rng(1):
+Mach ~ U[0.7, 3.0], alpha from {-5, -4.5, ..., 5} deg; FP32, HLLC + MUSCL
+(Venkatakrishnan) + SRK2, global CFL dt, freestream start. One bench step
+advances every case of the batch by ``--chunk`` SRK2 steps (default 50).
+
+value   cell-updates/s (one cell advanced one full SRK2 step), state resident
+        in HBM, device time from CUDA events on the solver stream.
+e2e     the same through the public API with host buffers: every step uploads
+        the 256 initial fields from pinned host memory (esr_set_case), runs
+        the chunk, and reads every final field back (esr_get_state).
+roofline  the dominant kernel (K2 flux/update) against the measured HBM copy
+        bandwidth; algorithmic bytes per launch = (40 + 64/B) B per cell and
+        case, half of the (80 + 128/B) B of a full SRK2 cell-update.
+
+--impl reference times the oracle (the NumPy restatement of the reference's
+JAX solver; the reference itself needs JAX, absent on these hosts) on the
+host cores on a bounded sample of the same workload.
+
+Under torchrun every rank runs its own 256-case batch (weak scaling; cases
+are independent, no data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "converged HR cases/s at ≤0.5% CD err, warm-start vs plain; cell-upd/s; GB/s"
+UNIT = "cell-updates/s"
+MESH_CACHE = Path(os.environ.get("EULERSR_MESH_CACHE", Path(tempfile.gettempdir()) / "eulersr_meshes"))
+
+
+def get_mesh(geom: str, h: float):
+    from eulersr_b200.mesh import Mesh
+    from eulersr_b200.meshing import build_mesh
+    MESH_CACHE.mkdir(parents=True, exist_ok=True)
+    p = MESH_CACHE / f"{geom}_h{h}.npz"
+    if p.exists():
+        return Mesh.load(p)
+    m = build_mesh(geom, h)
+    m.save(p)
+    return m
+
+
+def batch_cases(n, seed=1):
+    rng = np.random.default_rng(seed)
+    mach = rng.uniform(0.7, 3.0, n)
+    aoa = rng.choice(np.arange(-5, 5.01, 0.5), n)
+    return mach, aoa
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = Path(tempfile.gettempdir()) / f"eulersr_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace('.', '').isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        loaded = [x for x in sm if x > 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_oracle_sample(mesh, mach, aoa, seconds=12.0):
+    """Time the NumPy oracle's SRK2 step on one case of the workload mesh."""
+    from oracle import euler_oracle as O
+    om = O.build_oracle_mesh(mesh.points, mesh.tris, mesh.neighbors, mesh.faces, mesh.face_markers,
+                             mesh.face_connectivity, dtype=np.float32, metadata=mesh.metadata)
+    cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=float(mach), aoa=float(aoa), case=mesh.metadata['case'])
+    W, inlet = O.initialize(mesh.n_cells, cfg, np.float32)
+    dt = O.get_dt(W, om, CFL=0.6)
+    W = O.time_step_srk2(W, om, dt, inlet)   # warm-up
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        W = O.time_step_srk2(W, om, dt, inlet)
+        n += 1
+    el = time.perf_counter() - t0
+    return mesh.n_cells * n / el, n, el
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    mesh = get_mesh("naca0012", args.h)
+    mach, aoa = batch_cases(args.cases)
+    ncores = os.cpu_count() or 1
+    vals = []
+    per_step = max(4.0, 60.0 / max(1, args.steps + args.warmup))
+    for i in range(args.warmup + args.steps):
+        v, n, el = cpu_oracle_sample(mesh, mach[i % len(mach)], aoa[i % len(aoa)], seconds=per_step)
+        if i >= args.warmup:
+            vals.append((v, n, el))
+    value = float(np.mean([v for v, _, _ in vals]))
+    sample = (f"NumPy oracle (restatement of the reference JAX solver), float32, one case of the workload "
+              f"mesh ({mesh.n_cells} cells) per step, {vals[-1][1]} SRK2 steps in {vals[-1][2]:.1f} s")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean([e for _, _, e in vals]) * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Mach/alpha draws, freestream start)",
+            "config": workload_config(args, mesh),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": f"host has {ncores} cores; the oracle is single-threaded NumPy"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, mesh):
+    return {"workload": f"naca0012 h={args.h} HR ({mesh.n_cells} cells) x {args.cases} cases "
+                        f"(Mach~U[0.7,3] seed 1, alpha in -5..5 step 0.5), SRK2 chunk of {args.chunk} steps",
+            "cells": int(mesh.n_cells), "cases_per_gpu": args.cases, "srk2_steps_per_bench_step": args.chunk,
+            "scheme": "HLLC + MUSCL/Venkatakrishnan + SRK2, global dt, CFL 0.6 (0.45 transonic)",
+            "l2": "working set > L2 (state 3x + face states 3x of 16 B per cell and case)",
+            "parallelism": f"cases sharded, {args.cases} per GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cases", type=int, default=256)
+    ap.add_argument("--chunk", type=int, default=50)
+    ap.add_argument("--h", type=float, default=0.025)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        barrier(world)
+        return rc
+
+    from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
+    mesh = get_mesh("naca0012", args.h)
+    mach_all, aoa_all = batch_cases(args.cases * world)
+    mach, aoa = mach_all[rank::world], aoa_all[rank::world]
+    dm = DeviceMesh(mesh)
+    cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, dtype=np.float32)
+             for m, a in zip(mach, aoa)]
+    s = Solver(dm, len(cases), precision="f32", device=local if world > 1 else 0)
+    for b, c in enumerate(cases):
+        s.set_case(b, c)
+    s.synchronize()
+    B, N = len(cases), mesh.n_cells
+
+    # warm-up (graph capture happens in the first chunk)
+    for _ in range(args.warmup):
+        s.step(args.chunk)
+    clocks = ClockSampler(local)
+    barrier(world)
+    s.synchronize()
+    l0 = s.kernel_launches()
+    clocks.start()
+    ms = 0.0
+    for _ in range(args.steps):
+        s.step(args.chunk)          # CUDA events on the solver stream around each chunk
+        ms += s.elapsed_ms()
+    s.synchronize()
+    clk = clocks.stop()
+    launches = s.kernel_launches() - l0
+    barrier(world)
+    ms_max = allreduce_max(ms, world)
+    cu_total = allreduce_sum(float(N * B * args.chunk * args.steps), world)
+    value = cu_total / (ms_max * 1e-3)
+    alg_step_bytes = 80 + 128 / B
+
+    # dominant kernel: K2 flux/update, timed per launch with events on its stream
+    kt = s.profile_step(8)
+    hbm, peak_kind = peaks()
+    alg_k2 = (40 + 64 / B) * N * B
+    k2_gbs = alg_k2 / (kt["flux_ms"] * 1e-3) / 1e9
+    traffic = None
+    for pf in sorted((ROOT / "profiles").glob("k_flux_*.md")):
+        for line in pf.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_item_per_launch"):
+                traffic = float(line.split("=")[1].split()[0]) * N * B
+                roofline_src = pf.name
+    roofline = {"bound": "hbm", "achieved": k2_gbs, "peak": hbm, "unit": "GB/s", "frac": k2_gbs / hbm,
+                "traffic": traffic, "traffic_source": "ncu capture summarized in profiles/ (scaled by items)", "kernel": "k_flux (K2)", "peak_source": peak_kind,
+                "kernel_ms": kt["flux_ms"], "recon_ms": kt["recon_ms"],
+                "alg_bytes_per_launch": alg_k2}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import torch
+            pinned = [torch.empty((N, 4), dtype=torch.float64, pin_memory=True).numpy() for _ in range(B)]
+        except Exception:
+            pinned = [np.empty((N, 4)) for _ in range(B)]
+        from eulersr_b200.solver import freestream
+        for b, c in enumerate(cases):
+            pinned[b][:] = freestream(c.mach, c.aoa_deg, dtype=np.float32).astype(np.float64)[None, :]
+        outs = pinned  # results land in the same pinned buffers
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for b, c in enumerate(cases):
+                s.set_case(b, c, W_init=pinned[b])
+            s.step(args.chunk)
+            for b in range(B):
+                outs[b][:] = s.get_state(b)
+        s.synchronize()
+        el = time.perf_counter() - t0
+        el = allreduce_max(el, world)
+        e2e_val = allreduce_sum(float(N * B * args.chunk * e2e_steps), world) / el
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(B * N * 4 * 8),
+               "d2h_bytes_per_step": int(B * N * 4 * 8),
+               "api": "esr_set_case (host init field) + esr_step + esr_get_state per case"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, el = cpu_oracle_sample(mesh, mach[0], aoa[0], seconds=12.0)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"NumPy oracle float32, 1 case x {n} SRK2 steps on the {N}-cell mesh ({el:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Mach/alpha draws on a generated NACA0012 mesh, freestream start)",
+                "config": workload_config(args, mesh),
+                "alg_gbs_per_step": value * alg_step_bytes / 1e9,
+                "alg_bytes_per_cell_update": alg_step_bytes,
+                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": int(launches),
+                "kernel_times_ms": kt}
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -66,6 +66,15 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class KernelTimes(C.Structure):
+    _fields_ = [("recon_ms", C.c_double), ("flux_ms", C.c_double), ("other_ms", C.c_double),
+                ("recon_launches", C.c_int32), ("flux_launches", C.c_int32), ("other_launches", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class EsrError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"eulersr error {code}: {msg}")
@@ -100,6 +109,7 @@ _SIGS = {
     "esr_synchronize": (C.c_int, [C.c_void_p]),
     "esr_last_elapsed_ms": (C.c_int, [C.c_void_p, _f64p]),
     "esr_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "esr_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
     "esr_idw_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,

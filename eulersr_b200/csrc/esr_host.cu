@@ -125,6 +125,20 @@ struct SolverT : SolverBase {
   int g_plain_len = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
+  // per-launch event pairs while profiling (kind 0 recon, 1 flux, 2 other)
+  struct Tap { cudaEvent_t a, b; int kind; };
+  std::vector<Tap>* taps = nullptr;
+  void tap_begin(int kind) {
+    if (!taps) return;
+    Tap t{nullptr, nullptr, kind};
+    cudaEventCreate(&t.a);
+    cudaEventCreate(&t.b);
+    cudaEventRecord(t.a, stream);
+    taps->push_back(t);
+  }
+  void tap_end() {
+    if (taps && !taps->empty()) cudaEventRecord(taps->back().b, stream);
+  }
 
   ~SolverT() override {
     if (g_run) cudaGraphExecDestroy(g_run);
@@ -290,8 +304,10 @@ struct SolverT : SolverBase {
   // ---------------------------------------------------------------- kernels
   template <int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
   void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
+    tap_begin(1);
     k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, win, wbase, wout, FV.p,
                                                                         total, cs, kc, pos, dt_local.p);
+    tap_end();
     ++launches;
   }
   template <int STAGE>
@@ -312,8 +328,10 @@ struct SolverT : SolverBase {
       }
       return;
     }
+    tap_begin(0);
     if (write_dt) k_recon<T, true, true><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
     else k_recon<T, true, false><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
+    tap_end();
     ++launches;
   }
   // one time step of every live slot, step index `pos` inside the chunk
@@ -365,8 +383,38 @@ struct SolverT : SolverBase {
     const Cases<T> cs = cases(true);
     for (int i = 0; i < len; ++i) step_kernels(cs, i);
     const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    tap_begin(2);
     k_advance<<<nb, tb, 0, stream>>>(ctl(), n_slots, len, 0);
+    tap_end();
     ++launches;
+  }
+  int profile(int nsteps, esr_kernel_times* out) {
+    if (nsteps <= 0) return fail(ESR_ERR_ARG, "profile_step: nsteps must be > 0");
+    std::vector<Tap> v;
+    v.reserve((size_t)nsteps * 5 + 4);
+    taps = &v;
+    issue_plain_chunk(nsteps);
+    taps = nullptr;
+    cudaError_t e = cudaStreamSynchronize(stream);
+    double ms[3] = {0, 0, 0};
+    int cnt[3] = {0, 0, 0};
+    for (Tap& t : v) {
+      float x = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&x, t.a, t.b);
+      ms[t.kind] += x;
+      cnt[t.kind] += 1;
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+    if (e != cudaSuccess) return fail(ESR_ERR_CUDA, cudaGetErrorString(e));
+    out->recon_ms = cnt[0] ? ms[0] / cnt[0] : 0.0;
+    out->flux_ms = cnt[1] ? ms[1] / cnt[1] : 0.0;
+    out->other_ms = cnt[2] ? ms[2] / cnt[2] : 0.0;
+    out->recon_launches = cnt[0];
+    out->flux_launches = cnt[1];
+    out->other_launches = cnt[2];
+    out->reserved = 0;
+    return ESR_OK;
   }
   int run_chunk_len() const {
     const int ce = std::max(1, P.check_every);
@@ -956,6 +1004,12 @@ int esr_kernel_launches(const esr_solver* solver, int64_t* n) {
   if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
   *n = solver->impl->launches;
   return ESR_OK;
+}
+int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out) {
+  if (!out) return fail(ESR_ERR_ARG, "profile_step: null output");
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.profile(nsteps, out); });
+  ESR_GUARD_END
 }
 int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases, const double* const* init_fields,
                     double* const* final_states, esr_result* results) {

@@ -256,6 +256,13 @@ class Solver:
         F.check(F.lib().esr_kernel_launches(self.handle, C.byref(v)))
         return int(v.value)
 
+    def profile_step(self, nsteps: int = 8) -> dict:
+        """Average device ms per kernel kind over ``nsteps`` plain steps
+        (CUDA events on the solver's stream around every launch)."""
+        kt = F.KernelTimes()
+        F.check(F.lib().esr_profile_step(self.handle, int(nsteps), C.byref(kt)))
+        return kt.as_dict()
+
     def batch_solve(self, cases, init_fields=None, want_states=False):
         """Solve every case through the slots with retire/refill; returns
         (results, final states or None)."""

@@ -189,6 +189,20 @@ int esr_last_elapsed_ms(esr_solver* solver, double* ms);
 /* Number of kernel launches issued by the solver since creation. */
 int esr_kernel_launches(const esr_solver* solver, int64_t* n);
 
+/* Average device time of each kernel kind over `nsteps` plain steps issued
+ * without graphs, CUDA events recorded on the solver's stream around every
+ * launch. The steps advance the state like esr_step. */
+typedef struct esr_kernel_times {
+    double recon_ms;          /* K1: gradient, limiter, MUSCL face states */
+    double flux_ms;           /* K2: face fluxes, residual, stage update */
+    double other_ms;          /* bookkeeping kernels */
+    int32_t recon_launches;
+    int32_t flux_launches;
+    int32_t other_launches;
+    int32_t reserved;
+} esr_kernel_times;
+int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out);
+
 /* Solve n_cases cases through the solver's slots: every slot retired by the
  * stop rule is refilled in place with the next queued case. init_fields[i]
  * is a (n_cells,4) conserved warm start or NULL; final_states[i] receives the
