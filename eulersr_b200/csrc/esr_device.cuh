@@ -50,9 +50,18 @@ struct Seg {                 // one mesh and its B case slots
   int pad;
 };
 
+// Precision policy. float64 kernels keep IEEE division and the reference's
+// exact operation sequence (the faithful twin). float32 kernels use the
+// approximate divide (div.approx, <= 2 ulp) and reciprocal-multiplies; their
+// results stay within the float32 parity tolerance of the oracle.
+template <typename T> __device__ __forceinline__ T dv(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float dv<float>(float a, float b) { return __fdividef(a, b); }
+template <typename T> constexpr bool kFast = sizeof(T) == 4;
+
 template <typename T>
 struct Consts {
   T gamma, gm1;              // run gamma and gamma - 1 rounded from double
+  T inv_gm1, inv_gm1_14;     // 1/(gamma-1), 1/(1.4-1) for the float32 path
   T gm1_14;                  // 1.4 - 1 (wall ghost and forces use gamma 1.4)
   T half, eps_lim, venk_eps; // 0.5, limiter threshold, Venkatakrishnan 1e-7
   T ss_eps, den_eps;         // HLLC 1e-6 wave-speed split, 1e-12 denominator guard
@@ -74,16 +83,24 @@ struct Cases {               // per global slot
 template <typename T>
 __device__ __forceinline__ void prim(const V4<T>& W, T gm1, T half, T P[4]) {
   T r = W.x;
-  T u = W.y / r;
-  T v = W.z / r;
+  T u, v;
+  if constexpr (kFast<T>) {
+    const T ri = __fdividef(1.0f, r);
+    u = W.y * ri;
+    v = W.z * ri;
+  } else {
+    u = W.y / r;
+    v = W.z / r;
+  }
   P[0] = r; P[1] = u; P[2] = v;
   P[3] = (W.w - half * r * (u * u + v * v)) * gm1;
 }
 // helper.py:25-35 getConserved (M = 1)
 template <typename T>
-__device__ __forceinline__ V4<T> cons(const T P[4], T gm1, T half) {
+__device__ __forceinline__ V4<T> cons(const T P[4], T gm1, T inv_gm1, T half) {
   T r = P[0], u = P[1], v = P[2];
-  return mk4<T>(r, r * u, r * v, P[3] / gm1 + half * r * (u * u + v * v));
+  const T e = kFast<T> ? P[3] * inv_gm1 : P[3] / gm1;
+  return mk4<T>(r, r * u, r * v, e + half * r * (u * u + v * v));
 }
 
 // helper.py:196-204 slip wall ghost (gamma 1.4, background value 0)
@@ -93,7 +110,7 @@ __device__ __forceinline__ V4<T> wall_ghost(const V4<T>& Wc, T nx, T ny, const C
   prim<T>(Wc, k.gm1_14, k.half, P);
   T vn = P[1] * nx + P[2] * ny;
   T Q[4] = {P[0], P[1] - T(2) * vn * nx, P[2] - T(2) * vn * ny, P[3]};
-  return cons<T>(Q, k.gm1_14, k.half);
+  return cons<T>(Q, k.gm1_14, k.inv_gm1_14, k.half);
 }
 // helper.py:179-194 subsonic inlet ghost: rho,u,v imposed, p from the cell (gamma 1.4)
 template <typename T>
@@ -101,7 +118,7 @@ __device__ __forceinline__ V4<T> subsonic_ghost(const V4<T>& Wc, const Consts<T>
   T P[4];
   prim<T>(Wc, k.gm1_14, k.half, P);
   T Q[4] = {k.sub_rho, k.sub_u, k.sub_v, P[3]};
-  return cons<T>(Q, k.gm1_14, k.half);
+  return cons<T>(Q, k.gm1_14, k.inv_gm1_14, k.half);
 }
 // helper.py:233-256 BC_state for one boundary slot (conserved ghost)
 template <typename T>
@@ -116,7 +133,7 @@ __device__ __forceinline__ V4<T> ghost_cons(int kind, const V4<T>& Wc, T nx, T n
 // euler_solver.py:36-39 Venkatakrishnan with K = 0
 template <typename T>
 __device__ __forceinline__ T venkat(T a, T b, T eps) {
-  return (a * a + T(2) * a * b) / (a * a + T(2) * b * b + a * b + eps);
+  return dv<T>(a * a + T(2) * a * b, a * a + T(2) * b * b + a * b + eps);
 }
 
 // ------------------------------------------------------------------ fluxes
@@ -132,8 +149,8 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const T tx = -ny, ty = nx;
   const T utL = uL * tx + vL * ty;
   const T utR = uR * tx + vR * ty;
-  const T aL = sqrt(fabs(k.gamma * pL / rL));
-  const T aR = sqrt(fabs(k.gamma * pR / rR));
+  const T aL = sqrt(fabs(dv<T>(k.gamma * pL, rL)));
+  const T aR = sqrt(fabs(dv<T>(k.gamma * pR, rR)));
   T SL = fmin(unL - aL, unR - aR);
   T SR = fmax(unL + aL, unR + aR);
   if (SL == SR) SL = SL - k.ss_eps;
@@ -145,7 +162,7 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const T Fc2 = k.half * (FL2 + FR2), Fc3 = k.half * (FL3 + FR3);
   T den = rL * (SL - unL) - rR * (SR - unR);
   if (den == T(0)) den = k.den_eps;
-  const T Ss = (pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR)) / den;
+  const T Ss = dv<T>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
   const T PsL = pL + rL * (SL - unL) * (Ss - unL);
   const T PsR = pR + rR * (SR - unR) * (Ss - unR);
   const T Ps = k.half * (PsL + PsR);
@@ -156,9 +173,16 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const bool left = c1 || c2;
   const T rK = left ? rL : rR, unK = left ? unL : unR, SK = left ? SL : SR;
   const T EK = left ? EL : ER, pK = left ? pL : pR, utK = left ? utL : utR;
-  const T rs = rK * (SK - unK) / (SK - Ss);
+  T rs, Us3;
+  if constexpr (kFast<T>) {
+    const T inv = __fdividef(1.0f, SK - Ss);
+    rs = rK * (SK - unK) * inv;
+    Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) * inv;
+  } else {
+    rs = rK * (SK - unK) / (SK - Ss);
+    Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) / (SK - Ss);
+  }
   const T Us0 = rs, Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
-  const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) / (SK - Ss);
   T H0, H1, H2, H3;
   if (c1) { H0 = FL0; H1 = FL1; H2 = FL2; H3 = FL3; }
   else if (c2) { H0 = FL0 + SL * (Us0 - WL.x); H1 = FL1 + SL * (Us1 - WL.y); H2 = FL2 + SL * (Us2 - WL.z); H3 = FL3 + SL * (Us3 - WL.w); }
@@ -176,8 +200,8 @@ __device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4
   const T unR = PR[1] * nx + PR[2] * ny;
   const T FL0 = PL[0] * unL, FL1 = PL[0] * PL[1] * unL + PL[3] * nx, FL2 = PL[0] * PL[2] * unL + PL[3] * ny, FL3 = (WL.w + PL[3]) * unL;
   const T FR0 = PR[0] * unR, FR1 = PR[0] * PR[1] * unR + PR[3] * nx, FR2 = PR[0] * PR[2] * unR + PR[3] * ny, FR3 = (WR.w + PR[3]) * unR;
-  const T CL = sqrt(fabs(k.gamma * PL[3] / PL[0])) + fabs(unL);
-  const T CR = sqrt(fabs(k.gamma * PR[3] / PR[0])) + fabs(unR);
+  const T CL = sqrt(fabs(dv<T>(k.gamma * PL[3], PL[0]))) + fabs(unL);
+  const T CR = sqrt(fabs(dv<T>(k.gamma * PR[3], PR[0]))) + fabs(unR);
   const T C = fmax(CR, CL);
   F[0] = k.half * (FL0 + FR0) - k.half * C * (WR.x - WL.x);
   F[1] = k.half * (FL1 + FR1) - k.half * C * (WR.y - WL.y);
@@ -317,14 +341,23 @@ __global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, c
       } else {
         prim<T>(ghost_cons<T>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
       }
-      WL = cons<T>(qL, kc.gm1, kc.half);
-      WR = cons<T>(qR, kc.gm1, kc.half);
+      WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
+      WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
+      if constexpr (kFast<T>) {
+        // float32: the face primitives are used as reconstructed (the
+        // reference converts them to conserved and back, a rounding-level step)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) { PL[v] = qL[v]; PR[v] = qR[v]; }
+      } else {
+        prim<T>(WL, kc.gm1, kc.half, PL);
+        prim<T>(WR, kc.gm1, kc.half, PR);
+      }
     } else {
       WL = Wc;
       WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T>(kind, Wc, nx, ny, inlet, kc);
+      prim<T>(WL, kc.gm1, kc.half, PL);
+      prim<T>(WR, kc.gm1, kc.half, PR);
     }
-    prim<T>(WL, kc.gm1, kc.half, PL);
-    prim<T>(WR, kc.gm1, kc.half, PR);
     T F[4];
     if (FLUX == 0) hllc<T>(WL, PL, WR, PR, nx, ny, kc, F);
     else rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
@@ -334,10 +367,10 @@ __global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, c
   }
   const T area = geo(s, G_AREA, c);
   const T sig = cs.strength[g] * geo(s, G_BLEND3, c);
-  const T R0 = acc[0] / area - sig * (inlet.x - Wc.x);
-  const T R1 = acc[1] / area - sig * (inlet.y - Wc.y);
-  const T R2 = acc[2] / area - sig * (inlet.z - Wc.z);
-  const T R3 = acc[3] / area - sig * (inlet.w - Wc.w);
+  const T R0 = dv<T>(acc[0], area) - sig * (inlet.x - Wc.x);
+  const T R1 = dv<T>(acc[1], area) - sig * (inlet.y - Wc.y);
+  const T R2 = dv<T>(acc[2], area) - sig * (inlet.z - Wc.z);
+  const T R3 = dv<T>(acc[3], area) - sig * (inlet.w - Wc.w);
   const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
   V4<T> o;
   if (STAGE == ST_FIRST) {

@@ -174,6 +174,8 @@ struct SolverT : SolverBase {
     kc.gamma = (T)g;
     kc.gm1 = (T)(g - 1.0);
     kc.gm1_14 = (T)(1.4 - 1.0);
+    kc.inv_gm1 = (T)(1.0 / (g - 1.0));
+    kc.inv_gm1_14 = (T)(1.0 / (1.4 - 1.0));
     kc.half = (T)0.5;
     kc.eps_lim = sizeof(T) == 8 ? (T)1e-12 : (T)1e-7;
     kc.venk_eps = (T)1e-7;
