@@ -491,7 +491,7 @@ struct CaseCtl {             // mutable per-slot control words (device)
 };
 
 // Which slots need a stop-rule check after `pos` steps of the chunk.
-__global__ void k_mark_due(CaseCtl cc, int n_slots, int pos, int check_every) {
+static __global__ void k_mark_due(CaseCtl cc, int n_slots, int pos, int check_every) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_slots) return;
   int d = 0;
@@ -510,7 +510,7 @@ __device__ __forceinline__ long long globaltimer() {
 
 // euler/main.py:147-158: rel, streak, confirmation and the stopping step.
 // STOP_RULE 0: rel = ||dW|| / (block * (||Wref|| + 1e-16)); 1: density-residual RMS
-__global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* __restrict__ partial, int n_chunks,
+static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* __restrict__ partial, int n_chunks,
                         const int* __restrict__ ncells, double threshold, int patience, int stop_rule) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_slots || !cc.due[g]) return;
@@ -547,7 +547,7 @@ __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* __restr
 }
 
 // chunk end without checks: every live slot advanced `len` steps
-__global__ void k_advance(CaseCtl cc, int n_slots, int len, int stop_at_nmax) {
+static __global__ void k_advance(CaseCtl cc, int n_slots, int len, int stop_at_nmax) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_slots || !cc.active[g]) return;
   const int done = min(cc.step[g] + len, cc.nmax[g]);
@@ -674,7 +674,7 @@ __global__ void k_copy_out_device(const V4<T>* __restrict__ W, const int* __rest
 // ------------------------------------------------------------------- IDW
 // eval/core.py:135-142 with utils/metrics.py:9-14: weights from float64
 // distances, float32 weighted sum over the k neighbours in order.
-__global__ void k_idw(const float* __restrict__ src, int n_vars, const int* __restrict__ idx,
+static __global__ void k_idw(const float* __restrict__ src, int n_vars, const int* __restrict__ idx,
                       const float* __restrict__ dist, int n_dst, int k, float* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_dst) return;
