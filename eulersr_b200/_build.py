@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "libeulersr.so"
 
-SOURCES = ["esr_host.cu", "esr_mesh.cpp", "esr_mlp.cu"]
+SOURCES = ["esr_host.cu", "esr_mesh.cpp", "esr_noalloc.cu", "esr_mlp.cu"]
 HEADERS = ["esr_device.cuh", "esr_internal.h", "esr_layout.h", "esr_mlp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -112,6 +112,7 @@ _SIGS = {
     "esr_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
+    "esr_rel_change_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_idw_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                 C.c_void_p, C.c_void_p]),
 }

@@ -68,6 +68,8 @@ constexpr int kReduceCells = 2048;  // cells per reduction block
 
 using namespace esr;
 
+int esr::report_error(int code, const std::string& msg) { return fail(code, msg); }
+
 // ------------------------------------------------------------------ solver
 struct SolverBase {
   virtual ~SolverBase() = default;

@@ -22,6 +22,8 @@ struct HostMesh {
 };
 
 int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err);
+// records `msg` as the calling thread's esr_last_error() and returns `code`
+int report_error(int code, const std::string& msg);
 std::vector<int> rcm_order(int n, const std::vector<int>& nbr);
 
 }  // namespace esr

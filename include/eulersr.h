@@ -211,6 +211,21 @@ int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases,
                     const double* const* init_fields, double* const* final_states,
                     esr_result* results);
 
+/* Relative change ||A - B||_F / (||B||_F + 1e-16) of two device fields of
+ * n_rows x 4 values (float4 rows for ESR_PREC_F32, double4 rows for
+ * ESR_PREC_F64, 16-byte aligned), written to the device double *d_out on
+ * `stream`. No counterpart in the reference: it is the allocation-free form
+ * of the solver's stop-rule norm, for callers that cannot allocate device
+ * memory when they need it (a host allocator that owns the whole device
+ * budget, a pre-sized arena that forbids allocation after start-up). Its
+ * scratch is a fixed 16 KiB device array inside the library: at most
+ * 2,097,152 rows (larger n_rows is rejected with ESR_ERR_ARG); every GPU that
+ * loads the library holds the array until exit; the first call on a device
+ * looks up the array's address once (make it before any stream capture);
+ * calls that overlap on the GPU race on the shared array. */
+int esr_rel_change_noalloc(const void* d_A, const void* d_B, int64_t n_rows, int32_t precision,
+                           double* d_out, void* stream);
+
 /* IDW (k neighbours, weights 1/(d^2+1e-12) normalised) of a source field onto
  * target points; all pointers are device pointers, float32, row-major. */
 int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars,
