@@ -397,7 +397,12 @@ def load_reference_pickle(path) -> Mesh:
     raw = Path(path).read_bytes()
     buf = io.BytesIO(raw)
     version = np.lib.format.read_magic(buf)
-    np.lib.format._read_array_header(buf, version)
+    if version == (1, 0):
+        np.lib.format.read_array_header_1_0(buf, max_header_size=1 << 20)
+    elif version == (2, 0):
+        np.lib.format.read_array_header_2_0(buf, max_header_size=1 << 20)
+    else:
+        np.lib.format._read_array_header(buf, version, max_header_size=1 << 20)
     obj = _ReferenceUnpickler(buf).load()
     if isinstance(obj, np.ndarray):
         obj = obj.item()

@@ -1,0 +1,85 @@
+"""The C ABI library: loads, exports every declared symbol, prepares meshes on
+the host and rejects bad input with the reference's error classes (CPU only;
+no compute call needs a GPU here)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+def test_library_exports_every_header_symbol():
+    from eulersr_b200 import _ffi as F
+    L = F.lib()
+    names = F.header_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert L.esr_api_version() == 1
+
+
+def test_mesh_prepare_on_host(diamond02):
+    from eulersr_b200.solver import DeviceMesh
+    dm = DeviceMesh(diamond02)
+    assert dm.n_cells == diamond02.n_cells
+    perm = dm.permutation()
+    assert np.array_equal(np.sort(perm), np.arange(diamond02.n_cells))
+    wf, _, _ = diamond02.wall_owner_data()
+    assert dm.info.n_wall_faces == len(wf)
+    assert dm.info.n_boundary_slots == int((diamond02.neighbors < 0).sum())
+    assert dm.info.y_min == pytest.approx(0.0) and dm.info.y_max == pytest.approx(4.0)
+
+
+def test_mesh_rejects_periodic_marker(diamond02):
+    from eulersr_b200 import _ffi as F
+    from eulersr_b200.mesh import Mesh
+    from eulersr_b200.solver import DeviceMesh
+    fm = diamond02.face_markers.copy()
+    fm[fm == 4] = 1
+    bad = Mesh.from_arrays(diamond02.points, diamond02.tris, diamond02.neighbors, diamond02.faces, fm,
+                           diamond02.face_connectivity, dict(diamond02.metadata))
+    with pytest.raises(F.EsrError) as e:
+        DeviceMesh(bad)
+    assert e.value.code == F.ESR_ERR_ARG and "periodic" in str(e.value)
+
+
+def test_mesh_rejects_out_of_range(diamond02):
+    from eulersr_b200 import _ffi as F
+    from eulersr_b200.mesh import Mesh
+    from eulersr_b200.solver import DeviceMesh
+    nb = diamond02.neighbors.copy()
+    nb[0, 0] = diamond02.n_cells + 5
+    bad = Mesh.__new__(Mesh)
+    bad.__dict__.update(diamond02.__dict__)
+    bad.neighbors = nb
+    with pytest.raises(F.EsrError) as e:
+        DeviceMesh(bad)
+    assert e.value.code == F.ESR_ERR_ARG
+
+
+def test_solver_argument_errors_before_cuda(diamond02):
+    """Unknown flux / reconstruction names fail like the reference's
+    ValueError (euler_solver.py:122,139) without touching the device."""
+    from eulersr_b200.solver import Solver
+    with pytest.raises(ValueError, match="Unknown flux type"):
+        Solver(diamond02, 1, flux="roe")
+    with pytest.raises(ValueError, match="Unknown reconstruction scheme"):
+        Solver(diamond02, 1, reconstruction="weno")
+
+
+def test_rcm_c_matches_contract(diamond02):
+    """The library's renumbering is a permutation that keeps neighbours close."""
+    from eulersr_b200.solver import DeviceMesh
+    rng = np.random.default_rng(0)
+    shuffled = diamond02.renumbered(rng.permutation(diamond02.n_cells))
+
+    def bandwidth(m, perm=None):
+        inv = np.arange(m.n_cells)
+        if perm is not None:
+            inv = np.empty_like(perm)
+            inv[perm] = np.arange(len(perm))
+        c, k = np.nonzero(m.neighbors >= 0)
+        return int(np.abs(inv[c] - inv[m.neighbors[c, k]]).max())
+    perm = DeviceMesh(shuffled).permutation()
+    assert np.array_equal(np.sort(perm), np.arange(diamond02.n_cells))
+    assert bandwidth(shuffled, perm) <= 3 * bandwidth(diamond02)
+    assert bandwidth(shuffled, perm) < bandwidth(shuffled) / 5
