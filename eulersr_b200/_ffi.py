@@ -54,13 +54,16 @@ class Params(C.Structure):
 class Case(C.Structure):
     _fields_ = [("mesh", C.c_int32), ("reserved", C.c_int32), ("mach", C.c_double), ("aoa_deg", C.c_double),
                 ("cfl", C.c_double), ("tf", C.c_double), ("max_steps", C.c_int64), ("inlet", C.c_double * 4),
-                ("rho_inf", C.c_double), ("u_inf", C.c_double), ("l_ref", C.c_double)]
+                ("rho_inf", C.c_double), ("u_inf", C.c_double), ("l_ref", C.c_double),
+                ("eng_track", C.c_int32), ("eng_patience", C.c_int32), ("eng_target_cd", C.c_double),
+                ("eng_target_cl", C.c_double), ("eng_cd_tol", C.c_double), ("eng_cl_tol", C.c_double)]
 
 
 class Result(C.Structure):
     _fields_ = [("status", C.c_int32), ("converged", C.c_int32), ("stopping_step", C.c_int32),
                 ("steps", C.c_int32), ("n_max", C.c_int32), ("case_index", C.c_int32), ("dt", C.c_double),
-                ("last_rel", C.c_double), ("cd", C.c_double), ("cl", C.c_double), ("solve_time_s", C.c_double)]
+                ("last_rel", C.c_double), ("cd", C.c_double), ("cl", C.c_double), ("solve_time_s", C.c_double),
+                ("eng_converged", C.c_int32), ("eng_stopping_step", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -106,6 +109,7 @@ _SIGS = {
     "esr_residual_probe": (C.c_int, [C.c_void_p, _f64p]),
     "esr_forces": (C.c_int, [C.c_void_p, _f64p, _f64p]),
     "esr_entropy": (C.c_int, [C.c_void_p, _f64p]),
+    "esr_gradients": (C.c_int, [C.c_void_p, C.c_int32, _f64p]),
     "esr_synchronize": (C.c_int, [C.c_void_p]),
     "esr_last_elapsed_ms": (C.c_int, [C.c_void_p, _f64p]),
     "esr_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),

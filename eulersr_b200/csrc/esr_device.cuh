@@ -300,6 +300,41 @@ __global__ void __launch_bounds__(256) k_recon(const Seg<T>* __restrict__ segs, 
   }
 }
 
+// Unlimited LSQ gradient of the primitives with boundary ghosts, as the
+// bundle export computes it (euler/utils.py:33-39 -> helper.py:136-153), for
+// one slot; out[(c*4 + v)*2 + d] in the caller's cell order.
+template <typename T>
+__global__ void k_grad_export(const Seg<T>* __restrict__ segs, int seg, int b, const V4<T>* __restrict__ W,
+                              const V4<T>* __restrict__ inlet_p, const int* __restrict__ inv, int g_slot,
+                              Consts<T> kc, double* __restrict__ out) {
+  const Seg<T> s = segs[seg];
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;   // caller order
+  if (cc >= s.n_cells) return;
+  const int c = inv[cc];
+  const long long gi = s.off + (long long)c * s.B + b;
+  const V4<T> Wc = W[gi];
+  T Pc[4];
+  prim<T>(Wc, kc.gm1, kc.half, Pc);
+  const int4 nb = __ldg(s.nbr + c);
+  const int nbk[3] = {nb.x, nb.y, nb.z};
+  const V4<T> inlet = inlet_p[g_slot];
+  T Pk[3][4];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int kind = slot_kind(nb.w, k);
+    V4<T> Wk;
+    if (kind == K_INTERIOR) Wk = W[s.off + (long long)nbk[k] * s.B + b];
+    else Wk = ghost_cons<T>(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc);
+    prim<T>(Wk, kc.gm1, kc.half, Pk[k]);
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
+    out[((size_t)cc * 4 + v) * 2 + 0] = (double)(geo(s, G_C0X, c) * d0 + geo(s, G_C1X, c) * d1 + geo(s, G_C2X, c) * d2);
+    out[((size_t)cc * 4 + v) * 2 + 1] = (double)(geo(s, G_C0Y, c) * d0 + geo(s, G_C1Y, c) * d1 + geo(s, G_C2Y, c) * d2);
+  }
+}
+
 // ----------------------------------------------------------------- K2 flux
 enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
 
@@ -310,7 +345,7 @@ __global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, c
                                               const V4<T>* __restrict__ Win, const V4<T>* __restrict__ Wbase,
                                               V4<T>* __restrict__ Wout, const V4<T>* __restrict__ FV,
                                               long long total, Cases<T> cs, Consts<T> kc, int pos,
-                                              const T* __restrict__ dt_local) {
+                                              const T* __restrict__ dt_local, T* __restrict__ res_out) {
   const int2 bt = blk[blockIdx.x];
   const Seg<T> s = segs[bt.x];
   const int item = bt.y + threadIdx.x;
@@ -372,6 +407,8 @@ __global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, c
   const T R2 = dv<T>(acc[2], area) - sig * (inlet.z - Wc.z);
   const T R3 = dv<T>(acc[3], area) - sig * (inlet.w - Wc.w);
   const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+  // density residual of the state the step starts from (density-L2 stop rule)
+  if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
   V4<T> o;
   if (STAGE == ST_FIRST) {
     o = mk4<T>(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
@@ -402,7 +439,7 @@ __global__ void k_commit(const Seg<T>* __restrict__ segs, const int2* __restrict
 }
 
 // ------------------------------------------------------ per-case reductions
-enum RedOp { RED_NORM = 0, RED_DTMIN = 1, RED_ENTROPY = 2, RED_DIFF = 3 };
+enum RedOp { RED_NORM = 0, RED_DTMIN = 1, RED_ENTROPY = 2, RED_DIFF = 3, RED_RESSQ = 4 };
 
 struct CaseMap {             // global slot -> (segment, slot)
   const int* seg;
@@ -452,6 +489,10 @@ __global__ void __launch_bounds__(256) k_case_reduce(const Seg<T>* __restrict__ 
       }
       const T d = geo(s, G_AREA, c) / lam;
       a0 = fmin(a0, (double)d);
+    } else if (OP == RED_RESSQ) {   // Wref carries the density residual array
+      const double r = (double)((const T*)Wref)[gi];
+      a0 += r * r;
+      a1 += 1.0;
     } else {  // entropy
       const T r = w.x, u = w.y / r, v = w.z / r;
       const T p = (w.w - kc.half * r * (u * u + v * v)) * kc.gm1;
@@ -488,7 +529,31 @@ struct CaseCtl {             // mutable per-slot control words (device)
   double* last_rel;
   long long* t_start;        // globaltimer at the case start (ns)
   long long* t_end;
+  // engineering criterion (euler/main.py:66-113,160-171)
+  const int* eng_track;
+  const int* eng_patience;
+  const double4* eng_t;      // target cd, target cl, |cd| tolerance, |cl| tolerance
+  int* eng_streak;
+  int* eng_start;
+  int* eng_stop;
+  int* eng_stopping;
+  const double* forces;      // cd, cl per slot at the current check
 };
+
+// step-0 engineering state of freshly filled slots (euler/main.py:107-111)
+static __global__ void k_eng_init(CaseCtl cc, const int* __restrict__ fill, int n_slots) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !fill[g]) return;
+  int ok = 0;
+  if (cc.eng_track[g]) {
+    const double4 t = cc.eng_t[g];
+    ok = fabs(cc.forces[2 * g] - t.x) <= t.z && fabs(cc.forces[2 * g + 1] - t.y) <= t.w;
+  }
+  cc.eng_streak[g] = ok;
+  cc.eng_start[g] = 0;
+  cc.eng_stop[g] = 0;
+  cc.eng_stopping[g] = cc.nmax[g];
+}
 
 // Which slots need a stop-rule check after `pos` steps of the chunk.
 static __global__ void k_mark_due(CaseCtl cc, int n_slots, int pos, int check_every) {
@@ -511,7 +576,8 @@ __device__ __forceinline__ long long globaltimer() {
 // euler/main.py:147-158: rel, streak, confirmation and the stopping step.
 // STOP_RULE 0: rel = ||dW|| / (block * (||Wref|| + 1e-16)); 1: density-residual RMS
 static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* __restrict__ partial, int n_chunks,
-                        const int* __restrict__ ncells, double threshold, int patience, int stop_rule) {
+                        const int* __restrict__ ncells, double threshold, int patience, int stop_rule,
+                        int check_every) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_slots || !cc.due[g]) return;
   double s0 = 0.0, s1 = 0.0;
@@ -537,6 +603,30 @@ static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* 
   if (!finite) st = 4;
   else if (nstreak >= patience) st = 2;
   else if (done >= cc.nmax[g]) st = 3;
+  bool eng_under = false;
+  if (cc.eng_track[g]) {
+    const double4 t = cc.eng_t[g];
+    eng_under = fabs(cc.forces[2 * g] - t.x) <= t.z && fabs(cc.forces[2 * g + 1] - t.y) <= t.w;
+    const int es = cc.eng_streak[g];
+    const int nes = eng_under ? es + 1 : 0;
+    if (eng_under && es == 0) cc.eng_start[g] = done;
+    cc.eng_streak[g] = nes;
+    if (nes >= cc.eng_patience[g] && !cc.eng_stop[g]) {
+      cc.eng_stop[g] = 1;
+      cc.eng_stopping[g] = cc.eng_start[g];
+    }
+    // The reference keeps checking the frozen field after the stop rule
+    // fires until step N: the criterion can still confirm on that field.
+    if (st == 2 && !cc.eng_stop[g] && eng_under) {
+      const int ce = max(1, check_every);
+      const int N = cc.nmax[g];
+      const int remaining = done >= N ? 0 : N / ce - done / ce + ((N % ce) ? 1 : 0);
+      if (nes + remaining >= cc.eng_patience[g]) {
+        cc.eng_stop[g] = 1;
+        cc.eng_stopping[g] = cc.eng_start[g];
+      }
+    }
+  }
   if (st) {
     cc.status[g] = st;
     cc.stopping_step[g] = (st == 2) ? cc.streak_start[g] : cc.nmax[g];
@@ -590,8 +680,10 @@ __global__ void k_dt_finish(const int* __restrict__ fill, int n_slots, const dou
 // (helper.py:366-415): sum_w p(cell_w) n_w ds_w / (q_inf L_ref), p at gamma 1.4
 template <typename T>
 __global__ void k_forces(const Seg<T>* __restrict__ segs, CaseMap cm, const V4<T>* __restrict__ W,
-                         const double* __restrict__ qref, double* __restrict__ out, Consts<T> kc) {
+                         const double* __restrict__ qref, double* __restrict__ out, Consts<T> kc,
+                         const int* __restrict__ only_a, const int* __restrict__ only_b) {
   const int g = blockIdx.x;
+  if ((only_a && !only_a[g]) || (only_b && !only_b[g])) return;   // optional slot filters
   const Seg<T> s = segs[cm.seg[g]];
   const int b = cm.slot[g];
   double ax = 0.0, ay = 0.0;

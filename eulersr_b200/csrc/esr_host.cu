@@ -112,6 +112,8 @@ struct SolverT : SolverBase {
   DevBuf<long long> max_steps, t_start, t_end;
   DevBuf<int> active, step, nmax, nmax_inf, ref_step, streak, streak_start, stopping, status, due, fill;
   DevBuf<double> last_rel;
+  DevBuf<int> eng_track, eng_patience, eng_streak, eng_start, eng_stop, eng_stopping;
+  DevBuf<double4> eng_t;
   DevBuf<double2> partial;
   DevBuf<double> stage_rows;  // host rows staging for set/get state
 
@@ -161,6 +163,8 @@ struct SolverT : SolverBase {
     c.active = active.p; c.step = step.p; c.nmax = nmax.p; c.ref_step = ref_step.p; c.streak = streak.p;
     c.streak_start = streak_start.p; c.stopping_step = stopping.p; c.status = status.p; c.due = due.p;
     c.last_rel = last_rel.p; c.t_start = t_start.p; c.t_end = t_end.p;
+    c.eng_track = eng_track.p; c.eng_patience = eng_patience.p; c.eng_t = eng_t.p; c.eng_streak = eng_streak.p;
+    c.eng_start = eng_start.p; c.eng_stop = eng_stop.p; c.eng_stopping = eng_stopping.p; c.forces = forces.p;
     return c;
   }
   CaseMap cmap() { return CaseMap{d_case_seg.p, d_case_slot.p}; }
@@ -283,6 +287,13 @@ struct SolverT : SolverBase {
     for (DevBuf<int>* b : {&active, &step, &nmax, &nmax_inf, &ref_step, &streak, &streak_start, &stopping, &status, &due, &fill})
       ESR_TRY(b->alloc(n_slots));
     ESR_TRY(last_rel.alloc(n_slots));
+    for (DevBuf<int>* b : {&eng_track, &eng_patience, &eng_streak, &eng_start, &eng_stop, &eng_stopping}) {
+      ESR_TRY(b->alloc(n_slots));
+      ESR_CUDA(cudaMemsetAsync(b->p, 0, n_slots * sizeof(int), stream));
+    }
+    ESR_TRY(eng_t.alloc(n_slots));
+    ESR_CUDA(cudaMemsetAsync(eng_t.p, 0, n_slots * sizeof(double4), stream));
+    ESR_CUDA(cudaMemsetAsync(forces.p, 0, 2 * n_slots * sizeof(double), stream));
     ESR_TRY(partial.alloc((size_t)n_slots * n_chunks));
     for (DevBuf<int>* b : {&active, &step, &nmax, &ref_step, &streak, &streak_start, &stopping, &status, &due, &fill})
       ESR_CUDA(cudaMemsetAsync(b->p, 0, n_slots * sizeof(int), stream));
@@ -310,7 +321,7 @@ struct SolverT : SolverBase {
   void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
     tap_begin(1);
     k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, win, wbase, wout, FV.p,
-                                                                        total, cs, kc, pos, dt_local.p);
+                                                                        total, cs, kc, pos, dt_local.p, res.p);
     tap_end();
     ++launches;
   }
@@ -366,11 +377,16 @@ struct SolverT : SolverBase {
     const int tb = 128, nb = (n_slots + tb - 1) / tb;
     k_mark_due<<<nb, tb, 0, stream>>>(ctl(), n_slots, pos, std::max(1, P.check_every));
     dim3 grid(n_chunks, n_slots);
-    k_case_reduce<T, RED_NORM><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, Wref.p, due.p, kReduceCells,
-                                                                    partial.p, n_chunks, kc);
+    if (P.stop_rule == ESR_STOP_DENSITY_L2)
+      k_case_reduce<T, RED_RESSQ><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, (V*)res.p, due.p,
+                                                                       kReduceCells, partial.p, n_chunks, kc);
+    else
+      k_case_reduce<T, RED_NORM><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, Wref.p, due.p,
+                                                                      kReduceCells, partial.p, n_chunks, kc);
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, due.p, eng_track.p);
     k_check<<<nb, tb, 0, stream>>>(ctl(), n_slots, pos, partial.p, n_chunks, d_ncells.p, P.threshold,
-                                   std::max(1, P.patience), 0);
-    launches += 3;
+                                   std::max(1, P.patience), P.stop_rule, std::max(1, P.check_every));
+    launches += 4;
   }
   void issue_run_chunk(int len) {
     const Cases<T> cs = cases(false);
@@ -450,7 +466,7 @@ struct SolverT : SolverBase {
       const int ce = std::max(1, P.check_every);
       int cps = 0;
       for (int i = 0; i < len; ++i) if ((i + 1) % ce == 0 || i + 1 == len) ++cps;
-      n += 3LL * cps;
+      n += 4LL * cps;
     }
     return n;
   }
@@ -504,6 +520,15 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpyAsync(tf.p + slot, &tfv, sizeof(double), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemcpyAsync(max_steps.p + slot, &ms, sizeof(long long), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemcpyAsync(qref.p + slot, &qv, sizeof(double), cudaMemcpyHostToDevice, stream));
+    // engineering criterion: relative tolerances of euler/main.py:72-73
+    const int etrack = c->eng_track ? 1 : 0;
+    const int epat = std::max(1, c->eng_patience > 0 ? c->eng_patience : P.patience);
+    const double4 et = make_double4(c->eng_target_cd, c->eng_target_cl,
+                                    c->eng_cd_tol * std::max(std::fabs(c->eng_target_cd), 1e-8),
+                                    c->eng_cl_tol * std::max(std::fabs(c->eng_target_cl), 1e-8));
+    ESR_CUDA(cudaMemcpyAsync(eng_track.p + slot, &etrack, sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(eng_patience.p + slot, &epat, sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(eng_t.p + slot, &et, sizeof(double4), cudaMemcpyHostToDevice, stream));
     const int tb = 256, nb = (N + tb - 1) / tb;
     if (W_init) {
       if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
@@ -549,7 +574,9 @@ struct SolverT : SolverBase {
     const int tb = 128, nb = (n_slots + tb - 1) / tb;
     k_dt_finish<T><<<nb, tb, 0, stream>>>(fill.p, n_slots, partial.p, n_chunks, cfl.p, tf.p, max_steps.p, dt.p, ctl(),
                                           P.dt_mode == ESR_DT_LOCAL);
-    launches += 2;
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, fill.p, eng_track.p);
+    k_eng_init<<<nb, tb, 0, stream>>>(ctl(), fill.p, n_slots);
+    launches += 4;
     ESR_CUDA(cudaGetLastError());
     return ESR_OK;
   }
@@ -655,7 +682,7 @@ struct SolverT : SolverBase {
     return ESR_OK;
   }
   int compute_forces() {
-    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc);
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, nullptr, nullptr);
     ++launches;
     ESR_CUDA(cudaGetLastError());
     return ESR_OK;
@@ -675,9 +702,15 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpyAsync(d.data(), dt.p, n_slots * sizeof(T), cudaMemcpyDeviceToHost, stream));
     ESR_CUDA(cudaMemcpyAsync(ts.data(), t_start.p, n_slots * sizeof(long long), cudaMemcpyDeviceToHost, stream));
     ESR_CUDA(cudaMemcpyAsync(te.data(), t_end.p, n_slots * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+    std::vector<int> etr(n_slots), est(n_slots), esp(n_slots);
+    ESR_CUDA(cudaMemcpyAsync(etr.data(), eng_track.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(est.data(), eng_stop.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaMemcpyAsync(esp.data(), eng_stopping.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
     ESR_CUDA(cudaStreamSynchronize(stream));
     for (int g = 0; g < n_slots; ++g) {
       esr_result& r = out[g];
+      r.eng_converged = etr[g] ? est[g] : 0;
+      r.eng_stopping_step = etr[g] ? (est[g] ? esp[g] : nm[g]) : 0;
       r.status = st[g];
       r.converged = st[g] == ESR_CASE_CONVERGED;
       r.stopping_step = (st[g] == ESR_CASE_CONVERGED || st[g] == ESR_CASE_MAXSTEP || st[g] == ESR_CASE_NONFINITE) ? sstep[g] : nm[g];
@@ -721,6 +754,20 @@ struct SolverT : SolverBase {
       for (int i = 0; i < n_chunks; ++i) { s0 += pt[(size_t)g * n_chunks + i].x; s1 += pt[(size_t)g * n_chunks + i].y; }
       rel[g] = on[g] ? std::sqrt(s0) / (std::sqrt(s1) + 1e-16) : 0.0;
     }
+    return ESR_OK;
+  }
+  int gradients(int slot, double* out) {
+    int m, b;
+    ESR_TRY(mesh_of_slot(slot, m, b));
+    MeshDev& md = *meshes[m];
+    const int N = md.hm->n_cells, tb = 128, nb = (N + tb - 1) / tb;
+    DevBuf<double> g;
+    ESR_TRY(g.alloc((size_t)8 * N));
+    k_grad_export<T><<<nb, tb, 0, stream>>>(d_segs.p, m, b, W.p, inlet.p, md.inv.p, slot, kc, g.p);
+    ++launches;
+    ESR_CUDA(cudaGetLastError());
+    ESR_CUDA(cudaMemcpyAsync(out, g.p, (size_t)8 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
     return ESR_OK;
   }
   int entropy(double* S) {
@@ -889,7 +936,7 @@ int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_me
   if (p.reconstruction != ESR_RECON_MUSCL && p.reconstruction != ESR_RECON_CONSTANT) return fail(ESR_ERR_ARG, "Unknown reconstruction scheme");
   if (p.time_scheme < ESR_TIME_SRK2 || p.time_scheme > ESR_TIME_RK2) return fail(ESR_ERR_ARG, "unknown time scheme");
   if (p.dt_mode != ESR_DT_GLOBAL && p.dt_mode != ESR_DT_LOCAL) return fail(ESR_ERR_ARG, "unknown dt mode");
-  if (p.stop_rule != ESR_STOP_REFERENCE) return fail(ESR_ERR_ARG, "stop rule not supported by this build");
+  if (p.stop_rule != ESR_STOP_REFERENCE && p.stop_rule != ESR_STOP_DENSITY_L2) return fail(ESR_ERR_ARG, "unknown stop rule");
   if (!(p.gamma > 1.0)) return fail(ESR_ERR_ARG, "gamma must be > 1");
   auto s = std::make_unique<esr_solver>();
   s->precision = p.precision;
@@ -989,6 +1036,12 @@ int esr_forces(esr_solver* solver, double* cd, double* cl) {
     for (int g = 0; g < s.n_slots; ++g) { cd[g] = fo[2 * g]; cl[g] = fo[2 * g + 1]; }
     return ESR_OK;
   });
+}
+int esr_gradients(esr_solver* solver, int32_t slot, double* grad) {
+  if (!grad) return fail(ESR_ERR_ARG, "gradients: null output");
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.gradients(slot, grad); });
+  ESR_GUARD_END
 }
 int esr_entropy(esr_solver* solver, double* total) {
   if (!total) return fail(ESR_ERR_ARG, "entropy: null output");

@@ -50,6 +50,11 @@ class FlowCase:
     l_ref: float = 1.0
     clamp: bool = True
     dtype: type = np.float64
+    eng_target_cd: float | None = None     # engineering criterion (euler/main.py:66-113)
+    eng_target_cl: float | None = None
+    eng_cd_tol: float = 0.001
+    eng_cl_tol: float = 0.001
+    eng_patience: int = 0                  # 0: the solver's stop-rule patience
 
     def to_c(self) -> F.Case:
         c = F.Case()
@@ -65,6 +70,13 @@ class FlowCase:
         c.rho_inf = float(self.rho_inf)
         c.u_inf = float(self.mach * math.sqrt(self.gamma * self.p_inf / self.rho_inf))
         c.l_ref = float(self.l_ref)
+        if self.eng_target_cd is not None and self.eng_target_cl is not None:
+            c.eng_track = 1
+            c.eng_patience = int(self.eng_patience)
+            c.eng_target_cd = float(self.eng_target_cd)
+            c.eng_target_cl = float(self.eng_target_cl)
+            c.eng_cd_tol = float(self.eng_cd_tol)
+            c.eng_cl_tol = float(self.eng_cl_tol)
         return c
 
 
@@ -237,6 +249,12 @@ class Solver:
         cl = np.empty(self.n_slots)
         F.check(F.lib().esr_forces(self.handle, F.ptr(cd, C.c_double), F.ptr(cl, C.c_double)))
         return cd, cl
+
+    def gradients(self, slot: int = 0) -> np.ndarray:
+        """(N, 4, 2) unlimited LSQ gradient of the primitives (bundle export)."""
+        out = np.empty((self._n_cells(slot), 4, 2), dtype=np.float64)
+        F.check(F.lib().esr_gradients(self.handle, slot, F.ptr(out, C.c_double)))
+        return out
 
     def entropy(self) -> np.ndarray:
         out = np.empty(self.n_slots)

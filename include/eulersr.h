@@ -130,6 +130,13 @@ typedef struct esr_case {
     double rho_inf;           /* force reference density */
     double u_inf;             /* force reference speed |U_inf| */
     double l_ref;             /* force reference length (obstacle_length) */
+    /* engineering criterion tracked beside the stop rule, never stopping the
+     * case (euler/main.py:66-113,160-171): |cd - target_cd| <= cd_tol *
+     * max(|target_cd|, 1e-8) and the same for cl, `eng_patience` checks in a row */
+    int32_t eng_track;
+    int32_t eng_patience;
+    double eng_target_cd, eng_target_cl;
+    double eng_cd_tol, eng_cl_tol;
 } esr_case;
 
 typedef struct esr_result {
@@ -143,6 +150,8 @@ typedef struct esr_result {
     double last_rel;          /* last stop-rule value */
     double cd, cl;            /* body-axis pressure force coefficients at the end */
     double solve_time_s;      /* device time from the case's start to its retirement */
+    int32_t eng_converged;    /* engineering criterion confirmed (0 when not tracked) */
+    int32_t eng_stopping_step;/* first step of its confirming streak, else N */
 } esr_result;
 
 typedef struct esr_mesh esr_mesh;
@@ -182,6 +191,10 @@ int esr_get_results(esr_solver* solver, esr_result* results_per_slot);
 int esr_residual_probe(esr_solver* solver, double* rel_per_slot);
 int esr_forces(esr_solver* solver, double* cd_per_slot, double* cl_per_slot);
 int esr_entropy(esr_solver* solver, double* total_per_slot);
+/* Unlimited LSQ gradient of the primitives of one slot, boundary ghosts
+ * included: grad[(cell*4 + var)*2 + dim], caller's cell order. Replaces the
+ * host gradient of the bundle export (euler/utils.py:33-39, helper.py:136-153). */
+int esr_gradients(esr_solver* solver, int32_t slot, double* grad);
 int esr_synchronize(esr_solver* solver);
 /* Device milliseconds of the solver's stream between the last two esr_run /
  * esr_step / esr_batch_solve boundaries. */

@@ -402,6 +402,17 @@ def time_step_srk2(W, mesh, dt, inlet, **kw):
     return h * (W + W1 - dt * k2)
 
 
+def time_step_srk2_local(W, mesh, cfl, inlet, gamma=1.4, **kw):
+    """SRK2 with the per-cell CFL step of the state at the start of the step
+    (the local-time-step option; the reference itself uses one global dt)."""
+    h = W.dtype.type(0.5)
+    dt = get_local_dt(W, mesh, CFL=cfl, gamma=gamma)[:, None]
+    k1 = residual(W, mesh, inlet, gamma=gamma, **kw)
+    W1 = W - dt * k1
+    k2 = residual(W1, mesh, inlet, gamma=gamma, **kw)
+    return h * (W + W1 - dt * k2)
+
+
 def time_step_ee(W, mesh, dt, inlet, **kw):
     """euler_solver.py:630-633."""
     return W - dt * residual(W, mesh, inlet, **kw)
@@ -458,7 +469,10 @@ def force_coefficients(W, mesh: OracleMesh, rho_inf, U_inf, L_ref, marker=None):
     if marker is None:
         marker = int(mesh.metadata.get('force_marker', 2))
     P = get_primitive(W)[:, 3]
-    faces, cells, slots = wall_owner_data(mesh, marker)
+    cache = mesh.metadata.setdefault('_wall_owner_cache', {})
+    if marker not in cache:
+        cache[marker] = wall_owner_data(mesh, marker)
+    faces, cells, slots = cache[marker]
     n = mesh.normals[cells, slots]
     ds = mesh.surface[faces]
     q = 0.5 * rho_inf * U_inf ** 2
@@ -493,6 +507,8 @@ class OracleRun:
     last_rel: float
     final_residual: float
     rel_history: list
+    eng_converged: bool | None = None
+    eng_stopping_step: int | None = None
 
 
 def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None = None,
@@ -504,8 +520,10 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
     step N, rel = ||W - W_ref|| / (steps * (||W_ref|| + 1e-16)) (``:150-152``);
     ``patience`` consecutive checks under the threshold stop the run and the
     stopping step is the first step of that streak (``:153-158``). Stopped steps
-    keep W (``:146``). ``stop_rule='density_l2'`` replaces rel by the density
-    residual L2 ||rho_{n} - rho_{n-1}||/sqrt(N) / dt of the last step.
+    keep W (``:146``) while checks continue to step N, which is where the
+    engineering criterion (``engineering_target_cd/cl`` in cfg) can still
+    confirm. ``stop_rule='density_l2'`` replaces rel by the RMS over cells of
+    the density residual of the state before the last step.
     ``max_steps`` caps N for tests.
     """
     cfl = float(cfg['CFL'])
@@ -522,6 +540,20 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
     thr = float(cfg['stationarity_threshold'])
     every = int(cfg['stationarity_check_every'])
     patience = max(1, int(cfg.get('stationarity_patience', 1)))
+    # engineering criterion tracked beside the stop rule (euler/main.py:66-113,160-171)
+    tcd, tcl = cfg.get('engineering_target_cd'), cfg.get('engineering_target_cl')
+    track = tcd is not None and tcl is not None
+    if track:
+        cd_tol = float(cfg.get('engineering_cd_tol', 0.001)) * max(abs(tcd), 1e-8)
+        cl_tol = float(cfg.get('engineering_cl_tol', 0.001)) * max(abs(tcl), 1e-8)
+        e_pat = max(1, int(cfg.get('engineering_patience', patience)))
+        U_inf = cfg['Mach'] * math.sqrt(gamma * cfg['p_inf'] / cfg['rho_inf'])
+        L_ref = mesh.metadata['obstacle_length']
+
+        def eng_ok(Wx):
+            cd, cl = force_coefficients(Wx, mesh, cfg['rho_inf'], U_inf, L_ref)
+            return abs(cd - tcd) <= cd_tol and abs(cl - tcl) <= cl_tol
+        e_streak, e_start, e_stop, e_stopping = (1 if eng_ok(W) else 0), 0, False, N
     W_ref = W
     ref_step = 0
     last_rel = math.inf
@@ -532,6 +564,8 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
     hist = []
     steps_taken = 0
     for step in range(1, N + 1):
+        if stop and not track:
+            break          # nothing observable changes once stopped
         W_prev = W
         if not stop:
             W = fn(W, mesh, dt, inlet, **kw)
@@ -539,7 +573,8 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
         if step % every == 0 or step == N:
             block = max(1, step - ref_step)
             if stop_rule == 'density_l2':
-                rel = float(np.sqrt(np.mean((W[:, 0].astype(np.float64) - W_prev[:, 0]) ** 2)) / float(dt))
+                R = residual(W_prev, mesh, inlet, **kw)
+                rel = float(np.sqrt(np.mean(R[:, 0].astype(np.float64) ** 2)))
             else:
                 rel = float(np.linalg.norm(W - W_ref) / (block * (np.linalg.norm(W_ref) + 1e-16)))
             under = rel <= thr
@@ -547,20 +582,30 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
             if under and streak == 0:
                 streak_start = step
             confirmed = new_streak >= patience and not stop
+            if track:
+                e_under = eng_ok(W)
+                new_e = e_streak + 1 if e_under else 0
+                if e_under and e_streak == 0:
+                    e_start = step
+                if new_e >= e_pat and not e_stop:
+                    e_stop, e_stopping = True, e_start
+                e_streak = new_e
             if confirmed:
                 stop = True
                 stopping_step = streak_start
             streak = new_streak
             W_ref = W
             ref_step = step
-            last_rel = rel
-            hist.append((step, rel))
-            if stop:
+            if not (stop and not confirmed):
+                last_rel = rel
+                hist.append((step, rel))
+            if stop and track and e_stop:
                 break
     W_probe = fn(W, mesh, dt, inlet, **kw)
     final_res = float(np.linalg.norm(W_probe - W) / (np.linalg.norm(W) + 1e-16))
     return OracleRun(W=W, dt=float(dt), n_max=N, converged=stop, stopping_step=int(stopping_step),
-                     steps_taken=steps_taken, last_rel=last_rel, final_residual=final_res, rel_history=hist)
+                     steps_taken=steps_taken, last_rel=last_rel, final_residual=final_res, rel_history=hist,
+                     eng_converged=(e_stop if track else None), eng_stopping_step=(e_stopping if track else None))
 
 
 # ----------------------------------------------------------------------------
