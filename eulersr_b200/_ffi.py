@@ -116,6 +116,23 @@ _SIGS = {
     "esr_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
+    "esr_gemm_bf16": (C.c_int, [C.c_int32] * 5 + [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
+                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.c_int32, C.c_int32, C.c_void_p]),
+    "esr_mlp_head_fwd": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
+    "esr_mlp_head_bwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "esr_mlp_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_float,
+                                   C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "esr_mlp_decode": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                 C.c_void_p, C.c_void_p]),
+    "esr_mlp_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    "esr_reduce_splits": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
+    "esr_colsum_bf16": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "esr_adamw": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
+                            C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_rel_change_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_idw_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                 C.c_void_p, C.c_void_p]),

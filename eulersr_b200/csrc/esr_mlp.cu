@@ -1,0 +1,483 @@
+// esr_mlp.cu -- BF16 training and inference kernels of the warm-start MLP.
+//
+// The network corrects an IDW interpolation of the coarse solution cell by
+// cell: 32 input features (13 used) -> 256 -> 3 residual blocks of 256 ->
+// 4 outputs. Its 256-wide layers are GEMMs of rows (cells) x 256 x 256 run
+// on the tensor cores by one kernel template:
+//   C[M x N] = A[M x K] * B[K x N], BF16 operands, FP32 accumulation
+//   (mma.sync m16n8k16), 128 x 128 x 32 CTA tiles, 8 warps of 64 x 32,
+//   3-stage cp.async pipeline, ldmatrix (.trans for the transposed operands)
+// with fused epilogues:
+//   EPI_F32   store the FP32 tile (split-K partials of the weight gradients)
+//   EPI_FWD   z = acc + bias; out = residual + relu(z)   (z kept for backward)
+//   EPI_BWD   dh = acc + dh_next; dz_prev = dh * (z_prev > 0)
+// The 4-wide head, the loss, AdamW and the fixed-order reductions are plain
+// SIMT kernels. Every reduction is deterministic (no atomics).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "esr_internal.h"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
+constexpr int PAD = 8;
+constexpr int LD_K = BK + PAD;     // row stride of K-contiguous tiles (elements)
+constexpr int LD_MN = BM + PAD;    // row stride of M/N-contiguous tiles
+
+enum { EPI_F32 = 0, EPI_FWD = 1, EPI_BWD = 2 };
+
+struct Epi {
+  const float* bias;     // FWD: per-column bias
+  const bf16* res;       // FWD: residual input; BWD: dh of the next layer
+  const bf16* aux;       // BWD: z of the previous layer (relu mask)
+  void* out0;            // F32: float partials; FWD: activation out; BWD: dh
+  bf16* out1;            // FWD: z; BWD: dz_prev
+  int ldo;               // leading dimension of res/aux/out0/out1
+  long long split_stride;// F32: elements between split-K partial tiles
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void ldsm_x4(unsigned r[4], const void* p) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(s));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned r[4], const void* p) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(s));
+}
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// A(m,k): A_T ? A[k*lda + m] : A[m*lda + k];  B(k,n): B_T ? B[k*ldb + n] : B[n*ldb + k]
+template <bool A_T, bool B_T, int EPI>
+__global__ void __launch_bounds__(THREADS) k_gemm(int M, int N, int K_split, const bf16* __restrict__ A, int lda,
+                                                  const bf16* __restrict__ B, int ldb, Epi e) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int A_ELEMS = A_T ? BK * LD_MN : BM * LD_K;
+  constexpr int B_ELEMS = B_T ? BK * LD_MN : BN * LD_K;
+  bf16* sA = reinterpret_cast<bf16*>(smem_raw);
+  bf16* sB = sA + STAGES * A_ELEMS;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int m_blk = blockIdx.y * BM, n_blk = blockIdx.x * BN;
+  const int k_begin = blockIdx.z * K_split;
+  const int KT = K_split / BK;
+
+  auto load_tile = [&](int stage, int kt) {
+    const int k0 = k_begin + kt * BK;
+    bf16* a = sA + stage * A_ELEMS;
+    bf16* b = sB + stage * B_ELEMS;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int c = tid + i * THREADS;   // 512 chunks of 8 elements per operand tile
+      if (!A_T) {
+        const int r = c >> 2, kc = (c & 3) * 8;
+        cp_async16(a + r * LD_K + kc, A + (size_t)(m_blk + r) * lda + k0 + kc);
+      } else {
+        const int r = c >> 4, mc = (c & 15) * 8;
+        cp_async16(a + r * LD_MN + mc, A + (size_t)(k0 + r) * lda + m_blk + mc);
+      }
+      if (!B_T) {
+        const int r = c >> 2, kc = (c & 3) * 8;
+        cp_async16(b + r * LD_K + kc, B + (size_t)(n_blk + r) * ldb + k0 + kc);
+      } else {
+        const int r = c >> 4, nc = (c & 15) * 8;
+        cp_async16(b + r * LD_MN + nc, B + (size_t)(k0 + r) * ldb + n_blk + nc);
+      }
+    }
+  };
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int pf = kt + STAGES - 1;
+    if (pf < KT) load_tile(pf % STAGES, pf);
+    cp_async_commit();
+    const bf16* a = sA + (kt % STAGES) * A_ELEMS;
+    const bf16* b = sB + (kt % STAGES) * B_ELEMS;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      unsigned af[4][4], bfr[2][4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        const int m0 = wm * 64 + mi * 16;
+        if (!A_T) ldsm_x4(af[mi], a + (m0 + (lane & 15)) * LD_K + kk + (lane >> 4) * 8);
+        else ldsm_x4_t(af[mi], a + (kk + (lane & 7) + (lane >> 4) * 8) * LD_MN + m0 + ((lane >> 3) & 1) * 8);
+      }
+#pragma unroll
+      for (int nj = 0; nj < 2; ++nj) {
+        const int n0 = wn * 32 + nj * 16;
+        if (!B_T) ldsm_x4(bfr[nj], b + (n0 + (lane & 7) + (lane >> 4) * 8) * LD_K + kk + ((lane >> 3) & 1) * 8);
+        else ldsm_x4_t(bfr[nj], b + (kk + (lane & 7) + ((lane >> 3) & 1) * 8) * LD_MN + n0 + (lane >> 4) * 8);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+          mma_bf16(acc[mi][ni], af[mi], bfr[ni >> 1][(ni & 1) * 2], bfr[ni >> 1][(ni & 1) * 2 + 1]);
+    }
+  }
+  cp_async_wait<0>();
+
+  const int g = lane >> 2, tig = lane & 3;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = m_blk + wm * 64 + mi * 16 + g + h * 8;
+        const int n = n_blk + wn * 32 + ni * 8 + tig * 2;
+        const float v0 = acc[mi][ni][2 * h], v1 = acc[mi][ni][2 * h + 1];
+        const size_t o = (size_t)m * e.ldo + n;
+        if (EPI == EPI_F32) {
+          float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
+          *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
+        } else if (EPI == EPI_FWD) {
+          const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
+          float r0 = 0.f, r1 = 0.f;
+          if (e.res) {
+            const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+            r0 = __bfloat162float(r.x);
+            r1 = __bfloat162float(r.y);
+          }
+          *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
+          *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
+              __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
+        } else {
+          float d0 = v0, d1 = v1;
+          if (e.res) {
+            const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+            d0 += __bfloat162float(r.x);
+            d1 += __bfloat162float(r.y);
+          }
+          *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
+          if (e.aux) {
+            const __nv_bfloat162 z = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
+            *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
+                __bfloat162float(z.x) > 0.f ? d0 : 0.f, __bfloat162float(z.y) > 0.f ? d1 : 0.f);
+          }
+        }
+      }
+}
+
+// ------------------------------------------------------------- SIMT kernels
+// y[r][j] = sum_k H[r][k] W[j][k] + b[j], 4 outputs, FP32 accumulation
+__global__ void k_head_fwd(const bf16* __restrict__ H, int rows, int K, const float* __restrict__ W,
+                           const float* __restrict__ b, const float* __restrict__ base, float* __restrict__ y) {
+  const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int k = lane; k < K; k += 32) {
+    const float h = __bfloat162float(H[(size_t)r * K + k]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) s[j] += h * W[j * K + k];
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+  if (lane < 4) y[(size_t)r * 4 + lane] = s[lane] + b[lane] + (base ? base[(size_t)r * 4 + lane] : 0.f);
+}
+
+// dH[r][k] = sum_j dY[r][j] W[j][k] as BF16, and dz = dH * (z > 0) of the
+// last hidden pre-activation
+__global__ void k_head_bwd_dx(const float* __restrict__ dY, int rows, int K, const float* __restrict__ W,
+                              const bf16* __restrict__ z, bf16* __restrict__ dH, bf16* __restrict__ dZ) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)rows * K) return;
+  const int r = (int)(i / K), k = (int)(i % K);
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) s += dY[(size_t)r * 4 + j] * W[j * K + k];
+  dH[i] = __float2bfloat16(s);
+  dZ[i] = __float2bfloat16(__bfloat162float(z[i]) > 0.f ? s : 0.f);
+}
+
+// Per-cell inputs of one case (BF16 rows of `ld` columns, zero padded):
+// [x, y, wall distance, wall normal x, y (5 static), IDW primitives
+// normalised (4), asinh(IDW dp/dx / s_p), asinh(dp/dy / s_p) (2), M_n, alpha_n]
+__global__ void k_features(const float* __restrict__ stat5, const float* __restrict__ idw_prim,
+                           const float* __restrict__ idw_gradp, int rows, float mach_n, float aoa_n,
+                           const float* __restrict__ mu, const float* __restrict__ sig, int ld, bf16* __restrict__ X) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  bf16* x = X + (size_t)r * ld;
+  for (int j = 0; j < 5; ++j) x[j] = __float2bfloat16(stat5[(size_t)r * 5 + j]);
+  for (int v = 0; v < 4; ++v) x[5 + v] = __float2bfloat16((idw_prim[(size_t)r * 4 + v] - mu[v]) / sig[v]);
+  const float sp = sig[3] + 1e-8f;
+  x[9] = __float2bfloat16(asinhf(idw_gradp[(size_t)r * 2] / sp));
+  x[10] = __float2bfloat16(asinhf(idw_gradp[(size_t)r * 2 + 1] / sp));
+  x[11] = __float2bfloat16(mach_n);
+  x[12] = __float2bfloat16(aoa_n);
+  for (int j = 13; j < ld; ++j) x[j] = __float2bfloat16(0.f);
+}
+
+// normalised primitive prediction -> conserved state (float64 rows), with
+// density and pressure kept above `floor_frac` of their freestream values
+__global__ void k_decode(const float* __restrict__ pred_n, int rows, const float* __restrict__ mu,
+                         const float* __restrict__ sig, float gamma, float rho_floor, float p_floor,
+                         double* __restrict__ W) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const float rho = fmaxf(pred_n[(size_t)r * 4] * sig[0] + mu[0], rho_floor);
+  const float u = pred_n[(size_t)r * 4 + 1] * sig[1] + mu[1];
+  const float v = pred_n[(size_t)r * 4 + 2] * sig[2] + mu[2];
+  const float p = fmaxf(pred_n[(size_t)r * 4 + 3] * sig[3] + mu[3], p_floor);
+  W[(size_t)r * 4] = rho;
+  W[(size_t)r * 4 + 1] = (double)rho * u;
+  W[(size_t)r * 4 + 2] = (double)rho * v;
+  W[(size_t)r * 4 + 3] = (double)p / (gamma - 1.0) + 0.5 * (double)rho * ((double)u * u + (double)v * v);
+}
+
+// per-block partials of dW_head[j][k] = sum_r dY[r][j] H[r][k] and db[j] = sum_r dY[r][j]
+__global__ void k_head_bwd_dw(const float* __restrict__ dY, const bf16* __restrict__ H, int rows, int K,
+                              int rows_per_block, float* __restrict__ part) {
+  const int k = threadIdx.x;            // blockDim.x == K (256)
+  const int r0 = blockIdx.x * rows_per_block, r1 = min(rows, r0 + rows_per_block);
+  float s[4] = {0.f, 0.f, 0.f, 0.f}, sb[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int r = r0; r < r1; ++r) {
+    const float h = __bfloat162float(H[(size_t)r * K + k]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float d = dY[(size_t)r * 4 + j];
+      s[j] += d * h;
+      sb[j] += d;
+    }
+  }
+  float* p = part + (size_t)blockIdx.x * (4 * K + 4);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) p[j * K + k] = s[j];
+  if (k < 4) p[4 * K + k] = sb[k];
+}
+
+// out[i] = sum_s part[s * stride + i] in split order
+__global__ void k_reduce_splits(const float* __restrict__ part, int splits, long long stride, long long n,
+                                float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.f;
+  for (int z = 0; z < splits; ++z) s += part[(size_t)z * stride + i];
+  out[i] = s;
+}
+
+// column sums of a BF16 [rows x C] matrix in fixed row blocks (bias gradients)
+__global__ void k_colsum_part(const bf16* __restrict__ X, int rows, int C, int rows_per_block, float* __restrict__ part) {
+  const int c = blockIdx.y * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const int r0 = blockIdx.x * rows_per_block, r1 = min(rows, r0 + rows_per_block);
+  float s = 0.f;
+  for (int r = r0; r < r1; ++r) s += __bfloat162float(X[(size_t)r * C + c]);
+  part[(size_t)blockIdx.x * C + c] = s;
+}
+
+// shock-weighted relative MSE (loss.py:20-23) on pred = base + head:
+// L = mean_v [ sum_r w_r (p - t)^2 / R / (mean_r t^2 + 1e-8) ]; dpred written;
+// per-block partial sums of the loss numerators
+__global__ void k_loss(const float* __restrict__ pred, const float* __restrict__ tgt, const float* __restrict__ w,
+                       int rows, const float* __restrict__ inv_den, float* __restrict__ dpred,
+                       float* __restrict__ part) {
+  __shared__ float sh[256];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.f;
+  if (r < rows) {
+    const float wr = w ? w[r] : 1.f;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const float d = pred[(size_t)r * 4 + v] - tgt[(size_t)r * 4 + v];
+      l += wr * d * d * inv_den[v];
+      dpred[(size_t)r * 4 + v] = 2.f * wr * d * inv_den[v] / (4.f * rows);
+    }
+  }
+  sh[threadIdx.x] = l;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0] / (4.f * rows);
+}
+
+// AdamW on FP32 master weights with a BF16 (or FP32) working copy
+__global__ void k_adamw(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                        float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float wd,
+                        float bc1, float bc2, bf16* __restrict__ p_bf16) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / bc1, vh = vi / bc2;
+  const float pi = p[i] * (1.f - lr * wd) - lr * mh / (sqrtf(vh) + eps);
+  p[i] = pi;
+  if (p_bf16) p_bf16[i] = __float2bfloat16(pi);
+}
+
+int mfail(int code, const std::string& msg) { return esr::report_error(code, msg); }
+
+template <bool AT, bool BT, int EPI>
+int launch_gemm(int M, int N, int K, int splits, const bf16* A, int lda, const bf16* B, int ldb, const Epi& e,
+                cudaStream_t st) {
+  constexpr int A_ELEMS = AT ? BK * LD_MN : BM * LD_K;
+  constexpr int B_ELEMS = BT ? BK * LD_MN : BN * LD_K;
+  const int smem = STAGES * (A_ELEMS + B_ELEMS) * (int)sizeof(bf16);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_gemm<AT, BT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set = true;
+  }
+  dim3 grid(N / BN, M / BM, splits);
+  k_gemm<AT, BT, EPI><<<grid, THREADS, smem, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+  return ESR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// C = A * B with the epilogue `epi` (0 F32 split-K partials, 1 forward, 2 backward).
+// trans_a: A stored [K][M] (lda >= M); else [M][K] (lda >= K).
+// trans_b: B stored [K][N] (ldb >= N); else [N][K] (ldb >= K).
+// M, N multiples of 128; K a multiple of 32 * splits; rows 16-byte aligned.
+int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
+                  const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res, const void* aux,
+                  void* out0, void* out1, int32_t ldo, int32_t splits, void* stream) {
+  if (!A || !B || !out0) return mfail(ESR_ERR_ARG, "gemm: null operand");
+  if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN) return mfail(ESR_ERR_ARG, "gemm: M and N must be multiples of 128");
+  if (splits < 1 || K % (BK * splits)) return mfail(ESR_ERR_ARG, "gemm: K must be a multiple of 32 x splits");
+  if (lda % 8 || ldb % 8 || ldo % 2) return mfail(ESR_ERR_ARG, "gemm: leading dimensions must keep 16-byte rows");
+  if ((trans_a ? lda < M : lda < K) || (trans_b ? ldb < N : ldb < K) || ldo < N)
+    return mfail(ESR_ERR_ARG, "gemm: leading dimension too small");
+  if (((uintptr_t)A | (uintptr_t)B) & 15) return mfail(ESR_ERR_ARG, "gemm: operands must be 16-byte aligned");
+  if (epi == EPI_FWD && (!bias || !out1)) return mfail(ESR_ERR_ARG, "gemm: forward epilogue needs bias and z output");
+  if (epi == EPI_BWD && aux && !out1) return mfail(ESR_ERR_ARG, "gemm: backward epilogue with z needs dz output");
+  if (epi != EPI_F32 && splits != 1) return mfail(ESR_ERR_ARG, "gemm: split-K only with the F32 epilogue");
+  Epi e{bias, (const bf16*)res, (const bf16*)aux, out0, (bf16*)out1, ldo, (long long)M * ldo};
+  cudaStream_t st = (cudaStream_t)stream;
+  const bf16* a = (const bf16*)A;
+  const bf16* b = (const bf16*)B;
+#define ESR_GEMM_CASE(TA, TB, E) \
+  if (!!trans_a == TA && !!trans_b == TB && epi == E) launch_gemm<TA, TB, E>(M, N, K, splits, a, lda, b, ldb, e, st); else
+  ESR_GEMM_CASE(false, false, EPI_FWD)
+  ESR_GEMM_CASE(false, true, EPI_BWD)
+  ESR_GEMM_CASE(true, true, EPI_F32)
+  ESR_GEMM_CASE(false, false, EPI_F32)
+  ESR_GEMM_CASE(false, true, EPI_F32)
+  ESR_GEMM_CASE(false, false, EPI_BWD)
+  return mfail(ESR_ERR_ARG, "gemm: unsupported layout/epilogue combination");
+#undef ESR_GEMM_CASE
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, std::string("gemm: ") + cudaGetErrorString(err));
+}
+
+// 4-wide head: y = H W^T + b (+ base); H [rows x K] BF16, W [4 x K] FP32
+int esr_mlp_head_fwd(const void* H, int32_t rows, int32_t K, const float* W, const float* b, const float* base,
+                     float* y, void* stream) {
+  if (!H || !W || !b || !y || rows <= 0 || K <= 0) return mfail(ESR_ERR_ARG, "head_fwd: bad argument");
+  const int wpb = 8;
+  k_head_fwd<<<(rows + wpb - 1) / wpb, wpb * 32, 0, (cudaStream_t)stream>>>((const bf16*)H, rows, K, W, b, base, y);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+// head backward: dH = dY W and dZ = dH * (z > 0) (BF16), dW/db partials per
+// block of `rpb` rows (4*K + 4 floats per block)
+int esr_mlp_head_bwd(const float* dY, const void* H, const void* Z, int32_t rows, int32_t K, const float* W, void* dH,
+                     void* dZ, float* part, int32_t rpb, void* stream) {
+  if (!dY || !H || !Z || !W || !dH || !dZ || !part || rows <= 0 || K != 256 || rpb <= 0)
+    return mfail(ESR_ERR_ARG, "head_bwd: bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)rows * K;
+  k_head_bwd_dx<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dY, rows, K, W, (const bf16*)Z, (bf16*)dH, (bf16*)dZ);
+  k_head_bwd_dw<<<(rows + rpb - 1) / rpb, K, 0, st>>>(dY, (const bf16*)H, rows, K, rpb, part);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_mlp_features(const float* stat5, const float* idw_prim, const float* idw_gradp, int32_t rows, float mach_n,
+                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, void* stream) {
+  if (!stat5 || !idw_prim || !idw_gradp || !mu || !sig || !X || rows <= 0 || ld < 13)
+    return mfail(ESR_ERR_ARG, "features: bad argument");
+  k_features<<<(rows + 127) / 128, 128, 0, (cudaStream_t)stream>>>(stat5, idw_prim, idw_gradp, rows, mach_n, aoa_n,
+                                                                   mu, sig, ld, (bf16*)X);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_mlp_decode(const float* pred_n, int32_t rows, const float* mu, const float* sig, float gamma, float rho_floor,
+                   float p_floor, double* W, void* stream) {
+  if (!pred_n || !mu || !sig || !W || rows <= 0) return mfail(ESR_ERR_ARG, "decode: bad argument");
+  k_decode<<<(rows + 127) / 128, 128, 0, (cudaStream_t)stream>>>(pred_n, rows, mu, sig, gamma, rho_floor, p_floor, W);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_reduce_splits(const float* part, int32_t splits, int64_t stride, int64_t n, float* out, void* stream) {
+  if (!part || !out || splits <= 0 || n <= 0 || stride < n) return mfail(ESR_ERR_ARG, "reduce_splits: bad argument");
+  k_reduce_splits<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(part, splits, stride, n, out);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_colsum_bf16(const void* X, int32_t rows, int32_t C, int32_t rpb, float* part, void* stream) {
+  if (!X || !part || rows <= 0 || C <= 0 || rpb <= 0) return mfail(ESR_ERR_ARG, "colsum: bad argument");
+  dim3 grid((rows + rpb - 1) / rpb, (C + 127) / 128);
+  k_colsum_part<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16*)X, rows, C, rpb, part);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_mlp_loss(const float* pred, const float* tgt, const float* w, int32_t rows, const float* inv_den,
+                 float* dpred, float* part, void* stream) {
+  if (!pred || !tgt || !inv_den || !dpred || !part || rows <= 0) return mfail(ESR_ERR_ARG, "loss: bad argument");
+  k_loss<<<(rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(pred, tgt, w, rows, inv_den, dpred, part);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+int esr_adamw(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+              float wd, int32_t step, void* p_bf16, void* stream) {
+  if (!p || !g || !m || !v || n <= 0 || step < 1) return mfail(ESR_ERR_ARG, "adamw: bad argument");
+  const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
+  k_adamw<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, wd, bc1, bc2,
+                                                                         (bf16*)p_bf16);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
+}
+
+}  // extern "C"

@@ -245,6 +245,42 @@ int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars,
                   const int32_t* d_idx, const float* d_dist, int32_t n_dst, int32_t k,
                   float* d_out, void* stream);
 
+/* ---- learned warm start: BF16 training/inference kernels of the residual
+ * MLP that corrects the IDW interpolation (replaces the DAM/AMNet forward of
+ * models/dam.py:306-308 with a 4 x 256 residual MLP; loss of loss.py:20-23).
+ * All pointers are device pointers; `stream` is a cudaStream_t or NULL. */
+
+/* C[M x N] = A[M x K] B[K x N] on the tensor cores, BF16 operands, FP32
+ * accumulation. trans_a: A stored [K][M] else [M][K]; trans_b: B stored
+ * [K][N] else [N][K] (a torch Linear weight). epi 0: FP32 partial tiles
+ * (out0 + split * M * ldo); epi 1: z = acc + bias -> out1, out0 = res +
+ * relu(z); epi 2: dh = acc + res -> out0, out1 = dh * (aux > 0).
+ * M, N multiples of 128, K a multiple of 32 * splits. */
+int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
+                  const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res, const void* aux,
+                  void* out0, void* out1, int32_t ldo, int32_t splits, void* stream);
+/* 4-wide output layer: y = H W^T + b (+ base), H BF16 [rows x K], W FP32 [4 x K] */
+int esr_mlp_head_fwd(const void* H, int32_t rows, int32_t K, const float* W, const float* b, const float* base,
+                     float* y, void* stream);
+/* its backward: dH = dY W, dZ = dH * (Z > 0) (BF16), dW/db partials per `rpb` rows */
+int esr_mlp_head_bwd(const float* dY, const void* H, const void* Z, int32_t rows, int32_t K, const float* W, void* dH,
+                     void* dZ, float* part, int32_t rpb, void* stream);
+/* per-cell input rows (13 features, zero padded to ld columns, BF16) */
+int esr_mlp_features(const float* stat5, const float* idw_prim, const float* idw_gradp, int32_t rows, float mach_n,
+                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, void* stream);
+/* normalised primitive prediction -> conserved float64 rows (density and pressure floored) */
+int esr_mlp_decode(const float* pred_n, int32_t rows, const float* mu, const float* sig, float gamma, float rho_floor,
+                   float p_floor, double* W, void* stream);
+/* shock-weighted relative MSE: per-block loss partials and d loss / d pred */
+int esr_mlp_loss(const float* pred, const float* tgt, const float* w, int32_t rows, const float* inv_den,
+                 float* dpred, float* part, void* stream);
+/* fixed-order sums: out[i] = sum_s part[s*stride + i]; column sums of BF16 rows */
+int esr_reduce_splits(const float* part, int32_t splits, int64_t stride, int64_t n, float* out, void* stream);
+int esr_colsum_bf16(const void* X, int32_t rows, int32_t C, int32_t rpb, float* part, void* stream);
+/* AdamW on FP32 master weights, refreshing an optional BF16 copy */
+int esr_adamw(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+              float wd, int32_t step, void* p_bf16, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
