@@ -23,7 +23,7 @@ FLUX = {"hllc": 0, "hll": 0, "rusanov": 1}
 RECON = {"muscl": 0, "second_order": 0, "2nd_order": 0, "constant": 1, "first_order": 1, "none": 1, "godunov": 1}
 TIME = {"SRK2": 0, "SSP_RK2": 0, "EE": 1, "RK2": 2}
 DT_MODE = {"global": 0, "local": 1}
-STOP_RULE = {"reference": 0, "density_l2": 1}
+STOP_RULE = {"reference": 0, "density_l2": 1, "engineering": 2}
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
@@ -124,7 +124,7 @@ _SIGS = {
     "esr_mlp_head_bwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "esr_mlp_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_float,
-                                   C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+                                   C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "esr_mlp_decode": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
                                  C.c_void_p, C.c_void_p]),
     "esr_mlp_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,

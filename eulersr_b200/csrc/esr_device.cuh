@@ -601,7 +601,7 @@ static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* 
   cc.ref_step[g] = done;
   int st = 0;
   if (!finite) st = 4;
-  else if (nstreak >= patience) st = 2;
+  else if (stop_rule != 2 && nstreak >= patience) st = 2;
   else if (done >= cc.nmax[g]) st = 3;
   bool eng_under = false;
   if (cc.eng_track[g]) {
@@ -614,6 +614,10 @@ static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* 
     if (nes >= cc.eng_patience[g] && !cc.eng_stop[g]) {
       cc.eng_stop[g] = 1;
       cc.eng_stopping[g] = cc.eng_start[g];
+      if (stop_rule == 2 && finite) {   // the criterion itself ends the case
+        st = 2;
+        cc.streak_start[g] = cc.eng_start[g];
+      }
     }
     // The reference keeps checking the frozen field after the stop rule
     // fires until step N: the criterion can still confirm on that field.

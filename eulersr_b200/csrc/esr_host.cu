@@ -936,7 +936,8 @@ int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_me
   if (p.reconstruction != ESR_RECON_MUSCL && p.reconstruction != ESR_RECON_CONSTANT) return fail(ESR_ERR_ARG, "Unknown reconstruction scheme");
   if (p.time_scheme < ESR_TIME_SRK2 || p.time_scheme > ESR_TIME_RK2) return fail(ESR_ERR_ARG, "unknown time scheme");
   if (p.dt_mode != ESR_DT_GLOBAL && p.dt_mode != ESR_DT_LOCAL) return fail(ESR_ERR_ARG, "unknown dt mode");
-  if (p.stop_rule != ESR_STOP_REFERENCE && p.stop_rule != ESR_STOP_DENSITY_L2) return fail(ESR_ERR_ARG, "unknown stop rule");
+  if (p.stop_rule != ESR_STOP_REFERENCE && p.stop_rule != ESR_STOP_DENSITY_L2 && p.stop_rule != ESR_STOP_ENGINEERING)
+    return fail(ESR_ERR_ARG, "unknown stop rule");
   if (!(p.gamma > 1.0)) return fail(ESR_ERR_ARG, "gamma must be > 1");
   auto s = std::make_unique<esr_solver>();
   s->precision = p.precision;

@@ -232,12 +232,17 @@ __global__ void k_head_bwd_dx(const float* __restrict__ dY, int rows, int K, con
 // normalised (4), asinh(IDW dp/dx / s_p), asinh(dp/dy / s_p) (2), M_n, alpha_n]
 __global__ void k_features(const float* __restrict__ stat5, const float* __restrict__ idw_prim,
                            const float* __restrict__ idw_gradp, int rows, float mach_n, float aoa_n,
-                           const float* __restrict__ mu, const float* __restrict__ sig, int ld, bf16* __restrict__ X) {
+                           const float* __restrict__ mu, const float* __restrict__ sig, int ld, bf16* __restrict__ X,
+                           float* __restrict__ base) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rows) return;
   bf16* x = X + (size_t)r * ld;
   for (int j = 0; j < 5; ++j) x[j] = __float2bfloat16(stat5[(size_t)r * 5 + j]);
-  for (int v = 0; v < 4; ++v) x[5 + v] = __float2bfloat16((idw_prim[(size_t)r * 4 + v] - mu[v]) / sig[v]);
+  for (int v = 0; v < 4; ++v) {
+    const float q = (idw_prim[(size_t)r * 4 + v] - mu[v]) / sig[v];
+    x[5 + v] = __float2bfloat16(q);
+    if (base) base[(size_t)r * 4 + v] = q;   // the IDW prediction the MLP corrects
+  }
   const float sp = sig[3] + 1e-8f;
   x[9] = __float2bfloat16(asinhf(idw_gradp[(size_t)r * 2] / sp));
   x[10] = __float2bfloat16(asinhf(idw_gradp[(size_t)r * 2 + 1] / sp));
@@ -430,11 +435,11 @@ int esr_mlp_head_bwd(const float* dY, const void* H, const void* Z, int32_t rows
 }
 
 int esr_mlp_features(const float* stat5, const float* idw_prim, const float* idw_gradp, int32_t rows, float mach_n,
-                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, void* stream) {
+                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, float* base, void* stream) {
   if (!stat5 || !idw_prim || !idw_gradp || !mu || !sig || !X || rows <= 0 || ld < 13)
     return mfail(ESR_ERR_ARG, "features: bad argument");
   k_features<<<(rows + 127) / 128, 128, 0, (cudaStream_t)stream>>>(stat5, idw_prim, idw_gradp, rows, mach_n, aoa_n,
-                                                                   mu, sig, ld, (bf16*)X);
+                                                                   mu, sig, ld, (bf16*)X, base);
   cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, cudaGetErrorString(err));
 }

@@ -1,0 +1,210 @@
+"""Config 5: train the warm-start model and compare warm vs cold HR solves.
+
+    python -m eulersr_b200.warmstart.run --n-train 512 --n-eval 128 --out warm.json
+
+Geometry NACA2412, HR h=0.025, LR h=0.1; cases (Mach ~ U[0.7, 3], alpha ~
+U[-5, 5]) from default_rng(3): the first n_train train, the next n_eval are
+held out. All solves use the local CFL step (CFL 0.6, 0.45 transonic).
+
+Accuracy protocol. The per-step change statistic of the reference's stop rule
+flattens on a limiter-chatter floor (~2e-5 on these meshes) well before the
+force coefficients settle, so it cannot certify CD accuracy. Each held-out
+case therefore gets a reference CD from a long solve (``--ref-steps`` steps,
+then 5,000 more: cases whose CD still moves by more than 0.1 % are unsteady
+and count as failures for every start; an FP64 subset checks the FP32
+values), and every start (cold freestream, IDW, IDW+MLP) runs with the stop
+rule that ends a case once its CD has stayed within 0.5 % of that reference
+for 8 checks 25 steps apart (200 steps): the iteration at which the solve is
+converged to that accuracy. All cases stream through ``--slots`` slots with
+retire/refill; converged cases/s counts the cases that got there over the
+whole pipeline time (LR solve + inference + HR solve). The reference residual
+rule (``--threshold``) is run as well and reported with the CD error its stop
+leaves.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from ..mesh import Mesh
+from ..meshing import build_mesh
+from ..solver import DeviceMesh, FlowCase, Solver
+from .features import MeshPair
+from .mlp import MLP
+from .pipeline import WarmStart, build_training_set, draw_cases, eval_loss, pressure_gradients, primitives, train
+
+
+def cached_mesh(geom, h):
+    d = Path(os.environ.get("EULERSR_MESH_CACHE", Path(tempfile.gettempdir()) / "eulersr_meshes"))
+    d.mkdir(parents=True, exist_ok=True)
+    p = d / f"{geom}_h{h}.npz"
+    if p.exists():
+        return Mesh.load(p)
+    m = build_mesh(geom, h)
+    m.save(p)
+    return m
+
+
+def solve(dm, machs, aoas, *, slots=256, precision="f32", stop_rule="reference", threshold=1e-30, check_every=25,
+          patience=8, max_steps=20000, cd_targets=None, cd_tol=0.005, init_fields=None, want_states=False):
+    """Batched solve with retire/refill; returns (results, states, wall seconds)."""
+    dtype = np.float64 if precision == "f64" else np.float32
+    cases = []
+    for i, (m, a) in enumerate(zip(machs, aoas)):
+        kw = {}
+        if cd_targets is not None:
+            kw = dict(eng_target_cd=float(cd_targets[i]), eng_target_cl=0.0, eng_cd_tol=cd_tol, eng_cl_tol=1e12,
+                      eng_patience=patience)
+        cases.append(FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, max_steps=max_steps, dtype=dtype, **kw))
+    s = Solver(dm, min(slots, max(1, len(cases))), precision=precision, dt_mode="local", stop_rule=stop_rule,
+               threshold=threshold, check_every=check_every, patience=patience)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res, states = s.batch_solve(cases, init_fields=init_fields, want_states=want_states)
+    wall = time.perf_counter() - t0
+    s.close()
+    return res, states, wall
+
+
+def _summ(res, truth_cd, wall, extra_time=0.0, tol=0.005, steady=None):
+    steps = np.array([r["stopping_step"] for r in res])
+    conv = np.array([r["status"] == 2 for r in res])
+    if steady is not None:
+        conv = conv & steady
+    cd = np.array([r["cd"] for r in res])
+    err = np.abs(cd - truth_cd) / np.maximum(np.abs(truth_cd), 1e-8)
+    ok = conv & (err <= tol)
+    t = wall + extra_time
+    return {"median_iterations": float(np.median(steps)), "mean_iterations": float(steps.mean()),
+            "stopped_by_rule": int(conv.sum()), "cd_err_median": float(np.median(err)),
+            "cd_err_max": float(err.max()), "converged_within_0.5pct": int(ok.sum()), "pipeline_s": float(t),
+            "converged_cases_per_s": float(ok.sum() / t) if t > 0 else None}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--geom", default="naca2412")
+    ap.add_argument("--h-hr", type=float, default=0.025)
+    ap.add_argument("--h-lr", type=float, default=0.1)
+    ap.add_argument("--n-train", type=int, default=512)
+    ap.add_argument("--n-eval", type=int, default=256)
+    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--lr-steps", type=int, default=6000)
+    ap.add_argument("--target-steps", type=int, default=20000)
+    ap.add_argument("--ref-steps", type=int, default=30000)
+    ap.add_argument("--max-steps", type=int, default=30000)
+    ap.add_argument("--threshold", type=float, default=3e-5)
+    ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--single-sample", type=int, default=8)
+    ap.add_argument("--f64-check", type=int, default=16)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    rep = {"config": vars(a), "protocol": "local CFL dt; stop once CD stays within 0.5% of a long-solve reference "
+                                          "for 8 checks 25 steps apart; unsteady references excluded"}
+    T = {}
+    t0 = time.perf_counter()
+    hr, lr = cached_mesh(a.geom, a.h_hr), cached_mesh(a.geom, a.h_lr)
+    pair = MeshPair.build(hr, lr)
+    dm_hr, dm_lr = DeviceMesh(hr), DeviceMesh(lr)
+    T["setup_s"] = time.perf_counter() - t0
+    rep["cells"] = {"hr": hr.n_cells, "lr": lr.n_cells}
+    (mt, at), (me, ae) = draw_cases(a.n_train, a.n_eval, seed=3)
+    n_all = a.n_train + a.n_eval
+
+    # ---- LR solutions for every case (the warm start's input)
+    lr_res, lr_states, T["lr_solve_all_s"] = solve(dm_lr, np.r_[mt, me], np.r_[at, ae], max_steps=a.lr_steps,
+                                                   want_states=True)
+    lr_gp = pressure_gradients(lr, dm_lr, lr_states, np.r_[mt, me], np.r_[at, ae])
+    lr_s_per_case = T["lr_solve_all_s"] / n_all
+    # ---- HR training targets
+    _, hr_states, T["hr_targets_s"] = solve(dm_hr, mt, at, max_steps=a.target_steps, want_states=True)
+    hr_gp = pressure_gradients(hr, dm_hr, hr_states, mt, at)
+    # ---- model
+    ws = WarmStart(pair)
+    data, mu, sig = build_training_set(ws, lr_states[:a.n_train], lr_gp[:a.n_train], hr_states, hr_gp, mt, at)
+    del hr_states
+    mlp = MLP(seed=0)
+    ws.mlp = mlp
+    rep["train_rows"] = int(data.X.shape[0])
+    loss_idw = eval_loss(None, data)
+    hist, T["train_s"] = train(mlp, data, steps=a.train_steps)
+    rep["loss"] = {"idw_train": loss_idw, "mlp_train": eval_loss(mlp, data), "history": hist}
+    del data
+    torch.cuda.empty_cache()
+
+    # ---- held-out reference CDs (long solves + 5,000 more steps), FP64 check on a subset
+    ref_a, ref_states, T["reference_s"] = solve(dm_hr, me, ae, max_steps=a.ref_steps, want_states=True)
+    ref_b, _, t_b = solve(dm_hr, me, ae, max_steps=5000, init_fields=ref_states)
+    T["reference_s"] += t_b
+    del ref_states
+    cd_a = np.array([r["cd"] for r in ref_a])
+    truth = np.array([r["cd"] for r in ref_b])
+    steady = np.abs(truth - cd_a) <= 1e-3 * np.abs(truth)
+    rep["reference_steady_cases"] = int(steady.sum())
+    k64 = min(a.f64_check, a.n_eval)
+    ref64, _, T["reference_f64_s"] = solve(dm_hr, me[:k64], ae[:k64], precision="f64", max_steps=a.ref_steps)
+    cd64 = np.array([r["cd"] for r in ref64])
+    rel64 = np.abs(cd_a[:k64] - cd64) / np.abs(cd64)
+    rep["reference_f32_vs_f64_cd_relerr"] = {"steady_max": float(rel64[steady[:k64]].max()) if steady[:k64].any() else None,
+                                             "all_max": float(rel64.max())}
+
+    # ---- inference
+    lr_e, gp_e = lr_states[a.n_train:], lr_gp[a.n_train:]
+    inits = {}
+    for name, use in (("idw", False), ("mlp", True)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        inits[name] = [ws.predict_state(primitives(W).astype(np.float32), g, m, al, use_mlp=use)
+                       for W, g, m, al in zip(lr_e, gp_e, me, ae)]
+        torch.cuda.synchronize()
+        T[f"infer_{name}_s"] = time.perf_counter() - t
+    lr_eval_s = lr_s_per_case * a.n_eval
+
+    # ---- convergence to 0.5 % CD accuracy, every start
+    starts = {}
+    res, _, t = solve(dm_hr, me, ae, slots=a.slots, stop_rule="engineering", max_steps=a.max_steps,
+                      cd_targets=truth)
+    starts["cold_batched"] = _summ(res, truth, t, steady=steady)
+    for name in ("idw", "mlp"):
+        res, _, t = solve(dm_hr, me, ae, slots=a.slots, stop_rule="engineering", max_steps=a.max_steps,
+                          cd_targets=truth, init_fields=inits[name])
+        starts[f"{name}_batched"] = _summ(res, truth, t, lr_eval_s + T[f"infer_{name}_s"], steady=steady)
+    # plain single-case solves from freestream, one case per launch, on a sample
+    k = min(a.single_sample, a.n_eval)
+    single, wall1 = [], 0.0
+    for i in range(k):
+        r, _, t = solve(dm_hr, me[i:i + 1], ae[i:i + 1], slots=1, stop_rule="engineering", max_steps=a.max_steps,
+                        cd_targets=truth[i:i + 1])
+        single += r
+        wall1 += t
+    starts["cold_single_case"] = _summ(single, truth[:k], wall1, steady=steady[:k])
+    rep["starts_cd_accuracy"] = starts
+    base_rate = starts["cold_single_case"]["converged_cases_per_s"] or 0.0
+    rep["converged_cases_per_s_vs_single_cold"] = {
+        n: (v["converged_cases_per_s"] / base_rate if base_rate else None) for n, v in starts.items()}
+    rep["iterations_ratio_vs_cold"] = {n: starts["cold_batched"]["median_iterations"] / max(v["median_iterations"], 1)
+                                       for n, v in starts.items()}
+    # ---- the reference residual rule, for comparison
+    resid = {}
+    for name, init in (("cold", None), ("idw", inits["idw"]), ("mlp", inits["mlp"])):
+        res, _, t = solve(dm_hr, me, ae, slots=a.slots, threshold=a.threshold, check_every=5, patience=3,
+                          max_steps=a.max_steps, init_fields=init)
+        resid[name] = _summ(res, truth, t, 0.0 if init is None else lr_eval_s + T[f"infer_{name}_s"], steady=steady)
+    rep["residual_rule"] = resid
+    rep["timings_s"] = T
+    txt = json.dumps(rep, indent=1, default=float)
+    print(txt)
+    if a.out:
+        Path(a.out).write_text(txt)
+    return rep
+
+
+if __name__ == "__main__":
+    main()

@@ -69,6 +69,8 @@ extern "C" {
 #define ESR_DT_LOCAL 1         /* per-cell CFL dt recomputed every step */
 #define ESR_STOP_REFERENCE 0   /* ||W_n - W_ref||_F / (steps (||W_ref||_F + 1e-16)) */
 #define ESR_STOP_DENSITY_L2 1  /* RMS over cells of the density residual */
+#define ESR_STOP_ENGINEERING 2 /* stop when the engineering criterion (force coefficients
+                                * within tolerance of given targets) is confirmed */
 
 /* Mesh description; all host arrays are owned by the caller and copied. */
 typedef struct esr_mesh_desc {
@@ -265,9 +267,10 @@ int esr_mlp_head_fwd(const void* H, int32_t rows, int32_t K, const float* W, con
 /* its backward: dH = dY W, dZ = dH * (Z > 0) (BF16), dW/db partials per `rpb` rows */
 int esr_mlp_head_bwd(const float* dY, const void* H, const void* Z, int32_t rows, int32_t K, const float* W, void* dH,
                      void* dZ, float* part, int32_t rpb, void* stream);
-/* per-cell input rows (13 features, zero padded to ld columns, BF16) */
+/* per-cell input rows (13 features, zero padded to ld columns, BF16) and,
+ * when base != NULL, the normalised IDW primitives the MLP corrects (FP32) */
 int esr_mlp_features(const float* stat5, const float* idw_prim, const float* idw_gradp, int32_t rows, float mach_n,
-                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, void* stream);
+                     float aoa_n, const float* mu, const float* sig, int32_t ld, void* X, float* base, void* stream);
 /* normalised primitive prediction -> conserved float64 rows (density and pressure floored) */
 int esr_mlp_decode(const float* pred_n, int32_t rows, const float* mu, const float* sig, float gamma, float rho_floor,
                    float p_floor, double* W, void* stream);

@@ -581,7 +581,7 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
             new_streak = streak + 1 if under else 0
             if under and streak == 0:
                 streak_start = step
-            confirmed = new_streak >= patience and not stop
+            confirmed = new_streak >= patience and not stop and stop_rule != 'engineering'
             if track:
                 e_under = eng_ok(W)
                 new_e = e_streak + 1 if e_under else 0
@@ -589,6 +589,8 @@ def run(W, mesh: OracleMesh, inlet, cfg: dict[str, Any], max_steps: int | None =
                     e_start = step
                 if new_e >= e_pat and not e_stop:
                     e_stop, e_stopping = True, e_start
+                    if stop_rule == 'engineering' and not stop:
+                        confirmed, streak_start = True, e_start
                 e_streak = new_e
             if confirmed:
                 stop = True

@@ -215,3 +215,26 @@ def test_diamond_shock_expansion_validation(diamond_hr):
     assert abs(beta - th.beta_upper_deg) < 0.83, (beta, th.beta_upper_deg)
     assert abs(r32['cd'] - r64['cd']) <= 1e-4 * abs(r64['cd'])
     assert abs(r64['cl']) < 2e-3
+
+
+def test_engineering_stop_rule_matches_oracle(diamond02):
+    """ESR_STOP_ENGINEERING: the case ends when CD/CL stay within tolerance
+    of their targets for `patience` checks; same step as the oracle."""
+    from eulersr_b200.solver import Solver, FlowCase
+    from oracle import euler_oracle as O
+    base = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=2.5, aoa=5.0, case='diamond', CFL=0.6, tf=3.0,
+                stationarity_threshold=1e-12, stationarity_check_every=5, stationarity_patience=3)
+    om = oracle_mesh(diamond02, np.float64)
+    W0, inl = O.initialize(diamond02.n_cells, base)
+    longrun = O.run(W0, om, inl, dict(base), max_steps=600)
+    cd, cl = O.force_coefficients(longrun.W, om, 1.0, 2.5 * math.sqrt(1.4), 1.0)
+    cfg = dict(base, engineering_target_cd=cd, engineering_target_cl=cl, engineering_cd_tol=0.005,
+               engineering_cl_tol=0.005, engineering_patience=3)
+    ro = O.run(W0, om, inl, dict(cfg), stop_rule='engineering')
+    s = Solver(diamond02, 1, precision='f64', stop_rule='engineering', threshold=1e-12, check_every=5, patience=3)
+    s.set_case(0, FlowCase(mach=2.5, aoa_deg=5.0, cfl=0.6, tf=3.0, eng_target_cd=cd, eng_target_cl=cl,
+                           eng_cd_tol=0.005, eng_cl_tol=0.005, eng_patience=3))
+    r = s.run()[0]
+    assert ro.converged and bool(r['converged'])
+    assert r['stopping_step'] == ro.stopping_step == ro.eng_stopping_step
+    assert rel_err(s.get_state(0), ro.W) <= 1e-10
