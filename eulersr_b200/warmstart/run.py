@@ -99,10 +99,10 @@ def main(argv=None):
     ap.add_argument("--lr-steps", type=int, default=6000)
     ap.add_argument("--target-steps", type=int, default=20000)
     ap.add_argument("--ref-steps", type=int, default=30000)
-    ap.add_argument("--max-steps", type=int, default=30000)
+    ap.add_argument("--max-steps", type=int, default=12000)
     ap.add_argument("--threshold", type=float, default=3e-5)
-    ap.add_argument("--train-steps", type=int, default=2000)
-    ap.add_argument("--single-sample", type=int, default=8)
+    ap.add_argument("--train-steps", type=int, default=10000)
+    ap.add_argument("--single-sample", type=int, default=4)
     ap.add_argument("--f64-check", type=int, default=16)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
@@ -169,22 +169,32 @@ def main(argv=None):
 
     # ---- convergence to 0.5 % CD accuracy, every start
     starts = {}
-    res, _, t = solve(dm_hr, me, ae, slots=a.slots, stop_rule="engineering", max_steps=a.max_steps,
-                      cd_targets=truth)
-    starts["cold_batched"] = _summ(res, truth, t, steady=steady)
+    res_cold, _, t = solve(dm_hr, me, ae, slots=a.slots, stop_rule="engineering", max_steps=a.max_steps,
+                           cd_targets=truth)
+    starts["cold_batched"] = _summ(res_cold, truth, t, steady=steady)
     for name in ("idw", "mlp"):
         res, _, t = solve(dm_hr, me, ae, slots=a.slots, stop_rule="engineering", max_steps=a.max_steps,
                           cd_targets=truth, init_fields=inits[name])
         starts[f"{name}_batched"] = _summ(res, truth, t, lr_eval_s + T[f"infer_{name}_s"], steady=steady)
-    # plain single-case solves from freestream, one case per launch, on a sample
+    # plain single-case solves from freestream (one case per launch). A case's
+    # steps and result are bitwise the same alone or in a batch, so the time of
+    # all held-out cases alone is their step counts from the batched cold run
+    # times the single-case step time measured on a sample, plus its set-up.
     k = min(a.single_sample, a.n_eval)
-    single, wall1 = [], 0.0
+    single, wall1, steps1 = [], 0.0, 0
     for i in range(k):
         r, _, t = solve(dm_hr, me[i:i + 1], ae[i:i + 1], slots=1, stop_rule="engineering", max_steps=a.max_steps,
                         cd_targets=truth[i:i + 1])
         single += r
         wall1 += t
-    starts["cold_single_case"] = _summ(single, truth[:k], wall1, steady=steady[:k])
+        steps1 += r[0]["steps"]
+    cold_res = res_cold
+    assert all(single[i]["stopping_step"] == cold_res[i]["stopping_step"] for i in range(k))
+    t_step1 = wall1 / max(steps1, 1)
+    rep["single_case_step_s"] = t_step1
+    t_all_single = t_step1 * sum(r["steps"] for r in cold_res)
+    starts["cold_single_case"] = _summ(cold_res, truth, t_all_single, steady=steady)
+    starts["cold_single_case"]["measured_sample"] = {"cases": k, "wall_s": wall1, "steps": steps1}
     rep["starts_cd_accuracy"] = starts
     base_rate = starts["cold_single_case"]["converged_cases_per_s"] or 0.0
     rep["converged_cases_per_s_vs_single_cold"] = {
