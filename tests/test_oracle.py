@@ -161,3 +161,17 @@ def test_idw_weights_normalised():
     idx = rng.integers(0, 40, (50, 6))
     out = O.idw_predict(src, idx, d)
     assert out.shape == (50, 4) and out.dtype == np.float32
+
+
+def test_c_port_matches_numpy_oracle(diamond02):
+    """The multi-threaded C restatement (CPU baseline) agrees with the NumPy oracle."""
+    from oracle.cport import CpuCase
+    cc = CpuCase(diamond02, 2.5, 5.0, np.float64)
+    Wc = cc.srk2(cc.W0, 20)
+    om = cc.om
+    W = cc.W0
+    for _ in range(20):
+        W = O.time_step_srk2(W, om, cc.dt, cc.inlet)
+    assert rel_err(Wc, W) <= 1e-12
+    c32 = CpuCase(diamond02, 2.5, 5.0, np.float32)
+    assert rel_err(c32.srk2(c32.W0, 20), W) <= 1e-5
