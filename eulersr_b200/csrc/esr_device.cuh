@@ -680,6 +680,180 @@ __global__ void k_dt_finish(const int* __restrict__ fill, int n_slots, const dou
   cc.t_start[g] = globaltimer();
 }
 
+// ------------------------------------------------- device-side case queue
+// A batch of cases is uploaded once; every chunk of steps ends with a refill
+// sequence inside the same CUDA graph: slots whose case stopped write the
+// case's result record (and final state), then each mesh's free slots take
+// the next queued cases of that mesh in slot order, their state is set from
+// the freestream or an uploaded warm start, and dt, N and the step-0
+// engineering state are computed. The host only polls the done counter.
+template <typename T>
+struct Queue {
+  int n_meshes;
+  const int* qlist;            // case ids grouped by mesh, in submission order
+  const int* qoff;             // n_meshes + 1 offsets into qlist
+  int* qhead;                  // per mesh: next queue position
+  int* slot_case;              // per slot: running case id or -1
+  int* retiring;               // per slot scratch flag
+  // per case parameters
+  const V4<T>* c_inlet;
+  const T* c_strength;
+  const double* c_cfl;
+  const double* c_tf;
+  const long long* c_max_steps;
+  const double* c_qref;
+  const int* c_eng_track;
+  const int* c_eng_pat;
+  const double4* c_eng_t;
+  const double* init;          // warm-start rows (caller cell order), or null
+  const long long* init_off;   // per case first row in `init`, -1 = freestream
+  // per case results
+  int* r_status;
+  int* r_stop;
+  int* r_steps;
+  int* r_nmax;
+  double* r_dt;
+  double* r_rel;
+  double* r_cd;
+  double* r_cl;
+  double* r_time;
+  int* r_eng_conv;
+  int* r_eng_stop;
+  double* out;                 // final states (caller order) or null
+  const long long* out_off;    // per case first row in `out`
+  int* n_done;
+};
+
+// per-slot writable parameters that the queue fills
+template <typename T>
+struct SlotParams {
+  T* dt;
+  V4<T>* inlet;
+  T* strength;
+  double* cfl;
+  double* tf;
+  long long* max_steps;
+  double* qref;
+  int* eng_track;
+  int* eng_pat;
+  double4* eng_t;
+};
+
+static __global__ void k_mark_retiring(const int* __restrict__ status, int n_slots, int* __restrict__ slot_case,
+                                       int* __restrict__ retiring) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots) return;
+  retiring[g] = (slot_case[g] >= 0 && status[g] >= 2) ? 1 : 0;
+}
+
+// result record of every retiring slot's case (forces already computed)
+template <typename T>
+__global__ void k_retire(CaseCtl cc, Queue<T> q, const T* __restrict__ dt, const double* __restrict__ forces,
+                         int n_slots, int local_mode) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !q.retiring[g]) return;
+  const int c = q.slot_case[g];
+  const int st = cc.status[g];
+  q.r_status[c] = st;
+  q.r_stop[c] = cc.stopping_step[g];
+  q.r_steps[c] = cc.step[g];
+  q.r_nmax[c] = cc.nmax[g];
+  q.r_dt[c] = local_mode ? 0.0 : (double)dt[g];
+  q.r_rel[c] = cc.last_rel[g];
+  q.r_cd[c] = forces[2 * g];
+  q.r_cl[c] = forces[2 * g + 1];
+  q.r_time[c] = (cc.t_end[g] > cc.t_start[g]) ? (double)(cc.t_end[g] - cc.t_start[g]) * 1e-9 : 0.0;
+  const int tr = cc.eng_track[g];
+  q.r_eng_conv[c] = tr ? cc.eng_stop[g] : 0;
+  q.r_eng_stop[c] = tr ? (cc.eng_stop[g] ? cc.eng_stopping[g] : cc.nmax[g]) : 0;
+  atomicAdd(q.n_done, 1);   // a counter only; no result depends on its order
+}
+
+// final state of retiring slots into the output rows (caller cell order)
+template <typename T>
+__global__ void k_retire_states(const Seg<T>* __restrict__ segs, CaseMap cm, Queue<T> q, const V4<T>* __restrict__ W,
+                                const int* __restrict__ const* inv_of_seg) {
+  const int g = blockIdx.y;
+  if (!q.retiring[g] || q.out == nullptr) return;
+  const Seg<T> s = segs[cm.seg[g]];
+  const int b = cm.slot[g];
+  const int* inv = inv_of_seg[cm.seg[g]];
+  const long long base = q.out_off[q.slot_case[g]];
+  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < s.n_cells; cc += gridDim.x * blockDim.x) {
+    const V4<T> w = W[s.off + (long long)inv[cc] * s.B + b];
+    double* r = q.out + 4 * (base + cc);
+    r[0] = (double)w.x; r[1] = (double)w.y; r[2] = (double)w.z; r[3] = (double)w.w;
+  }
+}
+
+// one thread per mesh: free slots take the next queued cases, in slot order
+template <typename T>
+__global__ void k_assign(const Seg<T>* __restrict__ segs, int n_segs, Queue<T> q, SlotParams<T> sp, CaseCtl cc,
+                         int* __restrict__ fill) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n_segs) return;
+  const Seg<T> s = segs[m];
+  for (int b = 0; b < s.B; ++b) {
+    const int g = s.case0 + b;
+    fill[g] = 0;
+    if (q.slot_case[g] >= 0 && !q.retiring[g]) continue;   // still running
+    q.retiring[g] = 0;
+    if (q.qhead[m] >= q.qoff[m + 1] - q.qoff[m]) {
+      q.slot_case[g] = -1;
+      cc.active[g] = 0;
+      cc.status[g] = 0;
+      continue;
+    }
+    const int c = q.qlist[q.qoff[m] + q.qhead[m]];
+    q.qhead[m] += 1;
+    q.slot_case[g] = c;
+    fill[g] = 1;
+    sp.inlet[g] = q.c_inlet[c];
+    sp.strength[g] = q.c_strength[c];
+    sp.cfl[g] = q.c_cfl[c];
+    sp.tf[g] = q.c_tf[c];
+    sp.max_steps[g] = q.c_max_steps[c];
+    sp.qref[g] = q.c_qref[c];
+    sp.eng_track[g] = q.c_eng_track[c];
+    sp.eng_pat[g] = q.c_eng_pat[c];
+    sp.eng_t[g] = q.c_eng_t[c];
+    cc.step[g] = 0;
+    cc.ref_step[g] = 0;
+    cc.streak[g] = 0;
+    cc.streak_start[g] = 0;
+    cc.stopping_step[g] = 0;
+    cc.due[g] = 0;
+    cc.status[g] = 1;
+    cc.active[g] = 1;
+    cc.last_rel[g] = INFINITY;
+  }
+}
+
+// initial state of the slots just filled: warm-start rows or freestream
+template <typename T>
+__global__ void k_fill_slots(const Seg<T>* __restrict__ segs, CaseMap cm, Queue<T> q, const int* __restrict__ fill,
+                             const int* __restrict__ const* perm_of_seg, V4<T>* __restrict__ W,
+                             V4<T>* __restrict__ Wref) {
+  const int g = blockIdx.y;
+  if (!fill[g]) return;
+  const Seg<T> s = segs[cm.seg[g]];
+  const int b = cm.slot[g];
+  const int c = q.slot_case[g];
+  const long long off = (q.init != nullptr) ? q.init_off[c] : -1;
+  const int* perm = perm_of_seg[cm.seg[g]];
+  const V4<T> inl = q.c_inlet[c];
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < s.n_cells; cell += gridDim.x * blockDim.x) {
+    V4<T> w = inl;
+    if (off >= 0) {
+      const double* r = q.init + 4 * (off + perm[cell]);
+      w = mk4<T>((T)r[0], (T)r[1], (T)r[2], (T)r[3]);
+    }
+    const long long gi = s.off + (long long)cell * s.B + b;
+    W[gi] = w;
+    Wref[gi] = w;
+  }
+}
+
 // pressure force coefficients of every live-or-finished slot
 // (helper.py:366-415): sum_w p(cell_w) n_w ds_w / (q_inf L_ref), p at gamma 1.4
 template <typename T>

@@ -796,67 +796,244 @@ struct SolverT : SolverBase {
   }
 
   // ------------------------------------------- batch with retire / refill
+  // Per-case slot parameters (the same values set_case uploads for one slot).
+  void case_params(const esr_case& c, V& in, T& str, double& q, double4& et, int& etrack, int& epat) {
+    const HostMesh& hm = *meshes[c.mesh]->hm;
+    in = mk4<T>((T)c.inlet[0], (T)c.inlet[1], (T)c.inlet[2], (T)c.inlet[3]);
+    const T r = in.x, u = in.y / r, v = in.z / r;
+    const T p = (in.w - kc.half * r * (u * u + v * v)) * kc.gm1;
+    const T U = std::sqrt(u * u + v * v), a = std::sqrt(kc.gamma * p / r);
+    const T Ly = (T)hm.y_max - (T)hm.y_min;
+    str = (T)1.0 * (U + a) / ((T)0.2 * Ly);
+    if (!(std::isfinite((double)str))) str = T(0);
+    const double qq = 0.5 * c.rho_inf * c.u_inf * c.u_inf * c.l_ref;
+    q = qq > 0 ? qq : 1.0;
+    etrack = c.eng_track ? 1 : 0;
+    epat = std::max(1, c.eng_patience > 0 ? c.eng_patience : P.patience);
+    et = make_double4(c.eng_target_cd, c.eng_target_cl, c.eng_cd_tol * std::max(std::fabs(c.eng_target_cd), 1e-8),
+                      c.eng_cl_tol * std::max(std::fabs(c.eng_target_cl), 1e-8));
+  }
+
+  // The queue lives on the device: every captured chunk of steps ends with
+  // the refill sequence (retire -> assign -> fill -> dt), so the host only
+  // polls the done counter.
+  struct BatchBufs {
+    DevBuf<int> qlist, qoff, qhead, slot_case, retiring, c_eng_track, c_eng_pat, r_status, r_stop, r_steps, r_nmax,
+        r_eng_conv, r_eng_stop, n_done;
+    DevBuf<V> c_inlet;
+    DevBuf<T> c_strength;
+    DevBuf<double> c_cfl, c_tf, c_qref, r_dt, r_rel, r_cd, r_cl, r_time, init, out;
+    DevBuf<long long> c_max_steps, init_off, out_off;
+    DevBuf<double4> c_eng_t;
+  };
+  DevBuf<int> perm_all;
+  DevBuf<const int*> perm_ptrs, inv_ptrs;
+
+  void issue_refill(const Queue<T>& q, const SlotParams<T>& sp, bool with_states) {
+    const int tb = 128, nb = (n_slots + tb - 1) / tb;
+    k_mark_retiring<<<nb, tb, 0, stream>>>(status.p, n_slots, q.slot_case, q.retiring);
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, q.retiring, nullptr);
+    k_retire<T><<<nb, tb, 0, stream>>>(ctl(), q, dt.p, forces.p, n_slots, P.dt_mode == ESR_DT_LOCAL);
+    int max_cells = 0;
+    for (auto& md : meshes) max_cells = std::max(max_cells, md->hm->n_cells);
+    dim3 g2(std::min(64, (max_cells + 255) / 256), n_slots);
+    if (with_states) k_retire_states<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), q, W.p, inv_ptrs.p);
+    k_assign<T><<<(int)(meshes.size() + 31) / 32, 32, 0, stream>>>(d_segs.p, (int)meshes.size(), q, sp, ctl(), fill.p);
+    k_fill_slots<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), q, fill.p, perm_ptrs.p, W.p, Wref.p);
+    dim3 grid(n_chunks, n_slots);
+    k_case_reduce<T, RED_DTMIN><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, fill.p, kReduceCells,
+                                                                     partial.p, n_chunks, kc);
+    k_dt_finish<T><<<nb, tb, 0, stream>>>(fill.p, n_slots, partial.p, n_chunks, cfl.p, tf.p, max_steps.p, dt.p, ctl(),
+                                          P.dt_mode == ESR_DT_LOCAL);
+    k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, fill.p, eng_track.p);
+    k_eng_init<<<nb, tb, 0, stream>>>(ctl(), fill.p, n_slots);
+    launches += with_states ? 10 : 9;
+  }
+
   int batch(const esr_case* cs, int n, const double* const* init, double* const* finals, esr_result* out) {
+    const int nm = (int)meshes.size();
     for (int i = 0; i < n; ++i) {
-      if (cs[i].mesh < 0 || cs[i].mesh >= (int)meshes.size()) return fail(ESR_ERR_ARG, "batch: case mesh out of range");
+      if (cs[i].mesh < 0 || cs[i].mesh >= nm) return fail(ESR_ERR_ARG, "batch: case mesh out of range");
+      if (meshes[cs[i].mesh]->B < 1) return fail(ESR_ERR_ARG, "batch: case mesh has no slots");
+      if (!(cs[i].cfl > 0)) return fail(ESR_ERR_ARG, "batch: cfl must be > 0");
+      if (!(cs[i].tf > 0) && cs[i].max_steps <= 0) return fail(ESR_ERR_ARG, "batch: tf must be > 0");
       out[i] = esr_result{};
       out[i].case_index = i;
     }
-    // per-mesh queues
-    std::vector<std::vector<int>> queue(meshes.size());
-    for (int i = n - 1; i >= 0; --i) queue[cs[i].mesh].push_back(i);
-    for (int g = 0; g < n_slots; ++g) ESR_TRY(clear_slot(g));
-    ESR_CUDA(cudaEventRecord(ev0, stream));
-    auto refill = [&](int g) -> int {
-      int m, b;
-      ESR_TRY(mesh_of_slot(g, m, b));
-      if (queue[m].empty()) return ESR_OK;
-      const int i = queue[m].back();
-      queue[m].pop_back();
-      ESR_TRY(set_case(g, &cs[i], init ? init[i] : nullptr, true));
-      hcase_index[g] = i;
+    if (n == 0) return ESR_OK;
+    // device copies of the renumbering, once per solver
+    if (!perm_ptrs.p) {
+      size_t tot = 0;
+      for (auto& md : meshes) tot += md->hm->n_cells;
+      ESR_TRY(perm_all.alloc(tot));
+      std::vector<const int*> pp(nm), ip(nm);
+      size_t o = 0;
+      for (int m = 0; m < nm; ++m) {
+        const HostMesh& hm = *meshes[m]->hm;
+        ESR_CUDA(cudaMemcpy(perm_all.p + o, hm.perm.data(), hm.n_cells * sizeof(int), cudaMemcpyHostToDevice));
+        pp[m] = perm_all.p + o;
+        ip[m] = meshes[m]->inv.p;
+        o += hm.n_cells;
+      }
+      ESR_TRY(perm_ptrs.alloc(nm));
+      ESR_TRY(inv_ptrs.alloc(nm));
+      ESR_CUDA(cudaMemcpy(perm_ptrs.p, pp.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
+      ESR_CUDA(cudaMemcpy(inv_ptrs.p, ip.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
+    }
+    BatchBufs B;
+    // queue: cases grouped by mesh, submission order inside a mesh
+    std::vector<int> qlist, qoff(nm + 1, 0);
+    for (int m = 0; m < nm; ++m) {
+      qoff[m] = (int)qlist.size();
+      for (int i = 0; i < n; ++i) if (cs[i].mesh == m) qlist.push_back(i);
+    }
+    qoff[nm] = (int)qlist.size();
+    std::vector<V> hin(n);
+    std::vector<T> hstr(n);
+    std::vector<double> hcfl(n), htf(n), hq(n);
+    std::vector<long long> hms(n), hinit_off(n, -1), hout_off(n, 0);
+    std::vector<int> htr(n), hpat(n);
+    std::vector<double4> het(n);
+    long long init_rows = 0, out_rows = 0;
+    for (int i = 0; i < n; ++i) {
+      case_params(cs[i], hin[i], hstr[i], hq[i], het[i], htr[i], hpat[i]);
+      hcfl[i] = cs[i].cfl;
+      htf[i] = cs[i].tf;
+      hms[i] = cs[i].max_steps;
+      const int N = meshes[cs[i].mesh]->hm->n_cells;
+      if (init && init[i]) { hinit_off[i] = init_rows; init_rows += N; }
+      hout_off[i] = out_rows;
+      out_rows += N;
+    }
+    const bool want_states = finals != nullptr;
+    auto up = [&](auto& buf, const auto& v) -> int {
+      using E = typename std::decay_t<decltype(v)>::value_type;
+      ESR_TRY(buf.alloc(std::max<size_t>(v.size(), 1)));
+      if (!v.empty()) ESR_CUDA(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice, stream));
       return ESR_OK;
     };
-    for (int g = 0; g < n_slots; ++g) ESR_TRY(refill(g));
-    ESR_TRY(flush_fills());
-    std::vector<esr_result> slot_res(n_slots);
-    int remaining = n;
-    int poll = 2;
-    while (remaining > 0) {
-      for (int i = 0; i < poll; ++i) ESR_TRY(launch_run_chunk());
-      int live = 0;
-      std::vector<int> st;
-      ESR_TRY(any_active(live, &st));
-      bool harvest = false;
-      for (int g = 0; g < n_slots; ++g) if (hcase_index[g] >= 0 && st[g] >= ESR_CASE_CONVERGED) harvest = true;
-      if (harvest) {
-        ESR_TRY(results(slot_res.data()));
-        for (int g = 0; g < n_slots; ++g) {
-          if (hcase_index[g] < 0 || st[g] < ESR_CASE_CONVERGED) continue;
-          const int i = hcase_index[g];
-          out[i] = slot_res[g];
-          out[i].case_index = i;
-          if (finals && finals[i]) ESR_TRY(get_state(g, finals[i], false));
-          hcase_index[g] = -1;
-          --remaining;
-          ESR_TRY(refill(g));
-        }
-        ESR_TRY(flush_fills());
-        poll = 2;
-      } else {
-        poll = std::min(poll * 2, 16);
-      }
-      if (live == 0 && remaining > 0) {
-        bool any_filled = false;
-        for (int g = 0; g < n_slots; ++g) any_filled |= hcase_index[g] >= 0;
-        if (!any_filled) return fail(ESR_ERR_STATE, "batch: queue stalled");
-      }
+    ESR_TRY(up(B.qlist, qlist));
+    ESR_TRY(up(B.qoff, qoff));
+    ESR_TRY(up(B.c_inlet, hin));
+    ESR_TRY(up(B.c_strength, hstr));
+    ESR_TRY(up(B.c_cfl, hcfl));
+    ESR_TRY(up(B.c_tf, htf));
+    ESR_TRY(up(B.c_qref, hq));
+    ESR_TRY(up(B.c_max_steps, hms));
+    ESR_TRY(up(B.c_eng_track, htr));
+    ESR_TRY(up(B.c_eng_pat, hpat));
+    ESR_TRY(up(B.c_eng_t, het));
+    ESR_TRY(up(B.init_off, hinit_off));
+    ESR_TRY(up(B.out_off, hout_off));
+    for (DevBuf<int>* b : {&B.qhead, &B.n_done}) {
+      ESR_TRY(b->alloc(std::max(nm, 1)));
+      ESR_CUDA(cudaMemsetAsync(b->p, 0, std::max(nm, 1) * sizeof(int), stream));
     }
+    ESR_TRY(B.slot_case.alloc(n_slots));
+    ESR_TRY(B.retiring.alloc(n_slots));
+    std::vector<int> minus(n_slots, -1);
+    ESR_CUDA(cudaMemcpyAsync(B.slot_case.p, minus.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemsetAsync(B.retiring.p, 0, n_slots * sizeof(int), stream));
+    ESR_CUDA(cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream));
+    ESR_CUDA(cudaMemsetAsync(status.p, 0, n_slots * sizeof(int), stream));
+    for (DevBuf<int>* b : {&B.r_status, &B.r_stop, &B.r_steps, &B.r_nmax, &B.r_eng_conv, &B.r_eng_stop})
+      ESR_TRY(b->alloc(n));
+    for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time}) ESR_TRY(b->alloc(n));
+    if (init_rows > 0) {
+      ESR_TRY(B.init.alloc((size_t)4 * init_rows));
+      for (int i = 0; i < n; ++i)
+        if (init && init[i])
+          ESR_CUDA(cudaMemcpyAsync(B.init.p + 4 * hinit_off[i], init[i],
+                                   (size_t)4 * meshes[cs[i].mesh]->hm->n_cells * sizeof(double),
+                                   cudaMemcpyHostToDevice, stream));
+    }
+    if (want_states) ESR_TRY(B.out.alloc((size_t)4 * out_rows));
+    ESR_CUDA(cudaStreamSynchronize(stream));   // host vectors above are the copy sources
+    Queue<T> q{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
+               B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p,
+               init_rows > 0 ? B.init.p : nullptr, B.init_off.p, B.r_status.p, B.r_stop.p, B.r_steps.p, B.r_nmax.p,
+               B.r_dt.p, B.r_rel.p, B.r_cd.p, B.r_cl.p, B.r_time.p, B.r_eng_conv.p, B.r_eng_stop.p,
+               want_states ? B.out.p : nullptr, B.out_off.p, B.n_done.p};
+    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p};
+    ESR_CUDA(cudaEventRecord(ev0, stream));
+    issue_refill(q, sp, want_states);   // first fill of every slot
+    // the chunk graph of this batch: steps, checks, then the refill sequence
+    cudaGraphExec_t gexec = nullptr;
+    const int len = run_chunk_len();
+    if (P.use_graphs) {
+      cudaGraph_t graph = nullptr;
+      ESR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      const int64_t before = launches;
+      issue_run_chunk(len);
+      issue_refill(q, sp, want_states);
+      launches = before;
+      ESR_CUDA(cudaStreamEndCapture(stream, &graph));
+      cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    const int64_t per_chunk = chunk_launches(true, len) + (want_states ? 10 : 9);
+    int done = 0, poll = 4;
+    int rc = ESR_OK;
+    for (long long guard = 0; done < n; ++guard) {
+      for (int i = 0; i < poll; ++i) {
+        if (gexec) {
+          cudaError_t e = cudaGraphLaunch(gexec, stream);
+          if (e != cudaSuccess) { rc = fail(ESR_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
+          launches += per_chunk;
+        } else {
+          issue_run_chunk(len);
+          issue_refill(q, sp, want_states);
+        }
+      }
+      if (rc != ESR_OK) break;
+      cudaError_t e = cudaMemcpyAsync(&done, B.n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) { rc = fail(ESR_ERR_CUDA, std::string("batch poll: ") + cudaGetErrorString(e)); break; }
+      poll = std::min(poll * 2, 32);
+      if (guard > (1LL << 40)) { rc = fail(ESR_ERR_STATE, "batch: no progress"); break; }
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (rc != ESR_OK) return rc;
     ESR_CUDA(cudaEventRecord(ev1, stream));
-    ESR_CUDA(cudaEventSynchronize(ev1));
+    std::vector<int> st(n), sstop(n), ssteps(n), snmax(n), sec(n), ses(n);
+    std::vector<double> sdt(n), srel(n), scd(n), scl(n), stime(n);
+    auto down = [&](auto& v, const auto& buf) -> int {
+      using E = typename std::decay_t<decltype(v)>::value_type;
+      ESR_CUDA(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(E), cudaMemcpyDeviceToHost, stream));
+      return ESR_OK;
+    };
+    ESR_TRY(down(st, B.r_status)); ESR_TRY(down(sstop, B.r_stop)); ESR_TRY(down(ssteps, B.r_steps));
+    ESR_TRY(down(snmax, B.r_nmax)); ESR_TRY(down(sec, B.r_eng_conv)); ESR_TRY(down(ses, B.r_eng_stop));
+    ESR_TRY(down(sdt, B.r_dt)); ESR_TRY(down(srel, B.r_rel)); ESR_TRY(down(scd, B.r_cd)); ESR_TRY(down(scl, B.r_cl));
+    ESR_TRY(down(stime, B.r_time));
+    if (want_states)
+      for (int i = 0; i < n; ++i)
+        if (finals[i])
+          ESR_CUDA(cudaMemcpyAsync(finals[i], B.out.p + 4 * hout_off[i],
+                                   (size_t)4 * meshes[cs[i].mesh]->hm->n_cells * sizeof(double),
+                                   cudaMemcpyDeviceToHost, stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    for (int i = 0; i < n; ++i) {
+      esr_result& r = out[i];
+      r.status = st[i];
+      r.converged = st[i] == ESR_CASE_CONVERGED;
+      r.stopping_step = sstop[i];
+      r.steps = ssteps[i];
+      r.n_max = snmax[i];
+      r.case_index = i;
+      r.dt = sdt[i];
+      r.last_rel = srel[i];
+      r.cd = scd[i];
+      r.cl = scl[i];
+      r.solve_time_s = stime[i];
+      r.eng_converged = sec[i];
+      r.eng_stopping_step = ses[i];
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     last_ms = ms;
+    for (int g = 0; g < n_slots; ++g) hcase_index[g] = -1;
     return ESR_OK;
   }
 };

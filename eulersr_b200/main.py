@@ -170,9 +170,9 @@ def run(W, mesh, inlet, cfg, out_dirs):
     return W
 
 
-def export_snapshot(W, mesh: Mesh, s: Solver, t, cfg, out_dirs):
+def export_snapshot(W, mesh: Mesh, s: Solver, t, cfg, out_dirs, slot: int = 0):
     """euler/utils.py:21-69: .npy state and the bundle .npz (primitives, LSQ
-    primitive gradients from the device, Mach)."""
+    primitive gradients of solver slot ``slot`` from the device, Mach)."""
     exp, gamma = cfg["export"], cfg["gamma"]
     name = format_snapshot_name(cfg, t)
     res = Path(out_dirs["res"])
@@ -181,7 +181,7 @@ def export_snapshot(W, mesh: Mesh, s: Solver, t, cfg, out_dirs):
         np.save(res / f"{name}.npy", np.asarray(W))
     if exp.get("bundle", True):
         prims = _primitive(np.asarray(W, np.float64), gamma)
-        grad = s.gradients(0)
+        grad = s.gradients(slot)
         mach = np.sqrt(prims[:, 1] ** 2 + prims[:, 2] ** 2) / np.sqrt(gamma * prims[:, 3] / prims[:, 0])
         path = res / f"{name}.npz"
         if cfg.get("verbose", True):

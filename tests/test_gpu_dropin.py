@@ -238,3 +238,31 @@ def test_engineering_stop_rule_matches_oracle(diamond02):
     assert ro.converged and bool(r['converged'])
     assert r['stopping_step'] == ro.stopping_step == ro.eng_stopping_step
     assert rel_err(s.get_state(0), ro.W) <= 1e-10
+
+
+def test_grid_batch_matches_single_runs(diamond02, tmp_path, capsys):
+    """slurm/run_euler_grid.py on the batched solver: every case's summary,
+    bundle and returned state equal those of main.run for the same case
+    (two slots for five cases, so slots are refilled on the device)."""
+    from eulersr_b200 import grid as G
+    from eulersr_b200 import main as M
+    cfg = _cfg(precision='f32', tf=1.0, stationarity_threshold=5e-4, stationarity_check_every=10)
+    grid = [(1.5, -2.0), (1.5, 2.0), (2.5, 0.0), (0.9, 1.0), (3.0, 4.0)]
+    recs = G.run_grid(cfg, diamond02, grid, slots=2, out_root=tmp_path / 'batch')
+    capsys.readouterr()
+    assert len(recs) == len(grid)
+    for (mach, aoa), rec in zip(grid, recs):
+        c = G.build_case_cfg(cfg, 'diamond', mach, aoa)
+        W0, inlet = M.initialize(diamond02, c)
+        dirs = {'fig': tmp_path / 'f', 'res': tmp_path / 'single' / f'{mach}_{aoa}'}
+        W = M.run(W0, diamond02, inlet, c, dirs)
+        assert np.array_equal(W, rec['W'])
+        one = json.loads(next(dirs['res'].glob('summary_*.json')).read_text())
+        tag = f"AOA{aoa:.2f}"
+        batch = json.loads(next((tmp_path / 'batch').rglob(f'{tag}/summary_AOA{aoa:.2f}_M{mach:.2f}_*.json')).read_text())
+        for k in ('cd', 'cl', 'converged', 'stopping_step', 'stationarity_rel', 'deltaS', 'mach', 'aoa', 'n_cells'):
+            assert one[k] == batch[k], (mach, aoa, k, one[k], batch[k])
+        b1 = np.load(next(dirs['res'].glob('*.npz')))
+        b2 = np.load(next((tmp_path / 'batch').rglob(f'{tag}/AOA{aoa:.2f}_M{mach:.2f}_*.npz')))
+        for k in ('conservatives', 'primitives', 'primitives_grad', 'mach', 'time'):
+            assert np.array_equal(b1[k], b2[k]), k

@@ -142,19 +142,40 @@ def test_maxstep_cap(diamond02):
     assert r['steps'] == r['n_max'] == int(np.float32(0.05) / np.float32(r['dt'])) + 1
 
 
-def test_batch_equals_single(diamond02, naca02):
-    """A case solved inside a ragged two-mesh batch with retire/refill is
-    bitwise identical to the same case solved alone."""
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_batch_equals_single(diamond02, naca02, precision):
+    """Every case solved inside a ragged two-mesh batch, with the queue
+    retiring and refilling slots on the device, is bitwise identical to the
+    same case solved alone: state, stop step, status and force coefficients.
+    Case 4 starts from a warm field and case 1 tracks the engineering rule."""
     from eulersr_b200.solver import Solver, FlowCase
-    cases = [FlowCase(mach=m, aoa_deg=a, mesh=i % 2, cfl=0.6, tf=0.4)
-             for i, (m, a) in enumerate([(2.5, 5.0), (1.5, -2.0), (3.0, 1.0), (0.9, 0.5), (2.0, 0.0)])]
-    s = Solver([diamond02, naca02], [2, 1], precision='f32', threshold=1e-5, check_every=10)
-    res, states = s.batch_solve(cases, want_states=True)
-    for i in (0, 3):
-        c = cases[i]
-        one = Solver([diamond02, naca02][c.mesh], 1, precision='f32', threshold=1e-5, check_every=10)
-        one.set_case(0, FlowCase(mach=c.mach, aoa_deg=c.aoa_deg, cfl=0.6, tf=0.4))
+    dt_ = np.float32 if precision == 'f32' else np.float64
+    meshes = [diamond02, naca02]
+    spec = [(2.5, 5.0), (1.5, -2.0), (3.0, 1.0), (0.9, 0.5), (2.0, 0.0), (2.2, 3.0), (1.8, -1.0)]
+    cases = [FlowCase(mach=m, aoa_deg=a, mesh=i % 2, cfl=0.6, tf=0.4, dtype=dt_) for i, (m, a) in enumerate(spec)]
+    eng = dict(eng_target_cd=0.05, eng_target_cl=0.1, eng_cd_tol=0.5, eng_cl_tol=100.0, eng_patience=2)
+    for k, v in eng.items():
+        setattr(cases[1], k, v)
+    warm = Solver(diamond02, 1, precision=precision)
+    warm.set_case(0, FlowCase(mach=2.0, aoa_deg=0.0, cfl=0.6, tf=0.4, dtype=dt_))
+    warm.step(30)
+    init = [None] * len(cases)
+    init[4] = warm.get_state(0)
+    s = Solver(meshes, [2, 1], precision=precision, threshold=1e-5, check_every=10)
+    res, states = s.batch_solve(cases, init_fields=init, want_states=True)
+    assert sorted(r['case_index'] for r in res) == list(range(len(cases)))
+    for i, c in enumerate(cases):
+        one = Solver(meshes[c.mesh], 1, precision=precision, threshold=1e-5, check_every=10)
+        c1 = FlowCase(mach=c.mach, aoa_deg=c.aoa_deg, cfl=0.6, tf=0.4, dtype=dt_)
+        if i == 1:
+            for k, v in eng.items():
+                setattr(c1, k, v)
+        one.set_case(0, c1, init[i])
         r1 = one.run()[0]
-        assert r1['stopping_step'] == res[i]['stopping_step']
-        assert r1['status'] == res[i]['status']
-        assert np.array_equal(one.get_state(0), states[i])
+        for k in ('stopping_step', 'status', 'steps', 'n_max', 'cd', 'cl', 'eng_converged', 'eng_stopping_step'):
+            assert r1[k] == res[i][k], (i, k, r1[k], res[i][k])
+        assert np.array_equal(one.get_state(0), states[i]), i
+    # the same batch again on the same handle gives the same answer
+    res2, states2 = s.batch_solve(cases, init_fields=init, want_states=True)
+    assert all(np.array_equal(a, b) for a, b in zip(states, states2))
+    assert [r['stopping_step'] for r in res] == [r['stopping_step'] for r in res2]
