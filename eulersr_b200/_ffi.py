@@ -63,7 +63,7 @@ class Result(C.Structure):
     _fields_ = [("status", C.c_int32), ("converged", C.c_int32), ("stopping_step", C.c_int32),
                 ("steps", C.c_int32), ("n_max", C.c_int32), ("case_index", C.c_int32), ("dt", C.c_double),
                 ("last_rel", C.c_double), ("cd", C.c_double), ("cl", C.c_double), ("solve_time_s", C.c_double),
-                ("eng_converged", C.c_int32), ("eng_stopping_step", C.c_int32)]
+                ("eng_converged", C.c_int32), ("eng_stopping_step", C.c_int32), ("final_residual", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -76,6 +76,16 @@ class KernelTimes(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("n_candidates", C.c_int32), ("candidates", C.c_int32 * 4),
+                ("step_ms", C.c_double * 4)]
+
+    def as_dict(self):
+        n = int(self.n_candidates)
+        return {"block_size": int(self.block_size),
+                "step_ms": {int(self.candidates[i]): float(self.step_ms[i]) for i in range(n)}}
 
 
 class EsrError(RuntimeError):
@@ -114,6 +124,7 @@ _SIGS = {
     "esr_last_elapsed_ms": (C.c_int, [C.c_void_p, _f64p]),
     "esr_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "esr_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "esr_solver_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
     "esr_gemm_bf16": (C.c_int, [C.c_int32] * 5 + [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,

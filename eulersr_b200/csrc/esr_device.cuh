@@ -58,6 +58,18 @@ template <typename T> __device__ __forceinline__ T dv(T a, T b) { return a / b; 
 template <> __device__ __forceinline__ float dv<float>(float a, float b) { return __fdividef(a, b); }
 template <typename T> constexpr bool kFast = sizeof(T) == 4;
 
+// Resident 256-thread blocks per SM the float32 cell kernels are compiled for
+// (register caps 65536 / (256 x n)); float64 kernels take what they need.
+#ifndef ESR_K1_MINB
+#define ESR_K1_MINB 5
+#endif
+#ifndef ESR_K1_MINB_LOCAL
+#define ESR_K1_MINB_LOCAL 4
+#endif
+#ifndef ESR_K2_MINB
+#define ESR_K2_MINB 4
+#endif
+
 template <typename T>
 struct Consts {
   T gamma, gm1;              // run gamma and gamma - 1 rounded from double
@@ -156,10 +168,6 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   if (SL == SR) SL = SL - k.ss_eps;
   if (SL == SR) SR = SR + k.ss_eps;
   const T EL = WL.w, ER = WR.w;
-  const T FL0 = rL * unL, FL1 = rL * uL * unL + pL * nx, FL2 = rL * vL * unL + pL * ny, FL3 = (EL + pL) * unL;
-  const T FR0 = rR * unR, FR1 = rR * uR * unR + pR * nx, FR2 = rR * vR * unR + pR * ny, FR3 = (ER + pR) * unR;
-  const T Fc0 = k.half * (FL0 + FR0), Fc1 = k.half * (FL1 + FR1);
-  const T Fc2 = k.half * (FL2 + FR2), Fc3 = k.half * (FL3 + FR3);
   T den = rL * (SL - unL) - rR * (SR - unR);
   if (den == T(0)) den = k.den_eps;
   const T Ss = dv<T>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
@@ -173,23 +181,40 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const bool left = c1 || c2;
   const T rK = left ? rL : rR, unK = left ? unL : unR, SK = left ? SL : SR;
   const T EK = left ? EL : ER, pK = left ? pL : pR, utK = left ? utL : utR;
-  T rs, Us3;
   if constexpr (kFast<T>) {
-    const T inv = __fdividef(1.0f, SK - Ss);
-    rs = rK * (SK - unK) * inv;
-    Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) * inv;
+    // float32: the HLLC flux itself (the central-flux identity F = Fc - (Fc - H)
+    // is exact in real arithmetic) and only the physical flux of the selected side
+    const T uK = left ? uL : uR, vK = left ? vL : vR;
+    const V4<T> WK = left ? WL : WR;
+    const T FK0 = rK * unK, FK1 = rK * uK * unK + pK * nx, FK2 = rK * vK * unK + pK * ny, FK3 = (EK + pK) * unK;
+    if (left ? !c1 : c3) {
+      const T inv = __fdividef(1.0f, SK - Ss);
+      const T rs = rK * (SK - unK) * inv;
+      const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) * inv;
+      const T Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
+      F[0] = FK0 + SK * (rs - WK.x);
+      F[1] = FK1 + SK * (Us1 - WK.y);
+      F[2] = FK2 + SK * (Us2 - WK.z);
+      F[3] = FK3 + SK * (Us3 - WK.w);
+    } else {
+      F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
+    }
   } else {
-    rs = rK * (SK - unK) / (SK - Ss);
-    Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) / (SK - Ss);
+    const T FL0 = rL * unL, FL1 = rL * uL * unL + pL * nx, FL2 = rL * vL * unL + pL * ny, FL3 = (EL + pL) * unL;
+    const T FR0 = rR * unR, FR1 = rR * uR * unR + pR * nx, FR2 = rR * vR * unR + pR * ny, FR3 = (ER + pR) * unR;
+    const T Fc0 = k.half * (FL0 + FR0), Fc1 = k.half * (FL1 + FR1);
+    const T Fc2 = k.half * (FL2 + FR2), Fc3 = k.half * (FL3 + FR3);
+    const T rs = rK * (SK - unK) / (SK - Ss);
+    const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) / (SK - Ss);
+    const T Us0 = rs, Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
+    T H0, H1, H2, H3;
+    if (c1) { H0 = FL0; H1 = FL1; H2 = FL2; H3 = FL3; }
+    else if (c2) { H0 = FL0 + SL * (Us0 - WL.x); H1 = FL1 + SL * (Us1 - WL.y); H2 = FL2 + SL * (Us2 - WL.z); H3 = FL3 + SL * (Us3 - WL.w); }
+    else if (c3) { H0 = FR0 + SR * (Us0 - WR.x); H1 = FR1 + SR * (Us1 - WR.y); H2 = FR2 + SR * (Us2 - WR.z); H3 = FR3 + SR * (Us3 - WR.w); }
+    else { H0 = FR0; H1 = FR1; H2 = FR2; H3 = FR3; }
+    F[0] = Fc0 - (Fc0 - H0); F[1] = Fc1 - (Fc1 - H1);
+    F[2] = Fc2 - (Fc2 - H2); F[3] = Fc3 - (Fc3 - H3);
   }
-  const T Us0 = rs, Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
-  T H0, H1, H2, H3;
-  if (c1) { H0 = FL0; H1 = FL1; H2 = FL2; H3 = FL3; }
-  else if (c2) { H0 = FL0 + SL * (Us0 - WL.x); H1 = FL1 + SL * (Us1 - WL.y); H2 = FL2 + SL * (Us2 - WL.z); H3 = FL3 + SL * (Us3 - WL.w); }
-  else if (c3) { H0 = FR0 + SR * (Us0 - WR.x); H1 = FR1 + SR * (Us1 - WR.y); H2 = FR2 + SR * (Us2 - WR.z); H3 = FR3 + SR * (Us3 - WR.w); }
-  else { H0 = FR0; H1 = FR1; H2 = FR2; H3 = FR3; }
-  F[0] = Fc0 - (Fc0 - H0); F[1] = Fc1 - (Fc1 - H1);
-  F[2] = Fc2 - (Fc2 - H2); F[3] = Fc3 - (Fc3 - H3);
 }
 
 // euler_solver.py:203-240 Rusanov (plain branch) inside getFlux
@@ -219,7 +244,7 @@ __device__ __forceinline__ T geo(const Seg<T>& s, int f, int c) { return __ldg(s
 // With LOCALDT it also writes the per-cell CFL time step of the state.
 // MUSCL=false only computes the local dt (constant reconstruction needs no face states).
 template <typename T, bool MUSCL, bool LOCALDT>
-__global__ void __launch_bounds__(256) k_recon(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_LOCAL : ESR_K1_MINB) : 1) k_recon(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
                                                const V4<T>* __restrict__ W, V4<T>* __restrict__ FV,
                                                long long total, Cases<T> cs, Consts<T> kc, int pos,
                                                T* __restrict__ dt_local) {
@@ -341,7 +366,7 @@ enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
 // euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
 // then the stage update of :630-653.
 template <typename T, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
-__global__ void __launch_bounds__(256) k_flux(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(const Seg<T>* __restrict__ segs, const int2* __restrict__ blk,
                                               const V4<T>* __restrict__ Win, const V4<T>* __restrict__ Wbase,
                                               V4<T>* __restrict__ Wout, const V4<T>* __restrict__ FV,
                                               long long total, Cases<T> cs, Consts<T> kc, int pos,
@@ -719,6 +744,7 @@ struct Queue {
   double* r_time;
   int* r_eng_conv;
   int* r_eng_stop;
+  double* r_probe;             // one-step residual of the final state
   double* out;                 // final states (caller order) or null
   const long long* out_off;    // per case first row in `out`
   int* n_done;
@@ -767,6 +793,20 @@ __global__ void k_retire(CaseCtl cc, Queue<T> q, const T* __restrict__ dt, const
   q.r_eng_conv[c] = tr ? cc.eng_stop[g] : 0;
   q.r_eng_stop[c] = tr ? (cc.eng_stop[g] ? cc.eng_stopping[g] : cc.nmax[g]) : 0;
   atomicAdd(q.n_done, 1);   // a counter only; no result depends on its order
+}
+
+// euler/main.py:228-230 for every retiring slot: ||W' - W|| / (||W|| + 1e-16)
+// from the RED_DIFF partials of its probe step, summed in chunk order
+template <typename T>
+__global__ void k_probe_finish(Queue<T> q, const double2* __restrict__ partial, int n_chunks, int n_slots) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots || !q.retiring[g]) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = 0; i < n_chunks; ++i) {
+    s0 += partial[(size_t)g * n_chunks + i].x;
+    s1 += partial[(size_t)g * n_chunks + i].y;
+  }
+  q.r_probe[q.slot_case[g]] = sqrt(s0) / (sqrt(s1) + 1e-16);
 }
 
 // final state of retiring slots into the output rows (caller cell order)
@@ -854,6 +894,70 @@ __global__ void k_fill_slots(const Seg<T>* __restrict__ segs, CaseMap cm, Queue<
   }
 }
 
+// Once a mesh's queue is empty its running cases are packed into the lowest
+// slots, so that warps over the freed slots (32 slots of one cell) exit at
+// once in the step kernels. One thread per mesh pairs the lowest free slot
+// with the highest running one; move_src[dst] = src, -1 elsewhere.
+template <typename T>
+__global__ void k_compact_plan(const Seg<T>* __restrict__ segs, int n_segs, Queue<T> q, int* __restrict__ move_src) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n_segs) return;
+  const Seg<T> s = segs[m];
+  for (int b = 0; b < s.B; ++b) move_src[s.case0 + b] = -1;
+  if (q.qhead[m] < q.qoff[m + 1] - q.qoff[m]) return;   // cases still queued: no slot is free
+  int lo = 0, hi = s.B - 1;
+  for (;;) {
+    while (lo < hi && q.slot_case[s.case0 + lo] >= 0) ++lo;
+    while (hi > lo && q.slot_case[s.case0 + hi] < 0) --hi;
+    if (lo >= hi) break;
+    move_src[s.case0 + lo] = s.case0 + hi;
+    ++lo;
+    --hi;
+  }
+}
+
+// per-cell state of every moved case (grid: x over cells, y over slots)
+template <typename T>
+__global__ void k_compact_items(const Seg<T>* __restrict__ segs, CaseMap cm, const int* __restrict__ move_src,
+                                V4<T>* __restrict__ W, V4<T>* __restrict__ Wref) {
+  const int g = blockIdx.y;
+  const int src = move_src[g];
+  if (src < 0) return;
+  const Seg<T> s = segs[cm.seg[g]];
+  const int bd = cm.slot[g], bs = cm.slot[src];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < s.n_cells; c += gridDim.x * blockDim.x) {
+    const long long d = s.off + (long long)c * s.B + bd, o = s.off + (long long)c * s.B + bs;
+    W[d] = W[o];
+    Wref[d] = Wref[o];
+  }
+}
+
+// per-slot words of every moved case; the source slot is left empty
+template <typename T>
+__global__ void k_compact_slots(const int* __restrict__ move_src, int n_slots, Queue<T> q, SlotParams<T> sp,
+                                CaseCtl cc, double* __restrict__ forces) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_slots) return;
+  const int o = move_src[g];
+  if (o < 0) return;
+  q.slot_case[g] = q.slot_case[o];
+  sp.dt[g] = sp.dt[o]; sp.inlet[g] = sp.inlet[o]; sp.strength[g] = sp.strength[o]; sp.cfl[g] = sp.cfl[o];
+  sp.tf[g] = sp.tf[o]; sp.max_steps[g] = sp.max_steps[o]; sp.qref[g] = sp.qref[o];
+  sp.eng_track[g] = sp.eng_track[o]; sp.eng_pat[g] = sp.eng_pat[o]; sp.eng_t[g] = sp.eng_t[o];
+  cc.active[g] = cc.active[o]; cc.step[g] = cc.step[o]; cc.nmax[g] = cc.nmax[o]; cc.ref_step[g] = cc.ref_step[o];
+  cc.streak[g] = cc.streak[o]; cc.streak_start[g] = cc.streak_start[o]; cc.stopping_step[g] = cc.stopping_step[o];
+  cc.status[g] = cc.status[o]; cc.due[g] = cc.due[o]; cc.last_rel[g] = cc.last_rel[o];
+  cc.t_start[g] = cc.t_start[o]; cc.t_end[g] = cc.t_end[o];
+  cc.eng_streak[g] = cc.eng_streak[o]; cc.eng_start[g] = cc.eng_start[o]; cc.eng_stop[g] = cc.eng_stop[o];
+  cc.eng_stopping[g] = cc.eng_stopping[o];
+  forces[2 * g] = forces[2 * o];
+  forces[2 * g + 1] = forces[2 * o + 1];
+  q.slot_case[o] = -1;
+  cc.active[o] = 0;
+  cc.status[o] = 0;
+  cc.due[o] = 0;
+}
+
 // pressure force coefficients of every live-or-finished slot
 // (helper.py:366-415): sum_w p(cell_w) n_w ds_w / (q_inf L_ref), p at gamma 1.4
 template <typename T>
@@ -912,6 +1016,13 @@ __global__ void k_gather_state(const V4<T>* __restrict__ W, const int* __restric
 }
 
 // freestream fill of a slot: W = Wref = inlet
+// every item of W set to one state (the autotuner's workload)
+template <typename T>
+__global__ void k_fill_uniform(V4<T>* __restrict__ W, long long n, V4<T> w) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    W[i] = w;
+}
+
 template <typename T>
 __global__ void k_fill_freestream(V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, int n_cells, long long off, int B,
                                   int b, V4<T> w) {

@@ -104,7 +104,7 @@ struct SolverT : SolverBase {
   int n_blk = 0;
   DevBuf<int> d_case_seg, d_case_slot, d_ncells;
 
-  DevBuf<V> W, Wa, Wref, FV;
+  DevBuf<V> W, Wa, Wref, FV, Wp;   // Wp: probe step output (batch solves)
   DevBuf<T> dt_local, res;
   DevBuf<T> dt, strength;
   DevBuf<V> inlet;
@@ -215,14 +215,13 @@ struct SolverT : SolverBase {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     block = p->block_size > 0 ? p->block_size : 0;
-    if (block == 0) {
+    if (block == 0) {   // starting point; measured below
       block = 256;
       while (block > 64 && (total + block - 1) / block < 2 * sms) block /= 2;
     }
-    if (block != 64 && block != 128 && block != 256) return fail(ESR_ERR_ARG, "solver: block_size must be 64, 128 or 256");
+    if (block != 64 && block != 128 && block != 256) return fail(ESR_ERR_ARG, "solver: block_size must be 0, 64, 128 or 256");
     // upload meshes
     std::vector<Seg<T>> hsegs;
-    std::vector<int2> hblk;
     std::vector<int> hseg_of(n_slots), hslot_of(n_slots), hnc(n_slots);
     for (int m = 0; m < nm; ++m) {
       MeshDev& md = *meshes[m];
@@ -254,15 +253,11 @@ struct SolverT : SolverBase {
       s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
       s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
       hsegs.push_back(s);
-      const long long items = (long long)N * md.B;
-      for (long long b0 = 0; b0 < items; b0 += block) hblk.push_back(make_int2(m, (int)b0));
       for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
     }
-    n_blk = (int)hblk.size();
     ESR_TRY(d_segs.alloc(hsegs.size()));
     ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
-    ESR_TRY(d_blk.alloc(hblk.size()));
-    ESR_CUDA(cudaMemcpy(d_blk.p, hblk.data(), hblk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESR_TRY(build_blocks(block));
     ESR_TRY(d_case_seg.alloc(n_slots));
     ESR_TRY(d_case_slot.alloc(n_slots));
     ESR_TRY(d_ncells.alloc(n_slots));
@@ -305,6 +300,73 @@ struct SolverT : SolverBase {
     hcase.assign(n_slots, esr_case{});
     hcase_index.assign(n_slots, -1);
     ESR_CUDA(cudaStreamSynchronize(stream));
+    if (p->block_size == 0) ESR_TRY(autotune());
+    return ESR_OK;
+  }
+
+  // block table: one entry (mesh, first item) per block of `blk` items
+  int build_blocks(int blk) {
+    std::vector<int2> hblk;
+    for (int m = 0; m < (int)meshes.size(); ++m) {
+      const long long items = (long long)meshes[m]->hm->n_cells * meshes[m]->B;
+      for (long long b0 = 0; b0 < items; b0 += blk) hblk.push_back(make_int2(m, (int)b0));
+    }
+    ESR_TRY(d_blk.alloc(hblk.size()));
+    ESR_CUDA(cudaMemcpy(d_blk.p, hblk.data(), hblk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    n_blk = (int)hblk.size();
+    block = blk;
+    return ESR_OK;
+  }
+
+  // Autotuner: time one full step of every slot (the solver's own meshes,
+  // scheme and slot counts; a uniform finite state, all slots live) for each
+  // block size and keep the fastest. Results do not depend on the choice:
+  // every item is computed the same way whatever block it falls in.
+  esr_tuning tuning{};
+  int autotune() {
+    const V w0 = mk4<T>(T(1), T(0.5), T(0.1), T(2.5));
+    const int tb = 256;
+    k_fill_uniform<T><<<(int)std::min<long long>((total + tb - 1) / tb, 65535), tb, 0, stream>>>(W.p, total, w0);
+    std::vector<V> in(n_slots, w0);
+    std::vector<T> dts(n_slots, T(1e-4));
+    std::vector<int> on(n_slots, 1);
+    ESR_CUDA(cudaMemcpyAsync(inlet.p, in.data(), n_slots * sizeof(V), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(dt.p, dts.data(), n_slots * sizeof(T), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemcpyAsync(active.p, on.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
+    const Cases<T> cs = cases(true);
+    const int cand[3] = {64, 128, 256};
+    const int64_t before = launches;
+    double best = 1e300;
+    int best_blk = block;
+    tuning.n_candidates = 3;
+    for (int i = 0; i < 3; ++i) {
+      ESR_TRY(build_blocks(cand[i]));
+      step_kernels(cs, 0);   // warm-up
+      ESR_CUDA(cudaEventRecord(ev0, stream));
+      for (int r = 0; r < 3; ++r) step_kernels(cs, 0);
+      ESR_CUDA(cudaEventRecord(ev1, stream));
+      ESR_CUDA(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev0, ev1);
+      tuning.candidates[i] = cand[i];
+      tuning.step_ms[i] = ms / 3.0;
+      if (ms / 3.0 < best) { best = ms / 3.0; best_blk = cand[i]; }
+    }
+    launches = before;
+    ESR_TRY(build_blocks(best_blk));
+    tuning.block_size = best_blk;
+    ESR_CUDA(cudaMemsetAsync(W.p, 0, total * sizeof(V), stream));
+    ESR_CUDA(cudaMemsetAsync(Wa.p, 0, total * sizeof(V), stream));
+    ESR_CUDA(cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream));
+    ESR_CUDA(cudaMemsetAsync(dt.p, 0, n_slots * sizeof(T), stream));
+    ESR_CUDA(cudaMemsetAsync(inlet.p, 0, n_slots * sizeof(V), stream));
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int get_tuning(esr_tuning* out) {
+    *out = tuning;
+    if (out->block_size == 0) out->block_size = block;   // given, not measured
     return ESR_OK;
   }
 
@@ -372,6 +434,18 @@ struct SolverT : SolverBase {
         flux_dispatch<ST_SRK2_SECOND>(Wa.p, W.p, W.p, cs, pos);
         break;
     }
+  }
+  // One step of the slots active in `cs` written to scratch instead of W
+  // (the residual probe); returns the buffer that holds the stepped state.
+  V* probe_kernels(const Cases<T>& cs) {
+    const bool local = P.dt_mode == ESR_DT_LOCAL;
+    recon(W.p, cs, 0, local);
+    flux_dispatch<ST_FIRST>(W.p, nullptr, Wa.p, cs, 0);
+    if (P.time_scheme == ESR_TIME_EE) return Wa.p;
+    recon(Wa.p, cs, 0, false);
+    if (P.time_scheme == ESR_TIME_RK2) flux_dispatch<ST_RK2_SECOND>(Wa.p, W.p, Wp.p, cs, 0);
+    else flux_dispatch<ST_SRK2_SECOND>(Wa.p, W.p, Wp.p, cs, 0);
+    return Wp.p;
   }
   void check_point(int pos) {
     const int tb = 128, nb = (n_slots + tb - 1) / tb;
@@ -822,11 +896,11 @@ struct SolverT : SolverBase {
         r_eng_conv, r_eng_stop, n_done;
     DevBuf<V> c_inlet;
     DevBuf<T> c_strength;
-    DevBuf<double> c_cfl, c_tf, c_qref, r_dt, r_rel, r_cd, r_cl, r_time, init, out;
+    DevBuf<double> c_cfl, c_tf, c_qref, r_dt, r_rel, r_cd, r_cl, r_time, r_probe, init, out;
     DevBuf<long long> c_max_steps, init_off, out_off;
     DevBuf<double4> c_eng_t;
   };
-  DevBuf<int> perm_all;
+  DevBuf<int> perm_all, move_src;
   DevBuf<const int*> perm_ptrs, inv_ptrs;
 
   void issue_refill(const Queue<T>& q, const SlotParams<T>& sp, bool with_states) {
@@ -834,6 +908,14 @@ struct SolverT : SolverBase {
     k_mark_retiring<<<nb, tb, 0, stream>>>(status.p, n_slots, q.slot_case, q.retiring);
     k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, q.retiring, nullptr);
     k_retire<T><<<nb, tb, 0, stream>>>(ctl(), q, dt.p, forces.p, n_slots, P.dt_mode == ESR_DT_LOCAL);
+    // final one-step residual of each retiring case with its own dt
+    Cases<T> pc = cases(true);
+    pc.active = q.retiring;
+    const V* wp = probe_kernels(pc);
+    dim3 gr(n_chunks, n_slots);
+    k_case_reduce<T, RED_DIFF><<<gr, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), wp, W.p, q.retiring, kReduceCells,
+                                                                  partial.p, n_chunks, kc);
+    k_probe_finish<T><<<nb, tb, 0, stream>>>(q, partial.p, n_chunks, n_slots);
     int max_cells = 0;
     for (auto& md : meshes) max_cells = std::max(max_cells, md->hm->n_cells);
     dim3 g2(std::min(64, (max_cells + 255) / 256), n_slots);
@@ -847,7 +929,11 @@ struct SolverT : SolverBase {
                                           P.dt_mode == ESR_DT_LOCAL);
     k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, fill.p, eng_track.p);
     k_eng_init<<<nb, tb, 0, stream>>>(ctl(), fill.p, n_slots);
-    launches += with_states ? 10 : 9;
+    // pack running cases into the lowest slots once a mesh's queue is empty
+    k_compact_plan<T><<<(int)(meshes.size() + 31) / 32, 32, 0, stream>>>(d_segs.p, (int)meshes.size(), q, move_src.p);
+    k_compact_items<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), move_src.p, W.p, Wref.p);
+    k_compact_slots<T><<<nb, tb, 0, stream>>>(move_src.p, n_slots, q, sp, ctl(), forces.p);
+    launches += with_states ? 15 : 14;
   }
 
   int batch(const esr_case* cs, int n, const double* const* init, double* const* finals, esr_result* out) {
@@ -938,7 +1024,9 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemsetAsync(status.p, 0, n_slots * sizeof(int), stream));
     for (DevBuf<int>* b : {&B.r_status, &B.r_stop, &B.r_steps, &B.r_nmax, &B.r_eng_conv, &B.r_eng_stop})
       ESR_TRY(b->alloc(n));
-    for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time}) ESR_TRY(b->alloc(n));
+    for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time, &B.r_probe}) ESR_TRY(b->alloc(n));
+    if (Wp.n < (size_t)total) ESR_TRY(Wp.alloc(total));
+    if (move_src.n < (size_t)n_slots) ESR_TRY(move_src.alloc(n_slots));
     if (init_rows > 0) {
       ESR_TRY(B.init.alloc((size_t)4 * init_rows));
       for (int i = 0; i < n; ++i)
@@ -952,7 +1040,7 @@ struct SolverT : SolverBase {
     Queue<T> q{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
                B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p,
                init_rows > 0 ? B.init.p : nullptr, B.init_off.p, B.r_status.p, B.r_stop.p, B.r_steps.p, B.r_nmax.p,
-               B.r_dt.p, B.r_rel.p, B.r_cd.p, B.r_cl.p, B.r_time.p, B.r_eng_conv.p, B.r_eng_stop.p,
+               B.r_dt.p, B.r_rel.p, B.r_cd.p, B.r_cl.p, B.r_time.p, B.r_eng_conv.p, B.r_eng_stop.p, B.r_probe.p,
                want_states ? B.out.p : nullptr, B.out_off.p, B.n_done.p};
     SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p};
     ESR_CUDA(cudaEventRecord(ev0, stream));
@@ -960,19 +1048,20 @@ struct SolverT : SolverBase {
     // the chunk graph of this batch: steps, checks, then the refill sequence
     cudaGraphExec_t gexec = nullptr;
     const int len = run_chunk_len();
+    int64_t per_chunk = 0;
     if (P.use_graphs) {
       cudaGraph_t graph = nullptr;
       ESR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       const int64_t before = launches;
       issue_run_chunk(len);
       issue_refill(q, sp, want_states);
+      per_chunk = launches - before;
       launches = before;
       ESR_CUDA(cudaStreamEndCapture(stream, &graph));
       cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
     }
-    const int64_t per_chunk = chunk_launches(true, len) + (want_states ? 10 : 9);
     int done = 0, poll = 4;
     int rc = ESR_OK;
     for (long long guard = 0; done < n; ++guard) {
@@ -997,7 +1086,7 @@ struct SolverT : SolverBase {
     if (rc != ESR_OK) return rc;
     ESR_CUDA(cudaEventRecord(ev1, stream));
     std::vector<int> st(n), sstop(n), ssteps(n), snmax(n), sec(n), ses(n);
-    std::vector<double> sdt(n), srel(n), scd(n), scl(n), stime(n);
+    std::vector<double> sdt(n), srel(n), scd(n), scl(n), stime(n), sprobe(n);
     auto down = [&](auto& v, const auto& buf) -> int {
       using E = typename std::decay_t<decltype(v)>::value_type;
       ESR_CUDA(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(E), cudaMemcpyDeviceToHost, stream));
@@ -1007,6 +1096,7 @@ struct SolverT : SolverBase {
     ESR_TRY(down(snmax, B.r_nmax)); ESR_TRY(down(sec, B.r_eng_conv)); ESR_TRY(down(ses, B.r_eng_stop));
     ESR_TRY(down(sdt, B.r_dt)); ESR_TRY(down(srel, B.r_rel)); ESR_TRY(down(scd, B.r_cd)); ESR_TRY(down(scl, B.r_cl));
     ESR_TRY(down(stime, B.r_time));
+    ESR_TRY(down(sprobe, B.r_probe));
     if (want_states)
       for (int i = 0; i < n; ++i)
         if (finals[i])
@@ -1029,6 +1119,7 @@ struct SolverT : SolverBase {
       r.solve_time_s = stime[i];
       r.eng_converged = sec[i];
       r.eng_stopping_step = ses[i];
+      r.final_residual = sprobe[i];
     }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
@@ -1142,6 +1233,11 @@ int esr_solver_destroy(esr_solver* solver) {
 int esr_solver_num_slots(const esr_solver* solver, int32_t* n) {
   if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
   return dispatch(const_cast<esr_solver*>(solver), [&](auto& s) { *n = s.n_slots; return ESR_OK; });
+}
+
+int esr_solver_tuning(const esr_solver* solver, esr_tuning* out) {
+  if (!solver || !out) return fail(ESR_ERR_ARG, "null argument");
+  return dispatch(const_cast<esr_solver*>(solver), [&](auto& s) { return s.get_tuning(out); });
 }
 
 int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init) {

@@ -105,10 +105,10 @@ def run_grid(base_cfg, mesh, grid, slots=None, out_root=".", write=True):
     cases = [_flow_case(c, m, dtype) for c in cfgs]
     res, states = s.batch_solve(cases, want_states=True)
     records = []
-    # Per-case diagnostics on the device, B cases at a time: the freestream
-    # start gives dt and S0 (as main.run computes them), then the final state
-    # gives the one-step residual probe (euler/main.py:228-230), S and the
-    # LSQ gradients of the bundle.
+    # The batch returns each case's one-step residual probe of its final state
+    # (euler/main.py:228-230). Entropy before and after and the LSQ gradients
+    # of the bundle come from the device, B cases at a time: the freestream
+    # start gives S0 as main.run computes it, the final state S and gradients.
     for c0 in range(0, len(cases), B):
         idx = list(range(c0, min(c0 + B, len(cases))))
         for j, i in enumerate(idx):
@@ -118,13 +118,12 @@ def run_grid(base_cfg, mesh, grid, slots=None, out_root=".", write=True):
         S0 = s.entropy()
         for j, i in enumerate(idx):
             s.set_state(j, states[i])
-        probe = s.residual_probe()
         S1 = s.entropy()
         for j, i in enumerate(idx):
             cfg, r = cfgs[i], res[i]
             W = states[i].astype(dtype)
             final_time = int(r["stopping_step"]) * float(r["dt"])
-            rec = dict(cfg=cfg, result=r, final_residual=float(probe[j]), dS=float(S1[j] - S0[j]), W=W)
+            rec = dict(cfg=cfg, result=r, final_residual=float(r["final_residual"]), dS=float(S1[j] - S0[j]), W=W)
             records.append(rec)
             if write:
                 _write_case(rec, m, s, j, final_time, out_root, i + 1, len(cases))

@@ -274,6 +274,12 @@ class Solver:
         F.check(F.lib().esr_kernel_launches(self.handle, C.byref(v)))
         return int(v.value)
 
+    def tuning(self) -> dict:
+        """Block size in use and, when autotuned, the step time per candidate."""
+        t = F.Tuning()
+        F.check(F.lib().esr_solver_tuning(self.handle, C.byref(t)))
+        return t.as_dict()
+
     def profile_step(self, nsteps: int = 8) -> dict:
         """Average device ms per kernel kind over ``nsteps`` plain steps
         (CUDA events on the solver's stream around every launch)."""

@@ -1,4 +1,4 @@
-"""Learned warm start end to end.
+"""Learned warm start end to end: IDW of the LR solution plus a residual MLP.
 
 1. cases: (Mach ~ U[0.7, 3], alpha ~ U[-5, 5] deg) from default_rng(seed);
    the first n_train draws train, the next n_eval draws are held out;
@@ -9,25 +9,24 @@
    correction; loss = shock-weighted relative MSE with weights
    min(1 + |grad p_HR| / mean|grad p_HR|, 5) (preprocessing/dataset.py:168-170,
    loss.py:20-23); trained by the library's BF16 kernels with AdamW;
-4. evaluation (eval/convergence_case.py:30-142): for each held-out case the
-   HR FVM runs from freestream (cold), from IDW and from IDW+MLP to the same
-   stop rule (check every 5 steps, patience 3); reported: iterations, wall
-   time of the whole pipeline (LR solve + inference + warm HR solve) and the
-   CD error against a tightly converged reference solve.
+4. evaluation (eval/convergence_case.py:30-142, driven by ``run.py``): for
+   each held-out case the HR FVM runs from freestream (cold), from IDW and
+   from IDW+MLP to the same stop rule; reported: iterations, wall time of the
+   whole pipeline (LR solve + inference + warm HR solve) and the CD error
+   against a long reference solve.
 """
 from __future__ import annotations
 
 import ctypes as C
 import math
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 import torch
 
 from .. import _ffi as F
-from ..mesh import Mesh
-from ..solver import DeviceMesh, FlowCase, Solver
+from ..solver import FlowCase, Solver
 from .features import AOA_SCALE, MACH_MID, MACH_SCALE, MeshPair
 from .mlp import K_IN, MLP, ROW_TILE
 
@@ -45,36 +44,6 @@ def _p(t):
 
 def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
-
-
-@dataclass
-class SolveSpec:
-    threshold: float = 1e-5
-    check_every: int = 5
-    patience: int = 3
-    cfl: float = 0.6
-    tf: float = 1e9
-    max_steps: int = 40000
-    precision: str = "f32"
-    slots: int = 256
-
-
-def batch_solve(mesh, machs, aoas, spec: SolveSpec, init_fields=None, dm=None):
-    """Solve every (M, alpha) on one mesh through the batched solver; returns
-    (results, final states, device seconds)."""
-    dm = dm or DeviceMesh(mesh)
-    dtype = np.float64 if spec.precision == "f64" else np.float32
-    cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=spec.cfl, tf=spec.tf, max_steps=spec.max_steps,
-                      dtype=dtype, l_ref=float(mesh.metadata.get("obstacle_length", 1.0) or 1.0))
-             for m, a in zip(machs, aoas)]
-    s = Solver(dm, min(spec.slots, max(1, len(cases))), precision=spec.precision, threshold=spec.threshold,
-               check_every=spec.check_every, patience=spec.patience)
-    t0 = time.perf_counter()
-    res, states = s.batch_solve(cases, init_fields=init_fields, want_states=True)
-    wall = time.perf_counter() - t0
-    dev = s.elapsed_ms() * 1e-3
-    s.close()
-    return res, states, dev, wall
 
 
 def pressure_gradients(mesh, dm, states, machs, aoas):

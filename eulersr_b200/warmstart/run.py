@@ -1,4 +1,4 @@
-"""Config 5: train the warm-start model and compare warm vs cold HR solves.
+"""Learned warm start on NACA2412: train the model, compare warm vs cold HR solves.
 
     python -m eulersr_b200.warmstart.run --n-train 512 --n-eval 128 --out warm.json
 

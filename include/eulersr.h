@@ -115,7 +115,7 @@ typedef struct esr_params {
     int32_t patience;         /* consecutive checks under the threshold (>= 1) */
     int32_t device;           /* CUDA device ordinal */
     int32_t use_graphs;       /* 1: capture step chunks in CUDA graphs */
-    int32_t block_size;       /* threads per block for the cell kernels (0: autotuned) */
+    int32_t block_size;       /* threads per block for the cell kernels: 64, 128, 256, or 0 = autotuned */
     int32_t reserved;
 } esr_params;
 
@@ -154,6 +154,10 @@ typedef struct esr_result {
     double solve_time_s;      /* device time from the case's start to its retirement */
     int32_t eng_converged;    /* engineering criterion confirmed (0 when not tracked) */
     int32_t eng_stopping_step;/* first step of its confirming streak, else N */
+    double final_residual;    /* esr_batch_solve: one more step of the final state with the
+                                 case's own dt, ||W' - W||_F / (||W||_F + 1e-16)
+                                 (euler/main.py:228-230); esr_run leaves 0, use
+                                 esr_residual_probe */
 } esr_result;
 
 typedef struct esr_mesh esr_mesh;
@@ -179,6 +183,8 @@ int esr_solver_num_slots(const esr_solver* solver, int32_t* n_slots);
  * case's dt (global mode) and resets its stop-rule counters. */
 int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init);
 int esr_clear_slot(esr_solver* solver, int32_t slot);
+/* Slot `slot` restarts from state W (caller's cell order): stop-rule counters
+ * reset and dt recomputed from W, as esr_set_case with W_init does. */
 int esr_set_state(esr_solver* solver, int32_t slot, const double* W);
 int esr_get_state(esr_solver* solver, int32_t slot, double* W);
 /* device-resident float32/float64 state of a slot in the caller's cell order */
@@ -217,6 +223,17 @@ typedef struct esr_kernel_times {
     int32_t reserved;
 } esr_kernel_times;
 int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out);
+
+/* The autotuner's record: with esr_params.block_size = 0 the solver times one
+ * full step of all its slots for each candidate block size at creation and
+ * keeps the fastest (no reference counterpart: XLA picks launch shapes). */
+typedef struct esr_tuning {
+    int32_t block_size;       /* threads per block in use */
+    int32_t n_candidates;     /* 0 when block_size was given */
+    int32_t candidates[4];
+    double step_ms[4];        /* device ms of one step per candidate */
+} esr_tuning;
+int esr_solver_tuning(const esr_solver* solver, esr_tuning* out);
 
 /* Solve n_cases cases through the solver's slots: every slot retired by the
  * stop rule is refilled in place with the next queued case. init_fields[i]

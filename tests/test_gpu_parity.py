@@ -175,7 +175,30 @@ def test_batch_equals_single(diamond02, naca02, precision):
         for k in ('stopping_step', 'status', 'steps', 'n_max', 'cd', 'cl', 'eng_converged', 'eng_stopping_step'):
             assert r1[k] == res[i][k], (i, k, r1[k], res[i][k])
         assert np.array_equal(one.get_state(0), states[i]), i
+        # the probe of the retiring case (euler/main.py:228-230) with the case's own dt
+        assert res[i]['final_residual'] == one.residual_probe()[0], i
     # the same batch again on the same handle gives the same answer
     res2, states2 = s.batch_solve(cases, init_fields=init, want_states=True)
     assert all(np.array_equal(a, b) for a, b in zip(states, states2))
     assert [r['stopping_step'] for r in res] == [r['stopping_step'] for r in res2]
+
+def test_autotuner_and_block_invariance(naca02):
+    """The autotuner times every candidate block size and keeps the fastest;
+    the state after 30 steps is bitwise the same whatever the block size."""
+    from eulersr_b200.solver import Solver, FlowCase
+    states = []
+    for bs in (0, 64, 128, 256):
+        s = Solver(naca02, 3, precision='f32', block_size=bs)
+        t = s.tuning()
+        if bs == 0:
+            assert sorted(t['step_ms']) == [64, 128, 256]
+            assert all(v > 0 for v in t['step_ms'].values())
+            assert t['block_size'] == min(t['step_ms'], key=t['step_ms'].get)
+        else:
+            assert t['block_size'] == bs and t['step_ms'] == {}
+        for g, (m, a) in enumerate([(0.8, 1.0), (2.0, -3.0), (1.3, 2.5)]):
+            s.set_case(g, FlowCase(mach=m, aoa_deg=a, tf=1.0, dtype=np.float32))
+        s.step(30)
+        states.append([s.get_state(g) for g in range(3)])
+    for other in states[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(states[0], other))
