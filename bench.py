@@ -16,12 +16,17 @@ roofline  the dominant kernel (K2 flux/update) against the measured HBM copy
         bandwidth; algorithmic bytes per launch = (40 + 64/B) B per cell and
         case, half of the (80 + 128/B) B of a full SRK2 cell-update.
 
---impl reference times the oracle (the NumPy restatement of the reference's
-JAX solver; the reference itself needs JAX, absent on these hosts) on the
-host cores on a bounded sample of the same workload.
+--impl reference times the C/OpenMP restatement of the oracle (the
+reference's own CPU path is its JAX solver, absent on these hosts) on every
+host thread, on a bounded sample of the same workload.
 
-Under torchrun every rank runs its own 256-case batch (weak scaling; cases
-are independent, no data-path collective); the time is the max over ranks.
+--workload ragged runs the ragged multi-mesh batch instead: 12 meshes
+(diamond, NACA0012, NACA2412, NACA23012 at h = 0.1, 0.05, 0.025) and 1024
+cases (default_rng(2): Mach ~ U[0.7, 3], alpha ~ U[-5, 5]) dealt round-robin
+onto the meshes, all advanced by the same launches.
+
+Under torchrun every rank runs its own batch (weak scaling; cases are
+independent, no data-path collective); the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -191,8 +196,15 @@ def barrier(world):
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
-    mesh = get_mesh("naca0012", args.h)
-    mach, aoa = batch_cases(args.cases)
+    if args.workload == "ragged":
+        meshes, per = ragged_workload()
+        cfg_mesh, mesh = (meshes, per), meshes[-1]
+        mach = np.array([m for p in per for m, _ in p])
+        aoa = np.array([a for p in per for _, a in p])
+    else:
+        mesh = get_mesh("naca0012", args.h)
+        cfg_mesh = mesh
+        mach, aoa = batch_cases(args.cases)
     ncores = os.cpu_count() or 1
     vals = []
     per_step = max(3.0, 40.0 / max(1, args.steps + args.warmup))
@@ -208,7 +220,7 @@ def run_reference(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean([e for _, _, e in vals]) * 1e3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Mach/alpha draws, freestream start)",
-            "config": workload_config(args, mesh),
+            "config": workload_config(args, cfg_mesh),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": f"host has {ncores} cores"}
@@ -216,7 +228,34 @@ def run_reference(args, world, rank):
     return 0
 
 
+RAGGED_GEOMS = ("diamond", "naca0012", "naca2412", "naca23012")
+RAGGED_H = (0.1, 0.05, 0.025)
+
+
+def ragged_workload(n_cases=1024, seed=2, rank=0, world=1):
+    """The 12 meshes and, per mesh, the (Mach, alpha) of the cases dealt to it."""
+    meshes = [get_mesh(g, h) for g in RAGGED_GEOMS for h in RAGGED_H]
+    rng = np.random.default_rng(seed)
+    mach = rng.uniform(0.7, 3.0, n_cases * world)
+    aoa = rng.uniform(-5.0, 5.0, n_cases * world)
+    mach, aoa = mach[rank::world], aoa[rank::world]
+    per = [[] for _ in meshes]
+    for i in range(len(mach)):
+        per[i % len(meshes)].append((float(mach[i]), float(aoa[i])))
+    return meshes, per
+
+
 def workload_config(args, mesh):
+    if getattr(args, "workload", "naca") == "ragged":
+        meshes, per = mesh
+        cells = [m.n_cells for m in meshes]
+        return {"workload": f"ragged batch: 12 meshes ({', '.join(RAGGED_GEOMS)} x h in 0.1/0.05/0.025, "
+                            f"{min(cells)}-{max(cells)} cells) x {sum(len(p) for p in per)} cases "
+                            f"(default_rng(2): Mach~U[0.7,3], alpha~U[-5,5], round-robin), SRK2 chunk of {args.chunk} steps",
+                "cells": cells, "cases_per_mesh": [len(p) for p in per],
+                "cases_per_gpu": sum(len(p) for p in per), "srk2_steps_per_bench_step": args.chunk,
+                "scheme": "HLLC + MUSCL/Venkatakrishnan + SRK2, global dt, CFL 0.6 (0.45 transonic)",
+                "l2": "working set > L2", "parallelism": "cases sharded per GPU, all meshes in one launch"}
     return {"workload": f"naca0012 h={args.h} HR ({mesh.n_cells} cells) x {args.cases} cases "
                         f"(Mach~U[0.7,3] seed 1, alpha in -5..5 step 0.5), SRK2 chunk of {args.chunk} steps",
             "cells": int(mesh.n_cells), "cases_per_gpu": args.cases, "srk2_steps_per_bench_step": args.chunk,
@@ -236,6 +275,7 @@ def main():
     ap.add_argument("--h", type=float, default=0.025)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="naca", choices=["naca", "ragged"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -246,17 +286,30 @@ def main():
         return rc
 
     from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
-    mesh = get_mesh("naca0012", args.h)
-    mach_all, aoa_all = batch_cases(args.cases * world)
-    mach, aoa = mach_all[rank::world], aoa_all[rank::world]
-    dm = DeviceMesh(mesh)
-    cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, dtype=np.float32)
-             for m, a in zip(mach, aoa)]
-    s = Solver(dm, len(cases), precision="f32", device=local if world > 1 else 0)
+    if args.workload == "ragged":
+        meshes, per = ragged_workload(rank=rank, world=world)
+        cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=1e9, dtype=np.float32)
+                 for k, p in enumerate(per) for m, a in p]
+        s = Solver([DeviceMesh(m) for m in meshes], [len(p) for p in per], precision="f32",
+                   device=local if world > 1 else 0)
+        mesh = (meshes, per)
+        items = sum(m.n_cells * len(p) for m, p in zip(meshes, per))
+        B, N = len(cases), items / len(cases)       # N: mean cells per case
+        mach, aoa = [c.mach for c in cases], [c.aoa_deg for c in cases]
+        cpu_mesh = meshes[-1]
+    else:
+        mesh = get_mesh("naca0012", args.h)
+        mach_all, aoa_all = batch_cases(args.cases * world)
+        mach, aoa = mach_all[rank::world], aoa_all[rank::world]
+        cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, dtype=np.float32)
+                 for m, a in zip(mach, aoa)]
+        s = Solver(DeviceMesh(mesh), len(cases), precision="f32", device=local if world > 1 else 0)
+        B, N = len(cases), mesh.n_cells
+        cpu_mesh = mesh
     for b, c in enumerate(cases):
         s.set_case(b, c)
     s.synchronize()
-    B, N = len(cases), mesh.n_cells
+    tuning = s.tuning()
 
     # warm-up (graph capture happens in the first chunk)
     for _ in range(args.warmup):
@@ -277,35 +330,40 @@ def main():
     ms_max = allreduce_max(ms, world)
     cu_total = allreduce_sum(float(N * B * args.chunk * args.steps), world)
     value = cu_total / (ms_max * 1e-3)
-    alg_step_bytes = 80 + 128 / B
+    # geometry is shared by the cases of a mesh: 128 B per cell-step per mesh
+    B_eff = B if args.workload != "ragged" else B / len(mesh[0])
+    alg_step_bytes = 80 + 128 / B_eff
 
     # dominant kernel: K2 flux/update, timed per launch with events on its stream
     kt = s.profile_step(8)
     hbm, peak_kind = peaks()
-    alg_k2 = (40 + 64 / B) * N * B
+    alg_k2 = (40 + 64 / B_eff) * N * B
     k2_gbs = alg_k2 / (kt["flux_ms"] * 1e-3) / 1e9
     traffic = None
-    for pf in sorted((ROOT / "profiles").glob("k_flux_*.md")):
+    pf = ROOT / "profiles" / "k_flux_naca0012_h0.025_b128.md"
+    if pf.exists():
         for line in pf.read_text().splitlines():
             if line.startswith("traffic_bytes_per_item_per_launch"):
                 traffic = float(line.split("=")[1].split()[0]) * N * B
-                roofline_src = pf.name
     roofline = {"bound": "hbm", "achieved": k2_gbs, "peak": hbm, "unit": "GB/s", "frac": k2_gbs / hbm,
-                "traffic": traffic, "traffic_source": "ncu capture summarized in profiles/ (scaled by items)", "kernel": "k_flux (K2)", "peak_source": peak_kind,
-                "kernel_ms": kt["flux_ms"], "recon_ms": kt["recon_ms"],
-                "alg_bytes_per_launch": alg_k2}
+                "traffic": traffic, "traffic_source": f"ncu capture in profiles/{pf.name}, per item, scaled by items",
+                "kernel": "k_flux (K2)", "peak_source": peak_kind, "kernel_ms": kt["flux_ms"],
+                "recon_ms": kt["recon_ms"], "alg_bytes_per_launch": alg_k2,
+                "note": "K2 is issue-bound (~800 instructions per item); see profiles/"}
 
     # end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
+        sizes = [s._n_cells(b) for b in range(B)]
         try:
             import torch
-            pinned = [torch.empty((N, 4), dtype=torch.float64, pin_memory=True).numpy() for _ in range(B)]
+            pinned = [torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy() for n in sizes]
         except Exception:
-            pinned = [np.empty((N, 4)) for _ in range(B)]
+            pinned = [np.empty((n, 4)) for n in sizes]
         from eulersr_b200.solver import freestream
         for b, c in enumerate(cases):
             pinned[b][:] = freestream(c.mach, c.aoa_deg, dtype=np.float32).astype(np.float64)[None, :]
+        h2d = int(sum(p.nbytes for p in pinned))
         outs = pinned  # results land in the same pinned buffers
         e2e_steps = max(2, min(args.steps, 5))
         barrier(world)
@@ -320,22 +378,24 @@ def main():
         el = time.perf_counter() - t0
         el = allreduce_max(el, world)
         e2e_val = allreduce_sum(float(N * B * args.chunk * e2e_steps), world) / el
-        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(B * N * 4 * 8),
-               "d2h_bytes_per_step": int(B * N * 4 * 8),
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": h2d,
                "api": "esr_set_case (host init field) + esr_step + esr_get_state per case"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, n, el, thr, kind = cpu_oracle_sample(mesh, mach[0], aoa[0], seconds=12.0)
+        v, n, el, thr, kind = cpu_oracle_sample(cpu_mesh, mach[0], aoa[0], seconds=12.0)
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"{kind}, float32, 1 case x {n} SRK2 steps on the {N}-cell mesh ({el:.1f} s)"}
+               "sample": f"{kind}, float32, 1 case x {n} SRK2 steps on the {cpu_mesh.n_cells}-cell mesh ({el:.1f} s)"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded Mach/alpha draws on a generated NACA0012 mesh, freestream start)",
-                "config": workload_config(args, mesh),
+                "data": "synthetic (seeded Mach/alpha draws on meshes generated by the package's mesher, "
+                        "freestream start)",
+                "config": dict(workload_config(args, mesh), block_size=tuning["block_size"],
+                               autotune_step_ms=tuning["step_ms"]),
                 "alg_gbs_per_step": value * alg_step_bytes / 1e9,
                 "alg_bytes_per_cell_update": alg_step_bytes,
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,

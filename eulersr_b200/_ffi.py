@@ -96,6 +96,9 @@ class EsrError(RuntimeError):
 
 _LIB = None
 
+_GEMM_ARGS = [C.c_int32] * 5 + [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
+
 _SIGS = {
     "esr_api_version": (C.c_int32, []),
     "esr_last_error": (C.c_char_p, []),
@@ -127,9 +130,9 @@ _SIGS = {
     "esr_solver_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
-    "esr_gemm_bf16": (C.c_int, [C.c_int32] * 5 + [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
-                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                                   C.c_int32, C.c_int32, C.c_void_p]),
+    "esr_gemm_bf16": (C.c_int, _GEMM_ARGS),
+    "esr_gemm_bf16_mma_sync": (C.c_int, _GEMM_ARGS),
+    "esr_gemm_tc_status": (C.c_int, [C.POINTER(C.c_int32)]),
     "esr_mlp_head_fwd": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
     "esr_mlp_head_bwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,

@@ -353,6 +353,228 @@ __global__ void k_adamw(float* __restrict__ p, const float* __restrict__ g, floa
   if (p_bf16) p_bf16[i] = __float2bfloat16(pi);
 }
 
+// ------------------------------------------------------ tcgen05 GEMM path
+// The same C = A B with the fifth-generation tensor cores: operands staged
+// in shared memory in the 128-byte swizzled canonical layouts the UMMA
+// descriptors describe, one thread issues tcgen05.mma (128 x 128 x 16, BF16
+// in, FP32 accumulators in tensor memory), tcgen05.commit signals an
+// mbarrier per pipeline stage, and the epilogue reads the accumulators back
+// with tcgen05.ld. Tiles 128 x 128 x 64, 3 stages (96 KB), 256 threads.
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, THREADS = 256;
+constexpr int TILE_BYTES = BM * BK * 2;                 // 16 KB per operand and stage
+constexpr int SMEM_BYTES = 1024 + STAGES * 2 * TILE_BYTES + (STAGES + 1) * 8 + 16;
+constexpr long long kSpinLimit = 1LL << 20;             // bounded mbarrier polls
+
+__device__ int g_tc_error = 0;                          // set when a wait gave up
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+// true once the barrier's phase with this parity has completed; false after the spin limit
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  atomicExch(&g_tc_error, 1);
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// Shared-memory matrix descriptor, 128-byte swizzle. K-major: rows of 64
+// elements (128 B), 8-row groups 1024 B apart (SBO), LBO unused (1).
+// MN-major: 64-element MN groups `lbo` bytes apart, 8-row K groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;                // descriptor version of sm_100
+  d |= (uint64_t)2 << 61;                // SWIZZLE_128B
+  return d;
+}
+
+// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, majors, N, M
+template <bool A_MN, bool B_MN>
+__host__ __device__ constexpr uint32_t instr_desc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((A_MN ? 1u : 0u) << 15) | ((B_MN ? 1u : 0u) << 16) |
+         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t v[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Byte offset of the 16-byte chunk (row, chunk) of a swizzled tile.
+// K-major tile (128 rows x 64 K): row r, chunk c of 8 K-elements.
+__device__ __forceinline__ uint32_t off_k(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }
+// MN-major tile (64 K-rows x 128 MN): K-row k, chunk c of 8 MN-elements;
+// MN groups of 64 are 8 KB apart, K groups of 8 rows 1 KB apart.
+__device__ __forceinline__ uint32_t off_mn(int k, int c) {
+  return (c >> 3) * 8192 + (k >> 3) * 1024 + (k & 7) * 128 + (((c & 7) ^ (k & 7)) << 4);
+}
+
+template <bool A_T, bool B_T, int EPI>
+__global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, const bf16* __restrict__ A, int lda,
+                                                     const bf16* __restrict__ B, int ldb, Epi e) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = saddr(smem_raw);
+  const uint32_t tiles = (raw + 1023u) & ~1023u;                   // swizzle atoms need 1 KB alignment
+  unsigned char* gtiles = smem_raw + (tiles - raw);
+  const uint32_t bars = tiles + STAGES * 2 * TILE_BYTES;           // STAGES + 1 mbarriers
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * 2 * TILE_BYTES + (STAGES + 1) * 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m_blk = blockIdx.y * BM, n_blk = blockIdx.x * BN;
+  const int k_begin = blockIdx.z * K_split;
+  const int KT = K_split / BK;
+
+  if (tid == 0) {
+    for (int s = 0; s <= STAGES; ++s) mbar_init(bars + 8 * s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {   // 128 TMEM columns: the 128 x 128 FP32 accumulator
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(saddr(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  auto load_tile = [&](int stage, int kt) {
+    const int k0 = k_begin + kt * BK;
+    unsigned char* a = gtiles + stage * 2 * TILE_BYTES;
+    unsigned char* b = a + TILE_BYTES;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + i * THREADS;   // 1024 chunks of 16 B per operand tile
+      if (!A_T) {
+        const int r = c >> 3, ch = c & 7;
+        cp_async16(a + off_k(r, ch), A + (size_t)(m_blk + r) * lda + k0 + ch * 8);
+      } else {
+        const int k = c >> 4, ch = c & 15;
+        cp_async16(a + off_mn(k, ch), A + (size_t)(k0 + k) * lda + m_blk + ch * 8);
+      }
+      if (!B_T) {
+        const int r = c >> 3, ch = c & 7;
+        cp_async16(b + off_k(r, ch), B + (size_t)(n_blk + r) * ldb + k0 + ch * 8);
+      } else {
+        const int k = c >> 4, ch = c & 15;
+        cp_async16(b + off_mn(k, ch), B + (size_t)(k0 + k) * ldb + n_blk + ch * 8);
+      }
+    }
+  };
+
+  constexpr uint32_t idesc = instr_desc<A_T, B_T>();
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    fence_proxy_async();            // this thread's tile writes -> visible to the tensor core's async proxy
+    __syncthreads();
+    const int s = kt % STAGES;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a = tiles + s * 2 * TILE_BYTES, b = a + TILE_BYTES;
+#pragma unroll
+      for (int j = 0; j < BK / 16; ++j) {   // K = 16 per instruction
+        const uint64_t ad = A_T ? smem_desc(a + j * 2048, 8192, 1024) : smem_desc(a + j * 32, 16, 1024);
+        const uint64_t bd = B_T ? smem_desc(b + j * 2048, 8192, 1024) : smem_desc(b + j * 32, 16, 1024);
+        umma(tmem, ad, bd, idesc, (kt | j) != 0);
+      }
+      umma_commit(bars + 8 * s);     // arrives when these MMAs (and all earlier ones) are done
+    }
+    const int pf = kt + STAGES - 1;
+    if (pf < KT) {
+      // the stage being refilled was read by the MMAs of iteration kt - 1
+      if (kt >= 1) mbar_wait(bars + 8 * ((kt - 1) % STAGES), ((kt - 1) / STAGES) & 1);
+      load_tile(pf % STAGES, pf);
+    }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  mbar_wait(bars + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
+  tc_fence_after();
+
+  // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63
+  const int wq = warp & 3, col0 = (warp >> 2) * 64;
+  const int m = m_blk + wq * 32 + lane;
+#pragma unroll 1
+  for (int cc = 0; cc < 64; cc += 16) {
+    uint32_t v[16];
+    tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(col0 + cc), v);
+    const int nb = n_blk + col0 + cc;
+#pragma unroll
+    for (int q = 0; q < 16; q += 2) {
+      const int n = nb + q;
+      const float v0 = __uint_as_float(v[q]), v1 = __uint_as_float(v[q + 1]);
+      const size_t o = (size_t)m * e.ldo + n;
+      if (EPI == EPI_F32) {
+        float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
+        *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
+      } else if (EPI == EPI_FWD) {
+        const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
+        float r0 = 0.f, r1 = 0.f;
+        if (e.res) {
+          const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+          r0 = __bfloat162float(r.x);
+          r1 = __bfloat162float(r.y);
+        }
+        *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
+            __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
+      } else {
+        float d0 = v0, d1 = v1;
+        if (e.res) {
+          const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+          d0 += __bfloat162float(r.x);
+          d1 += __bfloat162float(r.y);
+        }
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
+        if (e.aux) {
+          const __nv_bfloat162 z = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
+          *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
+              __bfloat162float(z.x) > 0.f ? d0 : 0.f, __bfloat162float(z.y) > 0.f ? d1 : 0.f);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
+  }
+}
+
+}  // namespace tc
+
 int mfail(int code, const std::string& msg) { return esr::report_error(code, msg); }
 
 template <bool AT, bool BT, int EPI>
@@ -371,6 +593,19 @@ int launch_gemm(int M, int N, int K, int splits, const bf16* A, int lda, const b
   return ESR_OK;
 }
 
+template <bool AT, bool BT, int EPI>
+int launch_gemm_tc(int M, int N, int K, int splits, const bf16* A, int lda, const bf16* B, int ldb, const Epi& e,
+                   cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(tc::k_gemm_tc<AT, BT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    attr_set = true;
+  }
+  dim3 grid(N / tc::BN, M / tc::BM, splits);
+  tc::k_gemm_tc<AT, BT, EPI><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+  return ESR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -379,12 +614,15 @@ extern "C" {
 // trans_a: A stored [K][M] (lda >= M); else [M][K] (lda >= K).
 // trans_b: B stored [K][N] (ldb >= N); else [N][K] (ldb >= K).
 // M, N multiples of 128; K a multiple of 32 * splits; rows 16-byte aligned.
-int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
-                  const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res, const void* aux,
-                  void* out0, void* out1, int32_t ldo, int32_t splits, void* stream) {
+namespace {
+// argument checks shared by both GEMM paths; bk = K granularity of the kernel
+int gemm_check(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
+               const void* B, int32_t ldb, int32_t epi, const float* bias, const void* aux, void* out0, void* out1,
+               int32_t ldo, int32_t splits, int bk) {
   if (!A || !B || !out0) return mfail(ESR_ERR_ARG, "gemm: null operand");
   if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN) return mfail(ESR_ERR_ARG, "gemm: M and N must be multiples of 128");
-  if (splits < 1 || K % (BK * splits)) return mfail(ESR_ERR_ARG, "gemm: K must be a multiple of 32 x splits");
+  if (splits < 1 || K % (bk * splits))
+    return mfail(ESR_ERR_ARG, "gemm: K must be a multiple of " + std::to_string(bk) + " x splits");
   if (lda % 8 || ldb % 8 || ldo % 2) return mfail(ESR_ERR_ARG, "gemm: leading dimensions must keep 16-byte rows");
   if ((trans_a ? lda < M : lda < K) || (trans_b ? ldb < N : ldb < K) || ldo < N)
     return mfail(ESR_ERR_ARG, "gemm: leading dimension too small");
@@ -392,6 +630,38 @@ int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_
   if (epi == EPI_FWD && (!bias || !out1)) return mfail(ESR_ERR_ARG, "gemm: forward epilogue needs bias and z output");
   if (epi == EPI_BWD && aux && !out1) return mfail(ESR_ERR_ARG, "gemm: backward epilogue with z needs dz output");
   if (epi != EPI_F32 && splits != 1) return mfail(ESR_ERR_ARG, "gemm: split-K only with the F32 epilogue");
+  return ESR_OK;
+}
+}  // namespace
+
+int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
+                  const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res, const void* aux,
+                  void* out0, void* out1, int32_t ldo, int32_t splits, void* stream) {
+  const int rc = gemm_check(trans_a, trans_b, M, N, K, A, lda, B, ldb, epi, bias, aux, out0, out1, ldo, splits, tc::BK);
+  if (rc != ESR_OK) return rc;
+  Epi e{bias, (const bf16*)res, (const bf16*)aux, out0, (bf16*)out1, ldo, (long long)M * ldo};
+  cudaStream_t st = (cudaStream_t)stream;
+  const bf16* a = (const bf16*)A;
+  const bf16* b = (const bf16*)B;
+#define ESR_GEMM_CASE(TA, TB, E) \
+  if (!!trans_a == TA && !!trans_b == TB && epi == E) launch_gemm_tc<TA, TB, E>(M, N, K, splits, a, lda, b, ldb, e, st); else
+  ESR_GEMM_CASE(false, false, EPI_FWD)
+  ESR_GEMM_CASE(false, true, EPI_BWD)
+  ESR_GEMM_CASE(true, true, EPI_F32)
+  ESR_GEMM_CASE(false, false, EPI_F32)
+  ESR_GEMM_CASE(false, true, EPI_F32)
+  ESR_GEMM_CASE(false, false, EPI_BWD)
+  return mfail(ESR_ERR_ARG, "gemm: unsupported layout/epilogue combination");
+#undef ESR_GEMM_CASE
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, std::string("gemm: ") + cudaGetErrorString(err));
+}
+
+int esr_gemm_bf16_mma_sync(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A,
+                           int32_t lda, const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res,
+                           const void* aux, void* out0, void* out1, int32_t ldo, int32_t splits, void* stream) {
+  const int rc = gemm_check(trans_a, trans_b, M, N, K, A, lda, B, ldb, epi, bias, aux, out0, out1, ldo, splits, BK);
+  if (rc != ESR_OK) return rc;
   Epi e{bias, (const bf16*)res, (const bf16*)aux, out0, (bf16*)out1, ldo, (long long)M * ldo};
   cudaStream_t st = (cudaStream_t)stream;
   const bf16* a = (const bf16*)A;
@@ -408,6 +678,17 @@ int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_
 #undef ESR_GEMM_CASE
   cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? ESR_OK : mfail(ESR_ERR_CUDA, std::string("gemm: ") + cudaGetErrorString(err));
+}
+
+int esr_gemm_tc_status(int32_t* gave_up) {
+  if (!gave_up) return mfail(ESR_ERR_ARG, "gemm_tc_status: null output");
+  int v = 0;
+  const int zero = 0;
+  cudaError_t err = cudaMemcpyFromSymbol(&v, tc::g_tc_error, sizeof(int));
+  if (err == cudaSuccess) err = cudaMemcpyToSymbol(tc::g_tc_error, &zero, sizeof(int));
+  if (err != cudaSuccess) return mfail(ESR_ERR_CUDA, std::string("gemm_tc_status: ") + cudaGetErrorString(err));
+  *gave_up = v;
+  return ESR_OK;
 }
 
 // 4-wide head: y = H W^T + b (+ base); H [rows x K] BF16, W [4 x K] FP32

@@ -124,7 +124,7 @@ class MLP:
         st = _stream()
         if splits is None:
             splits = 1
-            while splits < 64 and rows % (32 * splits * 2) == 0 and rows // (splits * 2) >= 1024:
+            while splits < 64 and rows % (64 * splits * 2) == 0 and rows // (splits * 2) >= 1024:
                 splits *= 2
         rpb = 256
         nblk = (rows + rpb - 1) // rpb

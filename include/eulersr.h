@@ -269,15 +269,24 @@ int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars,
  * models/dam.py:306-308 with a 4 x 256 residual MLP; loss of loss.py:20-23).
  * All pointers are device pointers; `stream` is a cudaStream_t or NULL. */
 
-/* C[M x N] = A[M x K] B[K x N] on the tensor cores, BF16 operands, FP32
+/* C[M x N] = A[M x K] B[K x N] on the fifth-generation tensor cores
+ * (tcgen05.mma, accumulators in tensor memory), BF16 operands, FP32
  * accumulation. trans_a: A stored [K][M] else [M][K]; trans_b: B stored
  * [K][N] else [N][K] (a torch Linear weight). epi 0: FP32 partial tiles
  * (out0 + split * M * ldo); epi 1: z = acc + bias -> out1, out0 = res +
  * relu(z); epi 2: dh = acc + res -> out0, out1 = dh * (aux > 0).
- * M, N multiples of 128, K a multiple of 32 * splits. */
+ * M, N multiples of 128, K a multiple of 64 * splits. */
 int esr_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
                   const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res, const void* aux,
                   void* out0, void* out1, int32_t ldo, int32_t splits, void* stream);
+/* The same GEMM on the warp-level mma.sync path (K a multiple of 32 *
+ * splits), kept as the cross-check of the tcgen05 kernel. */
+int esr_gemm_bf16_mma_sync(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K, const void* A,
+                           int32_t lda, const void* B, int32_t ldb, int32_t epi, const float* bias, const void* res,
+                           const void* aux, void* out0, void* out1, int32_t ldo, int32_t splits, void* stream);
+/* Synchronous: 1 in *gave_up when a tcgen05 GEMM stopped waiting on its
+ * pipeline barriers (bounded waits) since the last call, then clears it. */
+int esr_gemm_tc_status(int32_t* gave_up);
 /* 4-wide output layer: y = H W^T + b (+ base), H BF16 [rows x K], W FP32 [4 x K] */
 int esr_mlp_head_fwd(const void* H, int32_t rows, int32_t K, const float* W, const float* b, const float* base,
                      float* y, void* stream);

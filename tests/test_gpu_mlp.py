@@ -91,3 +91,61 @@ def test_idw_kernel_matches_formula():
     torch.cuda.synchronize()
     ref = O.idw_predict(src, idx, dist)
     assert np.max(np.abs(out.cpu().numpy() - ref)) <= 2e-6 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("ta,tb,epi,M,N,K,splits", [
+    (0, 0, 1, 256, 256, 256, 1),     # forward: z = X W^T + b, h = res + relu(z)
+    (0, 0, 1, 128, 256, 128, 1),     # input layer (K = 128)
+    (0, 1, 2, 256, 128, 256, 1),     # backward dX with the relu mask
+    (1, 1, 0, 256, 128, 512, 2),     # weight gradient, split-K partials
+    (1, 1, 0, 128, 256, 2048, 4),    # long K: the stage barriers wrap several times
+    (0, 0, 0, 256, 256, 192, 1),     # K-blocks = stages
+    (0, 1, 0, 128, 256, 64, 1),      # a single K-block
+    (0, 0, 2, 128, 128, 320, 1),
+])
+def test_tcgen05_gemm_matches_mma_sync(ta, tb, epi, M, N, K, splits):
+    """The tcgen05 GEMM (operands in swizzled shared memory, accumulators in
+    tensor memory) against the mma.sync kernel and a float64 product of the
+    same BF16 operands, for every layout/epilogue the MLP uses."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    L = F.lib()
+    g = torch.Generator().manual_seed(M + N + K + 7 * epi)
+    A = torch.randn((K, M) if ta else (M, K), generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn((K, N) if tb else (N, K), generator=g).to(torch.bfloat16).cuda()
+    bias = torch.randn(N, generator=g).cuda()
+    res = torch.randn(M, N, generator=g).to(torch.bfloat16).cuda()
+    aux = torch.randn(M, N, generator=g).to(torch.bfloat16).cuda()
+    lda = M if ta else K
+    ldb = N if tb else K
+    p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+
+    def run(fn):
+        if epi == 0:
+            o0, o1 = torch.zeros(splits, M, N, device="cuda"), None
+        else:
+            o0, o1 = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda"), torch.zeros(M, N, dtype=torch.bfloat16, device="cuda")
+        F.check(fn(ta, tb, M, N, K, p(A), lda, p(B), ldb, epi, p(bias) if epi == 1 else None,
+                   p(res) if epi else None, p(aux) if epi == 2 else None, p(o0), p(o1), N, splits, None))
+        torch.cuda.synchronize()
+        return o0, o1
+
+    t0, t1 = run(L.esr_gemm_bf16)
+    r0, r1 = run(L.esr_gemm_bf16_mma_sync)
+    flag = C.c_int32(-1)
+    F.check(L.esr_gemm_tc_status(C.byref(flag)))
+    assert flag.value == 0
+    Ad = A.double().cpu()
+    Bd = B.double().cpu()
+    ref = (Ad.T if ta else Ad) @ (Bd if tb else Bd.T)
+    if epi == 0:
+        got = t0.double().sum(0).cpu()
+        assert _rel(got.numpy(), ref.numpy()) < 1e-5
+        assert _rel(got.numpy(), r0.double().sum(0).cpu().numpy()) < 1e-5
+    else:
+        # BF16 outputs: both paths agree to BF16 rounding
+        for a, b in ((t0, r0), (t1, r1)):
+            assert _rel(a.float().cpu().numpy(), b.float().cpu().numpy()) < 4e-3
+        if epi == 1:
+            z = ref + bias.double().cpu()
+            assert _rel(t1.double().cpu().numpy(), z.numpy()) < 4e-3
