@@ -359,11 +359,14 @@ __global__ void k_adamw(float* __restrict__ p, const float* __restrict__ g, floa
 // descriptors describe, one thread issues tcgen05.mma (128 x 128 x 16, BF16
 // in, FP32 accumulators in tensor memory), tcgen05.commit signals an
 // mbarrier per pipeline stage, and the epilogue reads the accumulators back
-// with tcgen05.ld. Tiles 128 x 128 x 64, 3 stages (96 KB), 256 threads.
+// with tcgen05.ld, stages them in shared memory and applies the epilogue in
+// row-contiguous order. Tiles 128 x 128 x 64, 3 stages (96 KB), 256 threads.
 namespace tc {
 
 constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, THREADS = 256;
 constexpr int TILE_BYTES = BM * BK * 2;                 // 16 KB per operand and stage
+constexpr int SLD = BN + 4;                             // row stride (floats) of the staged accumulator tile
+static_assert(BM * SLD * 4 <= STAGES * 2 * TILE_BYTES, "accumulator staging must fit the pipeline buffers");
 constexpr int SMEM_BYTES = 1024 + STAGES * 2 * TILE_BYTES + (STAGES + 1) * 8 + 16;
 constexpr long long kSpinLimit = 1LL << 20;             // bounded mbarrier polls
 
@@ -522,54 +525,66 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
   mbar_wait(bars + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
   tc_fence_after();
 
-  // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63
-  const int wq = warp & 3, col0 = (warp >> 2) * 64;
-  const int m = m_blk + wq * 32 + lane;
-#pragma unroll 1
-  for (int cc = 0; cc < 64; cc += 16) {
-    uint32_t v[16];
-    tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(col0 + cc), v);
-    const int nb = n_blk + col0 + cc;
+  // Accumulators -> shared memory (the pipeline buffers are free now): warp w
+  // reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63.
+  float* stile = reinterpret_cast<float*>(gtiles);
+  {
+    const int wq = warp & 3, col0 = (warp >> 2) * 64;
+    const int r = wq * 32 + lane;
 #pragma unroll
-    for (int q = 0; q < 16; q += 2) {
-      const int n = nb + q;
-      const float v0 = __uint_as_float(v[q]), v1 = __uint_as_float(v[q + 1]);
-      const size_t o = (size_t)m * e.ldo + n;
-      if (EPI == EPI_F32) {
-        float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
-        *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
-      } else if (EPI == EPI_FWD) {
-        const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
-        float r0 = 0.f, r1 = 0.f;
-        if (e.res) {
-          const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
-          r0 = __bfloat162float(r.x);
-          r1 = __bfloat162float(r.y);
-        }
-        *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
-        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
-            __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
-      } else {
-        float d0 = v0, d1 = v1;
-        if (e.res) {
-          const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
-          d0 += __bfloat162float(r.x);
-          d1 += __bfloat162float(r.y);
-        }
-        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
-        if (e.aux) {
-          const __nv_bfloat162 z = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
-          *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
-              __bfloat162float(z.x) > 0.f ? d0 : 0.f, __bfloat162float(z.y) > 0.f ? d1 : 0.f);
-        }
-      }
+    for (int cc = 0; cc < 64; cc += 16) {
+      uint32_t v[16];
+      tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(col0 + cc), v);
+      float4* dst = reinterpret_cast<float4*>(stile + r * SLD + col0 + cc);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                             __uint_as_float(v[4 * q + 3]));
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 0) {   // every tcgen05.ld has completed: release the accumulator
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
+  }
+  // epilogue in row-contiguous order: a warp covers 32 column pairs of one row
+#pragma unroll 4
+  for (int it = 0; it < (BM * BN / 2) / THREADS; ++it) {
+    const int q = it * THREADS + tid;
+    const int r = q / (BN / 2), cp = q % (BN / 2);
+    const int m = m_blk + r, n = n_blk + 2 * cp;
+    const float2 acc = *reinterpret_cast<const float2*>(stile + r * SLD + 2 * cp);
+    const float v0 = acc.x, v1 = acc.y;
+    const size_t o = (size_t)m * e.ldo + n;
+    if (EPI == EPI_F32) {
+      float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
+      *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
+    } else if (EPI == EPI_FWD) {
+      const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
+      float r0 = 0.f, r1 = 0.f;
+      if (e.res) {
+        const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+        r0 = __bfloat162float(rr.x);
+        r1 = __bfloat162float(rr.y);
+      }
+      *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
+      *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
+          __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
+    } else {
+      float d0 = v0, d1 = v1;
+      if (e.res) {
+        const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+        d0 += __bfloat162float(rr.x);
+        d1 += __bfloat162float(rr.y);
+      }
+      *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
+      if (e.aux) {
+        const __nv_bfloat162 zz = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
+        *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
+            __bfloat162float(zz.x) > 0.f ? d0 : 0.f, __bfloat162float(zz.y) > 0.f ? d1 : 0.f);
+      }
+    }
   }
 }
 

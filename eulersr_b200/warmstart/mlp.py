@@ -8,7 +8,7 @@ untrained model is exactly IDW.
 
 PyTorch only holds the device buffers (parameters, Adam moments,
 activations) and the stream; every forward, backward, loss and optimizer
-step is a kernel of ``libeulersr.so`` (esr_gemm_bf16 on the tensor cores,
+step is a kernel of ``libeulersr.so`` (esr_gemm_bf16 on the tcgen05 tensor cores,
 head/loss/AdamW/reduction kernels).
 """
 from __future__ import annotations
@@ -40,8 +40,10 @@ class MLP:
     SHAPES = [("W0", (H, K_IN)), ("b0", (H,)), ("W1", (H, H)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)),
               ("W3", (H, H)), ("b3", (H,)), ("W4", (N_OUT, H)), ("b4", (N_OUT,))]
 
-    def __init__(self, device="cuda", seed=0, n_features=13):
+    def __init__(self, device="cuda", seed=0, n_features=13, gemm="tcgen05"):
         self.L = F.lib()
+        # the 256-wide layers: tcgen05 kernel, or the mma.sync kernel kept as its cross-check
+        self.gemm = {"tcgen05": self.L.esr_gemm_bf16, "mma_sync": self.L.esr_gemm_bf16_mma_sync}[gemm]
         self.device = device
         self.n_features = n_features
         self.offsets = {}
@@ -104,10 +106,10 @@ class MLP:
         tag = "k" if keep else "f"
         h = [self._buf(f"{tag}h{l}", (rows, H), torch.bfloat16) for l in range(4)]
         z = [self._buf(f"{tag}z{l}", (rows, H), torch.bfloat16) for l in range(4)]
-        F.check(self.L.esr_gemm_bf16(0, 0, rows, H, K_IN, _p(X), K_IN, _p(self.view("W0", True)), K_IN, 1,
+        F.check(self.gemm(0, 0, rows, H, K_IN, _p(X), K_IN, _p(self.view("W0", True)), K_IN, 1,
                                      _p(self.view("b0")), None, None, _p(h[0]), _p(z[0]), H, 1, st))
         for l in range(1, 4):
-            F.check(self.L.esr_gemm_bf16(0, 0, rows, H, H, _p(h[l - 1]), H, _p(self.view(f"W{l}", True)), H, 1,
+            F.check(self.gemm(0, 0, rows, H, H, _p(h[l - 1]), H, _p(self.view(f"W{l}", True)), H, 1,
                                          _p(self.view(f"b{l}")), _p(h[l - 1]), None, _p(h[l]), _p(z[l]), H, 1, st))
         y = self._buf(f"{tag}y", (rows, N_OUT), torch.float32)
         F.check(self.L.esr_mlp_head_fwd(_p(h[3]), rows, H, _p(self.view("W4")), _p(self.view("b4")),
@@ -141,7 +143,7 @@ class MLP:
             kin = K_IN if l == 0 else H
             src = X if l == 0 else h[l - 1]
             # weight gradient dW_l = dz_l^T src (split-K over rows, fixed-order reduction)
-            F.check(self.L.esr_gemm_bf16(1, 1, H, kin, rows, _p(dz), H, _p(src), kin, 0, None, None, None,
+            F.check(self.gemm(1, 1, H, kin, rows, _p(dz), H, _p(src), kin, 0, None, None, None,
                                          _p(part), None, kin, splits, st))
             F.check(self.L.esr_reduce_splits(_p(part), splits, H * kin, H * kin, _p(self.gview(f"W{l}")), st))
             F.check(self.L.esr_colsum_bf16(_p(dz), rows, H, rpb, _p(cpart), st))
@@ -149,7 +151,7 @@ class MLP:
             if l > 0:
                 dh_prev = self._buf(f"dh{l - 1}", (rows, H), torch.bfloat16)
                 dz_prev = self._buf(f"dz{l - 1}", (rows, H), torch.bfloat16)
-                F.check(self.L.esr_gemm_bf16(0, 1, rows, H, H, _p(dz), H, _p(self.view(f"W{l}", True)), H, 2,
+                F.check(self.gemm(0, 1, rows, H, H, _p(dz), H, _p(self.view(f"W{l}", True)), H, 2,
                                              None, _p(dh), _p(z[l - 1]), _p(dh_prev), _p(dz_prev), H, 1, st))
                 dh, dz = dh_prev, dz_prev
 
