@@ -25,6 +25,12 @@ host thread, on a bounded sample of the same workload.
 cases (default_rng(2): Mach ~ U[0.7, 3], alpha ~ U[-5, 5]) dealt round-robin
 onto the meshes, all advanced by the same launches.
 
+--workload diamond runs single-case solves of the symmetric diamond instead:
+h = 0.1 (1,450 cells) is M=2.5, alpha=5, CFL 0.8 until the density residual
+L2 < 1e-6; h = 0.025 (19,384 cells) is M=2.0, alpha=0, CFL 0.6 with the
+reference stop rule (threshold 1e-5, checks every 25 steps); each bench step
+is one full solve from freestream (set-up, stepping, results).
+
 Under torchrun every rank runs its own batch (weak scaling; cases are
 independent, no data-path collective); the time is the max over ranks.
 """
@@ -264,6 +270,82 @@ def workload_config(args, mesh):
             "parallelism": f"cases sharded, {args.cases} per GPU"}
 
 
+def diamond_case(h):
+    """(Mach, alpha, CFL, stop rule, threshold, max steps) of the single-case diamond workloads."""
+    if h >= 0.1:
+        return 2.5, 5.0, 0.8, "density_l2", 1e-6, 40000
+    return 2.0, 0.0, 0.6, "reference", 1e-5, 40000
+
+
+def run_single(args, world, rank, local):
+    """One case per GPU solved from freestream to its stop rule, K times."""
+    from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
+    mesh = get_mesh("diamond", args.h)
+    mach, aoa, cfl, rule, thr, cap = diamond_case(args.h)
+    case = FlowCase(mach=mach, aoa_deg=aoa, cfl=cfl, tf=1e9, max_steps=cap, dtype=np.float32)
+    s = Solver(DeviceMesh(mesh), 1, precision="f32", stop_rule=rule, threshold=thr, check_every=25,
+               device=local if world > 1 else 0)
+    N = mesh.n_cells
+
+    def solve():
+        s.set_case(0, case)
+        return s.run()[0]
+    for _ in range(args.warmup):
+        r = solve()
+    clocks = ClockSampler(local)
+    barrier(world)
+    s.synchronize()
+    l0 = s.kernel_launches()
+    clocks.start()
+    ms, steps = 0.0, 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = solve()
+        ms += s.elapsed_ms()             # device time of the run (CUDA events on the solver stream)
+        steps += int(r["steps"])
+    s.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = s.kernel_launches() - l0
+    ms_max = allreduce_max(ms, world)
+    cu = allreduce_sum(float(N * steps), world)
+    value = cu / (ms_max * 1e-3)
+    kt = s.profile_step(8)
+    hbm, peak_kind = peaks()
+    alg_k2 = (40 + 64) * N
+    k2_gbs = alg_k2 / (kt["flux_ms"] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": k2_gbs, "peak": hbm, "unit": "GB/s", "frac": k2_gbs / hbm,
+                "traffic": None, "kernel": "k_flux (K2)", "peak_source": peak_kind, "kernel_ms": kt["flux_ms"],
+                "recon_ms": kt["recon_ms"], "alg_bytes_per_launch": alg_k2,
+                "note": "one case: the state is L2-resident and the launches are latency-bound"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, el, thr_, kind = cpu_oracle_sample(mesh, mach, aoa, seconds=12.0)
+        cpu = {"value": v, "unit": UNIT, "cores": thr_, "kind": "port",
+               "sample": f"{kind}, float32, {n} SRK2 steps of the case on the {N}-cell mesh ({el:.1f} s)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (diamond mesh generated by the package's mesher, freestream start)",
+                "config": {"workload": f"diamond h={args.h} ({N} cells), one case M={mach} alpha={aoa} CFL {cfl}, "
+                                       f"stop rule {rule} {thr}, one bench step = one full solve",
+                           "cells": N, "steps_per_solve": int(r["steps"]), "converged": bool(r["converged"]),
+                           "cd": r["cd"], "cl": r["cl"], "l2": "working set < L2 (one case)"},
+                "converged_cases_per_s": args.steps * world / (ms_max * 1e-3),
+                "e2e": {"value": cu / wall, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                        "api": "esr_set_case (freestream) + esr_run, results read back; wall clock"},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+                "kernel_times_ms": kt}
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -275,7 +357,7 @@ def main():
     ap.add_argument("--h", type=float, default=0.025)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="naca", choices=["naca", "ragged"])
+    ap.add_argument("--workload", default="naca", choices=["naca", "ragged", "diamond"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -286,6 +368,8 @@ def main():
         return rc
 
     from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
+    if args.workload == "diamond":
+        return run_single(args, world, rank, local)
     if args.workload == "ragged":
         meshes, per = ragged_workload(rank=rank, world=world)
         cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=1e9, dtype=np.float32)

@@ -10,7 +10,10 @@ each rank runs its own batched solver on its shard. The host side here
   (one all_gather over the process group: NCCL between GPUs, gloo on CPU);
 * reports a rank that failed: every rank contributes a status word to the
   gather, so the others learn of the failure at the collective instead of
-  waiting, and a short process-group timeout bounds the wait if a rank dies.
+  waiting, and a short process-group timeout bounds the wait if a rank dies;
+* averages the warm-start MLP's gradient over ranks for data-parallel
+  training (one all_reduce of the flat FP32 gradient per step; every rank
+  then takes the same AdamW step, so the replicas stay identical).
 
 This replaces the SLURM job arrays of ``slurm/run_euler_grid.sbatch`` (one
 job per angle, a serial Mach loop inside) by one process per GPU.
@@ -23,7 +26,7 @@ from dataclasses import dataclass
 import numpy as np
 
 RESULT_FIELDS = ("case_index", "status", "converged", "stopping_step", "steps", "n_max", "dt", "last_rel", "cd", "cl",
-                 "solve_time_s", "eng_converged", "eng_stopping_step")
+                 "solve_time_s", "eng_converged", "eng_stopping_step", "final_residual")
 
 
 def case_cost(mach, n_cells=1.0):
@@ -92,6 +95,24 @@ def records_to_dicts(rows):
     return [{k: (int(v) if k in ("case_index", "status", "converged", "stopping_step", "steps", "n_max",
                                   "eng_converged", "eng_stopping_step") else float(v))
              for k, v in zip(RESULT_FIELDS, row[:-1])} for row in rows]
+
+
+def allreduce_mean_(t, world: int):
+    """In place: the mean of ``t`` over all ranks (sum all_reduce, then / world)."""
+    if world <= 1:
+        return t
+    import torch.distributed as dist
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    t.div_(world)
+    return t
+
+
+def rank_batch(batch: int, world: int, rank: int) -> int:
+    """Rows of a global mini-batch that rank ``rank`` draws (equal shares, so
+    the mean of the rank means is the global mean)."""
+    if batch % world:
+        raise ValueError(f"global batch {batch} is not divisible by {world} ranks")
+    return batch // world
 
 
 def solve_sharded(solver_factory, cases, rank: int, world: int, n_cells=1.0, device="cpu"):

@@ -138,17 +138,23 @@ def build_training_set(ws: WarmStart, lr_states, lr_gradp, hr_states, hr_gradp, 
     return TrainData(torch.cat(Xs), torch.cat(bs), tgt, torch.cat(wts), inv_den.contiguous()), mu, sig
 
 
-def train(mlp: MLP, data: TrainData, steps=1500, batch=32768, lr=2e-3, seed=0, log_every=250):
-    g = torch.Generator(device=data.X.device).manual_seed(seed)
+def train(mlp: MLP, data: TrainData, steps=1500, batch=32768, lr=2e-3, seed=0, log_every=250, world=1, rank=0):
+    """AdamW on shock-weighted relative MSE. With ``world`` > 1 (one process
+    per GPU, torch.distributed initialised) each rank draws batch/world rows
+    of its own and the gradients are averaged over ranks before the step."""
+    from ..parallel import allreduce_mean_, rank_batch
+    local = rank_batch(batch, world, rank)
+    g = torch.Generator(device=data.X.device).manual_seed(seed * 1009 + rank)
     R = data.X.shape[0]
     hist = []
     t0 = time.perf_counter()
     for it in range(steps):
-        idx = torch.randint(0, R, (batch,), generator=g, device=data.X.device)
+        idx = torch.randint(0, R, (local,), generator=g, device=data.X.device)
         X, base, tgt, w = data.X[idx], data.base[idx], data.tgt[idx], data.w[idx]
         y, acts = mlp.forward(X, base, keep=True)
         L, dpred = mlp.loss(y, tgt, w, data.inv_den)
         mlp.backward(acts, dpred)
+        allreduce_mean_(mlp.g, world)
         cur = lr * 0.5 * (1 + math.cos(math.pi * it / steps))
         mlp.adamw(lr=cur, wd=1e-5)
         if it % log_every == 0 or it == steps - 1:

@@ -105,3 +105,40 @@ def test_rank_that_leaves_ends_the_collective_with_an_error():
     out = _run("hang")
     assert out[1][0] == "left"
     assert out[0][0] == "error"
+
+
+def _dp_worker(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from eulersr_b200.parallel import allreduce_mean_, rank_batch
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    try:
+        g = torch.arange(6, dtype=torch.float32) * (rank + 1)      # this rank's gradient
+        allreduce_mean_(g, world)
+        q.put((rank, g.tolist(), rank_batch(32768, world, rank)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_gradient_mean():
+    """Gradient averaging of data-parallel MLP training over two gloo ranks:
+    both ranks end with the same mean, so their AdamW steps stay identical."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = dict((r, (g, b)) for r, g, b in (q.get(timeout=120) for _ in range(2)))
+    for p in ps:
+        p.join(timeout=60)
+    expect = [1.5 * i for i in range(6)]
+    assert got[0][0] == expect and got[1][0] == expect
+    assert got[0][1] == got[1][1] == 16384
+    import pytest
+    from eulersr_b200.parallel import rank_batch
+    with pytest.raises(ValueError):
+        rank_batch(100, 3, 0)
