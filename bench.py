@@ -282,8 +282,10 @@ def run_single(args, world, rank, local):
     from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
     mesh = get_mesh("diamond", args.h)
     mach, aoa, cfl, rule, thr, cap = diamond_case(args.h)
-    case = FlowCase(mach=mach, aoa_deg=aoa, cfl=cfl, tf=1e9, max_steps=cap, dtype=np.float32)
-    s = Solver(DeviceMesh(mesh), 1, precision="f32", stop_rule=rule, threshold=thr, check_every=25,
+    prec = args.precision
+    case = FlowCase(mach=mach, aoa_deg=aoa, cfl=cfl, tf=1e9, max_steps=cap,
+                    dtype=np.float64 if prec == "f64" else np.float32)
+    s = Solver(DeviceMesh(mesh), 1, precision=prec, stop_rule=rule, threshold=thr, check_every=25,
                device=local if world > 1 else 0)
     N = mesh.n_cells
 
@@ -326,7 +328,7 @@ def run_single(args, world, rank, local):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "scaling": "weak", "vs_baseline": None, "dtype": prec,
                 "data": "synthetic (diamond mesh generated by the package's mesher, freestream start)",
                 "config": {"workload": f"diamond h={args.h} ({N} cells), one case M={mach} alpha={aoa} CFL {cfl}, "
                                        f"stop rule {rule} {thr}, one bench step = one full solve",
@@ -358,6 +360,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="naca", choices=["naca", "ragged", "diamond"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"], help="diamond workload only")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

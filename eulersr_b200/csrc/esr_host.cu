@@ -168,6 +168,8 @@ struct SolverT : SolverBase {
     return c;
   }
   CaseMap cmap() { return CaseMap{d_case_seg.p, d_case_slot.p}; }
+  Seg<T> hseg0{};   // host copy of the first segment (one-mesh block map)
+  BlockMap<T> bmap() { return BlockMap<T>{d_segs.p, d_blk.p, hseg0, meshes.size() == 1 ? 1 : 0}; }
 
   int init(const esr_mesh* const* ms, const int32_t* slots, int nm, const esr_params* p) {
     P = *p;
@@ -257,6 +259,7 @@ struct SolverT : SolverBase {
     }
     ESR_TRY(d_segs.alloc(hsegs.size()));
     ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
+    hseg0 = hsegs[0];
     ESR_TRY(build_blocks(block));
     ESR_TRY(d_case_seg.alloc(n_slots));
     ESR_TRY(d_case_slot.alloc(n_slots));
@@ -382,7 +385,7 @@ struct SolverT : SolverBase {
   template <int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
   void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
     tap_begin(1);
-    k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, win, wbase, wout, FV.p,
+    k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(bmap(), win, wbase, wout, FV.p,
                                                                         total, cs, kc, pos, dt_local.p, res.p);
     tap_end();
     ++launches;
@@ -400,14 +403,14 @@ struct SolverT : SolverBase {
   void recon(const V* w, const Cases<T>& cs, int pos, bool write_dt) {
     if (P.reconstruction != ESR_RECON_MUSCL) {
       if (write_dt) {  // constant reconstruction still needs the local dt
-        k_recon<T, false, true><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, nullptr, 0, cs, kc, pos, dt_local.p);
+        k_recon<T, false, true><<<n_blk, block, 0, stream>>>(bmap(), w, nullptr, 0, cs, kc, pos, dt_local.p);
         ++launches;
       }
       return;
     }
     tap_begin(0);
-    if (write_dt) k_recon<T, true, true><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
-    else k_recon<T, true, false><<<n_blk, block, 0, stream>>>(d_segs.p, d_blk.p, w, FV.p, total, cs, kc, pos, dt_local.p);
+    if (write_dt) k_recon<T, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    else k_recon<T, true, false><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
     tap_end();
     ++launches;
   }
