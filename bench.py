@@ -10,8 +10,8 @@ advances every case of the batch by ``--chunk`` SRK2 steps (default 50).
 value   cell-updates/s (one cell advanced one full SRK2 step), state resident
         in HBM, device time from CUDA events on the solver stream.
 e2e     the same through the public API with host buffers: every step uploads
-        the 256 initial fields from pinned host memory (esr_set_case), runs
-        the chunk, and reads every final field back (esr_get_state).
+        the 256 initial fields from pinned host memory (esr_set_cases), runs
+        the chunk, and reads every final field back (esr_get_states).
 roofline  the dominant kernel (K2 flux/update) against the measured HBM copy
         bandwidth; algorithmic bytes per launch = (40 + 64/B) B per cell and
         case, half of the (80 + 128/B) B of a full SRK2 cell-update.
@@ -453,21 +453,20 @@ def main():
         h2d = int(sum(p.nbytes for p in pinned))
         outs = pinned  # results land in the same pinned buffers
         e2e_steps = max(2, min(args.steps, 5))
+        slots = list(range(B))
         barrier(world)
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            for b, c in enumerate(cases):
-                s.set_case(b, c, W_init=pinned[b])
+            s.set_cases(slots, cases, pinned)      # every init field host -> device, one sync
             s.step(args.chunk)
-            for b in range(B):
-                outs[b][:] = s.get_state(b)
+            s.get_states(slots, outs)              # every final field device -> host, one sync
         s.synchronize()
         el = time.perf_counter() - t0
         el = allreduce_max(el, world)
         e2e_val = allreduce_sum(float(N * B * args.chunk * e2e_steps), world) / el
         e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": h2d,
-               "api": "esr_set_case (host init field) + esr_step + esr_get_state per case"}
+               "api": "esr_set_cases (pinned host init fields) + esr_step + esr_get_states"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

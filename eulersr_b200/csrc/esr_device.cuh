@@ -920,6 +920,45 @@ __global__ void k_fill_slots(const Seg<T>* __restrict__ segs, CaseMap cm, Queue<
   }
 }
 
+// per-slot start of a case (esr_set_cases): parameters and reset counters
+template <typename T>
+struct SlotInit {
+  V4<T> inlet;
+  double cfl, tf, qref;
+  long long max_steps;
+  double4 eng_t;
+  T strength;
+  int slot, eng_track, eng_pat;
+};
+
+template <typename T>
+__global__ void k_init_slots(const SlotInit<T>* __restrict__ si, int n, SlotParams<T> sp, CaseCtl cc,
+                             int* __restrict__ fill) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SlotInit<T> x = si[i];
+  const int g = x.slot;
+  sp.inlet[g] = x.inlet;
+  sp.strength[g] = x.strength;
+  sp.cfl[g] = x.cfl;
+  sp.tf[g] = x.tf;
+  sp.max_steps[g] = x.max_steps;
+  sp.qref[g] = x.qref;
+  sp.eng_track[g] = x.eng_track;
+  sp.eng_pat[g] = x.eng_pat;
+  sp.eng_t[g] = x.eng_t;
+  cc.step[g] = 0;
+  cc.ref_step[g] = 0;
+  cc.streak[g] = 0;
+  cc.streak_start[g] = 0;
+  cc.stopping_step[g] = 0;
+  cc.due[g] = 0;
+  cc.status[g] = 1;
+  cc.active[g] = 1;
+  cc.last_rel[g] = INFINITY;
+  fill[g] = 1;
+}
+
 // Once a mesh's queue is empty its running cases are packed into the lowest
 // slots, so that warps over the freed slots (32 slots of one cell) exit at
 // once in the step kernels. One thread per mesh pairs the lowest free slot

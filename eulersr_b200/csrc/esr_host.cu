@@ -657,6 +657,84 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaGetLastError());
     return ESR_OK;
   }
+  // ---------------------------------------------- many slots at once
+  DevBuf<double> stage_many;            // host rows of set_cases / get_states
+  DevBuf<SlotInit<T>> d_init;
+  int set_cases(int n, const int32_t* slots, const esr_case* cs, const double* const* W_init) {
+    if (n < 0 || (n > 0 && (!slots || !cs))) return fail(ESR_ERR_ARG, "set_cases: bad arguments");
+    if (n == 0) return ESR_OK;
+    std::vector<SlotInit<T>> hi(n);
+    std::vector<char> seen(n_slots, 0);
+    std::vector<long long> off(n, -1);
+    long long rows = 0;
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      if (seen[slots[i]]) return fail(ESR_ERR_ARG, "set_cases: a slot is listed twice");
+      seen[slots[i]] = 1;
+      esr_case c = cs[i];
+      c.mesh = m;   // the slot decides the mesh, as in esr_set_case
+      if (!(c.tf > 0) && c.max_steps <= 0) return fail(ESR_ERR_ARG, "set_cases: tf must be > 0");
+      if (!(c.cfl > 0)) return fail(ESR_ERR_ARG, "set_cases: cfl must be > 0");
+      SlotInit<T>& x = hi[i];
+      x.slot = slots[i];
+      case_params(c, x.inlet, x.strength, x.qref, x.eng_t, x.eng_track, x.eng_pat);
+      x.cfl = c.cfl;
+      x.tf = c.tf;
+      x.max_steps = c.max_steps;
+      hcase[slots[i]] = c;
+      if (W_init && W_init[i]) { off[i] = rows; rows += meshes[m]->hm->n_cells; }
+    }
+    if (rows > 0 && stage_many.n < (size_t)4 * rows) ESR_TRY(stage_many.alloc((size_t)4 * rows));
+    if (d_init.n < (size_t)n) ESR_TRY(d_init.alloc(n));
+    ESR_CUDA(cudaMemcpyAsync(d_init.p, hi.data(), n * sizeof(SlotInit<T>), cudaMemcpyHostToDevice, stream));
+    ESR_CUDA(cudaMemsetAsync(fill.p, 0, n_slots * sizeof(int), stream));
+    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p};
+    k_init_slots<T><<<(n + 127) / 128, 128, 0, stream>>>(d_init.p, n, sp, ctl(), fill.p);
+    ++launches;
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      MeshDev& md = *meshes[m];
+      const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
+      if (off[i] >= 0) {
+        double* st = stage_many.p + 4 * off[i];
+        ESR_CUDA(cudaMemcpyAsync(st, W_init[i], (size_t)4 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+        k_scatter_state<T><<<nb, tb, 0, stream>>>(st, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
+      } else {
+        k_fill_freestream<T><<<nb, tb, 0, stream>>>(W.p, Wref.p, N, md.off, md.B, b, hi[i].inlet);
+      }
+      ++launches;
+    }
+    ESR_TRY(finish_fill());
+    ESR_CUDA(cudaStreamSynchronize(stream));   // hi and the caller's fields are the copy sources
+    return ESR_OK;
+  }
+  int get_states(int n, const int32_t* slots, double* const* out) {
+    if (n < 0 || (n > 0 && (!slots || !out))) return fail(ESR_ERR_ARG, "get_states: bad arguments");
+    long long rows = 0;
+    std::vector<long long> off(n);
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      if (!out[i]) return fail(ESR_ERR_ARG, "get_states: null output");
+      off[i] = rows;
+      rows += meshes[m]->hm->n_cells;
+    }
+    if (rows > 0 && stage_many.n < (size_t)4 * rows) ESR_TRY(stage_many.alloc((size_t)4 * rows));
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      MeshDev& md = *meshes[m];
+      const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
+      double* st = stage_many.p + 4 * off[i];
+      k_gather_state<T><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, st);
+      ++launches;
+      ESR_CUDA(cudaMemcpyAsync(out[i], st, (size_t)4 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+    ESR_CUDA(cudaStreamSynchronize(stream));
+    return ESR_OK;
+  }
   int clear_slot(int slot) {
     int m, b;
     ESR_TRY(mesh_of_slot(slot, m, b));
@@ -1250,6 +1328,17 @@ int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const doub
     if (rc == ESR_OK) s.hcase_index[slot] = slot;
     return rc;
   });
+  ESR_GUARD_END
+}
+int esr_set_cases(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                  const double* const* W_init) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.set_cases(n, slots, cases, W_init); });
+  ESR_GUARD_END
+}
+int esr_get_states(esr_solver* solver, int32_t n, const int32_t* slots, double* const* out) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.get_states(n, slots, out); });
   ESR_GUARD_END
 }
 int esr_clear_slot(esr_solver* solver, int32_t slot) {

@@ -200,6 +200,40 @@ class Solver:
         else:
             F.check(F.lib().esr_set_case(self.handle, slot, C.byref(c), None))
 
+    def set_cases(self, slots, cases, W_inits=None):
+        """set_case for many slots at once (one synchronisation). ``W_inits``:
+        None or a list with an (n_cells, 4) field or None per slot; pinned
+        float64 host arrays copy fastest."""
+        n = len(slots)
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        carr = (F.Case * n)(*[c.to_c() for c in cases])
+        keep, arr = [], None
+        if W_inits is not None:
+            arr = (F._f64p * n)()
+            for i, W in enumerate(W_inits):
+                if W is None:
+                    continue
+                W = F.f64(W)
+                if W.shape != (self._n_cells(int(sl[i])), 4):
+                    raise ValueError(f"init field {i} has shape {W.shape}")
+                keep.append(W)
+                arr[i] = F.ptr(W, C.c_double)
+        F.check(F.lib().esr_set_cases(self.handle, n, F.ptr(sl, C.c_int32), carr, arr))
+
+    def get_states(self, slots, out=None):
+        """get_state for many slots at once into ``out`` (arrays (n_cells, 4)
+        float64, allocated when None); one synchronisation."""
+        n = len(slots)
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        if out is None:
+            out = [np.empty((self._n_cells(int(g)), 4)) for g in sl]
+        for g, o in zip(sl, out):
+            if o.shape != (self._n_cells(int(g)), 4) or o.dtype != np.float64 or not o.flags.c_contiguous:
+                raise ValueError("get_states: outputs must be C-contiguous float64 (n_cells, 4)")
+        arr = (F._f64p * n)(*[F.ptr(o, C.c_double) for o in out])
+        F.check(F.lib().esr_get_states(self.handle, n, F.ptr(sl, C.c_int32), arr))
+        return out
+
     def set_state(self, slot: int, W):
         W = F.f64(W)
         if W.shape != (self._n_cells(slot), 4):

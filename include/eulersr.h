@@ -183,6 +183,16 @@ int esr_solver_num_slots(const esr_solver* solver, int32_t* n_slots);
  * case's dt (global mode) and resets its stop-rule counters. */
 int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init);
 int esr_clear_slot(esr_solver* solver, int32_t slot);
+/* esr_set_case for n slots at once: slots[i] gets cases[i] and W_init[i]
+ * (W_init NULL, or a NULL entry: freestream). The host fields are copied
+ * asynchronously (pinned buffers copy fastest), the dt of every filled slot
+ * comes from one reduction, and the call synchronises once. A slot may be
+ * listed once; as in esr_set_case, the slot decides the mesh. */
+int esr_set_cases(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                  const double* const* W_init);
+/* esr_get_state for n slots at once into out[i] (caller's cell order); one
+ * synchronisation at the end. */
+int esr_get_states(esr_solver* solver, int32_t n, const int32_t* slots, double* const* out);
 /* Slot `slot` restarts from state W (caller's cell order): stop-rule counters
  * reset and dt recomputed from W, as esr_set_case with W_init does. */
 int esr_set_state(esr_solver* solver, int32_t slot, const double* W);

@@ -202,3 +202,33 @@ def test_autotuner_and_block_invariance(naca02):
         states.append([s.get_state(g) for g in range(3)])
     for other in states[1:]:
         assert all(np.array_equal(a, b) for a, b in zip(states[0], other))
+
+
+def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
+    """esr_set_cases / esr_get_states (many slots, one synchronisation) give
+    bitwise the same runs as esr_set_case / esr_get_state slot by slot, on a
+    two-mesh solver with warm-started and freestream slots."""
+    from eulersr_b200.solver import Solver, FlowCase
+    meshes = [diamond02, naca02]
+    spec = [(0, 2.5, 5.0), (0, 1.5, -2.0), (1, 0.9, 1.0), (1, 2.0, 0.0), (1, 3.0, -4.0)]
+    cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=0.5, dtype=np.float32) for k, m, a in spec]
+    slots = [0, 1, 2, 3, 4]
+    pre = Solver(naca02, 1, precision='f32')
+    pre.set_case(0, FlowCase(mach=2.0, aoa_deg=0.0, tf=0.5, dtype=np.float32))
+    pre.step(15)
+    warm = [None, None, None, pre.get_state(0), None]
+    a = Solver(meshes, [2, 3], precision='f32', threshold=1e-5, check_every=10)
+    b = Solver(meshes, [2, 3], precision='f32', threshold=1e-5, check_every=10)
+    for g, c, w in zip(slots, cases, warm):
+        a.set_case(g, c, w)
+    b.set_cases(slots[::-1], cases[::-1], warm[::-1])
+    assert np.array_equal(a.dt(), b.dt())
+    a.step(40)
+    b.step(40)
+    got = b.get_states(slots)
+    for g in slots:
+        assert np.array_equal(a.get_state(g), got[g]), g
+    ra, rb = a.run(), b.run()
+    assert [r['stopping_step'] for r in ra] == [r['stopping_step'] for r in rb]
+    with pytest.raises(Exception):
+        b.set_cases([0, 0], cases[:2])
