@@ -47,8 +47,17 @@ struct Seg {                 // one mesh and its B case slots
   const T* wall_ny;
   const T* wall_ds;          // face length
   int n_wall;
+  int b_shift;               // item / B = (umulhi(item, b_magic) + item) >> b_shift
+  unsigned b_magic;
   int pad;
 };
+
+// cell of an item of segment s without an integer divide (items < 2^31;
+// multiplier and shift chosen on the host, checked there against n / B)
+template <typename T>
+__device__ __forceinline__ int cell_of(const Seg<T>& s, int item) {
+  return (int)((__umulhi((unsigned)item, s.b_magic) + (unsigned)item) >> s.b_shift);
+}
 
 // Which segment and first item a block of the cell kernels covers. A
 // one-mesh solver passes its segment by value (kernel parameters live in the
@@ -241,6 +250,51 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   }
 }
 
+// float32 HLLC from the face primitives alone: the same arithmetic as the
+// fast branch of hllc() with the conserved variables formed only for the side
+// the wave fan selects (bitwise the same flux).
+template <typename T>
+__device__ __forceinline__ void hllc_fast(const T PL[4], const T PR[4], T nx, T ny, const Consts<T>& k, T F[4]) {
+  const T rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
+  const T rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
+  const T unL = uL * nx + vL * ny;
+  const T unR = uR * nx + vR * ny;
+  const T tx = -ny, ty = nx;
+  const T aL = sqrt(fabs(dv<T>(k.gamma * pL, rL)));
+  const T aR = sqrt(fabs(dv<T>(k.gamma * pR, rR)));
+  T SL = fmin(unL - aL, unR - aR);
+  T SR = fmax(unL + aL, unR + aR);
+  if (SL == SR) SL = SL - k.ss_eps;
+  if (SL == SR) SR = SR + k.ss_eps;
+  T den = rL * (SL - unL) - rR * (SR - unR);
+  if (den == T(0)) den = k.den_eps;
+  const T Ss = dv<T>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
+  const T PsL = pL + rL * (SL - unL) * (Ss - unL);
+  const T PsR = pR + rR * (SR - unR) * (Ss - unR);
+  const T Ps = k.half * (PsL + PsR);
+  const bool c1 = SL >= T(0);
+  const bool c2 = (SL <= T(0)) && (Ss >= T(0));
+  const bool c3 = (Ss <= T(0)) && (SR >= T(0));
+  const bool left = c1 || c2;
+  const T rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
+  const T unK = left ? unL : unR, SK = left ? SL : SR;
+  const T EK = pK * k.inv_gm1 + k.half * rK * (uK * uK + vK * vK);   // cons() of the selected side
+  const T FK0 = rK * unK, FK1 = rK * uK * unK + pK * nx, FK2 = rK * vK * unK + pK * ny, FK3 = (EK + pK) * unK;
+  if (left ? !c1 : c3) {
+    const T utK = uK * tx + vK * ty;
+    const T inv = __fdividef(1.0f, SK - Ss);
+    const T rs = rK * (SK - unK) * inv;
+    const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) * inv;
+    const T Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
+    F[0] = FK0 + SK * (rs - rK);
+    F[1] = FK1 + SK * (Us1 - rK * uK);
+    F[2] = FK2 + SK * (Us2 - rK * vK);
+    F[3] = FK3 + SK * (Us3 - EK);
+  } else {
+    F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
+  }
+}
+
 // euler_solver.py:203-240 Rusanov (plain branch) inside getFlux
 template <typename T>
 __device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
@@ -277,7 +331,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
   block_origin(bm, s, first);
   const int item = first + threadIdx.x;
   if (item >= s.n_cells * s.B) return;
-  const int c = item / s.B;
+  const int c = cell_of(s, item);
   const int b = item - c * s.B;
   const int g = s.case0 + b;
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
@@ -401,7 +455,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
   block_origin(bm, s, first);
   const int item = first + threadIdx.x;
   if (item >= s.n_cells * s.B) return;
-  const int c = item / s.B;
+  const int c = cell_of(s, item);
   const int b = item - c * s.B;
   const int g = s.case0 + b;
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
@@ -427,14 +481,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
       } else {
         prim<T>(ghost_cons<T>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
       }
-      WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
-      WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
       if constexpr (kFast<T>) {
         // float32: the face primitives are used as reconstructed (the
-        // reference converts them to conserved and back, a rounding-level step)
+        // reference converts them to conserved and back, a rounding-level
+        // step); HLLC forms the conserved state of the selected side itself
 #pragma unroll
         for (int v = 0; v < 4; ++v) { PL[v] = qL[v]; PR[v] = qR[v]; }
+        if (FLUX != 0) {
+          WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
+          WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
+        }
       } else {
+        WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
+        WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
         prim<T>(WL, kc.gm1, kc.half, PL);
         prim<T>(WR, kc.gm1, kc.half, PR);
       }
@@ -445,8 +504,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
       prim<T>(WR, kc.gm1, kc.half, PR);
     }
     T F[4];
-    if (FLUX == 0) hllc<T>(WL, PL, WR, PR, nx, ny, kc, F);
-    else rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
+    if (FLUX == 0) {
+      if constexpr (kFast<T> && MUSCL) hllc_fast<T>(PL, PR, nx, ny, kc, F);
+      else hllc<T>(WL, PL, WR, PR, nx, ny, kc, F);
+    } else {
+      rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
+    }
     const T sk = geo(s, G_S0 + k, c);
     if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
     else { acc[0] = acc[0] + sk * F[0]; acc[1] = acc[1] + sk * F[1]; acc[2] = acc[2] + sk * F[2]; acc[3] = acc[3] + sk * F[3]; }
@@ -483,7 +546,7 @@ __global__ void k_commit(const Seg<T>* __restrict__ segs, const int2* __restrict
   const Seg<T> s = segs[bt.x];
   const int item = bt.y + threadIdx.x;
   if (item >= s.n_cells * s.B) return;
-  const int c = item / s.B;
+  const int c = cell_of(s, item);
   const int g = s.case0 + (item - c * s.B);
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
   dst[s.off + item] = src[s.off + item];

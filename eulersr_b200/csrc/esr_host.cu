@@ -254,6 +254,7 @@ struct SolverT : SolverBase {
       s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = N; s.off = md.off;
       s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
       s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
+      ESR_TRY(set_divider(s));
       hsegs.push_back(s);
       for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
     }
@@ -304,6 +305,25 @@ struct SolverT : SolverBase {
     hcase_index.assign(n_slots, -1);
     ESR_CUDA(cudaStreamSynchronize(stream));
     if (p->block_size == 0) ESR_TRY(autotune());
+    return ESR_OK;
+  }
+
+  // item -> cell without a divide: q = (umulhi(n, m) + n) >> l with
+  // l = ceil(log2 B), m = floor(2^32 (2^l - B) / B) + 1 (exact for n < 2^31)
+  static int set_divider(Seg<T>& s) {
+    const uint32_t d = (uint32_t)s.B;
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    const uint64_t m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+    if (m > 0xFFFFFFFFull) return fail(ESR_ERR_ARG, "solver: slot count has no 32-bit divider");
+    s.b_magic = (uint32_t)m;
+    s.b_shift = l;
+    const uint64_t items = (uint64_t)s.n_cells * d;
+    if (items >= (1ull << 31)) return fail(ESR_ERR_ARG, "solver: cells x slots of one mesh must stay below 2^31");
+    for (uint64_t n : {uint64_t(0), uint64_t(d - 1), uint64_t(d), items - 1, items / 2 + 1}) {
+      const uint32_t q = (uint32_t)((((n * s.b_magic) >> 32) + n) >> l);
+      if (n < items && q != n / d) return fail(ESR_ERR_STATE, "solver: item divider check failed");
+    }
     return ESR_OK;
   }
 
