@@ -38,10 +38,10 @@ struct Seg {                 // one mesh and its B case slots
   int n_cells;
   int B;                     // case slots on this mesh
   int case0;                 // global slot index of slot 0
-  int geo_stride;
+  int geo_stride;            // G_COUNT (values per cell record)
   long long off;             // first item of this segment in the state arrays
   const int4* nbr;           // x,y,z neighbour cell (-1 boundary), w packed slot info
-  const T* geo;              // G_COUNT * geo_stride
+  const T* geo;              // per-cell records of G_COUNT values
   const int* wall_cell;      // force faces: owner cell
   const T* wall_nx;          // owner's outward unit normal
   const T* wall_ny;
@@ -313,7 +313,19 @@ __device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4
 }
 
 template <typename T>
-__device__ __forceinline__ T geo(const Seg<T>& s, int f, int c) { return __ldg(s.geo + (size_t)f * s.geo_stride + c); }
+__device__ __forceinline__ T geo(const Seg<T>& s, int f, int c) { return __ldg(s.geo + (size_t)c * G_COUNT + f); }
+
+// N4 consecutive groups of 4 geometry values of cell c, from group g0, as
+// vector loads (the per-cell record is 16-byte aligned)
+template <typename T, int N4>
+__device__ __forceinline__ void geo_groups(const Seg<T>& s, int c, int g0, T out[4 * N4]) {
+  const V4<T>* p = reinterpret_cast<const V4<T>*>(s.geo + (size_t)c * G_COUNT) + g0;
+#pragma unroll
+  for (int i = 0; i < N4; ++i) {
+    const V4<T> v = p[i];
+    out[4 * i] = v.x; out[4 * i + 1] = v.y; out[4 * i + 2] = v.z; out[4 * i + 3] = v.w;
+  }
+}
 
 // --------------------------------------------------------------- K1 recon
 // euler_solver.py:106-122 build_reconstruction for MUSCL: BC ghosts, LSQ
@@ -340,15 +352,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
   T Pc[4];
   prim<T>(Wc, kc.gm1, kc.half, Pc);
   if (LOCALDT) {
+    T gn[12];
+    geo_groups<T, 3>(s, c, 0, gn);
     const T cel = sqrt(fabs(kc.gamma * Pc[3] / Pc[0]));
     T lam = T(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const T un = Pc[1] * geo(s, G_N0X + 2 * k, c) + Pc[2] * geo(s, G_N0Y + 2 * k, c);
-      const T term = (cel + fabs(un)) * geo(s, G_S0 + k, c);
+      const T un = Pc[1] * gn[G_N0X + 2 * k] + Pc[2] * gn[G_N0Y + 2 * k];
+      const T term = (cel + fabs(un)) * gn[G_S0 + k];
       lam = (k == 0) ? term : lam + term;
     }
-    dt_local[gi] = geo(s, G_AREA, c) / lam * cs.dt[g];   // cs.dt holds the case CFL in local mode
+    dt_local[gi] = gn[G_AREA] / lam * cs.dt[g];   // cs.dt holds the case CFL in local mode
   }
   if (!MUSCL) return;
   const int4 nb = __ldg(s.nbr + c);
@@ -364,16 +378,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
     prim<T>(Wk, kc.gm1, kc.half, Pk[k]);
   }
   T gx[4], gy[4];
-  const T c0x = geo(s, G_C0X, c), c0y = geo(s, G_C0Y, c), c1x = geo(s, G_C1X, c), c1y = geo(s, G_C1Y, c);
-  const T c2x = geo(s, G_C2X, c), c2y = geo(s, G_C2Y, c);
+  T gc[12];   // LSQ coefficients and face offsets (groups 3-5)
+  geo_groups<T, 3>(s, c, 3, gc);
+  const T c0x = gc[G_C0X - 12], c0y = gc[G_C0Y - 12], c1x = gc[G_C1X - 12], c1y = gc[G_C1Y - 12];
+  const T c2x = gc[G_C2X - 12], c2y = gc[G_C2Y - 12];
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
     gx[v] = c0x * d0 + c1x * d1 + c2x * d2;
     gy[v] = c0y * d0 + c1y * d1 + c2y * d2;
   }
-  const T fx[3] = {geo(s, G_F0X, c), geo(s, G_F1X, c), geo(s, G_F2X, c)};
-  const T fy[3] = {geo(s, G_F0Y, c), geo(s, G_F1Y, c), geo(s, G_F2Y, c)};
+  const T fx[3] = {gc[G_F0X - 12], gc[G_F1X - 12], gc[G_F2X - 12]};
+  const T fy[3] = {gc[G_F0Y - 12], gc[G_F1Y - 12], gc[G_F2Y - 12]};
   T phi[4], D[3][4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
@@ -464,11 +480,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
   const int4 nb = __ldg(s.nbr + c);
   const int nbk[3] = {nb.x, nb.y, nb.z};
   const V4<T> inlet = cs.inlet[g];
+  T gk[12];   // normals, face lengths, area, blend (groups 0-2)
+  geo_groups<T, 3>(s, c, 0, gk);
   T acc[4];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int kind = slot_kind(nb.w, k);
-    const T nx = geo(s, G_N0X + 2 * k, c), ny = geo(s, G_N0Y + 2 * k, c);
+    const T nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
     V4<T> WL, WR;
     T PL[4], PR[4];
     if (MUSCL) {
@@ -510,12 +528,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
     } else {
       rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
     }
-    const T sk = geo(s, G_S0 + k, c);
+    const T sk = gk[G_S0 + k];
     if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
     else { acc[0] = acc[0] + sk * F[0]; acc[1] = acc[1] + sk * F[1]; acc[2] = acc[2] + sk * F[2]; acc[3] = acc[3] + sk * F[3]; }
   }
-  const T area = geo(s, G_AREA, c);
-  const T sig = cs.strength[g] * geo(s, G_BLEND3, c);
+  const T area = gk[G_AREA];
+  const T sig = cs.strength[g] * gk[G_BLEND3];
   const T R0 = dv<T>(acc[0], area) - sig * (inlet.x - Wc.x);
   const T R1 = dv<T>(acc[1], area) - sig * (inlet.y - Wc.y);
   const T R2 = dv<T>(acc[2], area) - sig * (inlet.z - Wc.z);

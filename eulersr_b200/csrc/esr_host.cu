@@ -251,7 +251,7 @@ struct SolverT : SolverBase {
       ESR_TRY(md.inv.alloc(N));
       ESR_CUDA(cudaMemcpy(md.inv.p, hm.inv.data(), N * sizeof(int), cudaMemcpyHostToDevice));
       Seg<T> s{};
-      s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = N; s.off = md.off;
+      s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = G_COUNT; s.off = md.off;
       s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
       s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
       ESR_TRY(set_divider(s));

@@ -13,7 +13,7 @@ struct HostMesh {
   double y_min = 0, y_max = 0;
   std::vector<int> perm;          // new -> old
   std::vector<int> inv;           // old -> new
-  std::vector<double> geo;        // G_COUNT x n_cells, renumbered
+  std::vector<double> geo;        // n_cells records of G_COUNT values, renumbered
   std::vector<int> nbr;           // 4 x n_cells (x,y,z neighbours, w packed)
   std::vector<int> wall_cell;     // renumbered owner cell of each force face
   std::vector<double> wall_n;     // (nx, ny) per force face

@@ -3,15 +3,19 @@
 
 namespace esr {
 
-// per-cell geometry fields, stored structure-of-arrays: geo[field * stride + cell]
+// per-cell geometry, G_COUNT = 24 values per cell stored cell by cell
+// (geo[cell * G_COUNT + field]) in groups of 4 for vector loads: groups 0-2
+// are what the flux kernel reads, groups 3-5 what the reconstruction reads
 enum GeoField {
-  G_C0X, G_C0Y, G_C1X, G_C1Y, G_C2X, G_C2Y,   // LSQ: grad = sum_k c_k (P_k - P_c)
-  G_F0X, G_F0Y, G_F1X, G_F1Y, G_F2X, G_F2Y,   // face midpoint - barycentre
-  G_N0X, G_N0Y, G_N1X, G_N1Y, G_N2X, G_N2Y,   // outward unit normals
-  G_S0, G_S1, G_S2,                           // face lengths
-  G_AREA, G_BLEND3,                           // cell area, sponge blend^3
+  G_N0X, G_N0Y, G_N1X, G_N1Y,                 // outward unit normals
+  G_N2X, G_N2Y, G_S0, G_S1,                   // ... and face lengths
+  G_S2, G_AREA, G_BLEND3, G_PAD,              // cell area, sponge blend^3
+  G_C0X, G_C0Y, G_C1X, G_C1Y,                 // LSQ: grad = sum_k c_k (P_k - P_c)
+  G_C2X, G_C2Y, G_F0X, G_F0Y,                 // face midpoint - barycentre
+  G_F1X, G_F1Y, G_F2X, G_F2Y,
   G_COUNT
 };
+static_assert(G_COUNT == 24, "geometry groups of 4");
 
 // slot kinds (face markers of euler/jax_fvm/src/mesh.py:47-52)
 enum SlotKind { K_INTERIOR = 0, K_WALL = 2, K_INLET = 3, K_OUTLET = 4, K_SUBSONIC = 5 };

@@ -93,7 +93,7 @@ int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err) {
   hm.n_faces = F;
   hm.geo.assign((size_t)G_COUNT * N, 0.0);
   hm.nbr.assign((size_t)4 * N, 0);
-  auto G = [&](int f, int c) -> double& { return hm.geo[(size_t)f * N + c]; };
+  auto G = [&](int f, int c) -> double& { return hm.geo[(size_t)c * G_COUNT + f]; };
 
   // face geometry
   std::vector<double> fmid(2 * F), flen(F);

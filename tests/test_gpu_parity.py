@@ -232,3 +232,27 @@ def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
     assert [r['stopping_step'] for r in ra] == [r['stopping_step'] for r in rb]
     with pytest.raises(Exception):
         b.set_cases([0, 0], cases[:2])
+
+
+def test_batch_edge_cases(diamond02):
+    """Queue edge cases of esr_batch_solve: an empty case list, a case capped
+    by max_steps (MAXSTEP), a case that blows up (CFL 40: NONFINITE, retired
+    at its next check without disturbing the others), and more cases than
+    slots on one slot; every finite case equals its single-case solve."""
+    from eulersr_b200.solver import Solver, FlowCase
+    s = Solver(diamond02, 1, precision='f32', threshold=1e-5, check_every=10)
+    res, states = s.batch_solve([], want_states=True)
+    assert res == [] and states == []
+    cases = [FlowCase(mach=2.5, aoa_deg=5.0, cfl=0.6, tf=10.0, max_steps=7, dtype=np.float32),
+             FlowCase(mach=2.0, aoa_deg=1.0, cfl=40.0, tf=10.0, max_steps=400, dtype=np.float32),
+             FlowCase(mach=1.5, aoa_deg=-1.0, cfl=0.6, tf=0.3, dtype=np.float32)]
+    res, states = s.batch_solve(cases, want_states=True)
+    assert res[0]['status'] == 3 and res[0]['steps'] == 7 and res[0]['n_max'] == 7
+    assert res[1]['status'] == 4 and not res[1]['converged']
+    assert res[2]['status'] in (2, 3)
+    for i in (0, 2):
+        one = Solver(diamond02, 1, precision='f32', threshold=1e-5, check_every=10)
+        one.set_case(0, cases[i])
+        r1 = one.run()[0]
+        assert r1['stopping_step'] == res[i]['stopping_step'] and r1['status'] == res[i]['status']
+        assert np.array_equal(one.get_state(0), states[i])
