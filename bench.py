@@ -364,11 +364,12 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
-    world, rank, local = dist_setup()
     if args.impl == "reference":
-        rc = run_reference(args, world, rank)
-        barrier(world)
-        return rc
+        # the reference's CPU path: rank 0 alone times it; other ranks exit at once
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank)
+    world, rank, local = dist_setup()
 
     from eulersr_b200.solver import Solver, FlowCase, DeviceMesh
     if args.workload == "diamond":
