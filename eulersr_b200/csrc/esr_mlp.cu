@@ -363,12 +363,23 @@ __global__ void k_adamw(float* __restrict__ p, const float* __restrict__ g, floa
 // row-contiguous order. Tiles 128 x 128 x 64, 3 stages (96 KB), 256 threads.
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, THREADS = 256;
-constexpr int TILE_BYTES = BM * BK * 2;                 // 16 KB per operand and stage
-constexpr int SLD = BN + 4;                             // row stride (floats) of the staged accumulator tile
-static_assert(BM * SLD * 4 <= STAGES * 2 * TILE_BYTES, "accumulator staging must fit the pipeline buffers");
-constexpr int SMEM_BYTES = 1024 + STAGES * 2 * TILE_BYTES + (STAGES + 1) * 8 + 16;
+constexpr int BM = 128, BK = 64, THREADS = 256;
+constexpr int A_BYTES = BM * BK * 2;                    // 16 KB of A per stage
+constexpr int SLD = 128 + 4;                            // row stride (floats) of a staged 128-column accumulator half
 constexpr long long kSpinLimit = 1LL << 20;             // bounded mbarrier polls
+
+// Tile width 128 (3 stages) or 256 (2 stages): a 256-wide tile reads each
+// 128-row block of A once for the whole 256-column output; both use 96 KB of
+// pipeline buffers, so two CTAs fit on an SM.
+template <int TBN>
+struct Cfg {
+  static constexpr int BN = TBN;
+  static constexpr int STAGES = TBN == 256 ? 2 : 3;
+  static constexpr int B_BYTES = TBN * BK * 2;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + (STAGES + 1) * 8 + 16;
+  static_assert(BM * SLD * 4 <= STAGES * STAGE_BYTES, "accumulator staging must fit the pipeline buffers");
+};
 
 __device__ int g_tc_error = 0;                          // set when a wait gave up
 
@@ -407,10 +418,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
 }
 
 // kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, majors, N, M
-template <bool A_MN, bool B_MN>
+template <bool A_MN, bool B_MN, int N>
 __host__ __device__ constexpr uint32_t instr_desc() {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((A_MN ? 1u : 0u) << 15) | ((B_MN ? 1u : 0u) << 16) |
-         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
@@ -440,15 +451,17 @@ __device__ __forceinline__ uint32_t off_mn(int k, int c) {
   return (c >> 3) * 8192 + (k >> 3) * 1024 + (k & 7) * 128 + (((c & 7) ^ (k & 7)) << 4);
 }
 
-template <bool A_T, bool B_T, int EPI>
+template <bool A_T, bool B_T, int EPI, int TBN>
 __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, const bf16* __restrict__ A, int lda,
                                                      const bf16* __restrict__ B, int ldb, Epi e) {
+  using C = Cfg<TBN>;
+  constexpr int BN = C::BN, STAGES = C::STAGES, STAGE_BYTES = C::STAGE_BYTES;
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = saddr(smem_raw);
   const uint32_t tiles = (raw + 1023u) & ~1023u;                   // swizzle atoms need 1 KB alignment
   unsigned char* gtiles = smem_raw + (tiles - raw);
-  const uint32_t bars = tiles + STAGES * 2 * TILE_BYTES;           // STAGES + 1 mbarriers
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * 2 * TILE_BYTES + (STAGES + 1) * 8);
+  const uint32_t bars = tiles + STAGES * STAGE_BYTES;              // STAGES + 1 mbarriers
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * STAGE_BYTES + (STAGES + 1) * 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m_blk = blockIdx.y * BM, n_blk = blockIdx.x * BN;
   const int k_begin = blockIdx.z * K_split;
@@ -458,8 +471,8 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
     for (int s = 0; s <= STAGES; ++s) mbar_init(bars + 8 * s, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) {   // 128 TMEM columns: the 128 x 128 FP32 accumulator
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(saddr(tmem_slot)));
+  if (warp == 0) {   // BN TMEM columns: the 128 x BN FP32 accumulator
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(tmem_slot)), "n"(BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   tc_fence_before();
@@ -469,11 +482,11 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
 
   auto load_tile = [&](int stage, int kt) {
     const int k0 = k_begin + kt * BK;
-    unsigned char* a = gtiles + stage * 2 * TILE_BYTES;
-    unsigned char* b = a + TILE_BYTES;
+    unsigned char* a = gtiles + stage * STAGE_BYTES;
+    unsigned char* b = a + A_BYTES;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int c = tid + i * THREADS;   // 1024 chunks of 16 B per operand tile
+      const int c = tid + i * THREADS;   // 1024 chunks of 16 B in the A tile
       if (!A_T) {
         const int r = c >> 3, ch = c & 7;
         cp_async16(a + off_k(r, ch), A + (size_t)(m_blk + r) * lda + k0 + ch * 8);
@@ -481,17 +494,21 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
         const int k = c >> 4, ch = c & 15;
         cp_async16(a + off_mn(k, ch), A + (size_t)(k0 + k) * lda + m_blk + ch * 8);
       }
+    }
+#pragma unroll
+    for (int i = 0; i < BN / 32; ++i) {
+      const int c = tid + i * THREADS;   // BN * 8 chunks in the B tile
       if (!B_T) {
         const int r = c >> 3, ch = c & 7;
         cp_async16(b + off_k(r, ch), B + (size_t)(n_blk + r) * ldb + k0 + ch * 8);
       } else {
-        const int k = c >> 4, ch = c & 15;
+        const int k = c / (BN / 8), ch = c % (BN / 8);
         cp_async16(b + off_mn(k, ch), B + (size_t)(k0 + k) * ldb + n_blk + ch * 8);
       }
     }
   };
 
-  constexpr uint32_t idesc = instr_desc<A_T, B_T>();
+  constexpr uint32_t idesc = instr_desc<A_T, B_T, BN>();
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
     if (s < KT) load_tile(s, s);
@@ -504,7 +521,7 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
     const int s = kt % STAGES;
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t a = tiles + s * 2 * TILE_BYTES, b = a + TILE_BYTES;
+      const uint32_t a = tiles + s * STAGE_BYTES, b = a + A_BYTES;
 #pragma unroll
       for (int j = 0; j < BK / 16; ++j) {   // K = 16 per instruction
         const uint64_t ad = A_T ? smem_desc(a + j * 2048, 8192, 1024) : smem_desc(a + j * 32, 16, 1024);
@@ -525,64 +542,69 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
   mbar_wait(bars + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
   tc_fence_after();
 
-  // Accumulators -> shared memory (the pipeline buffers are free now): warp w
-  // reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63.
+  // Accumulators -> shared memory (the pipeline buffers are free now), 128
+  // columns at a time: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows) and
+  // columns 64 (w / 4) .. +63 of the half.
   float* stile = reinterpret_cast<float*>(gtiles);
-  {
-    const int wq = warp & 3, col0 = (warp >> 2) * 64;
-    const int r = wq * 32 + lane;
+#pragma unroll 1
+  for (int h = 0; h < BN / 128; ++h) {
+    if (h > 0) __syncthreads();   // the previous half has been stored
+    {
+      const int wq = warp & 3, col0 = (warp >> 2) * 64;
+      const int r = wq * 32 + lane;
 #pragma unroll
-    for (int cc = 0; cc < 64; cc += 16) {
-      uint32_t v[16];
-      tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(col0 + cc), v);
-      float4* dst = reinterpret_cast<float4*>(stile + r * SLD + col0 + cc);
+      for (int cc = 0; cc < 64; cc += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(h * 128 + col0 + cc), v);
+        float4* dst = reinterpret_cast<float4*>(stile + r * SLD + col0 + cc);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                             __uint_as_float(v[4 * q + 3]));
+        for (int q = 0; q < 4; ++q)
+          dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                               __uint_as_float(v[4 * q + 3]));
+      }
     }
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) {   // every tcgen05.ld has completed: release the accumulator
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
-  }
-  // epilogue in row-contiguous order: a warp covers 32 column pairs of one row
+    tc_fence_before();
+    __syncthreads();
+    if (h == BN / 128 - 1 && warp == 0) {   // every tcgen05.ld has completed: release the accumulator
+      tc_fence_after();
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(BN));
+    }
+    // epilogue in row-contiguous order: a warp covers 32 column pairs of one row
 #pragma unroll 4
-  for (int it = 0; it < (BM * BN / 2) / THREADS; ++it) {
-    const int q = it * THREADS + tid;
-    const int r = q / (BN / 2), cp = q % (BN / 2);
-    const int m = m_blk + r, n = n_blk + 2 * cp;
-    const float2 acc = *reinterpret_cast<const float2*>(stile + r * SLD + 2 * cp);
-    const float v0 = acc.x, v1 = acc.y;
-    const size_t o = (size_t)m * e.ldo + n;
-    if (EPI == EPI_F32) {
-      float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
-      *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
-    } else if (EPI == EPI_FWD) {
-      const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
-      float r0 = 0.f, r1 = 0.f;
-      if (e.res) {
-        const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
-        r0 = __bfloat162float(rr.x);
-        r1 = __bfloat162float(rr.y);
-      }
-      *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
-      *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
-          __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
-    } else {
-      float d0 = v0, d1 = v1;
-      if (e.res) {
-        const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
-        d0 += __bfloat162float(rr.x);
-        d1 += __bfloat162float(rr.y);
-      }
-      *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
-      if (e.aux) {
-        const __nv_bfloat162 zz = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
-        *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
-            __bfloat162float(zz.x) > 0.f ? d0 : 0.f, __bfloat162float(zz.y) > 0.f ? d1 : 0.f);
+    for (int it = 0; it < (BM * 128 / 2) / THREADS; ++it) {
+      const int q = it * THREADS + tid;
+      const int r = q / 64, cp = q % 64;
+      const int m = m_blk + r, n = n_blk + h * 128 + 2 * cp;
+      const float2 acc = *reinterpret_cast<const float2*>(stile + r * SLD + 2 * cp);
+      const float v0 = acc.x, v1 = acc.y;
+      const size_t o = (size_t)m * e.ldo + n;
+      if (EPI == EPI_F32) {
+        float* out = static_cast<float*>(e.out0) + (size_t)blockIdx.z * e.split_stride;
+        *reinterpret_cast<float2*>(out + o) = make_float2(v0, v1);
+      } else if (EPI == EPI_FWD) {
+        const float z0 = v0 + e.bias[n], z1 = v1 + e.bias[n + 1];
+        float r0 = 0.f, r1 = 0.f;
+        if (e.res) {
+          const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+          r0 = __bfloat162float(rr.x);
+          r1 = __bfloat162float(rr.y);
+        }
+        *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(z0, z1);
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) =
+            __floats2bfloat162_rn(r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
+      } else {
+        float d0 = v0, d1 = v1;
+        if (e.res) {
+          const __nv_bfloat162 rr = *reinterpret_cast<const __nv_bfloat162*>(e.res + o);
+          d0 += __bfloat162float(rr.x);
+          d1 += __bfloat162float(rr.y);
+        }
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(e.out0) + o) = __floats2bfloat162_rn(d0, d1);
+        if (e.aux) {
+          const __nv_bfloat162 zz = *reinterpret_cast<const __nv_bfloat162*>(e.aux + o);
+          *reinterpret_cast<__nv_bfloat162*>(e.out1 + o) = __floats2bfloat162_rn(
+              __bfloat162float(zz.x) > 0.f ? d0 : 0.f, __bfloat162float(zz.y) > 0.f ? d1 : 0.f);
+        }
       }
     }
   }
@@ -613,11 +635,19 @@ int launch_gemm_tc(int M, int N, int K, int splits, const bf16* A, int lda, cons
                    cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(tc::k_gemm_tc<AT, BT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    cudaFuncSetAttribute(tc::k_gemm_tc<AT, BT, EPI, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<128>::SMEM);
+    cudaFuncSetAttribute(tc::k_gemm_tc<AT, BT, EPI, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<256>::SMEM);
     attr_set = true;
   }
-  dim3 grid(N / tc::BN, M / tc::BM, splits);
-  tc::k_gemm_tc<AT, BT, EPI><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+  if (N % 256 == 0) {   // the whole 256-wide output row block per CTA
+    dim3 grid(N / 256, M / tc::BM, splits);
+    tc::k_gemm_tc<AT, BT, EPI, 256><<<grid, tc::THREADS, tc::Cfg<256>::SMEM, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+  } else {
+    dim3 grid(N / 128, M / tc::BM, splits);
+    tc::k_gemm_tc<AT, BT, EPI, 128><<<grid, tc::THREADS, tc::Cfg<128>::SMEM, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+  }
   return ESR_OK;
 }
 
