@@ -641,7 +641,9 @@ int launch_gemm_tc(int M, int N, int K, int splits, const bf16* A, int lda, cons
                          tc::Cfg<256>::SMEM);
     attr_set = true;
   }
-  if (N % 256 == 0) {   // the whole 256-wide output row block per CTA
+  // 256-wide tiles (A read once per row block) when there are still enough
+  // of them to give every SM one; otherwise 128-wide tiles for parallelism
+  if (N % 256 == 0 && (long long)(M / tc::BM) * (N / 256) * splits >= 148) {
     dim3 grid(N / 256, M / tc::BM, splits);
     tc::k_gemm_tc<AT, BT, EPI, 256><<<grid, tc::THREADS, tc::Cfg<256>::SMEM, st>>>(M, N, K / splits, A, lda, B, ldb, e);
   } else {
