@@ -30,6 +30,7 @@ from __future__ import annotations
 import io
 import json
 import pickle
+import os
 from pathlib import Path
 from typing import Any
 
@@ -312,7 +313,10 @@ class Mesh:
         """Write the extended ``graph.npz``."""
         path = Path(path)
         path.parent.mkdir(parents=True, exist_ok=True)
-        np.savez_compressed(path, **self.graph_arrays(W_snapshots, inlet_state))
+        # write aside and rename: several processes may cache the same mesh at once
+        tmp = path.with_name(f".{path.stem}.{os.getpid()}.tmp.npz")
+        np.savez_compressed(tmp, **self.graph_arrays(W_snapshots, inlet_state))
+        os.replace(tmp, path)
         return path
 
     @classmethod

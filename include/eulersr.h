@@ -24,6 +24,12 @@
  *   esr_batch_solve      the serial grid loop of slurm/run_euler_grid.py:94-104,
  *                        run as one batch with retire/refill
  *   esr_idw_apply        eval/core.py:135-142 predict_idw (weights utils/metrics.py:9-14)
+ *   esr_set_cases /      esr_set_case / esr_get_state for many slots at once (the
+ *   esr_get_states       per-case initialize + np.asarray(W) of the grid loop)
+ *   esr_gemm_bf16 and    the network forward/backward that produces the warm start
+ *   the esr_mlp_*        (models/dam.py:306-308 with loss.py:20-23), here a residual
+ *                        MLP on IDW
+ *   esr_solver_tuning    no counterpart (XLA chooses launch shapes itself)
  *
  * Threading: a solver handle owns one CUDA stream and must not be used from
  * two threads at once. Handles of different solvers are independent.
