@@ -1,6 +1,6 @@
 """Learned warm start on NACA2412: train the model, compare warm vs cold HR solves.
 
-    python -m eulersr_b200.warmstart.run --n-train 512 --n-eval 128 --out warm.json
+    python -m eulersr_b200.warmstart.run --n-train 2048 --n-eval 256 --out warm.json
 
 Geometry NACA2412, HR h=0.025, LR h=0.1; cases (Mach ~ U[0.7, 3], alpha ~
 U[-5, 5]) from default_rng(3): the first n_train train, the next n_eval are
@@ -93,7 +93,7 @@ def main(argv=None):
     ap.add_argument("--geom", default="naca2412")
     ap.add_argument("--h-hr", type=float, default=0.025)
     ap.add_argument("--h-lr", type=float, default=0.1)
-    ap.add_argument("--n-train", type=int, default=512)
+    ap.add_argument("--n-train", type=int, default=2048)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--lr-steps", type=int, default=6000)
