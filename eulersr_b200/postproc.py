@@ -150,3 +150,35 @@ def shock_angle_deg(mesh, W, le=(1.0, 2.0), chord=1.0, gamma=1.4, p_inf=1.0, x_r
     X, Y = np.asarray(pts).T
     slope = np.polyfit(X, Y, 1)[0]
     return math.degrees(math.atan(slope))
+
+
+def validate_diamond(h=0.025, machs=(1.5, 2.0), precision="f64"):
+    """Converged diamond solves (alpha 0) against shock-expansion theory, as
+    euler/postproc/theory_validation_diamond.py does: CD error and the
+    leading-edge shock-angle error per Mach. Needs the GPU library."""
+    import numpy as np
+    from .meshing import build_mesh
+    from .solver import FlowCase, Solver
+    mesh = build_mesh("diamond", h)
+    rows = []
+    for M in machs:
+        th = diamond_theory(M, 0.0, half_angle_deg=5.0)
+        s = Solver(mesh, 1, precision=precision, threshold=1e-5, check_every=25)
+        s.set_case(0, FlowCase(mach=M, aoa_deg=0.0, cfl=0.6, tf=30.0,
+                               dtype=np.float64 if precision == "f64" else np.float32))
+        r = s.run()[0]
+        beta = shock_angle_deg(mesh, s.get_state(0), le=(1.0, 2.0))
+        rows.append({"mach": M, "cells": mesh.n_cells, "converged": bool(r["converged"]), "steps": int(r["steps"]),
+                     "cd": float(r["cd"]), "cd_theory": th.cd, "cd_err": abs(r["cd"] - th.cd) / th.cd,
+                     "beta_deg": float(beta), "beta_theory_deg": th.beta_upper_deg,
+                     "beta_err_deg": abs(beta - th.beta_upper_deg)})
+        s.close()
+    return rows
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+    prec = sys.argv[1] if len(sys.argv) > 1 else "f64"
+    for row in validate_diamond(precision=prec):
+        print(json.dumps(row))

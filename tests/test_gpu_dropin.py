@@ -190,7 +190,7 @@ def diamond_hr():
 
 
 def test_diamond_shock_expansion_validation(diamond_hr):
-    """Configs 1-2 checks at the reference's published validation point
+    """The diamond checks at the reference's published validation point
     (diamond h=0.025, M=1.5, alpha=0; README.md:54-55 reports 1.8 % CD error
     and a 0.83 deg shock-angle error): converged CD vs shock-expansion theory,
     the leading-edge shock angle, and FP32 vs the FP64 build of the same
