@@ -95,7 +95,7 @@ def main(argv=None):
     ap.add_argument("--h-lr", type=float, default=0.1)
     ap.add_argument("--n-train", type=int, default=2048)
     ap.add_argument("--n-eval", type=int, default=256)
-    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--slots", type=int, default=32)
     ap.add_argument("--lr-steps", type=int, default=6000)
     ap.add_argument("--target-steps", type=int, default=20000)
     ap.add_argument("--ref-steps", type=int, default=30000)
