@@ -56,7 +56,8 @@ class Case(C.Structure):
                 ("cfl", C.c_double), ("tf", C.c_double), ("max_steps", C.c_int64), ("inlet", C.c_double * 4),
                 ("rho_inf", C.c_double), ("u_inf", C.c_double), ("l_ref", C.c_double),
                 ("eng_track", C.c_int32), ("eng_patience", C.c_int32), ("eng_target_cd", C.c_double),
-                ("eng_target_cl", C.c_double), ("eng_cd_tol", C.c_double), ("eng_cl_tol", C.c_double)]
+                ("eng_target_cl", C.c_double), ("eng_cd_tol", C.c_double), ("eng_cl_tol", C.c_double),
+                ("threshold", C.c_double)]
 
 
 class Result(C.Structure):

@@ -670,6 +670,7 @@ struct CaseCtl {             // mutable per-slot control words (device)
   int* eng_stop;
   int* eng_stopping;
   const double* forces;      // cd, cl per slot at the current check
+  const double* thr;         // per-slot stop-rule threshold, <= 0: the solver's
 };
 
 // step-0 engineering state of freshly filled slots (euler/main.py:107-111)
@@ -725,7 +726,8 @@ static __global__ void k_check(CaseCtl cc, int n_slots, int pos, const double2* 
   else rel = sqrt(s0 / (double)ncells[g]);
   cc.last_rel[g] = rel;
   const bool finite = isfinite(s0) && isfinite(s1);
-  const bool under = rel <= threshold;
+  const double th = cc.thr[g] > 0.0 ? cc.thr[g] : threshold;
+  const bool under = rel <= th;
   const int streak = cc.streak[g];
   const int nstreak = under ? streak + 1 : 0;
   if (under && streak == 0) cc.streak_start[g] = done;
@@ -837,6 +839,7 @@ struct Queue {
   const int* c_eng_track;
   const int* c_eng_pat;
   const double4* c_eng_t;
+  const double* c_thr;
   const double* init;          // warm-start rows (caller cell order), or null
   const long long* init_off;   // per case first row in `init`, -1 = freestream
   // per case results
@@ -870,6 +873,7 @@ struct SlotParams {
   int* eng_track;
   int* eng_pat;
   double4* eng_t;
+  double* thr;
 };
 
 static __global__ void k_mark_retiring(const int* __restrict__ status, int n_slots, int* __restrict__ slot_case,
@@ -964,6 +968,7 @@ __global__ void k_assign(const Seg<T>* __restrict__ segs, int n_segs, Queue<T> q
     sp.eng_track[g] = q.c_eng_track[c];
     sp.eng_pat[g] = q.c_eng_pat[c];
     sp.eng_t[g] = q.c_eng_t[c];
+    sp.thr[g] = q.c_thr[c];
     cc.step[g] = 0;
     cc.ref_step[g] = 0;
     cc.streak[g] = 0;
@@ -1005,7 +1010,7 @@ __global__ void k_fill_slots(const Seg<T>* __restrict__ segs, CaseMap cm, Queue<
 template <typename T>
 struct SlotInit {
   V4<T> inlet;
-  double cfl, tf, qref;
+  double cfl, tf, qref, thr;
   long long max_steps;
   double4 eng_t;
   T strength;
@@ -1028,6 +1033,7 @@ __global__ void k_init_slots(const SlotInit<T>* __restrict__ si, int n, SlotPara
   sp.eng_track[g] = x.eng_track;
   sp.eng_pat[g] = x.eng_pat;
   sp.eng_t[g] = x.eng_t;
+  sp.thr[g] = x.thr;
   cc.step[g] = 0;
   cc.ref_step[g] = 0;
   cc.streak[g] = 0;
@@ -1090,6 +1096,7 @@ __global__ void k_compact_slots(const int* __restrict__ move_src, int n_slots, Q
   sp.dt[g] = sp.dt[o]; sp.inlet[g] = sp.inlet[o]; sp.strength[g] = sp.strength[o]; sp.cfl[g] = sp.cfl[o];
   sp.tf[g] = sp.tf[o]; sp.max_steps[g] = sp.max_steps[o]; sp.qref[g] = sp.qref[o];
   sp.eng_track[g] = sp.eng_track[o]; sp.eng_pat[g] = sp.eng_pat[o]; sp.eng_t[g] = sp.eng_t[o];
+  sp.thr[g] = sp.thr[o];
   cc.active[g] = cc.active[o]; cc.step[g] = cc.step[o]; cc.nmax[g] = cc.nmax[o]; cc.ref_step[g] = cc.ref_step[o];
   cc.streak[g] = cc.streak[o]; cc.streak_start[g] = cc.streak_start[o]; cc.stopping_step[g] = cc.stopping_step[o];
   cc.status[g] = cc.status[o]; cc.due[g] = cc.due[o]; cc.last_rel[g] = cc.last_rel[o];

@@ -111,7 +111,7 @@ struct SolverT : SolverBase {
   DevBuf<double> cfl, tf, qref, forces;
   DevBuf<long long> max_steps, t_start, t_end;
   DevBuf<int> active, step, nmax, nmax_inf, ref_step, streak, streak_start, stopping, status, due, fill;
-  DevBuf<double> last_rel;
+  DevBuf<double> last_rel, thr;
   DevBuf<int> eng_track, eng_patience, eng_streak, eng_start, eng_stop, eng_stopping;
   DevBuf<double4> eng_t;
   DevBuf<double2> partial;
@@ -165,6 +165,7 @@ struct SolverT : SolverBase {
     c.last_rel = last_rel.p; c.t_start = t_start.p; c.t_end = t_end.p;
     c.eng_track = eng_track.p; c.eng_patience = eng_patience.p; c.eng_t = eng_t.p; c.eng_streak = eng_streak.p;
     c.eng_start = eng_start.p; c.eng_stop = eng_stop.p; c.eng_stopping = eng_stopping.p; c.forces = forces.p;
+    c.thr = thr.p;
     return c;
   }
   CaseMap cmap() { return CaseMap{d_case_seg.p, d_case_slot.p}; }
@@ -286,6 +287,8 @@ struct SolverT : SolverBase {
     for (DevBuf<int>* b : {&active, &step, &nmax, &nmax_inf, &ref_step, &streak, &streak_start, &stopping, &status, &due, &fill})
       ESR_TRY(b->alloc(n_slots));
     ESR_TRY(last_rel.alloc(n_slots));
+    ESR_TRY(thr.alloc(n_slots));
+    ESR_CUDA(cudaMemsetAsync(thr.p, 0, n_slots * sizeof(double), stream));
     for (DevBuf<int>* b : {&eng_track, &eng_patience, &eng_streak, &eng_start, &eng_stop, &eng_stopping}) {
       ESR_TRY(b->alloc(n_slots));
       ESR_CUDA(cudaMemsetAsync(b->p, 0, n_slots * sizeof(int), stream));
@@ -626,6 +629,8 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpyAsync(eng_track.p + slot, &etrack, sizeof(int), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemcpyAsync(eng_patience.p + slot, &epat, sizeof(int), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemcpyAsync(eng_t.p + slot, &et, sizeof(double4), cudaMemcpyHostToDevice, stream));
+    const double th = c->threshold;
+    ESR_CUDA(cudaMemcpyAsync(thr.p + slot, &th, sizeof(double), cudaMemcpyHostToDevice, stream));
     const int tb = 256, nb = (N + tb - 1) / tb;
     if (W_init) {
       if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
@@ -701,6 +706,7 @@ struct SolverT : SolverBase {
       case_params(c, x.inlet, x.strength, x.qref, x.eng_t, x.eng_track, x.eng_pat);
       x.cfl = c.cfl;
       x.tf = c.tf;
+      x.thr = c.threshold;
       x.max_steps = c.max_steps;
       hcase[slots[i]] = c;
       if (W_init && W_init[i]) { off[i] = rows; rows += meshes[m]->hm->n_cells; }
@@ -709,7 +715,7 @@ struct SolverT : SolverBase {
     if (d_init.n < (size_t)n) ESR_TRY(d_init.alloc(n));
     ESR_CUDA(cudaMemcpyAsync(d_init.p, hi.data(), n * sizeof(SlotInit<T>), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemsetAsync(fill.p, 0, n_slots * sizeof(int), stream));
-    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p};
+    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
     k_init_slots<T><<<(n + 127) / 128, 128, 0, stream>>>(d_init.p, n, sp, ctl(), fill.p);
     ++launches;
     for (int i = 0; i < n; ++i) {
@@ -997,7 +1003,7 @@ struct SolverT : SolverBase {
         r_eng_conv, r_eng_stop, n_done;
     DevBuf<V> c_inlet;
     DevBuf<T> c_strength;
-    DevBuf<double> c_cfl, c_tf, c_qref, r_dt, r_rel, r_cd, r_cl, r_time, r_probe, init, out;
+    DevBuf<double> c_cfl, c_tf, c_qref, c_thr, r_dt, r_rel, r_cd, r_cl, r_time, r_probe, init, out;
     DevBuf<long long> c_max_steps, init_off, out_off;
     DevBuf<double4> c_eng_t;
   };
@@ -1077,7 +1083,7 @@ struct SolverT : SolverBase {
     qoff[nm] = (int)qlist.size();
     std::vector<V> hin(n);
     std::vector<T> hstr(n);
-    std::vector<double> hcfl(n), htf(n), hq(n);
+    std::vector<double> hcfl(n), htf(n), hq(n), hthr(n);
     std::vector<long long> hms(n), hinit_off(n, -1), hout_off(n, 0);
     std::vector<int> htr(n), hpat(n);
     std::vector<double4> het(n);
@@ -1086,6 +1092,7 @@ struct SolverT : SolverBase {
       case_params(cs[i], hin[i], hstr[i], hq[i], het[i], htr[i], hpat[i]);
       hcfl[i] = cs[i].cfl;
       htf[i] = cs[i].tf;
+      hthr[i] = cs[i].threshold;
       hms[i] = cs[i].max_steps;
       const int N = meshes[cs[i].mesh]->hm->n_cells;
       if (init && init[i]) { hinit_off[i] = init_rows; init_rows += N; }
@@ -1106,6 +1113,7 @@ struct SolverT : SolverBase {
     ESR_TRY(up(B.c_cfl, hcfl));
     ESR_TRY(up(B.c_tf, htf));
     ESR_TRY(up(B.c_qref, hq));
+    ESR_TRY(up(B.c_thr, hthr));
     ESR_TRY(up(B.c_max_steps, hms));
     ESR_TRY(up(B.c_eng_track, htr));
     ESR_TRY(up(B.c_eng_pat, hpat));
@@ -1139,11 +1147,11 @@ struct SolverT : SolverBase {
     if (want_states) ESR_TRY(B.out.alloc((size_t)4 * out_rows));
     ESR_CUDA(cudaStreamSynchronize(stream));   // host vectors above are the copy sources
     Queue<T> q{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
-               B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p,
+               B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p, B.c_thr.p,
                init_rows > 0 ? B.init.p : nullptr, B.init_off.p, B.r_status.p, B.r_stop.p, B.r_steps.p, B.r_nmax.p,
                B.r_dt.p, B.r_rel.p, B.r_cd.p, B.r_cl.p, B.r_time.p, B.r_eng_conv.p, B.r_eng_stop.p, B.r_probe.p,
                want_states ? B.out.p : nullptr, B.out_off.p, B.n_done.p};
-    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p};
+    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
     ESR_CUDA(cudaEventRecord(ev0, stream));
     issue_refill(q, sp, want_states);   // first fill of every slot
     // the chunk graph of this batch: steps, checks, then the refill sequence

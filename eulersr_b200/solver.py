@@ -55,6 +55,7 @@ class FlowCase:
     eng_cd_tol: float = 0.001
     eng_cl_tol: float = 0.001
     eng_patience: int = 0                  # 0: the solver's stop-rule patience
+    threshold: float | None = None         # this case's stop-rule threshold (None: the solver's)
 
     def to_c(self) -> F.Case:
         c = F.Case()
@@ -70,6 +71,7 @@ class FlowCase:
         c.rho_inf = float(self.rho_inf)
         c.u_inf = float(self.mach * math.sqrt(self.gamma * self.p_inf / self.rho_inf))
         c.l_ref = float(self.l_ref)
+        c.threshold = float(self.threshold) if self.threshold is not None else 0.0
         if self.eng_target_cd is not None and self.eng_target_cl is not None:
             c.eng_track = 1
             c.eng_patience = int(self.eng_patience)

@@ -145,6 +145,10 @@ typedef struct esr_case {
     int32_t eng_patience;
     double eng_target_cd, eng_target_cl;
     double eng_cd_tol, eng_cl_tol;
+    /* stop-rule threshold of this case; <= 0: the solver's esr_params.threshold
+     * (eval/convergence_case.py:61-65 gives each case its own: the reference
+     * field's one-step residual x 1.001) */
+    double threshold;
 } esr_case;
 
 typedef struct esr_result {

@@ -256,3 +256,21 @@ def test_batch_edge_cases(diamond02):
         r1 = one.run()[0]
         assert r1['stopping_step'] == res[i]['stopping_step'] and r1['status'] == res[i]['status']
         assert np.array_equal(one.get_state(0), states[i])
+
+
+def test_per_case_threshold(diamond02):
+    """esr_case.threshold overrides the solver's stop-rule threshold for that
+    case (batch and single-slot paths alike), as eval/convergence_case.py
+    gives each case its own."""
+    from eulersr_b200.solver import Solver, FlowCase
+    thr = [3e-4, 5e-5, None]
+    cases = [FlowCase(mach=2.0, aoa_deg=2.0, cfl=0.6, tf=2.0, threshold=t, dtype=np.float32) for t in thr]
+    s = Solver(diamond02, 2, precision='f32', threshold=1e-3, check_every=10, patience=2)
+    res, _ = s.batch_solve(cases)
+    for c, t, r in zip(cases, thr, res):
+        one = Solver(diamond02, 1, precision='f32', threshold=t if t is not None else 1e-3, check_every=10,
+                     patience=2)
+        one.set_case(0, FlowCase(mach=2.0, aoa_deg=2.0, cfl=0.6, tf=2.0, dtype=np.float32))
+        r1 = one.run()[0]
+        assert (r1['stopping_step'], r1['status']) == (r['stopping_step'], r['status']), (t, r1, r)
+    assert res[1]['stopping_step'] > res[0]['stopping_step'] > res[2]['stopping_step']
