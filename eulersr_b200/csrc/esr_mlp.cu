@@ -14,7 +14,9 @@
 // The 4-wide head, the loss, AdamW and the fixed-order reductions are plain
 // SIMT kernels. Every reduction is deterministic (no atomics).
 #include <cuda_bf16.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include <string>
@@ -354,13 +356,13 @@ __global__ void k_adamw(float* __restrict__ p, const float* __restrict__ g, floa
 }
 
 // ------------------------------------------------------ tcgen05 GEMM path
-// The same C = A B with the fifth-generation tensor cores: operands staged
-// in shared memory in the 128-byte swizzled canonical layouts the UMMA
-// descriptors describe, one thread issues tcgen05.mma (128 x 128 x 16, BF16
-// in, FP32 accumulators in tensor memory), tcgen05.commit signals an
-// mbarrier per pipeline stage, and the epilogue reads the accumulators back
-// with tcgen05.ld, stages them in shared memory and applies the epilogue in
-// row-contiguous order. Tiles 128 x 128 x 64, 3 stages (96 KB), 256 threads.
+// The same C = A B with the fifth-generation tensor cores: TMA boxes bring
+// the operands into shared memory in the 128-byte swizzled canonical layouts
+// the UMMA descriptors describe, one thread issues the loads and
+// tcgen05.mma (128 x N x 16, BF16 in, FP32 accumulators in tensor memory),
+// mbarriers track each stage (tiles landed / MMAs done reading), and the
+// epilogue reads the accumulators back with tcgen05.ld, stages them in shared
+// memory and applies the epilogue in row-contiguous order.
 namespace tc {
 
 constexpr int BM = 128, BK = 64, THREADS = 256;
@@ -377,7 +379,7 @@ struct Cfg {
   static constexpr int STAGES = TBN == 256 ? 2 : 3;
   static constexpr int B_BYTES = TBN * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + (STAGES + 1) * 8 + 16;
+  static constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 2 * STAGES * 8 + 16;
   static_assert(BM * SLD * 4 <= STAGES * STAGE_BYTES, "accumulator staging must fit the pipeline buffers");
 };
 
@@ -400,7 +402,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   atomicExch(&g_tc_error, 1);
   return false;
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
@@ -433,6 +434,17 @@ __device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b, uint
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
 }
+// TMA: one 2-D box of a tensor map into shared memory, completion counted in
+// bytes on an mbarrier (no multicast)
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t v[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
@@ -442,33 +454,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t v[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// Byte offset of the 16-byte chunk (row, chunk) of a swizzled tile.
-// K-major tile (128 rows x 64 K): row r, chunk c of 8 K-elements.
-__device__ __forceinline__ uint32_t off_k(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }
-// MN-major tile (64 K-rows x 128 MN): K-row k, chunk c of 8 MN-elements;
-// MN groups of 64 are 8 KB apart, K groups of 8 rows 1 KB apart.
-__device__ __forceinline__ uint32_t off_mn(int k, int c) {
-  return (c >> 3) * 8192 + (k >> 3) * 1024 + (k & 7) * 128 + (((c & 7) ^ (k & 7)) << 4);
-}
+// Shared-memory tile layouts (what the TMA boxes with the 128-byte swizzle
+// produce and the UMMA descriptors describe). K-major tile (rows x 64 K):
+// row r at r * 128 B, its 16-byte chunk c at ((c ^ (r & 7)) * 16). MN-major
+// tile (64 K-rows x MN): groups of 64 MN elements 8 KB apart, K-row k of a
+// group at (k >> 3) * 1024 + (k & 7) * 128 B, chunk c at ((c ^ (k & 7)) * 16).
 
 template <bool A_T, bool B_T, int EPI, int TBN>
-__global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, const bf16* __restrict__ A, int lda,
-                                                     const bf16* __restrict__ B, int ldb, Epi e) {
+__global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, const __grid_constant__ CUtensorMap tmA,
+                                                     const __grid_constant__ CUtensorMap tmB, Epi e) {
   using C = Cfg<TBN>;
   constexpr int BN = C::BN, STAGES = C::STAGES, STAGE_BYTES = C::STAGE_BYTES;
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = saddr(smem_raw);
   const uint32_t tiles = (raw + 1023u) & ~1023u;                   // swizzle atoms need 1 KB alignment
   unsigned char* gtiles = smem_raw + (tiles - raw);
-  const uint32_t bars = tiles + STAGES * STAGE_BYTES;              // STAGES + 1 mbarriers
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * STAGE_BYTES + (STAGES + 1) * 8);
+  const uint32_t empty = tiles + STAGES * STAGE_BYTES;             // per stage: MMAs done reading it
+  const uint32_t full = empty + STAGES * 8;                        // per stage: its tiles have landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * STAGE_BYTES + 2 * STAGES * 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m_blk = blockIdx.y * BM, n_blk = blockIdx.x * BN;
   const int k_begin = blockIdx.z * K_split;
   const int KT = K_split / BK;
 
   if (tid == 0) {
-    for (int s = 0; s <= STAGES; ++s) mbar_init(bars + 8 * s, 1);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(empty + 8 * s, 1);
+      mbar_init(full + 8 * s, 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {   // BN TMEM columns: the 128 x BN FP32 accumulator
@@ -480,66 +493,47 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  auto load_tile = [&](int stage, int kt) {
-    const int k0 = k_begin + kt * BK;
-    unsigned char* a = gtiles + stage * STAGE_BYTES;
-    unsigned char* b = a + A_BYTES;
+  // One thread is both the TMA producer and the MMA issuer; the other warps
+  // wait for the last MMA and then run the epilogue.
+  if (warp == 0) {
+    if (lane == 0) {
+      // the tiles of K-block kt into stage s: K-major boxes are 64 K x rows,
+      // MN-major boxes 64 MN x 64 K, one per 64-element MN group (8 KB apart)
+      auto produce = [&](int kt, int s) {
+        const int k0 = k_begin + kt * BK;
+        const uint32_t a = tiles + s * STAGE_BYTES, b = a + A_BYTES, bar = full + 8 * s;
+        mbar_expect_tx(bar, STAGE_BYTES);
+        if (!A_T) tma_load_2d(a, &tmA, k0, m_blk, bar);
+        else for (int g = 0; g < BM / 64; ++g) tma_load_2d(a + g * 8192, &tmA, m_blk + 64 * g, k0, bar);
+        if (!B_T) tma_load_2d(b, &tmB, k0, n_blk, bar);
+        else for (int g = 0; g < BN / 64; ++g) tma_load_2d(b + g * 8192, &tmB, n_blk + 64 * g, k0, bar);
+      };
+      constexpr uint32_t idesc = instr_desc<A_T, B_T, BN>();
+      for (int p = 0; p < STAGES && p < KT; ++p) produce(p, p);
+      for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt % STAGES;
+        mbar_wait(full + 8 * s, (kt / STAGES) & 1);
+        tc_fence_after();
+        const uint32_t a = tiles + s * STAGE_BYTES, b = a + A_BYTES;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = tid + i * THREADS;   // 1024 chunks of 16 B in the A tile
-      if (!A_T) {
-        const int r = c >> 3, ch = c & 7;
-        cp_async16(a + off_k(r, ch), A + (size_t)(m_blk + r) * lda + k0 + ch * 8);
-      } else {
-        const int k = c >> 4, ch = c & 15;
-        cp_async16(a + off_mn(k, ch), A + (size_t)(k0 + k) * lda + m_blk + ch * 8);
+        for (int j = 0; j < BK / 16; ++j) {   // K = 16 per instruction
+          const uint64_t ad = A_T ? smem_desc(a + j * 2048, 8192, 1024) : smem_desc(a + j * 32, 16, 1024);
+          const uint64_t bd = B_T ? smem_desc(b + j * 2048, 8192, 1024) : smem_desc(b + j * 32, 16, 1024);
+          umma(tmem, ad, bd, idesc, (kt | j) != 0);
+        }
+        umma_commit(empty + 8 * s);   // arrives when these MMAs (and all earlier ones) are done
+        // refill the stage the MMAs of the previous K-block read, once they are done
+        const int nxt = kt - 1 + STAGES;
+        if (kt >= 1 && nxt < KT) {
+          const int ps = (kt - 1) % STAGES;
+          mbar_wait(empty + 8 * ps, ((kt - 1) / STAGES) & 1);
+          produce(nxt, ps);
+        }
       }
     }
-#pragma unroll
-    for (int i = 0; i < BN / 32; ++i) {
-      const int c = tid + i * THREADS;   // BN * 8 chunks in the B tile
-      if (!B_T) {
-        const int r = c >> 3, ch = c & 7;
-        cp_async16(b + off_k(r, ch), B + (size_t)(n_blk + r) * ldb + k0 + ch * 8);
-      } else {
-        const int k = c / (BN / 8), ch = c % (BN / 8);
-        cp_async16(b + off_mn(k, ch), B + (size_t)(k0 + k) * ldb + n_blk + ch * 8);
-      }
-    }
-  };
-
-  constexpr uint32_t idesc = instr_desc<A_T, B_T, BN>();
-#pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < KT) load_tile(s, s);
-    cp_async_commit();
+    __syncwarp();
   }
-  for (int kt = 0; kt < KT; ++kt) {
-    cp_async_wait<STAGES - 2>();
-    fence_proxy_async();            // this thread's tile writes -> visible to the tensor core's async proxy
-    __syncthreads();
-    const int s = kt % STAGES;
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t a = tiles + s * STAGE_BYTES, b = a + A_BYTES;
-#pragma unroll
-      for (int j = 0; j < BK / 16; ++j) {   // K = 16 per instruction
-        const uint64_t ad = A_T ? smem_desc(a + j * 2048, 8192, 1024) : smem_desc(a + j * 32, 16, 1024);
-        const uint64_t bd = B_T ? smem_desc(b + j * 2048, 8192, 1024) : smem_desc(b + j * 32, 16, 1024);
-        umma(tmem, ad, bd, idesc, (kt | j) != 0);
-      }
-      umma_commit(bars + 8 * s);     // arrives when these MMAs (and all earlier ones) are done
-    }
-    const int pf = kt + STAGES - 1;
-    if (pf < KT) {
-      // the stage being refilled was read by the MMAs of iteration kt - 1
-      if (kt >= 1) mbar_wait(bars + 8 * ((kt - 1) % STAGES), ((kt - 1) / STAGES) & 1);
-      load_tile(pf % STAGES, pf);
-    }
-    cp_async_commit();
-  }
-  cp_async_wait<0>();
-  mbar_wait(bars + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
+  mbar_wait(empty + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
   tc_fence_after();
 
   // Accumulators -> shared memory (the pipeline buffers are free now), 128
@@ -630,6 +624,31 @@ int launch_gemm(int M, int N, int K, int splits, const bf16* A, int lda, const b
   return ESR_OK;
 }
 
+// 2-D BF16 tensor map: `inner` contiguous elements per row, `outer` rows,
+// rows `ld` elements apart; boxes of box_in x box_out with the 128-byte swizzle
+// the UMMA descriptors expect
+int make_map(CUtensorMap* map, const bf16* base, uint64_t inner, uint64_t outer, uint64_t ld, uint32_t box_in,
+             uint32_t box_out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q{};
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return mfail(ESR_ERR_CUDA, "gemm: cuTensorMapEncodeTiled is not available");
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[2] = {inner, outer};
+  const cuuint64_t strides[1] = {ld * sizeof(bf16)};
+  const cuuint32_t box[2] = {box_in, box_out};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return mfail(ESR_ERR_ARG, "gemm: tensor map rejected (error " + std::to_string((int)r) + ")");
+  return ESR_OK;
+}
+
 template <bool AT, bool BT, int EPI>
 int launch_gemm_tc(int M, int N, int K, int splits, const bf16* A, int lda, const bf16* B, int ldb, const Epi& e,
                    cudaStream_t st) {
@@ -643,12 +662,18 @@ int launch_gemm_tc(int M, int N, int K, int splits, const bf16* A, int lda, cons
   }
   // 256-wide tiles (A read once per row block) when there are still enough
   // of them to give every SM one; otherwise 128-wide tiles for parallelism
-  if (N % 256 == 0 && (long long)(M / tc::BM) * (N / 256) * splits >= 148) {
+  const int tbn = (N % 256 == 0 && (long long)(M / tc::BM) * (N / 256) * splits >= 148) ? 256 : 128;
+  CUtensorMap ma, mb;
+  int rc = AT ? make_map(&ma, A, M, K, lda, 64, 64) : make_map(&ma, A, K, M, lda, 64, tc::BM);
+  if (rc != ESR_OK) return rc;
+  rc = BT ? make_map(&mb, B, N, K, ldb, 64, 64) : make_map(&mb, B, K, N, ldb, 64, tbn);
+  if (rc != ESR_OK) return rc;
+  if (tbn == 256) {
     dim3 grid(N / 256, M / tc::BM, splits);
-    tc::k_gemm_tc<AT, BT, EPI, 256><<<grid, tc::THREADS, tc::Cfg<256>::SMEM, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+    tc::k_gemm_tc<AT, BT, EPI, 256><<<grid, tc::THREADS, tc::Cfg<256>::SMEM, st>>>(M, N, K / splits, ma, mb, e);
   } else {
     dim3 grid(N / 128, M / tc::BM, splits);
-    tc::k_gemm_tc<AT, BT, EPI, 128><<<grid, tc::THREADS, tc::Cfg<128>::SMEM, st>>>(M, N, K / splits, A, lda, B, ldb, e);
+    tc::k_gemm_tc<AT, BT, EPI, 128><<<grid, tc::THREADS, tc::Cfg<128>::SMEM, st>>>(M, N, K / splits, ma, mb, e);
   }
   return ESR_OK;
 }
