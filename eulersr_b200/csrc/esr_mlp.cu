@@ -379,7 +379,7 @@ struct Cfg {
   static constexpr int STAGES = TBN == 256 ? 2 : 3;
   static constexpr int B_BYTES = TBN * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 2 * STAGES * 8 + 16;
+  static constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + (2 * STAGES + 1) * 8 + 16;
   static_assert(BM * SLD * 4 <= STAGES * STAGE_BYTES, "accumulator staging must fit the pipeline buffers");
 };
 
@@ -471,7 +471,8 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
   unsigned char* gtiles = smem_raw + (tiles - raw);
   const uint32_t empty = tiles + STAGES * STAGE_BYTES;             // per stage: MMAs done reading it
   const uint32_t full = empty + STAGES * 8;                        // per stage: its tiles have landed
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * STAGE_BYTES + 2 * STAGES * 8);
+  const uint32_t done = full + STAGES * 8;                         // all MMAs of the tile are done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gtiles + STAGES * STAGE_BYTES + (2 * STAGES + 1) * 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m_blk = blockIdx.y * BM, n_blk = blockIdx.x * BN;
   const int k_begin = blockIdx.z * K_split;
@@ -482,6 +483,7 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
       mbar_init(empty + 8 * s, 1);
       mbar_init(full + 8 * s, 1);
     }
+    mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {   // BN TMEM columns: the 128 x BN FP32 accumulator
@@ -530,10 +532,14 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
           produce(nxt, ps);
         }
       }
+      umma_commit(done);   // its one phase completes when every MMA of the tile has
     }
     __syncwarp();
   }
-  mbar_wait(empty + 8 * ((KT - 1) % STAGES), ((KT - 1) / STAGES) & 1);
+  // The other warps reach this wait while the mainloop is still running. A
+  // stage barrier cannot serve here: waiting on parity 1 of a barrier still in
+  // its first phase returns at once. `done` completes exactly once.
+  mbar_wait(done, 0);
   tc_fence_after();
 
   // Accumulators -> shared memory (the pipeline buffers are free now), 128
