@@ -83,3 +83,40 @@ def test_rcm_c_matches_contract(diamond02):
     assert np.array_equal(np.sort(perm), np.arange(diamond02.n_cells))
     assert bandwidth(shuffled, perm) <= 3 * bandwidth(diamond02)
     assert bandwidth(shuffled, perm) < bandwidth(shuffled) / 5
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every ctypes mirror in _ffi.py has the size and field offsets the C
+    compiler gives the header's struct (so a field added on one side only is
+    caught without a GPU)."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+    from eulersr_b200 import _ffi as F
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = {"esr_mesh_desc": F.MeshDesc, "esr_mesh_info": F.MeshInfo, "esr_params": F.Params,
+             "esr_case": F.Case, "esr_result": F.Result, "esr_kernel_times": F.KernelTimes,
+             "esr_tuning": F.Tuning}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "eulersr.h"', 'int main(void) {']
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    inc = Path(__file__).resolve().parents[1] / "include"
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(inc), str(src), "-o", str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            parts = line.split()
+            got[(parts[0], parts[1])] = int(parts[2])
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
