@@ -10,8 +10,9 @@ advances every case of the batch by ``--chunk`` SRK2 steps (default 50).
 value   cell-updates/s (one cell advanced one full SRK2 step), state resident
         in HBM, device time from CUDA events on the solver stream.
 e2e     the same through the public API with host buffers: every step uploads
-        the 256 initial fields from pinned host memory (esr_set_cases), runs
-        the chunk, and reads every final field back (esr_get_states).
+        the 256 initial fields (float32) from pinned host memory
+        (esr_set_cases_f32), runs the chunk, and reads every final field back
+        (esr_get_states_f32).
 roofline  the dominant kernel (K2 flux/update) against the measured HBM copy
         bandwidth; algorithmic bytes per launch = (40 + 64/B) B per cell and
         case, half of the (80 + 128/B) B of a full SRK2 cell-update.
@@ -443,14 +444,15 @@ def main():
     e2e = None
     if not args.no_e2e:
         sizes = [s._n_cells(b) for b in range(B)]
+        # float32 host fields for the float32 solver (the values it stores)
         try:
             import torch
-            pinned = [torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy() for n in sizes]
+            pinned = [torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy() for n in sizes]
         except Exception:
-            pinned = [np.empty((n, 4)) for n in sizes]
+            pinned = [np.empty((n, 4), dtype=np.float32) for n in sizes]
         from eulersr_b200.solver import freestream
         for b, c in enumerate(cases):
-            pinned[b][:] = freestream(c.mach, c.aoa_deg, dtype=np.float32).astype(np.float64)[None, :]
+            pinned[b][:] = freestream(c.mach, c.aoa_deg, dtype=np.float32)[None, :]
         h2d = int(sum(p.nbytes for p in pinned))
         outs = pinned  # results land in the same pinned buffers
         e2e_steps = max(2, min(args.steps, 5))
@@ -467,7 +469,7 @@ def main():
         e2e_val = allreduce_sum(float(N * B * args.chunk * e2e_steps), world) / el
         e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": h2d,
-               "api": "esr_set_cases (pinned host init fields) + esr_step + esr_get_states"}
+               "api": "esr_set_cases_f32 (pinned float32 host init fields) + esr_step + esr_get_states_f32"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

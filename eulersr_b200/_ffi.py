@@ -131,6 +131,8 @@ _SIGS = {
     "esr_solver_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "esr_set_cases": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(Case), C.c_void_p]),
     "esr_get_states": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "esr_set_cases_f32": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(Case), C.c_void_p]),
+    "esr_get_states_f32": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
     "esr_gemm_bf16": (C.c_int, _GEMM_ARGS),

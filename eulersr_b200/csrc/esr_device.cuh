@@ -1144,31 +1144,30 @@ __global__ void k_forces(const Seg<T>* __restrict__ segs, CaseMap cm, const V4<T
 }
 
 // ----------------------------------------------------------- state movers
-// host-order float64 rows -> device precision, cell c of the caller's order
-// goes to renumbered cell inv[c]
-template <typename T>
-__global__ void k_scatter_state(const double* __restrict__ src, const int* __restrict__ inv, int n_cells,
+// host-order rows (float64, or float32) -> device precision, cell c of the
+// caller's order goes to renumbered cell inv[c]
+template <typename T, typename S = double>
+__global__ void k_scatter_state(const S* __restrict__ src, const int* __restrict__ inv, int n_cells,
                                 V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, long long off, int B, int b) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_cells) return;
-  const double* r = src + 4 * (size_t)c;
+  const S* r = src + 4 * (size_t)c;
   const V4<T> w = mk4<T>((T)r[0], (T)r[1], (T)r[2], (T)r[3]);
   const long long gi = off + (long long)inv[c] * B + b;
   W[gi] = w;
   if (Wref) Wref[gi] = w;
 }
 
-template <typename T>
+template <typename T, typename S = double>
 __global__ void k_gather_state(const V4<T>* __restrict__ W, const int* __restrict__ inv, int n_cells,
-                               long long off, int B, int b, double* __restrict__ dst) {
+                               long long off, int B, int b, S* __restrict__ dst) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_cells) return;
   const V4<T> w = W[off + (long long)inv[c] * B + b];
-  double* r = dst + 4 * (size_t)c;
-  r[0] = (double)w.x; r[1] = (double)w.y; r[2] = (double)w.z; r[3] = (double)w.w;
+  S* r = dst + 4 * (size_t)c;
+  r[0] = (S)w.x; r[1] = (S)w.y; r[2] = (S)w.z; r[3] = (S)w.w;
 }
 
-// freestream fill of a slot: W = Wref = inlet
 // every item of W set to one state (the autotuner's workload)
 template <typename T>
 __global__ void k_fill_uniform(V4<T>* __restrict__ W, long long n, V4<T> w) {
@@ -1176,6 +1175,7 @@ __global__ void k_fill_uniform(V4<T>* __restrict__ W, long long n, V4<T> w) {
     W[i] = w;
 }
 
+// freestream fill of a slot: W = Wref = inlet
 template <typename T>
 __global__ void k_fill_freestream(V4<T>* __restrict__ W, V4<T>* __restrict__ Wref, int n_cells, long long off, int B,
                                   int b, V4<T> w) {

@@ -685,7 +685,9 @@ struct SolverT : SolverBase {
   // ---------------------------------------------- many slots at once
   DevBuf<double> stage_many;            // host rows of set_cases / get_states
   DevBuf<SlotInit<T>> d_init;
-  int set_cases(int n, const int32_t* slots, const esr_case* cs, const double* const* W_init) {
+  // S: the type of the caller's host rows (double, or float for float32 fields)
+  template <typename S>
+  int set_cases(int n, const int32_t* slots, const esr_case* cs, const S* const* W_init) {
     if (n < 0 || (n > 0 && (!slots || !cs))) return fail(ESR_ERR_ARG, "set_cases: bad arguments");
     if (n == 0) return ESR_OK;
     std::vector<SlotInit<T>> hi(n);
@@ -712,6 +714,7 @@ struct SolverT : SolverBase {
       if (W_init && W_init[i]) { off[i] = rows; rows += meshes[m]->hm->n_cells; }
     }
     if (rows > 0 && stage_many.n < (size_t)4 * rows) ESR_TRY(stage_many.alloc((size_t)4 * rows));
+    S* stage = reinterpret_cast<S*>(stage_many.p);   // room for 4 rows of doubles is room for floats
     if (d_init.n < (size_t)n) ESR_TRY(d_init.alloc(n));
     ESR_CUDA(cudaMemcpyAsync(d_init.p, hi.data(), n * sizeof(SlotInit<T>), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemsetAsync(fill.p, 0, n_slots * sizeof(int), stream));
@@ -724,9 +727,9 @@ struct SolverT : SolverBase {
       MeshDev& md = *meshes[m];
       const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
       if (off[i] >= 0) {
-        double* st = stage_many.p + 4 * off[i];
-        ESR_CUDA(cudaMemcpyAsync(st, W_init[i], (size_t)4 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
-        k_scatter_state<T><<<nb, tb, 0, stream>>>(st, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
+        S* st = stage + 4 * off[i];
+        ESR_CUDA(cudaMemcpyAsync(st, W_init[i], (size_t)4 * N * sizeof(S), cudaMemcpyHostToDevice, stream));
+        k_scatter_state<T, S><<<nb, tb, 0, stream>>>(st, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
       } else {
         k_fill_freestream<T><<<nb, tb, 0, stream>>>(W.p, Wref.p, N, md.off, md.B, b, hi[i].inlet);
       }
@@ -736,7 +739,8 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaStreamSynchronize(stream));   // hi and the caller's fields are the copy sources
     return ESR_OK;
   }
-  int get_states(int n, const int32_t* slots, double* const* out) {
+  template <typename S>
+  int get_states(int n, const int32_t* slots, S* const* out) {
     if (n < 0 || (n > 0 && (!slots || !out))) return fail(ESR_ERR_ARG, "get_states: bad arguments");
     long long rows = 0;
     std::vector<long long> off(n);
@@ -753,10 +757,10 @@ struct SolverT : SolverBase {
       ESR_TRY(mesh_of_slot(slots[i], m, b));
       MeshDev& md = *meshes[m];
       const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
-      double* st = stage_many.p + 4 * off[i];
-      k_gather_state<T><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, st);
+      S* st = reinterpret_cast<S*>(stage_many.p) + 4 * off[i];
+      k_gather_state<T, S><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, st);
       ++launches;
-      ESR_CUDA(cudaMemcpyAsync(out[i], st, (size_t)4 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      ESR_CUDA(cudaMemcpyAsync(out[i], st, (size_t)4 * N * sizeof(S), cudaMemcpyDeviceToHost, stream));
     }
     ESR_CUDA(cudaStreamSynchronize(stream));
     return ESR_OK;
@@ -1365,6 +1369,17 @@ int esr_set_cases(esr_solver* solver, int32_t n, const int32_t* slots, const esr
   ESR_GUARD_END
 }
 int esr_get_states(esr_solver* solver, int32_t n, const int32_t* slots, double* const* out) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.get_states(n, slots, out); });
+  ESR_GUARD_END
+}
+int esr_set_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                      const float* const* W_init) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.set_cases(n, slots, cases, W_init); });
+  ESR_GUARD_END
+}
+int esr_get_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out) {
   ESR_GUARD_BEGIN
   return dispatch(solver, [&](auto& s) { return s.get_states(n, slots, out); });
   ESR_GUARD_END

@@ -204,36 +204,46 @@ class Solver:
 
     def set_cases(self, slots, cases, W_inits=None):
         """set_case for many slots at once (one synchronisation). ``W_inits``:
-        None or a list with an (n_cells, 4) field or None per slot; pinned
-        float64 host arrays copy fastest."""
+        None or a list with an (n_cells, 4) field or None per slot. Fields that
+        are all float32 go through the float32 entry point (half the bytes);
+        pinned host arrays copy fastest."""
         n = len(slots)
         sl = np.ascontiguousarray(slots, dtype=np.int32)
         carr = (F.Case * n)(*[c.to_c() for c in cases])
+        given = [W for W in (W_inits or []) if W is not None]
+        f32 = bool(given) and all(np.asarray(W).dtype == np.float32 for W in given)
+        ctype = C.c_float if f32 else C.c_double
         keep, arr = [], None
         if W_inits is not None:
-            arr = (F._f64p * n)()
+            arr = (C.POINTER(ctype) * n)()
             for i, W in enumerate(W_inits):
                 if W is None:
                     continue
-                W = F.f64(W)
+                W = np.ascontiguousarray(W, dtype=np.float32 if f32 else np.float64)
                 if W.shape != (self._n_cells(int(sl[i])), 4):
                     raise ValueError(f"init field {i} has shape {W.shape}")
                 keep.append(W)
-                arr[i] = F.ptr(W, C.c_double)
-        F.check(F.lib().esr_set_cases(self.handle, n, F.ptr(sl, C.c_int32), carr, arr))
+                arr[i] = F.ptr(W, ctype)
+        fn = F.lib().esr_set_cases_f32 if f32 else F.lib().esr_set_cases
+        F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), carr, arr))
 
-    def get_states(self, slots, out=None):
-        """get_state for many slots at once into ``out`` (arrays (n_cells, 4)
-        float64, allocated when None); one synchronisation."""
+    def get_states(self, slots, out=None, dtype=np.float64):
+        """get_state for many slots at once into ``out`` (C-contiguous
+        (n_cells, 4) arrays of one dtype, float64 or float32; allocated with
+        ``dtype`` when None); one synchronisation."""
         n = len(slots)
         sl = np.ascontiguousarray(slots, dtype=np.int32)
         if out is None:
-            out = [np.empty((self._n_cells(int(g)), 4)) for g in sl]
+            out = [np.empty((self._n_cells(int(g)), 4), dtype=dtype) for g in sl]
+        f32 = out[0].dtype == np.float32 if n else False
+        want = np.float32 if f32 else np.float64
         for g, o in zip(sl, out):
-            if o.shape != (self._n_cells(int(g)), 4) or o.dtype != np.float64 or not o.flags.c_contiguous:
-                raise ValueError("get_states: outputs must be C-contiguous float64 (n_cells, 4)")
-        arr = (F._f64p * n)(*[F.ptr(o, C.c_double) for o in out])
-        F.check(F.lib().esr_get_states(self.handle, n, F.ptr(sl, C.c_int32), arr))
+            if o.shape != (self._n_cells(int(g)), 4) or o.dtype != want or not o.flags.c_contiguous:
+                raise ValueError("get_states: outputs must be C-contiguous (n_cells, 4) arrays of one dtype")
+        ctype = C.c_float if f32 else C.c_double
+        arr = (C.POINTER(ctype) * n)(*[F.ptr(o, ctype) for o in out])
+        fn = F.lib().esr_get_states_f32 if f32 else F.lib().esr_get_states
+        F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), arr))
         return out
 
     def set_state(self, slot: int, W):

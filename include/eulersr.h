@@ -203,6 +203,11 @@ int esr_set_cases(esr_solver* solver, int32_t n, const int32_t* slots, const esr
 /* esr_get_state for n slots at once into out[i] (caller's cell order); one
  * synchronisation at the end. */
 int esr_get_states(esr_solver* solver, int32_t n, const int32_t* slots, double* const* out);
+/* The same with float32 host fields (half the bytes over PCIe; a float32
+ * solver stores exactly these values). */
+int esr_set_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                      const float* const* W_init);
+int esr_get_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out);
 /* Slot `slot` restarts from state W (caller's cell order): stop-rule counters
  * reset and dt recomputed from W, as esr_set_case with W_init does. */
 int esr_set_state(esr_solver* solver, int32_t slot, const double* W);

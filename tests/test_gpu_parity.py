@@ -232,6 +232,15 @@ def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
     assert [r['stopping_step'] for r in ra] == [r['stopping_step'] for r in rb]
     with pytest.raises(Exception):
         b.set_cases([0, 0], cases[:2])
+    # float32 host fields: the float32 solver stores exactly the same values
+    c32 = Solver(meshes, [2, 3], precision='f32', threshold=1e-5, check_every=10)
+    warm32 = [None if w is None else w.astype(np.float32) for w in warm]
+    c32.set_cases(slots, cases, warm32)
+    c32.step(40)
+    got32 = c32.get_states(slots, dtype=np.float32)
+    for g in slots:
+        assert got32[g].dtype == np.float32
+        assert np.array_equal(got32[g], got[g].astype(np.float32)), g
 
 
 def test_batch_edge_cases(diamond02):
