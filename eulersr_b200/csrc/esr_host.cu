@@ -118,7 +118,6 @@ struct SolverT : SolverBase {
   DevBuf<double> stage_rows;  // host rows staging for set/get state
 
   // host mirrors of per-slot case data
-  std::vector<esr_case> hcase;
   std::vector<int> hcase_index;
   Consts<T> kc{};
 
@@ -304,7 +303,6 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemsetAsync(dt.p, 0, n_slots * sizeof(T), stream));
     ESR_CUDA(cudaMemsetAsync(strength.p, 0, n_slots * sizeof(T), stream));
     ESR_CUDA(cudaMemsetAsync(inlet.p, 0, n_slots * sizeof(V), stream));
-    hcase.assign(n_slots, esr_case{});
     hcase_index.assign(n_slots, -1);
     ESR_CUDA(cudaStreamSynchronize(stream));
     if (p->block_size == 0) ESR_TRY(autotune());
@@ -598,7 +596,6 @@ struct SolverT : SolverBase {
     MeshDev& md = *meshes[m];
     const HostMesh& hm = *md.hm;
     const int N = hm.n_cells;
-    hcase[slot] = *c;
     // per-slot constants: inlet, sponge strength (helper.py:279-285), force reference
     const V in = mk4<T>((T)c->inlet[0], (T)c->inlet[1], (T)c->inlet[2], (T)c->inlet[3]);
     const T r = in.x, u = in.y / r, v = in.z / r;
@@ -710,9 +707,10 @@ struct SolverT : SolverBase {
       x.tf = c.tf;
       x.thr = c.threshold;
       x.max_steps = c.max_steps;
-      hcase[slots[i]] = c;
       if (W_init && W_init[i]) { off[i] = rows; rows += meshes[m]->hm->n_cells; }
     }
+    // every case is valid: only now does the host bookkeeping change
+    for (int i = 0; i < n; ++i) hcase_index[slots[i]] = slots[i];
     if (rows > 0 && stage_many.n < (size_t)4 * rows) ESR_TRY(stage_many.alloc((size_t)4 * rows));
     S* stage = reinterpret_cast<S*>(stage_many.p);   // room for 4 rows of doubles is room for floats
     if (d_init.n < (size_t)n) ESR_TRY(d_init.alloc(n));

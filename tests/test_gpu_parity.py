@@ -230,8 +230,17 @@ def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
         assert np.array_equal(a.get_state(g), got[g]), g
     ra, rb = a.run(), b.run()
     assert [r['stopping_step'] for r in ra] == [r['stopping_step'] for r in rb]
+    assert [r['case_index'] for r in ra] == [r['case_index'] for r in rb] == slots
     with pytest.raises(Exception):
         b.set_cases([0, 0], cases[:2])
+    # a call with an invalid case changes nothing, not even the valid slots before it
+    before = b.get_states(slots)
+    bad = FlowCase(mach=2.0, aoa_deg=0.0, mesh=1, cfl=-1.0, tf=0.5, dtype=np.float32)
+    with pytest.raises(Exception):
+        b.set_cases([0, 2], [cases[0], bad])
+    after = b.get_states(slots)
+    for g in slots:
+        assert np.array_equal(before[g], after[g]), g
     # float32 host fields: the float32 solver stores exactly the same values
     c32 = Solver(meshes, [2, 3], precision='f32', threshold=1e-5, check_every=10)
     warm32 = [None if w is None else w.astype(np.float32) for w in warm]
