@@ -2,7 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY. Nothing in the shipped package imports this module;
 only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of
-``bench.py`` use it, and only as the checker.
+``bench.py`` use it, and only to check the CUDA results (or, in bench.py,
+as the timed CPU baseline), never as the thing measured or shipped.
 
 Parity status: **unpinned** against the reference itself. The reference runs on
 JAX 0.4.38 (``pyproject.toml:14``), which is not installed here or on the GPU
