@@ -135,6 +135,10 @@ _SIGS = {
     "esr_get_states_f32": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.POINTER(_f64p),
                                   C.POINTER(Result)]),
+    "esr_batch_submit": (C.c_int, [C.c_void_p, C.POINTER(Case), C.c_int32, C.POINTER(_f64p), C.c_int32]),
+    "esr_batch_poll": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "esr_batch_results": (C.c_int, [C.c_void_p, C.POINTER(_f64p), C.POINTER(Result)]),
+    "esr_batch_cancel": (C.c_int, [C.c_void_p]),
     "esr_gemm_bf16": (C.c_int, _GEMM_ARGS),
     "esr_gemm_bf16_mma_sync": (C.c_int, _GEMM_ARGS),
     "esr_gemm_tc_status": (C.c_int, [C.POINTER(C.c_int32)]),

@@ -74,6 +74,7 @@ int esr::report_error(int code, const std::string& msg) { return fail(code, msg)
 struct SolverBase {
   virtual ~SolverBase() = default;
   int64_t launches = 0;
+  bool batch_busy = false;   // a submitted batch owns the slots until its results are read or it is cancelled
 };
 
 template <typename T>
@@ -144,6 +145,10 @@ struct SolverT : SolverBase {
   }
 
   ~SolverT() override {
+    if (pend) {   // a batch still pending: let its work finish before its buffers go
+      cudaStreamSynchronize(stream);
+      pend.reset();
+    }
     if (g_run) cudaGraphExecDestroy(g_run);
     if (g_plain) cudaGraphExecDestroy(g_plain);
     if (ev0) cudaEventDestroy(ev0);
@@ -1045,17 +1050,75 @@ struct SolverT : SolverBase {
     launches += with_states ? 15 : 14;
   }
 
-  int batch(const esr_case* cs, int n, const double* const* init, double* const* finals, esr_result* out) {
+  // A batch in flight: its queue and result buffers, the captured chunk graph
+  // and the host's polling state, held between esr_batch_submit and
+  // esr_batch_results (esr_batch_solve runs the three steps in one call).
+  struct PendingBatch {
+    BatchBufs B;
+    Queue<T> q{};
+    SlotParams<T> sp{};
+    std::vector<int> case_mesh;
+    std::vector<long long> out_off;
+    int n = 0;
+    bool want_states = false;
+    cudaGraphExec_t gexec = nullptr;
+    int len = 0;
+    int64_t per_chunk = 0;
+    int poll = 4;
+    long long guard = 0;
+    int done = 0;
+    ~PendingBatch() { if (gexec) cudaGraphExecDestroy(gexec); }
+  };
+  std::unique_ptr<PendingBatch> pend;
+
+  // Release the pending batch. clear_slots: the batch was abandoned before it
+  // finished, so its running cases are stopped (their slots go inactive).
+  int batch_cancel(bool clear_slots = true) {
+    int rc = ESR_OK;
+    if (pend) {
+      if (clear_slots && pend->n > 0) {
+        cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream);
+      }
+      // nothing of the batch may still run when its buffers are freed
+      cudaError_t e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch_cancel: ") + cudaGetErrorString(e));
+    }
+    pend.reset();
+    batch_busy = false;
+    for (int g = 0; g < n_slots; ++g) hcase_index[g] = -1;
+    return rc;
+  }
+
+  int batch_submit(const esr_case* cs, int n, const double* const* init, bool want_states) {
+    if (pend) return fail(ESR_ERR_STATE, "batch_submit: a batch is already pending");
     const int nm = (int)meshes.size();
     for (int i = 0; i < n; ++i) {
       if (cs[i].mesh < 0 || cs[i].mesh >= nm) return fail(ESR_ERR_ARG, "batch: case mesh out of range");
       if (meshes[cs[i].mesh]->B < 1) return fail(ESR_ERR_ARG, "batch: case mesh has no slots");
       if (!(cs[i].cfl > 0)) return fail(ESR_ERR_ARG, "batch: cfl must be > 0");
       if (!(cs[i].tf > 0) && cs[i].max_steps <= 0) return fail(ESR_ERR_ARG, "batch: tf must be > 0");
-      out[i] = esr_result{};
-      out[i].case_index = i;
     }
-    if (n == 0) return ESR_OK;
+    auto owned = std::make_unique<PendingBatch>();
+    PendingBatch& pb = *owned;
+    pb.n = n;
+    pb.want_states = want_states;
+    if (n == 0) {   // nothing to run: the slots are left as they are
+      pend = std::move(owned);
+      batch_busy = true;
+      return ESR_OK;
+    }
+    int rc = submit_fill(pb, cs, init);
+    if (rc != ESR_OK) {   // owned (and its buffers) go once the stream is idle
+      cudaStreamSynchronize(stream);
+      return rc;
+    }
+    pend = std::move(owned);
+    batch_busy = true;
+    return ESR_OK;
+  }
+
+  int submit_fill(PendingBatch& pb, const esr_case* cs, const double* const* init) {
+    const int n = pb.n, nm = (int)meshes.size();
     // device copies of the renumbering, once per solver
     if (!perm_ptrs.p) {
       size_t tot = 0;
@@ -1075,7 +1138,7 @@ struct SolverT : SolverBase {
       ESR_CUDA(cudaMemcpy(perm_ptrs.p, pp.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
       ESR_CUDA(cudaMemcpy(inv_ptrs.p, ip.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
     }
-    BatchBufs B;
+    BatchBufs& B = pb.B;
     // queue: cases grouped by mesh, submission order inside a mesh
     std::vector<int> qlist, qoff(nm + 1, 0);
     for (int m = 0; m < nm; ++m) {
@@ -1090,18 +1153,21 @@ struct SolverT : SolverBase {
     std::vector<int> htr(n), hpat(n);
     std::vector<double4> het(n);
     long long init_rows = 0, out_rows = 0;
+    pb.case_mesh.resize(n);
     for (int i = 0; i < n; ++i) {
       case_params(cs[i], hin[i], hstr[i], hq[i], het[i], htr[i], hpat[i]);
       hcfl[i] = cs[i].cfl;
       htf[i] = cs[i].tf;
       hthr[i] = cs[i].threshold;
       hms[i] = cs[i].max_steps;
+      pb.case_mesh[i] = cs[i].mesh;
       const int N = meshes[cs[i].mesh]->hm->n_cells;
       if (init && init[i]) { hinit_off[i] = init_rows; init_rows += N; }
       hout_off[i] = out_rows;
       out_rows += N;
     }
-    const bool want_states = finals != nullptr;
+    pb.out_off = hout_off;
+    const bool want_states = pb.want_states;
     auto up = [&](auto& buf, const auto& v) -> int {
       using E = typename std::decay_t<decltype(v)>::value_type;
       ESR_TRY(buf.alloc(std::max<size_t>(v.size(), 1)));
@@ -1148,53 +1214,75 @@ struct SolverT : SolverBase {
     }
     if (want_states) ESR_TRY(B.out.alloc((size_t)4 * out_rows));
     ESR_CUDA(cudaStreamSynchronize(stream));   // host vectors above are the copy sources
-    Queue<T> q{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
+    pb.q = Queue<T>{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
                B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p, B.c_thr.p,
                init_rows > 0 ? B.init.p : nullptr, B.init_off.p, B.r_status.p, B.r_stop.p, B.r_steps.p, B.r_nmax.p,
                B.r_dt.p, B.r_rel.p, B.r_cd.p, B.r_cl.p, B.r_time.p, B.r_eng_conv.p, B.r_eng_stop.p, B.r_probe.p,
                want_states ? B.out.p : nullptr, B.out_off.p, B.n_done.p};
-    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
+    pb.sp = SlotParams<T>{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
     ESR_CUDA(cudaEventRecord(ev0, stream));
-    issue_refill(q, sp, want_states);   // first fill of every slot
+    issue_refill(pb.q, pb.sp, want_states);   // first fill of every slot
     // the chunk graph of this batch: steps, checks, then the refill sequence
-    cudaGraphExec_t gexec = nullptr;
-    const int len = run_chunk_len();
-    int64_t per_chunk = 0;
+    pb.len = run_chunk_len();
     if (P.use_graphs) {
       cudaGraph_t graph = nullptr;
       ESR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       const int64_t before = launches;
-      issue_run_chunk(len);
-      issue_refill(q, sp, want_states);
-      per_chunk = launches - before;
+      issue_run_chunk(pb.len);
+      issue_refill(pb.q, pb.sp, want_states);
+      pb.per_chunk = launches - before;
       launches = before;
       ESR_CUDA(cudaStreamEndCapture(stream, &graph));
-      cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
+      cudaError_t e = cudaGraphInstantiate(&pb.gexec, graph, 0);
       cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      if (e != cudaSuccess) { pb.gexec = nullptr; return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)); }
     }
-    int done = 0, poll = 4;
+    return ESR_OK;
+  }
+
+  // One polling round: a few chunks (doubling up to 32 per round), then the
+  // done counter. A failure abandons the batch.
+  int batch_poll(int* n_done) {
+    if (!pend) return fail(ESR_ERR_STATE, "batch_poll: no batch pending");
+    PendingBatch& pb = *pend;
     int rc = ESR_OK;
-    for (long long guard = 0; done < n; ++guard) {
-      for (int i = 0; i < poll; ++i) {
-        if (gexec) {
-          cudaError_t e = cudaGraphLaunch(gexec, stream);
-          if (e != cudaSuccess) { rc = fail(ESR_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
-          launches += per_chunk;
+    if (pb.done < pb.n) {
+      for (int i = 0; i < pb.poll && rc == ESR_OK; ++i) {
+        if (pb.gexec) {
+          cudaError_t e = cudaGraphLaunch(pb.gexec, stream);
+          if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+          else launches += pb.per_chunk;
         } else {
-          issue_run_chunk(len);
-          issue_refill(q, sp, want_states);
+          issue_run_chunk(pb.len);
+          issue_refill(pb.q, pb.sp, pb.want_states);
         }
       }
-      if (rc != ESR_OK) break;
-      cudaError_t e = cudaMemcpyAsync(&done, B.n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-      if (e != cudaSuccess) { rc = fail(ESR_ERR_CUDA, std::string("batch poll: ") + cudaGetErrorString(e)); break; }
-      poll = std::min(poll * 2, 32);
-      if (guard > (1LL << 40)) { rc = fail(ESR_ERR_STATE, "batch: no progress"); break; }
+      if (rc == ESR_OK) {
+        cudaError_t e = cudaMemcpyAsync(&pb.done, pb.B.n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch poll: ") + cudaGetErrorString(e));
+      }
+      pb.poll = std::min(pb.poll * 2, 32);
+      if (rc == ESR_OK && ++pb.guard > (1LL << 40)) rc = fail(ESR_ERR_STATE, "batch: no progress");
     }
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (rc != ESR_OK) return rc;
+    if (rc != ESR_OK) {
+      const std::string msg = g_last_error;
+      batch_cancel(true);
+      return fail(rc, msg);
+    }
+    if (n_done) *n_done = pb.done;
+    return ESR_OK;
+  }
+
+  int batch_results(esr_result* out, double* const* finals) {
+    if (!pend) return fail(ESR_ERR_STATE, "batch_results: no batch pending");
+    PendingBatch& pb = *pend;
+    if (pb.done < pb.n) return fail(ESR_ERR_STATE, "batch_results: the batch has not finished");
+    if (finals && !pb.want_states) return fail(ESR_ERR_ARG, "batch_results: final states were not requested at submit");
+    const int n = pb.n;
+    if (n > 0 && !out) return fail(ESR_ERR_ARG, "batch_results: null results");
+    if (n == 0) return batch_cancel(false);
+    BatchBufs& B = pb.B;
     ESR_CUDA(cudaEventRecord(ev1, stream));
     std::vector<int> st(n), sstop(n), ssteps(n), snmax(n), sec(n), ses(n);
     std::vector<double> sdt(n), srel(n), scd(n), scl(n), stime(n), sprobe(n);
@@ -1208,15 +1296,16 @@ struct SolverT : SolverBase {
     ESR_TRY(down(sdt, B.r_dt)); ESR_TRY(down(srel, B.r_rel)); ESR_TRY(down(scd, B.r_cd)); ESR_TRY(down(scl, B.r_cl));
     ESR_TRY(down(stime, B.r_time));
     ESR_TRY(down(sprobe, B.r_probe));
-    if (want_states)
+    if (finals)
       for (int i = 0; i < n; ++i)
         if (finals[i])
-          ESR_CUDA(cudaMemcpyAsync(finals[i], B.out.p + 4 * hout_off[i],
-                                   (size_t)4 * meshes[cs[i].mesh]->hm->n_cells * sizeof(double),
+          ESR_CUDA(cudaMemcpyAsync(finals[i], B.out.p + 4 * pb.out_off[i],
+                                   (size_t)4 * meshes[pb.case_mesh[i]]->hm->n_cells * sizeof(double),
                                    cudaMemcpyDeviceToHost, stream));
     ESR_CUDA(cudaStreamSynchronize(stream));
     for (int i = 0; i < n; ++i) {
       esr_result& r = out[i];
+      r = esr_result{};
       r.status = st[i];
       r.converged = st[i] == ESR_CASE_CONVERGED;
       r.stopping_step = sstop[i];
@@ -1235,8 +1324,13 @@ struct SolverT : SolverBase {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     last_ms = ms;
-    for (int g = 0; g < n_slots; ++g) hcase_index[g] = -1;
-    return ESR_OK;
+    return batch_cancel(false);   // releases the batch's buffers and graph
+  }
+
+  int batch(const esr_case* cs, int n, const double* const* init, double* const* finals, esr_result* out) {
+    ESR_TRY(batch_submit(cs, n, init, finals != nullptr));
+    while (pend && pend->done < pend->n) ESR_TRY(batch_poll(nullptr));
+    return batch_results(out, finals);
   }
 };
 
@@ -1252,11 +1346,18 @@ struct esr_solver {
   catch (const std::exception& e) { return fail(ESR_ERR_STATE, e.what()); } \
   catch (...) { return fail(ESR_ERR_STATE, "unknown C++ exception"); }
 
+// dispatch_any: calls that are valid while a submitted batch owns the slots
 template <typename F>
-static int dispatch(esr_solver* s, F&& f) {
+static int dispatch_any(esr_solver* s, F&& f) {
   if (!s || !s->impl) return fail(ESR_ERR_ARG, "null solver");
   if (s->precision == ESR_PREC_F64) return f(*static_cast<SolverT<double>*>(s->impl.get()));
   return f(*static_cast<SolverT<float>*>(s->impl.get()));
+}
+template <typename F>
+static int dispatch(esr_solver* s, F&& f) {
+  if (s && s->impl && s->impl->batch_busy)
+    return fail(ESR_ERR_STATE, "a submitted batch owns the solver's slots: read its results or cancel it first");
+  return dispatch_any(s, std::forward<F>(f));
 }
 
 extern "C" {
@@ -1343,12 +1444,12 @@ int esr_solver_destroy(esr_solver* solver) {
 
 int esr_solver_num_slots(const esr_solver* solver, int32_t* n) {
   if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
-  return dispatch(const_cast<esr_solver*>(solver), [&](auto& s) { *n = s.n_slots; return ESR_OK; });
+  return dispatch_any(const_cast<esr_solver*>(solver), [&](auto& s) { *n = s.n_slots; return ESR_OK; });
 }
 
 int esr_solver_tuning(const esr_solver* solver, esr_tuning* out) {
   if (!solver || !out) return fail(ESR_ERR_ARG, "null argument");
-  return dispatch(const_cast<esr_solver*>(solver), [&](auto& s) { return s.get_tuning(out); });
+  return dispatch_any(const_cast<esr_solver*>(solver), [&](auto& s) { return s.get_tuning(out); });
 }
 
 int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init) {
@@ -1455,14 +1556,14 @@ int esr_entropy(esr_solver* solver, double* total) {
   return dispatch(solver, [&](auto& s) { return s.entropy(total); });
 }
 int esr_synchronize(esr_solver* solver) {
-  return dispatch(solver, [&](auto& s) {
+  return dispatch_any(solver, [&](auto& s) {
     cudaError_t e = cudaStreamSynchronize(s.stream);
     return e == cudaSuccess ? ESR_OK : fail(ESR_ERR_CUDA, cudaGetErrorString(e));
   });
 }
 int esr_last_elapsed_ms(esr_solver* solver, double* ms) {
   if (!ms) return fail(ESR_ERR_ARG, "null output");
-  return dispatch(solver, [&](auto& s) { *ms = s.last_ms; return ESR_OK; });
+  return dispatch_any(solver, [&](auto& s) { *ms = s.last_ms; return ESR_OK; });
 }
 int esr_kernel_launches(const esr_solver* solver, int64_t* n) {
   if (!solver || !n) return fail(ESR_ERR_ARG, "null argument");
@@ -1480,6 +1581,33 @@ int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases, 
   ESR_GUARD_BEGIN
   if (!cases || n_cases < 0 || !results) return fail(ESR_ERR_ARG, "batch_solve: null argument");
   return dispatch(solver, [&](auto& s) { return s.batch(cases, n_cases, init_fields, final_states, results); });
+  ESR_GUARD_END
+}
+int esr_batch_submit(esr_solver* solver, const esr_case* cases, int32_t n_cases, const double* const* init_fields,
+                     int32_t want_states) {
+  ESR_GUARD_BEGIN
+  if (n_cases < 0 || (n_cases > 0 && !cases)) return fail(ESR_ERR_ARG, "batch_submit: null argument");
+  return dispatch(solver, [&](auto& s) { return s.batch_submit(cases, n_cases, init_fields, want_states != 0); });
+  ESR_GUARD_END
+}
+int esr_batch_poll(esr_solver* solver, int32_t* n_done) {
+  ESR_GUARD_BEGIN
+  return dispatch_any(solver, [&](auto& s) {
+    int d = 0;
+    const int rc = s.batch_poll(&d);
+    if (rc == ESR_OK && n_done) *n_done = d;
+    return rc;
+  });
+  ESR_GUARD_END
+}
+int esr_batch_results(esr_solver* solver, double* const* final_states, esr_result* results) {
+  ESR_GUARD_BEGIN
+  return dispatch_any(solver, [&](auto& s) { return s.batch_results(results, final_states); });
+  ESR_GUARD_END
+}
+int esr_batch_cancel(esr_solver* solver) {
+  ESR_GUARD_BEGIN
+  return dispatch_any(solver, [&](auto& s) { return s.batch_cancel(true); });
   ESR_GUARD_END
 }
 

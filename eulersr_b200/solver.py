@@ -356,6 +356,54 @@ class Solver:
         F.check(F.lib().esr_batch_solve(self.handle, carr, n, init_arr, fin_arr, res))
         return [r.as_dict() for r in res], states
 
+    def batch_submit(self, cases, init_fields=None, want_states=False):
+        """Start the batch of ``batch_solve`` and return at once; the fields
+        are copied before this returns. Until ``batch_results`` or
+        ``batch_cancel`` the batch owns the slots."""
+        n = len(cases)
+        carr = (F.Case * n)(*[c.to_c() for c in cases])
+        keep = []
+        init_arr = None
+        if init_fields is not None:
+            init_arr = (F._f64p * n)()
+            for i, f in enumerate(init_fields):
+                if f is not None:
+                    a = F.f64(f)
+                    keep.append(a)
+                    init_arr[i] = F.ptr(a, C.c_double)
+        F.check(F.lib().esr_batch_submit(self.handle, carr, n, init_arr, int(bool(want_states))))
+        self._pending = ([self.meshes[c.mesh].n_cells for c in cases], bool(want_states))
+
+    def batch_poll(self) -> int:
+        """Advance the submitted batch by a few chunks; returns the number of
+        finished cases."""
+        d = C.c_int32(0)
+        try:
+            F.check(F.lib().esr_batch_poll(self.handle, C.byref(d)))
+        except Exception:
+            self._pending = None   # a failing poll cancels the batch
+            raise
+        return int(d.value)
+
+    def batch_results(self):
+        """(results, final states or None) of the finished batch; releases it."""
+        cells, want = self._pending
+        n = len(cells)
+        res = (F.Result * max(n, 1))()
+        states = None
+        fin_arr = None
+        if want:
+            states = [np.empty((nc, 4)) for nc in cells]
+            fin_arr = (F._f64p * max(n, 1))(*[F.ptr(s, C.c_double) for s in states])
+        F.check(F.lib().esr_batch_results(self.handle, fin_arr, res))
+        self._pending = None
+        return [r.as_dict() for r in res[:n]], states
+
+    def batch_cancel(self):
+        """Abandon the submitted batch: running cases stop, slots go inactive."""
+        F.check(F.lib().esr_batch_cancel(self.handle))
+        self._pending = None
+
     def close(self):
         if getattr(self, 'handle', None):
             F.lib().esr_solver_destroy(self.handle)

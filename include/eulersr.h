@@ -23,6 +23,9 @@
  *   esr_entropy          euler/jax_fvm/src/helper.py:312-320 get_total_entropy
  *   esr_batch_solve      the serial grid loop of slurm/run_euler_grid.py:94-104,
  *                        run as one batch with retire/refill
+ *   esr_batch_submit /   the same batch in three non-blocking steps (the grid
+ *   _poll / _results /   loop's calls to euler.main.run, :103-104, issued
+ *   _cancel              together and collected when done)
  *   esr_idw_apply        eval/core.py:135-142 predict_idw (weights utils/metrics.py:9-14)
  *   esr_set_cases /      esr_set_case / esr_get_state for many slots at once (the
  *   esr_get_states       per-case initialize + np.asarray(W) of the grid loop)
@@ -267,6 +270,28 @@ int esr_solver_tuning(const esr_solver* solver, esr_tuning* out);
 int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases,
                     const double* const* init_fields, double* const* final_states,
                     esr_result* results);
+
+/* esr_batch_solve split so that the caller keeps its thread between polls
+ * (slurm/run_euler_grid.py:94-104 run as one batch, as above).
+ * esr_batch_submit uploads the cases (init_fields as in esr_batch_solve; the
+ * fields are copied before it returns), fills every slot and returns; from
+ * then on the batch owns the slots, and every other call on the solver except
+ * esr_batch_poll, esr_batch_results, esr_batch_cancel, esr_solver_num_slots,
+ * esr_solver_tuning, esr_synchronize, esr_last_elapsed_ms and
+ * esr_kernel_launches fails with ESR_ERR_STATE. want_states != 0 keeps every
+ * case's final state for esr_batch_results. esr_batch_poll advances the batch
+ * by a few captured chunks (doubling from 4 up to 32 per call), waits for
+ * them, and reports how many cases have finished; results are bitwise those
+ * of esr_batch_solve. esr_batch_results (valid once *n_done == n_cases)
+ * fills results[n_cases] and, when final_states is non-NULL, final_states[i]
+ * (NULL entries skipped), then releases the batch. esr_batch_cancel
+ * abandons a pending batch: running cases stop and their slots go inactive.
+ * A failing poll cancels the batch itself. */
+int esr_batch_submit(esr_solver* solver, const esr_case* cases, int32_t n_cases,
+                     const double* const* init_fields, int32_t want_states);
+int esr_batch_poll(esr_solver* solver, int32_t* n_done);
+int esr_batch_results(esr_solver* solver, double* const* final_states, esr_result* results);
+int esr_batch_cancel(esr_solver* solver);
 
 /* Relative change ||A - B||_F / (||B||_F + 1e-16) of two device fields of
  * n_rows x 4 values (float4 rows for ESR_PREC_F32, double4 rows for

@@ -182,6 +182,57 @@ def test_batch_equals_single(diamond02, naca02, precision):
     assert all(np.array_equal(a, b) for a, b in zip(states, states2))
     assert [r['stopping_step'] for r in res] == [r['stopping_step'] for r in res2]
 
+
+def test_batch_submit_poll_results(diamond02, naca02):
+    """esr_batch_submit / esr_batch_poll / esr_batch_results give bitwise the
+    results and final states of esr_batch_solve. While a batch owns the slots
+    other solver calls fail with ESR_ERR_STATE; results before the end fail;
+    a cancelled batch leaves the solver usable for the next batch."""
+    from eulersr_b200.solver import Solver, FlowCase
+    from eulersr_b200._ffi import EsrError
+    meshes = [diamond02, naca02]
+    spec = [(2.5, 5.0), (1.5, -2.0), (3.0, 1.0), (0.9, 0.5), (2.0, 0.0), (2.2, 3.0), (1.8, -1.0)]
+    cases = [FlowCase(mach=m, aoa_deg=a, mesh=i % 2, cfl=0.6, tf=0.4, dtype=np.float32)
+             for i, (m, a) in enumerate(spec)]
+    warm = Solver(diamond02, 1, precision='f32')
+    warm.set_case(0, FlowCase(mach=2.0, aoa_deg=0.0, cfl=0.6, tf=0.4, dtype=np.float32))
+    warm.step(30)
+    init = [None] * len(cases)
+    init[4] = warm.get_state(0)
+    s = Solver(meshes, [2, 1], precision='f32', threshold=1e-5, check_every=10)
+    ref, ref_states = s.batch_solve(cases, init_fields=init, want_states=True)
+    s.batch_submit(cases, init_fields=init, want_states=True)
+    with pytest.raises(EsrError):
+        s.step(1)
+    with pytest.raises(EsrError):
+        s.batch_submit(cases)
+    with pytest.raises(EsrError):
+        s.batch_results()
+    done, polls, seen = 0, 0, []
+    while done < len(cases):
+        done = s.batch_poll()
+        seen.append(done)
+        polls += 1
+        assert polls < 100000
+    assert seen == sorted(seen)
+    res, states = s.batch_results()
+    for k in ('stopping_step', 'status', 'steps', 'n_max', 'cd', 'cl', 'final_residual', 'case_index'):
+        assert [r[k] for r in res] == [r[k] for r in ref], k
+    assert all(np.array_equal(a, b) for a, b in zip(states, ref_states))
+    # cancel part-way, then the solver takes the next batch and single cases again
+    s.batch_submit(cases, init_fields=init)
+    s.batch_poll()
+    s.batch_cancel()
+    res3, _ = s.batch_solve(cases, init_fields=init)
+    assert [r['stopping_step'] for r in res3] == [r['stopping_step'] for r in ref]
+    s.set_case(0, cases[0])
+    s.step(2)
+    # an empty batch: nothing runs, the slots are left as they are
+    s.batch_submit([])
+    assert s.batch_poll() == 0
+    assert s.batch_results() == ([], None)
+
+
 def test_autotuner_and_block_invariance(naca02):
     """The autotuner times every candidate block size and keeps the fastest;
     the state after 30 steps is bitwise the same whatever the block size."""
