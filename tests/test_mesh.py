@@ -140,3 +140,24 @@ def test_reference_pickle_reader(tmp_path, diamond02):
     assert np.array_equal(got.neighbors, diamond02.neighbors)
     assert got.metadata['obstacle_length'] == 1.0
     assert np.allclose(got.area, diamond02.area)
+
+
+def test_generate_mesh_cli(tmp_path, capsys):
+    """The euler/generate_mesh.py command line: --geom / -h / --out-dir give
+    one <geom>_h<h>.npz per pair, placed as the reference places them."""
+    import math
+    from eulersr_b200.meshing import generate as G
+    assert G.main(["--geom", "diamond_txy", "diamond_alpha10", "naca2412", "-h", "0.3",
+                   "--out-dir", str(tmp_path), "--fig-dir", str(tmp_path / "figs")]) == 0
+    out = capsys.readouterr().out
+    assert out.count("Mesh saved : ") == 3
+    txy = Mesh.load(tmp_path / "diamond_txy_h0.3.npz")
+    assert txy.validate()
+    assert txy.metadata["case"] == "diamond_txy"
+    assert txy.metadata["center"] == {"cx": 2.0, "cy": 2.5}
+    a10 = Mesh.load(tmp_path / "diamond_alpha10_h0.3.npz")
+    assert math.isclose(a10.metadata["height"], math.tan(math.radians(10.0)))
+    naca = Mesh.load(tmp_path / "naca2412_h0.3.npz")
+    assert naca.metadata["case"] == "naca2412" and naca.n_cells > 0
+    with pytest.raises(SystemExit):
+        G.main(["--geom", "bump", "--out-dir", str(tmp_path)])
