@@ -152,6 +152,63 @@ def shock_angle_deg(mesh, W, le=(1.0, 2.0), chord=1.0, gamma=1.4, p_inf=1.0, x_r
     return math.degrees(math.atan(slope))
 
 
+def _primitives(W, gamma=1.4):
+    """Density, velocity and pressure of conserved rows (helper.py:25-36, M = 1)."""
+    W = np.asarray(W, np.float64)
+    rho = W[:, 0]
+    u, v = W[:, 1] / rho, W[:, 2] / rho
+    p = (W[:, 3] - 0.5 * rho * (u * u + v * v)) * (gamma - 1.0)
+    return rho, u, v, p
+
+
+def force_coefficients(mesh, W, mach, gamma=1.4, rho_inf=1.0, p_inf=1.0):
+    """(CD, CL) of a field on the host, as helper.py:366-415 computes them:
+    the owner cell's pressure (no reconstruction) times the owner's outward
+    normal and the face length, summed over the force-marker faces, over
+    0.5 rho U^2 L_ref in body axes, U = M sqrt(gamma p / rho)."""
+    _, _, _, p = _primitives(W, gamma)
+    faces, cells, slots = mesh.wall_owner_data()
+    n = mesh.normals[cells, slots]
+    ds = mesh.surface[faces]
+    u_inf = mach * math.sqrt(gamma * p_inf / rho_inf)
+    q = 0.5 * rho_inf * u_inf ** 2 * float(mesh.metadata.get("obstacle_length", 1.0) or 1.0)
+    return float(np.sum(p[cells] * n[:, 0] * ds) / q), float(np.sum(p[cells] * n[:, 1] * ds) / q)
+
+
+def wall_profile(mesh, W, gamma=1.4):
+    """Wall Mach and pressure along the lower body surface (helper.py:439-506):
+    wall faces whose midpoint lies at or below the domain's mid-height (all
+    wall faces when none does), sorted by midpoint x then y, each valued at its
+    first listing cell; ``s`` is the arc length along the sorted midpoints."""
+    mid = mesh.face_midpoints()
+    wall = np.isin(mesh.face_markers, mesh.wall_markers())
+    empty = np.empty(0)
+    if not wall.any():
+        return {"s": empty, "x": empty, "y": empty, "mach": empty, "pressure": empty,
+                "face_ids": np.empty(0, np.int32)}
+    y_mid = 0.5 * float(mesh.points[:, 1].min() + mesh.points[:, 1].max())
+    ids = np.nonzero(wall & (mid[:, 1] <= y_mid))[0]
+    if ids.size == 0:
+        ids = np.nonzero(wall)[0]
+    ids = ids[np.lexsort((mid[ids, 1], mid[ids, 0]))]
+    # first (cell, slot) listing each face, row-major, as the owner lookup does
+    fc = mesh.face_connectivity.reshape(-1)
+    first = np.full(mesh.n_faces, -1, np.int64)
+    order = np.argsort(fc, kind="stable")
+    fcs = fc[order]
+    starts = np.r_[0, np.nonzero(np.diff(fcs))[0] + 1]
+    first[fcs[starts]] = order[starts]
+    keep = first[ids] >= 0
+    ids = ids[keep]
+    cells = first[ids] // 3
+    rho, u, v, p = _primitives(W, gamma)
+    a = np.sqrt(np.maximum(gamma * p[cells] / rho[cells], 1e-14))
+    m = mid[ids]
+    seg = np.linalg.norm(np.diff(m, axis=0), axis=1) if len(ids) > 1 else empty
+    return {"s": np.concatenate(([0.0], np.cumsum(seg))) if len(ids) else empty, "x": m[:, 0], "y": m[:, 1],
+            "mach": np.hypot(u[cells], v[cells]) / a, "pressure": p[cells], "face_ids": ids.astype(np.int32)}
+
+
 def validate_diamond(h=0.025, machs=(1.5, 2.0), precision="f64"):
     """Converged diamond solves (alpha 0) against shock-expansion theory, as
     euler/postproc/theory_validation_diamond.py does: CD error and the
