@@ -12,6 +12,9 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the native library")
+    # temporary files of the tests stay inside the checkout
+    if not config.option.basetemp:
+        config.option.basetemp = str(ROOT / ".pytest_tmp")
 
 
 @pytest.fixture(scope="session")

@@ -97,3 +97,97 @@ def test_mesh_convergence_campaign(tmp_path):
     assert float(lines[-1].split(",")[-1]) == 0.0
     # the ratio-2 chain lacks h=0.1 here, so no GCI triplet
     assert gci_csv.read_text().splitlines() == ["label,mach,aoa,h_coarse,h_mid,h_fine,quantity,p_obs,extrap,gci_fine_pct"]
+
+
+@pytest.mark.parametrize("mach,aoa", [(2.0, 0.0), (2.5, 3.0)])
+def test_theory_forces_on_mesh_equal_analytic(mach, aoa):
+    """The theory's face pressures placed on the wall cells and integrated by
+    the force routine give the analytic shock-expansion CD and CL (the body's
+    faces are exact segments of the four panels)."""
+    from conftest import load_mesh
+    from eulersr_b200.postproc import diamond_theory
+    from eulersr_b200 import theory_validation as TV
+    m = load_mesh("diamond_h0.1")
+    cx, cy = m.metadata["center"]["cx"], m.metadata["center"]["cy"]
+    panels = TV.diamond_panels(mach, aoa, 5.0)
+    assert TV.all_attached(panels)
+    cd, cl = TV.theory_forces(m, panels, mach, cx, cy)
+    th = diamond_theory(mach, aoa, 5.0)
+    assert cd == pytest.approx(th.cd, rel=1e-9)
+    assert cl == pytest.approx(th.cl, rel=1e-9, abs=1e-12)
+    for n in TV.PANEL_NAMES:
+        assert panels[n].p_ratio_freestream == pytest.approx(th.p_faces[n], rel=1e-12)
+    # M=1.05 detaches the front shocks: the campaigns skip such points
+    assert not TV.all_attached(TV.diamond_panels(1.05, 0.0, 5.0))
+
+
+def test_measure_shock_angle_on_a_ridge():
+    """Cells whose |grad p| peaks along a line through the leading edge at
+    angle beta give back beta."""
+    from eulersr_b200 import theory_validation as TV
+    rng = np.random.default_rng(4)
+    cx, cy, chord, height = 1.5, 2.0, 1.0, math.tan(math.radians(5.0))
+    x_le = cx - 0.5 * chord
+    pts = np.column_stack([rng.uniform(x_le - 0.35, x_le + 0.45, 20000), rng.uniform(cy - 0.3, cy + 0.3, 20000)])
+    beta = math.radians(41.0)
+    for side, sgn in (("upper", 1.0), ("lower", -1.0)):
+        d = np.abs(np.sin(beta) * (pts[:, 0] - x_le) - np.cos(beta) * sgn * (pts[:, 1] - cy))
+        grad = np.column_stack([np.exp(-(d / 0.004) ** 2), np.zeros(len(pts))])
+        got = TV.measure_shock_angle(pts, grad, cx, cy, chord, height, 0.0, side)
+        assert got == pytest.approx(41.0, abs=0.3)
+    assert TV.measure_shock_angle(pts[:5], grad[:5], cx, cy, chord, height, 0.0, "upper") is None
+
+
+def test_theory_campaigns_on_bundles(tmp_path):
+    """Both campaigns over bundles laid out as the grid driver writes them: a
+    field that carries the theory's pressures on the wall cells has zero CD,
+    CL and plateau-Cp error; the CSVs have the reference's columns."""
+    from eulersr_b200.mesh import Mesh
+    from eulersr_b200.meshing import generate as G
+    from eulersr_b200 import mesh_convergence as MC
+    from eulersr_b200 import theory_validation as TV
+    mesh_dir, raw_dir = tmp_path / "meshes", tmp_path / "raw"
+    mach, aoa = 2.0, 0.0
+    chain = [0.2, 0.15]       # coarser levels have under 3 faces per panel: no plateau
+    for h in chain:
+        G.generate("diamond", h, mesh_dir)
+        m = Mesh.load(G.mesh_path(mesh_dir, "diamond", h))
+        cx, cy = m.metadata["center"]["cx"], m.metadata["center"]["cy"]
+        panels = TV.diamond_panels(mach, aoa, 5.0)
+        p = np.ones(m.n_cells)
+        first = TV._first_owner(m)
+        mid = m.face_midpoints()
+        for f in np.nonzero(m.face_markers == m.force_marker())[0]:
+            p[first[f] // 3] = panels[TV.panel_of(mid[f, 0], mid[f, 1], cx, cy)].p_ratio_freestream
+        W = np.zeros((m.n_cells, 4))
+        W[:, 0] = 1.0
+        W[:, 3] = p / 0.4
+        grad = np.zeros((m.n_cells, 4, 2))
+        d = raw_dir / MC.format_h(h) / "AOA0.00"
+        d.mkdir(parents=True)
+        np.savez(d / "AOA0.00_M2.00_HLLC_MUSCL_SRK2_t3.00.npz", conservatives=W, node_pos=m.barycenter,
+                 primitives_grad=grad)
+    pts = [("P6_mach2_symetrique", mach, aoa), ("P2_supersonique_marginal", 1.05, 0.0)]
+    path = TV.run_theory_validation(raw_dir, mesh_dir, tmp_path / "theory", points=pts, h=0.2)
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith("label,mach,aoa,Cd_fvm,Cd_theory")
+    assert len(lines) == 1 + 4                      # the detached point is skipped
+    for line in lines[1:]:
+        f = line.split(",")
+        assert float(f[3]) == pytest.approx(float(f[4]), abs=1e-6)    # CD
+        assert float(f[8]) == pytest.approx(float(f[9]), abs=1e-6)    # plateau Cp
+    errs, fit = TV.run_wall_convergence(raw_dir, mesh_dir, tmp_path / "wall", points=pts, h_all=chain)
+    rows = errs.read_text().splitlines()
+    assert len(rows) == 1 + len(chain)
+    for line in rows[1:]:
+        f = line.split(",")
+        assert float(f[7]) < 1e-9 and float(f[10]) < 1e-9 and float(f[11]) < 1e-9
+    assert fit.read_text().splitlines() == ["label,mach,aoa,quantity,p_order,r2,n_points"]
+
+
+def test_fit_order():
+    from eulersr_b200.theory_validation import fit_order
+    rows = [dict(h=h, e=3.0 * h ** 1.5) for h in (0.1, 0.05, 0.025, 0.0125, 0.2)]
+    p, r2, n = fit_order(rows, "e")
+    assert n == 4 and p == pytest.approx(1.5, abs=1e-10) and r2 == pytest.approx(1.0, abs=1e-12)
+    assert fit_order(rows[:2], "e")[0] is None
