@@ -1168,6 +1168,50 @@ __global__ void k_gather_state(const V4<T>* __restrict__ W, const int* __restric
   r[0] = (S)w.x; r[1] = (S)w.y; r[2] = (S)w.z; r[3] = (S)w.w;
 }
 
+// One slot's field in a staging buffer of host rows (caller cell order):
+// many slots move with one launch (grid.y = slot).
+template <typename T>
+struct SlotCopy {
+  long long stage_row;   // first row of the slot in the staging buffer; < 0: fill with w
+  const int* inv;        // caller cell -> solver cell of the slot's mesh
+  long long off;         // the mesh's first item
+  int n_cells, B, b, pad;
+  V4<T> w;               // freestream state of a fill
+};
+
+// W = Wref = the staged rows (or the freestream) of every slot of jobs
+template <typename T, typename S>
+__global__ void k_scatter_slots(const S* __restrict__ stage, const SlotCopy<T>* __restrict__ jobs,
+                                V4<T>* __restrict__ W, V4<T>* __restrict__ Wref) {
+  const SlotCopy<T> j = jobs[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= j.n_cells) return;
+  V4<T> w;
+  long long gi;
+  if (j.stage_row >= 0) {
+    const S* r = stage + 4 * (j.stage_row + c);
+    w = mk4<T>((T)r[0], (T)r[1], (T)r[2], (T)r[3]);
+    gi = j.off + (long long)j.inv[c] * j.B + j.b;
+  } else {
+    w = j.w;
+    gi = j.off + (long long)c * j.B + j.b;
+  }
+  W[gi] = w;
+  Wref[gi] = w;
+}
+
+// the staged rows of every slot of jobs from W, in caller cell order
+template <typename T, typename S>
+__global__ void k_gather_slots(const V4<T>* __restrict__ W, const SlotCopy<T>* __restrict__ jobs,
+                               S* __restrict__ stage) {
+  const SlotCopy<T> j = jobs[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= j.n_cells) return;
+  const V4<T> w = W[j.off + (long long)j.inv[c] * j.B + j.b];
+  S* r = stage + 4 * (j.stage_row + c);
+  r[0] = (S)w.x; r[1] = (S)w.y; r[2] = (S)w.z; r[3] = (S)w.w;
+}
+
 // every item of W set to one state (the autotuner's workload)
 template <typename T>
 __global__ void k_fill_uniform(V4<T>* __restrict__ W, long long n, V4<T> w) {

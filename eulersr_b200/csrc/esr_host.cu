@@ -687,6 +687,24 @@ struct SolverT : SolverBase {
   // ---------------------------------------------- many slots at once
   DevBuf<double> stage_many;            // host rows of set_cases / get_states
   DevBuf<SlotInit<T>> d_init;
+  DevBuf<SlotCopy<T>> d_jobs;
+  // Upload the slot table and launch fn(table, grid) once per 65,535 slots
+  // (the grid's y limit); grid.x covers the largest mesh. The caller
+  // synchronises the stream before the host table goes.
+  template <typename F>
+  int launch_slot_copies(const std::vector<SlotCopy<T>>& jobs, int max_n, F&& fn) {
+    const int n = (int)jobs.size();
+    if (n == 0 || max_n == 0) return ESR_OK;
+    if (d_jobs.n < (size_t)n) ESR_TRY(d_jobs.alloc(n));
+    ESR_CUDA(cudaMemcpyAsync(d_jobs.p, jobs.data(), n * sizeof(SlotCopy<T>), cudaMemcpyHostToDevice, stream));
+    for (int j0 = 0; j0 < n; j0 += 65535) {
+      const int nj = std::min(65535, n - j0);
+      fn(d_jobs.p + j0, dim3((max_n + 255) / 256, nj));
+      ++launches;
+    }
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
   // S: the type of the caller's host rows (double, or float for float32 fields)
   template <typename S>
   int set_cases(int n, const int32_t* slots, const esr_case* cs, const S* const* W_init) {
@@ -724,20 +742,22 @@ struct SolverT : SolverBase {
     SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
     k_init_slots<T><<<(n + 127) / 128, 128, 0, stream>>>(d_init.p, n, sp, ctl(), fill.p);
     ++launches;
+    // every field lands in the staging rows first, then one launch places them all
+    std::vector<SlotCopy<T>> jobs(n);
+    int max_n = 0;
     for (int i = 0; i < n; ++i) {
       int m, b;
       ESR_TRY(mesh_of_slot(slots[i], m, b));
       MeshDev& md = *meshes[m];
-      const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
-      if (off[i] >= 0) {
-        S* st = stage + 4 * off[i];
-        ESR_CUDA(cudaMemcpyAsync(st, W_init[i], (size_t)4 * N * sizeof(S), cudaMemcpyHostToDevice, stream));
-        k_scatter_state<T, S><<<nb, tb, 0, stream>>>(st, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
-      } else {
-        k_fill_freestream<T><<<nb, tb, 0, stream>>>(W.p, Wref.p, N, md.off, md.B, b, hi[i].inlet);
-      }
-      ++launches;
+      const int N = md.hm->n_cells;
+      if (off[i] >= 0)
+        ESR_CUDA(cudaMemcpyAsync(stage + 4 * off[i], W_init[i], (size_t)4 * N * sizeof(S), cudaMemcpyHostToDevice, stream));
+      jobs[i] = SlotCopy<T>{off[i] >= 0 ? off[i] : -1, md.inv.p, md.off, N, md.B, b, 0, hi[i].inlet};
+      max_n = std::max(max_n, N);
     }
+    ESR_TRY(launch_slot_copies(jobs, max_n, [&](const SlotCopy<T>* dj, dim3 grid) {
+      k_scatter_slots<T, S><<<grid, 256, 0, stream>>>(stage, dj, W.p, Wref.p);
+    }));
     ESR_TRY(finish_fill());
     ESR_CUDA(cudaStreamSynchronize(stream));   // hi and the caller's fields are the copy sources
     return ESR_OK;
@@ -755,16 +775,23 @@ struct SolverT : SolverBase {
       rows += meshes[m]->hm->n_cells;
     }
     if (rows > 0 && stage_many.n < (size_t)4 * rows) ESR_TRY(stage_many.alloc((size_t)4 * rows));
+    S* stage = reinterpret_cast<S*>(stage_many.p);
+    // one launch stages every slot's rows, then one copy per slot
+    std::vector<SlotCopy<T>> jobs(n);
+    int max_n = 0;
     for (int i = 0; i < n; ++i) {
       int m, b;
       ESR_TRY(mesh_of_slot(slots[i], m, b));
       MeshDev& md = *meshes[m];
-      const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
-      S* st = reinterpret_cast<S*>(stage_many.p) + 4 * off[i];
-      k_gather_state<T, S><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, st);
-      ++launches;
-      ESR_CUDA(cudaMemcpyAsync(out[i], st, (size_t)4 * N * sizeof(S), cudaMemcpyDeviceToHost, stream));
+      jobs[i] = SlotCopy<T>{off[i], md.inv.p, md.off, md.hm->n_cells, md.B, b, 0, V{}};
+      max_n = std::max(max_n, md.hm->n_cells);
     }
+    ESR_TRY(launch_slot_copies(jobs, max_n, [&](const SlotCopy<T>* dj, dim3 grid) {
+      k_gather_slots<T, S><<<grid, 256, 0, stream>>>(W.p, dj, stage);
+    }));
+    for (int i = 0; i < n; ++i)
+      ESR_CUDA(cudaMemcpyAsync(out[i], stage + 4 * off[i], (size_t)4 * jobs[i].n_cells * sizeof(S),
+                               cudaMemcpyDeviceToHost, stream));
     ESR_CUDA(cudaStreamSynchronize(stream));
     return ESR_OK;
   }

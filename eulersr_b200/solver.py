@@ -7,6 +7,7 @@ missing, the constructors raise.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import math
 from dataclasses import dataclass, field
 
@@ -21,13 +22,22 @@ def freestream(mach: float, aoa_deg: float = 0.0, gamma: float = 1.4, rho_inf: f
                dtype=np.float64):
     """Conserved freestream state (euler/main.py:28-41): primitive
     (rho, M c cos a, M c sin a, p) converted in ``dtype``."""
+    return np.asarray(_freestream_values(float(mach), float(aoa_deg), float(gamma), float(rho_inf), float(p_inf),
+                                         np.dtype(dtype).str), dtype=dtype)
+
+
+@functools.lru_cache(maxsize=65536)
+def _freestream_values(mach, aoa_deg, gamma, rho_inf, p_inf, dtype_str):
+    """freestream() as a tuple of Python floats (exact copies of the values
+    rounded in the dtype), cached: a batch re-submits the same cases."""
+    dtype = np.dtype(dtype_str)
     c_inf = (gamma * p_inf / rho_inf) ** 0.5
     a = math.radians(aoa_deg)
     prim = np.asarray([rho_inf, mach * c_inf * np.cos(a), mach * c_inf * np.sin(a), p_inf], dtype=dtype)
     t = prim.dtype.type
     rho, u, v, p = prim
     E = p / ((t(gamma) - 1) * t(1.0) ** 2) + t(0.5) * rho * (u ** 2 + v ** 2)
-    return np.asarray([rho, rho * u, rho * v, E], dtype=dtype)
+    return tuple(float(x) for x in np.asarray([rho, rho * u, rho * v, E], dtype=dtype))
 
 
 def clamp_cfl(mach: float, cfl: float) -> float:
@@ -65,9 +75,8 @@ class FlowCase:
         c.cfl = float(clamp_cfl(self.mach, self.cfl) if self.clamp else self.cfl)
         c.tf = float(self.tf)
         c.max_steps = int(self.max_steps)
-        inl = freestream(self.mach, self.aoa_deg, self.gamma, self.rho_inf, self.p_inf, self.dtype)
-        for i in range(4):
-            c.inlet[i] = float(inl[i])
+        c.inlet[:] = _freestream_values(float(self.mach), float(self.aoa_deg), float(self.gamma), float(self.rho_inf),
+                                        float(self.p_inf), np.dtype(self.dtype).str)
         c.rho_inf = float(self.rho_inf)
         c.u_inf = float(self.mach * math.sqrt(self.gamma * self.p_inf / self.rho_inf))
         c.l_ref = float(self.l_ref)
