@@ -303,6 +303,38 @@ def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
         assert np.array_equal(got32[g], got[g].astype(np.float32)), g
 
 
+def test_set_cases_get_states_float64_solver(diamond02, naca02):
+    """The batched transfers on a float64 solver (two meshes, warm and
+    freestream slots) equal the per-slot calls bitwise; float32 host fields
+    are widened exactly."""
+    from eulersr_b200.solver import Solver, FlowCase
+    meshes = [diamond02, naca02]
+    spec = [(0, 2.5, 5.0), (1, 0.9, 1.0), (1, 2.0, 0.0)]
+    cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=0.5) for k, m, a in spec]
+    slots = [0, 1, 2]
+    rng = np.random.default_rng(7)
+    warm = [None, None, np.tile(cases[2].to_c().inlet[:], (naca02.n_cells, 1))
+            * (1.0 + 0.01 * rng.standard_normal((naca02.n_cells, 1)))]
+    a = Solver(meshes, [1, 2], precision='f64', threshold=1e-5, check_every=10)
+    b = Solver(meshes, [1, 2], precision='f64', threshold=1e-5, check_every=10)
+    for g, c, w in zip(slots, cases, warm):
+        a.set_case(g, c, w)
+    b.set_cases(slots, cases, warm)
+    assert np.array_equal(a.dt(), b.dt())
+    a.step(20)
+    b.step(20)
+    got = b.get_states(slots)
+    for g in slots:
+        assert got[g].dtype == np.float64
+        assert np.array_equal(a.get_state(g), got[g]), g
+    w32 = [None, None, warm[2].astype(np.float32)]
+    c = Solver(meshes, [1, 2], precision='f64', threshold=1e-5, check_every=10)
+    c.set_cases(slots, cases, w32)
+    d = Solver(meshes, [1, 2], precision='f64', threshold=1e-5, check_every=10)
+    d.set_cases(slots, cases, [None, None, w32[2].astype(np.float64)])
+    assert all(np.array_equal(x, y) for x, y in zip(c.get_states(slots), d.get_states(slots)))
+
+
 def test_batch_edge_cases(diamond02):
     """Queue edge cases of esr_batch_solve: an empty case list, a case capped
     by max_steps (MAXSTEP), a case that blows up (CFL 40: NONFINITE, retired
