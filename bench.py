@@ -43,7 +43,6 @@ import math
 import os
 import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -54,19 +53,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "converged HR cases/s at ≤0.5% CD err, warm-start vs plain; cell-upd/s; GB/s"
 UNIT = "cell-updates/s"
-MESH_CACHE = Path(os.environ.get("EULERSR_MESH_CACHE", Path(tempfile.gettempdir()) / "eulersr_meshes"))
 
 
 def get_mesh(geom: str, h: float):
-    from eulersr_b200.mesh import Mesh
-    from eulersr_b200.meshing import build_mesh
-    MESH_CACHE.mkdir(parents=True, exist_ok=True)
-    p = MESH_CACHE / f"{geom}_h{h}.npz"
-    if p.exists():
-        return Mesh.load(p)
-    m = build_mesh(geom, h)
-    m.save(p)
-    return m
+    from eulersr_b200.meshing.generate import cached_mesh
+    return cached_mesh(geom, h)
 
 
 def batch_cases(n, seed=1):
@@ -93,10 +84,11 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = Path(tempfile.gettempdir()) / f"eulersr_clocks_{os.getpid()}.csv"
+        self.path = ROOT / ".bench_tmp" / f"clocks_{os.getpid()}.csv"
 
     def start(self):
         try:
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)

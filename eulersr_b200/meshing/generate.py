@@ -23,6 +23,7 @@ reference writes ``<geom>_h<h>.npy`` (``euler/meshing/diamond.py:111-117``).
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -52,6 +53,26 @@ GEOMS = {
     "diamond_alpha10": _diamond("diamond_alpha10", half_angle_deg=10.0),
     "diamond_big": _diamond("diamond_big", Lx=6.0, Ly=6.0),
 }
+
+
+def cache_dir() -> Path:
+    """Where generated meshes are kept between runs: $EULERSR_MESH_CACHE, else
+    ``.mesh_cache`` beside the package."""
+    env = os.environ.get("EULERSR_MESH_CACHE")
+    return Path(env) if env else Path(__file__).resolve().parents[2] / ".mesh_cache"
+
+
+def cached_mesh(geom: str, h: float):
+    """The mesh of ``geom`` at size h from the cache, built and stored on
+    first use (any geometry ``build_mesh`` knows, with its default box)."""
+    from ..mesh import Mesh
+    from .mesher import build_mesh
+    p = cache_dir() / f"{geom}_h{h}.npz"
+    if p.exists():
+        return Mesh.load(p)
+    m = build_mesh(geom, h)
+    m.save(p)
+    return m
 
 
 def mesh_path(out_dir, geom: str, h: float) -> Path:

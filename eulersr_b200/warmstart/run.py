@@ -27,31 +27,17 @@ from __future__ import annotations
 
 import argparse
 import json
-import os
-import tempfile
 import time
 from pathlib import Path
 
 import numpy as np
 import torch
 
-from ..mesh import Mesh
-from ..meshing import build_mesh
+from ..meshing.generate import cached_mesh
 from ..solver import DeviceMesh, FlowCase, Solver
 from .features import MeshPair
 from .mlp import MLP
 from .pipeline import WarmStart, build_training_set, draw_cases, eval_loss, pressure_gradients, primitives, train
-
-
-def cached_mesh(geom, h):
-    d = Path(os.environ.get("EULERSR_MESH_CACHE", Path(tempfile.gettempdir()) / "eulersr_meshes"))
-    d.mkdir(parents=True, exist_ok=True)
-    p = d / f"{geom}_h{h}.npz"
-    if p.exists():
-        return Mesh.load(p)
-    m = build_mesh(geom, h)
-    m.save(p)
-    return m
 
 
 def solve(dm, machs, aoas, *, slots=256, precision="f32", stop_rule="reference", threshold=1e-30, check_every=25,
