@@ -430,7 +430,7 @@ def main():
                 "traffic": traffic, "traffic_source": f"ncu capture in profiles/{pf.name}, per item, scaled by items",
                 "kernel": "k_flux (K2)", "peak_source": peak_kind, "kernel_ms": kt["flux_ms"],
                 "recon_ms": kt["recon_ms"], "alg_bytes_per_launch": alg_k2,
-                "note": "K2 is issue-bound (~800 instructions per item); see profiles/"}
+                "note": "K2 is issue-bound (~645 instructions per item and stage); see profiles/"}
 
     # end to end through the public API with host buffers
     e2e = None
