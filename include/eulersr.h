@@ -200,7 +200,9 @@ int esr_clear_slot(esr_solver* solver, int32_t slot);
  * (W_init NULL, or a NULL entry: freestream). The host fields are copied
  * asynchronously (pinned buffers copy fastest), the dt of every filled slot
  * comes from one reduction, and the call synchronises once. A slot may be
- * listed once; as in esr_set_case, the slot decides the mesh. */
+ * listed once; as in esr_set_case, the slot decides the mesh. Every case is
+ * checked before anything changes: a call that fails on an argument leaves
+ * every slot as it was. */
 int esr_set_cases(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
                   const double* const* W_init);
 /* esr_get_state for n slots at once into out[i] (caller's cell order); one
