@@ -115,6 +115,13 @@ class TrainData:
     inv_den: torch.Tensor
 
 
+def loss_weights(hr_gradp, factor=1.0):
+    """Shock weights of one case's rows (preprocessing/dataset.py:168-170,
+    shock_weight_factor 1 by default): min(1 + factor |grad p| / mean |grad p|, 5)."""
+    gp = np.sqrt((np.asarray(hr_gradp) ** 2).sum(-1))
+    return np.minimum(1.0 + factor * gp / (gp.mean() + 1e-8), 5.0).astype(np.float32)
+
+
 def build_training_set(ws: WarmStart, lr_states, lr_gradp, hr_states, hr_gradp, machs, aoas, gamma=1.4):
     """Stack every training case's rows on the GPU; sets ws.mu/ws.sig from the HR targets."""
     hr_prims = [primitives(W, gamma).astype(np.float32) for W in hr_states]
@@ -131,8 +138,7 @@ def build_training_set(ws: WarmStart, lr_states, lr_gradp, hr_states, hr_gradp, 
         bs.append(base[:n])
         t = (hr_prims[i] - mu) / sig
         ts.append(torch.from_numpy(t.astype(np.float32)).to(ws.device))
-        gp = np.sqrt((hr_gradp[i] ** 2).sum(-1))
-        wts.append(torch.from_numpy(np.minimum(1.0 + gp / (gp.mean() + 1e-8), 5.0).astype(np.float32)).to(ws.device))
+        wts.append(torch.from_numpy(loss_weights(hr_gradp[i])).to(ws.device))
     tgt = torch.cat(ts)
     inv_den = (1.0 / ((tgt.double() ** 2).mean(0) + 1e-8)).float()
     return TrainData(torch.cat(Xs), torch.cat(bs), tgt, torch.cat(wts), inv_den.contiguous()), mu, sig

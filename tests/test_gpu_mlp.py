@@ -93,6 +93,59 @@ def test_idw_kernel_matches_formula():
     assert np.max(np.abs(out.cpu().numpy() - ref)) <= 2e-6 * max(1.0, np.abs(ref).max())
 
 
+def test_feature_and_decode_kernels_match_formula():
+    """esr_mlp_features builds the 13 inputs of preprocessing/dataset.py:140-176
+    (geometry statics, IDW primitives normalised by mu/sig, asinh of the IDW
+    pressure gradient over sig_p, normalised Mach and alpha; zero padding) in
+    BF16 plus the float32 IDW base; esr_mlp_decode turns normalised primitives
+    back into conserved rows with the density/pressure floors."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    rng = np.random.default_rng(5)
+    rows, ld = 777, 128
+    stat5 = rng.standard_normal((rows, 5)).astype(np.float32)
+    prim = (rng.standard_normal((rows, 4)) * [0.3, 0.5, 0.2, 0.4] + [1.0, 2.0, 0.1, 1.0]).astype(np.float32)
+    gradp = (rng.standard_normal((rows, 2)) * 5.0).astype(np.float32)
+    mu = np.array([1.1, 1.9, 0.05, 0.9], np.float32)
+    sig = np.array([0.25, 0.6, 0.3, 0.5], np.float32)
+    mach_n, aoa_n = np.float32(0.37), np.float32(-0.6)
+    d = {k: torch.from_numpy(v).cuda() for k, v in dict(stat5=stat5, prim=prim, gradp=gradp, mu=mu, sig=sig).items()}
+    X = torch.full((rows, ld), 7.0, dtype=torch.bfloat16, device="cuda")
+    base = torch.empty((rows, 4), dtype=torch.float32, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())   # noqa: E731
+    F.check(F.lib().esr_mlp_features(p(d["stat5"]), p(d["prim"]), p(d["gradp"]), rows, float(mach_n), float(aoa_n),
+                                     p(d["mu"]), p(d["sig"]), ld, p(X), p(base), None))
+    torch.cuda.synchronize()
+    q = (prim - mu) / sig                                  # float32, correctly rounded on both sides
+    assert np.array_equal(base.cpu().numpy(), q)
+    want = np.zeros((rows, ld), np.float32)
+    want[:, :5] = stat5
+    want[:, 5:9] = q
+    want[:, 9:11] = np.arcsinh(gradp / (sig[3] + np.float32(1e-8)))
+    want[:, 11], want[:, 12] = mach_n, aoa_n
+    got = X.float().cpu().numpy()
+    bf = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(torch.bfloat16).float().numpy()   # noqa: E731
+    assert np.array_equal(got[:, :9], bf(want[:, :9]))
+    assert np.array_equal(got[:, 11:], bf(want[:, 11:]))
+    # asinh may differ from numpy's in the last float32 bit: one BF16 step at most
+    assert np.all(np.abs(got[:, 9:11] - bf(want[:, 9:11])) <= np.abs(bf(want[:, 9:11])) * 2.0 ** -7 + 1e-30)
+    # decode: rho = max(q0 sig0 + mu0, floor), u, v, p = max(q3 sig3 + mu3, floor) -> conserved float64
+    pred = rng.standard_normal((rows, 4)).astype(np.float32)
+    pred[:5, 0] = -10.0                                    # density below the floor
+    pred[5:10, 3] = -10.0                                  # pressure below the floor
+    W = torch.empty((rows, 4), dtype=torch.float64, device="cuda")
+    dp = torch.from_numpy(pred).cuda()
+    F.check(F.lib().esr_mlp_decode(p(dp), rows, p(d["mu"]), p(d["sig"]), 1.4, 0.05, 0.05, p(W), None))
+    torch.cuda.synchronize()
+    r = np.maximum(pred[:, 0].astype(np.float64) * sig[0] + mu[0], 0.05)
+    u = pred[:, 1].astype(np.float64) * sig[1] + mu[1]
+    v = pred[:, 2].astype(np.float64) * sig[2] + mu[2]
+    pr = np.maximum(pred[:, 3].astype(np.float64) * sig[3] + mu[3], 0.05)
+    ref = np.stack([r, r * u, r * v, pr / 0.4 + 0.5 * r * (u * u + v * v)], 1)
+    assert np.allclose(W.cpu().numpy(), ref, rtol=2e-6, atol=1e-6)
+    assert np.all(W.cpu().numpy()[:5, 0] == np.float32(0.05))
+
+
 @pytest.mark.parametrize("ta,tb,epi,M,N,K,splits", [
     (0, 0, 1, 256, 256, 256, 1),     # forward: z = X W^T + b, h = res + relu(z)
     (0, 0, 1, 128, 256, 128, 1),     # input layer (K = 128)

@@ -191,3 +191,15 @@ def test_fit_order():
     p, r2, n = fit_order(rows, "e")
     assert n == 4 and p == pytest.approx(1.5, abs=1e-10) and r2 == pytest.approx(1.0, abs=1e-12)
     assert fit_order(rows[:2], "e")[0] is None
+
+
+def test_loss_weights_formula():
+    """Shock weights of the training rows (preprocessing/dataset.py:168-170):
+    1 + |grad p| / mean |grad p|, capped at 5."""
+    from eulersr_b200.warmstart.pipeline import loss_weights
+    g = np.array([[0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [3.0, 4.0], [0.0, 1.0], [60.0, 80.0]], np.float32)
+    gp = np.array([0.0, 0.0, 0.0, 5.0, 1.0, 100.0])
+    want = np.minimum(1.0 + gp / gp.mean(), 5.0)
+    assert np.allclose(loss_weights(g), want, rtol=1e-6)
+    assert loss_weights(g).dtype == np.float32 and loss_weights(g).max() == 5.0
+    assert np.allclose(loss_weights(g, factor=0.0), 1.0)
