@@ -203,3 +203,28 @@ def test_loss_weights_formula():
     assert np.allclose(loss_weights(g), want, rtol=1e-6)
     assert loss_weights(g).dtype == np.float32 and loss_weights(g).max() == 5.0
     assert np.allclose(loss_weights(g, factor=0.0), 1.0)
+
+
+def test_wall_features_distance_and_normal():
+    """Distance to the nearest of 8 samples per wall face and the face normal
+    turned towards the query point (utils/aero.py:154-177), on the diamond."""
+    from conftest import load_mesh
+    from eulersr_b200.warmstart.features import wall_features
+    m = load_mesh("diamond_h0.1")
+    cx, cy = m.metadata["center"]["cx"], m.metadata["center"]["cy"]
+    chord, height = m.metadata["chord"], m.metadata["height"]
+    x_le, top = cx - chord / 2, cy + height / 2
+    eps = math.atan(height / chord)
+    # the upper-front face's outward normal and a point 0.1 off its middle
+    n_uf = np.array([-math.sin(eps), math.cos(eps)])
+    mid_uf = np.array([x_le + chord / 4, cy + height / 4])
+    q = np.array([[cx, top + 0.3], [x_le - 0.2, cy], mid_uf + 0.1 * n_uf, mid_uf - 0.03 * n_uf])
+    d, n = wall_features(m, q)
+    assert d[0] == pytest.approx(0.3, abs=1e-12) and n[0, 1] > 0.99   # the top vertex is a sample
+    assert d[1] == pytest.approx(0.2, abs=1e-12) and n[1, 0] < 0      # the leading edge is a sample
+    faces = m.faces[m.face_markers == m.force_marker()]
+    seg = np.linalg.norm(m.points[faces[:, 1]] - m.points[faces[:, 0]], axis=1).max()
+    assert 0.1 - 1e-12 <= d[2] <= math.hypot(0.1, seg / 14) + 1e-12     # samples 1/7 of a face apart
+    assert n[2] @ n_uf == pytest.approx(1.0, abs=1e-9)
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0)
+    assert n[3] @ n_uf == pytest.approx(-1.0, abs=1e-9)               # turned towards a point inside
