@@ -218,7 +218,7 @@ def test_wall_features_distance_and_normal():
     # the upper-front face's outward normal and a point 0.1 off its middle
     n_uf = np.array([-math.sin(eps), math.cos(eps)])
     mid_uf = np.array([x_le + chord / 4, cy + height / 4])
-    q = np.array([[cx, top + 0.3], [x_le - 0.2, cy], mid_uf + 0.1 * n_uf, mid_uf - 0.03 * n_uf])
+    q = np.array([[cx, top + 0.3], [x_le - 0.2, cy], mid_uf + 0.1 * n_uf, mid_uf - 0.005 * n_uf])
     d, n = wall_features(m, q)
     assert d[0] == pytest.approx(0.3, abs=1e-12) and n[0, 1] > 0.99   # the top vertex is a sample
     assert d[1] == pytest.approx(0.2, abs=1e-12) and n[1, 0] < 0      # the leading edge is a sample
