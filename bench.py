@@ -447,8 +447,12 @@ def main():
             pinned[b][:] = freestream(c.mach, c.aoa_deg, dtype=np.float32)[None, :]
         h2d = int(sum(p.nbytes for p in pinned))
         outs = pinned  # results land in the same pinned buffers
-        e2e_steps = max(2, min(args.steps, 5))
+        e2e_steps = max(3, args.steps)
         slots = list(range(B))
+        # one untimed round first: the staging buffers are allocated on first use
+        s.set_cases(slots, cases, pinned)
+        s.step(args.chunk)
+        s.get_states(slots, outs)
         barrier(world)
         t0 = time.perf_counter()
         for _ in range(e2e_steps):

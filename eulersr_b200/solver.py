@@ -218,23 +218,43 @@ class Solver:
         pinned host arrays copy fastest."""
         n = len(slots)
         sl = np.ascontiguousarray(slots, dtype=np.int32)
-        carr = (F.Case * n)(*[c.to_c() for c in cases])
+        carr = self._case_array(cases)
         given = [W for W in (W_inits or []) if W is not None]
         f32 = bool(given) and all(np.asarray(W).dtype == np.float32 for W in given)
-        ctype = C.c_float if f32 else C.c_double
         keep, arr = [], None
         if W_inits is not None:
-            arr = (C.POINTER(ctype) * n)()
+            want = np.float32 if f32 else np.float64
+            ncell = self._cells_of_slots(sl)
+            addr = np.zeros(n, dtype=np.uintp)
             for i, W in enumerate(W_inits):
                 if W is None:
                     continue
-                W = np.ascontiguousarray(W, dtype=np.float32 if f32 else np.float64)
-                if W.shape != (self._n_cells(int(sl[i])), 4):
+                W = np.ascontiguousarray(W, dtype=want)
+                if W.shape != (ncell[i], 4):
                     raise ValueError(f"init field {i} has shape {W.shape}")
                 keep.append(W)
-                arr[i] = F.ptr(W, ctype)
+                addr[i] = W.ctypes.data
+            arr = addr.ctypes.data
         fn = F.lib().esr_set_cases_f32 if f32 else F.lib().esr_set_cases
         F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), carr, arr))
+
+    def _case_array(self, cases):
+        """The C records of ``cases``, reused while every case's fields are
+        unchanged (a serving loop re-submits the same cases)."""
+        key = tuple(tuple(vars(c).values()) for c in cases)
+        cached = getattr(self, "_carr_cache", None)
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        carr = (F.Case * len(cases))(*[c.to_c() for c in cases])
+        self._carr_cache = (key, carr)
+        return carr
+
+    def _cells_of_slots(self, sl):
+        ncell = getattr(self, "_slot_cells", None)
+        if ncell is None:
+            ncell = np.array([self.meshes[int(m)].n_cells for m in self.slot_mesh], dtype=np.int64)
+            self._slot_cells = ncell
+        return ncell[np.asarray(sl, dtype=np.int64)]
 
     def get_states(self, slots, out=None, dtype=np.float64):
         """get_state for many slots at once into ``out`` (C-contiguous
@@ -242,17 +262,18 @@ class Solver:
         ``dtype`` when None); one synchronisation."""
         n = len(slots)
         sl = np.ascontiguousarray(slots, dtype=np.int32)
+        ncell = self._cells_of_slots(sl)
         if out is None:
-            out = [np.empty((self._n_cells(int(g)), 4), dtype=dtype) for g in sl]
+            out = [np.empty((int(k), 4), dtype=dtype) for k in ncell]
         f32 = out[0].dtype == np.float32 if n else False
         want = np.float32 if f32 else np.float64
-        for g, o in zip(sl, out):
-            if o.shape != (self._n_cells(int(g)), 4) or o.dtype != want or not o.flags.c_contiguous:
+        addr = np.zeros(n, dtype=np.uintp)
+        for i, o in enumerate(out):
+            if o.shape != (ncell[i], 4) or o.dtype != want or not o.flags.c_contiguous:
                 raise ValueError("get_states: outputs must be C-contiguous (n_cells, 4) arrays of one dtype")
-        ctype = C.c_float if f32 else C.c_double
-        arr = (C.POINTER(ctype) * n)(*[F.ptr(o, ctype) for o in out])
+            addr[i] = o.ctypes.data
         fn = F.lib().esr_get_states_f32 if f32 else F.lib().esr_get_states
-        F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), arr))
+        F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), addr.ctypes.data))
         return out
 
     def set_state(self, slot: int, W):
