@@ -16,7 +16,6 @@ runs do), float32 otherwise.
 from __future__ import annotations
 
 import json
-import math
 import os
 import time
 from pathlib import Path
@@ -26,7 +25,7 @@ import numpy as np
 from .config import AOA_CASES_LC, KNOWN_CASES_LC, build_config_from_cli, format_snapshot_name, \
     load_default_config, load_mesh, setup_dirs
 from .mesh import Mesh
-from .solver import DeviceMesh, FlowCase, Solver, clamp_cfl, freestream
+from .solver import DeviceMesh, FlowCase, Solver, freestream
 
 CFG = load_default_config()
 

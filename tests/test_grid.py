@@ -1,6 +1,4 @@
 """The grid driver's host logic (slurm/run_euler_grid.py:24-56,60-92) on CPU."""
-import pytest
-
 from conftest import ROOT
 from eulersr_b200 import grid as G
 
