@@ -51,7 +51,10 @@ std::vector<int> rcm_order(int n, const std::vector<int>& nbr) {
         int j = nbr[3 * c + k];
         if (j >= 0 && !seen[j]) nb[m++] = j;
       }
-      std::sort(nb, nb + m, [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+      // at most three: insertion sort by (degree, index)
+      auto before = [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); };
+      for (int i = 1; i < m; ++i)
+        for (int j = i; j > 0 && before(nb[j], nb[j - 1]); --j) std::swap(nb[j], nb[j - 1]);
       for (int i = 0; i < m; ++i) {
         seen[nb[i]] = 1;
         q.push_back(nb[i]);
