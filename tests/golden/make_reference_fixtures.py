@@ -1,0 +1,54 @@
+"""Golden vectors from EulerSR's own NumPy utilities, for the CPU tests.
+
+The reference's solver needs JAX, which is not installed, but three of its
+host utilities import with NumPy and SciPy alone; this script runs them on
+seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
+
+* ``utils/metrics.py:9-14`` idw_weights (p = 2 inverse-distance weights);
+* ``utils/aero.py:154-177`` wall_features (wall distance and normal);
+* ``utils/aero.py:28-72,85-110`` build_wall_cache + aero_coeffs (CL, CD).
+
+Run from the repository root with the reference checkout as the argument:
+
+    python tests/golden/make_reference_fixtures.py /root/reference
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+
+
+def main(ref_root: str) -> Path:
+    sys.path.insert(0, str(ROOT))
+    from eulersr_b200.mesh import Mesh
+    sys.dont_write_bytecode = True                     # nothing is written into the reference checkout
+    sys.path.insert(0, str(Path(ref_root)))
+    from utils.aero import aero_coeffs, build_wall_cache, wall_features
+    from utils.metrics import idw_weights
+
+    mesh = Mesh.load(HERE / "diamond_h0.2.npz")
+    rng = np.random.default_rng(11)
+    dist = rng.uniform(1e-4, 0.5, (500, 6))
+    dist[:5, 0] = 0.0                                  # coincident points: the eps term decides
+    w = idw_weights(dist)
+    query = np.concatenate([mesh.barycenter, rng.uniform([0.5, 1.5], [2.5, 2.5], (300, 2))])
+    wd, wn = wall_features(mesh, query)
+    n = mesh.n_cells
+    prim = np.stack([rng.uniform(0.5, 2.0, n), rng.uniform(0.5, 3.0, n), rng.uniform(-0.5, 0.5, n),
+                     rng.uniform(0.5, 3.0, n)], 1)
+    mach = 2.0
+    ac = aero_coeffs(prim, build_wall_cache(mesh), mach)
+    out = HERE / "reference_utils.npz"
+    np.savez_compressed(out, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
+                        aero_prim=prim, aero_mach=np.float64(mach), aero_cl=np.float64(ac["CL"]),
+                        aero_cd=np.float64(ac["CD"]))
+    return out
+
+
+if __name__ == "__main__":
+    print(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

@@ -1,0 +1,49 @@
+"""The oracle and the package's host utilities against golden vectors made
+by EulerSR's own NumPy code (tests/golden/make_reference_fixtures.py):
+IDW weights (utils/metrics.py:9-14), wall distance and normal
+(utils/aero.py:154-177) and the host CL/CD (utils/aero.py:85-110)."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_mesh
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return np.load(GOLDEN / "reference_utils.npz")
+
+
+def test_idw_matches_reference_weights(ref):
+    """The oracle's IDW weights equal the reference's, and its prediction is
+    those weights (rounded to float32, as eval/core.py:135-142 applies them)
+    on the neighbours' values; the GPU kernel is held to the oracle."""
+    from oracle import euler_oracle as O
+    dist, w = ref["idw_dist"], ref["idw_w"]
+    assert np.allclose(O.idw_weights(dist), w, rtol=1e-14, atol=0)
+    rng = np.random.default_rng(2)
+    src = rng.standard_normal((400, 4)).astype(np.float32)
+    idx = rng.integers(0, 400, dist.shape)
+    got = O.idw_predict(src, idx, dist)
+    want = (w.astype(np.float32)[:, :, None] * src[idx]).sum(axis=1)
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+
+
+def test_wall_features_match_reference(ref):
+    from eulersr_b200.warmstart.features import wall_features
+    mesh = load_mesh("diamond_h0.2")
+    d, n = wall_features(mesh, ref["wall_query"])
+    assert np.allclose(d, ref["wall_dist"], rtol=0, atol=1e-12)
+    assert np.allclose(n, ref["wall_normal"], rtol=0, atol=1e-9)
+
+
+def test_host_force_coefficients_match_reference(ref):
+    """postproc.force_coefficients against the reference's aero_coeffs, which
+    rounds the wall normals and lengths to float32 (hence 1e-6)."""
+    from eulersr_b200.postproc import force_coefficients
+    mesh = load_mesh("diamond_h0.2")
+    prim = ref["aero_prim"]
+    r, u, v, p = prim.T
+    W = np.stack([r, r * u, r * v, p / 0.4 + 0.5 * r * (u * u + v * v)], 1)
+    cd, cl = force_coefficients(mesh, W, float(ref["aero_mach"]))
+    assert cd == pytest.approx(float(ref["aero_cd"]), rel=1e-6, abs=1e-9)
+    assert cl == pytest.approx(float(ref["aero_cl"]), rel=1e-6, abs=1e-9)
