@@ -228,3 +228,19 @@ def test_wall_features_distance_and_normal():
     assert n[2] @ n_uf == pytest.approx(1.0, abs=1e-9)
     assert np.allclose(np.linalg.norm(n, axis=1), 1.0)
     assert n[3] @ n_uf == pytest.approx(-1.0, abs=1e-9)               # turned towards a point inside
+
+
+def test_gas_dynamics_textbook_values():
+    """Prandtl-Meyer angles and the M=2, 10-degree oblique shock and
+    expansion against the standard tables (gamma 1.4)."""
+    from eulersr_b200.postproc import expansion, oblique_shock, prandtl_meyer
+    for M, nu in ((1.5, 11.91), (2.0, 26.38), (3.0, 49.76)):
+        assert math.degrees(prandtl_meyer(M)) == pytest.approx(nu, abs=0.01)
+    beta, M2, pr = oblique_shock(2.0, math.radians(10.0))
+    assert math.degrees(beta) == pytest.approx(39.31, abs=0.01)
+    assert M2 == pytest.approx(1.64, abs=0.005) and pr == pytest.approx(1.7066, abs=1e-4)
+    M2e, pre = expansion(2.0, math.radians(10.0))
+    assert math.degrees(prandtl_meyer(M2e)) == pytest.approx(36.38, abs=0.01)
+    assert M2e == pytest.approx(2.385, abs=0.002)
+    # isentropic: p2/p1 from the stagnation-pressure ratio of the two Mach numbers
+    assert pre == pytest.approx(((1 + 0.2 * 4.0) / (1 + 0.2 * M2e ** 2)) ** 3.5, rel=1e-12)
