@@ -6,7 +6,11 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
 
 * ``utils/metrics.py:9-14`` idw_weights (p = 2 inverse-distance weights);
 * ``utils/aero.py:154-177`` wall_features (wall distance and normal);
-* ``utils/aero.py:28-72,85-110`` build_wall_cache + aero_coeffs (CL, CD).
+* ``utils/aero.py:28-72,85-110`` build_wall_cache + aero_coeffs (CL, CD);
+* ``euler/graph.py:5-108`` export_graph on the golden diamond mesh with one
+  seeded snapshot, written by the reference itself as ``reference_graph.npz``;
+* ``euler/config.py:24-30,82-103`` the default configuration and the output
+  naming (h tag, condition tag, snapshot name) into ``reference_config.json``.
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -14,6 +18,7 @@ Run from the repository root with the reference checkout as the argument:
 """
 from __future__ import annotations
 
+import json
 import sys
 from pathlib import Path
 
@@ -30,6 +35,9 @@ def main(ref_root: str) -> Path:
     sys.path.insert(0, str(Path(ref_root)))
     from utils.aero import aero_coeffs, build_wall_cache, wall_features
     from utils.metrics import idw_weights
+    sys.path.insert(0, str(Path(ref_root) / "euler"))
+    from graph import export_graph
+    import config as ref_config
 
     mesh = Mesh.load(HERE / "diamond_h0.2.npz")
     rng = np.random.default_rng(11)
@@ -43,8 +51,22 @@ def main(ref_root: str) -> Path:
                      rng.uniform(0.5, 3.0, n)], 1)
     mach = 2.0
     ac = aero_coeffs(prim, build_wall_cache(mesh), mach)
+    snap = rng.standard_normal((n, 4))
+    export_graph(mesh, {0.5: snap, 1.25: 2 * snap}, [1.0, 2.0, 0.1, 4.5], str(HERE / "reference_graph.npz"))
+    names = []
+    base = ref_config.load_default_config()
+    for case, m_c, a_c, t, h in (("diamond", 2.5, 5.0, 1.234, 0.025), ("naca0012", 0.8, -2.5, 10.0, 0.1),
+                                 ("bump", 1.4, 3.0, 0.5, 0.05), ("NACA2412", 3.0, 0.0, 123.456, None),
+                                 ("rae2822", 0.75, 2.31, 7.0, 0.0125)):
+        cfg = dict(base, case=case, Mach=m_c, aoa=a_c)
+        mesh_h = type("M", (), {"metadata": {} if h is None else {"h": h}})()
+        names.append(dict(case=case, Mach=m_c, aoa=a_c, t=t, h=h, h_tag=ref_config.format_h(mesh_h),
+                          condition=ref_config.format_condition_tag(cfg),
+                          snapshot=ref_config.format_snapshot_name(cfg, t)))
+    (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names}, indent=1,
+                                                           sort_keys=True) + "\n")
     out = HERE / "reference_utils.npz"
-    np.savez_compressed(out, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
+    np.savez_compressed(out, graph_snapshot=snap, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
                         aero_prim=prim, aero_mach=np.float64(mach), aero_cl=np.float64(ac["CL"]),
                         aero_cd=np.float64(ac["CD"]))
     return out

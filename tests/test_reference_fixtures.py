@@ -47,3 +47,37 @@ def test_host_force_coefficients_match_reference(ref):
     cd, cl = force_coefficients(mesh, W, float(ref["aero_mach"]))
     assert cd == pytest.approx(float(ref["aero_cd"]), rel=1e-6, abs=1e-9)
     assert cl == pytest.approx(float(ref["aero_cl"]), rel=1e-6, abs=1e-9)
+
+
+def test_graph_npz_matches_reference_export(ref):
+    """Every array the reference's euler/graph.py export_graph wrote for the
+    golden mesh (nodes, directed edges with their normals, lengths, vectors,
+    face ids, boundary markers and kinds, boundary faces, inlet state,
+    snapshots) is identical in the package's graph.npz."""
+    mesh = load_mesh("diamond_h0.2")
+    snap = ref["graph_snapshot"]
+    ours = mesh.graph_arrays({0.5: snap, 1.25: 2 * snap}, [1.0, 2.0, 0.1, 4.5])
+    theirs = np.load(GOLDEN / "reference_graph.npz")
+    assert set(theirs.files) <= set(ours)
+    for k in theirs.files:
+        assert ours[k].dtype == theirs[k].dtype, k
+        assert np.array_equal(ours[k], theirs[k]), k
+
+
+def test_config_defaults_and_output_names_match_reference():
+    """The default configuration (euler/config.toml through euler/config.py)
+    and the output names the reference builds from a configuration: mesh-size
+    tag, condition tag, snapshot name."""
+    import json
+    from eulersr_b200 import config as Cfg
+    ref = json.loads((GOLDEN / "reference_config.json").read_text())
+    ours = Cfg.load_default_config()
+    for k, v in ref["default"].items():
+        assert ours.get(k) == v, (k, ours.get(k), v)
+    base = dict(ours)
+    for r in ref["names"]:
+        cfg = dict(base, case=r["case"], Mach=r["Mach"], aoa=r["aoa"])
+        mesh = type("M", (), {"metadata": {} if r["h"] is None else {"h": r["h"]}})()
+        assert Cfg.format_h(mesh) == r["h_tag"]
+        assert Cfg.format_condition_tag(cfg) == r["condition"]
+        assert Cfg.format_snapshot_name(cfg, r["t"]) == r["snapshot"]
