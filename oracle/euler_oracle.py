@@ -11,8 +11,10 @@ hosts, and the reference ships no tests, fixtures or golden vectors. This
 module therefore restates the reference source line by line (citations below
 are ``path:line`` inside the EulerSR checkout) and is pinned instead by
 known-answer properties (freestream preservation, HLLC consistency, LSQ
-exactness on linear fields) and by the analytic diamond shock-expansion theory
-(``oracle/theory.py``).
+exactness on linear fields) and by the analytic diamond shock-expansion theory.
+Where the reference runs without JAX (its NumPy utilities), it is pinned
+directly: ``idw_weights`` below equals ``utils/metrics.py:9-14`` on the golden
+vectors of ``tests/golden/reference_utils.npz``.
 
 All arithmetic is done in the dtype of the input arrays (float32 or float64),
 as the reference does under ``JAX_ENABLE_X64`` false / true. Quirks that are
