@@ -94,7 +94,7 @@ template <typename T> constexpr bool kFast = sizeof(T) == 4;
 // Resident 256-thread blocks per SM the float32 cell kernels are compiled for
 // (register caps 65536 / (256 x n)); float64 kernels take what they need.
 #ifndef ESR_K1_MINB
-#define ESR_K1_MINB 6
+#define ESR_K1_MINB 8
 #endif
 #ifndef ESR_K1_MINB_LOCAL
 #define ESR_K1_MINB_LOCAL 4
