@@ -448,7 +448,7 @@ def main():
         outs = pinned  # results land in the same pinned buffers
         e2e_steps = max(3, args.steps)
         slots = list(range(B))
-        # one untimed round first: the staging buffers are allocated on first use
+        # one untimed pass first: the staging buffers are allocated on first use
         s.set_cases(slots, cases, pinned)
         s.step(args.chunk)
         s.get_states(slots, outs)

@@ -1267,7 +1267,7 @@ struct SolverT : SolverBase {
     return ESR_OK;
   }
 
-  // One polling round: a few chunks (doubling up to 32 per round), then the
+  // One poll: a few chunks (doubling up to 32 per call), then the
   // done counter. A failure abandons the batch.
   int batch_poll(int* n_done) {
     if (!pend) return fail(ESR_ERR_STATE, "batch_poll: no batch pending");
