@@ -120,3 +120,21 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_ctypes_signatures_match_header_prototypes():
+    """Every function the ctypes layer binds takes as many arguments as its
+    prototype in include/eulersr.h, and every prototype has a binding."""
+    import re
+    from eulersr_b200 import _ffi as F
+    txt = re.sub(r"/\*.*?\*/", "", F.HEADER.read_text(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(esr_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
+        params = " ".join(m.group(2).split())
+        protos[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    assert len(protos) >= 25
+    missing = sorted(set(protos) - set(F._SIGS))
+    assert not missing, missing
+    for name, (_, args) in F._SIGS.items():
+        assert name in protos, name
+        assert len(args) == protos[name], (name, len(args), protos[name])
