@@ -160,7 +160,8 @@ typedef struct esr_result {
     int32_t stopping_step;    /* first step of the confirming streak, else N */
     int32_t steps;            /* steps actually advanced */
     int32_t n_max;            /* N = int(tf/dt)+1 (capped by max_steps) */
-    int32_t case_index;       /* index into the submitted case list */
+    int32_t case_index;       /* batch solves: index into the submitted case list; esr_run /
+                                 esr_get_results: the slot of a case set on it, else -1 */
     double dt;                /* global dt of the case (0 in local mode) */
     double last_rel;          /* last stop-rule value */
     double cd, cl;            /* body-axis pressure force coefficients at the end */
