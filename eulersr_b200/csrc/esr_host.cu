@@ -1101,15 +1101,12 @@ struct SolverT : SolverBase {
   // Release the pending batch. clear_slots: the batch was abandoned before it
   // finished, so its running cases are stopped (their slots go inactive).
   int batch_cancel(bool clear_slots = true) {
+    if (!pend) return ESR_OK;   // nothing pending: nothing changes
     int rc = ESR_OK;
-    if (pend) {
-      if (clear_slots && pend->n > 0) {
-        cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream);
-      }
-      // nothing of the batch may still run when its buffers are freed
-      cudaError_t e = cudaStreamSynchronize(stream);
-      if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch_cancel: ") + cudaGetErrorString(e));
-    }
+    if (clear_slots && pend->n > 0) cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream);
+    // nothing of the batch may still run when its buffers are freed
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch_cancel: ") + cudaGetErrorString(e));
     pend.reset();
     batch_busy = false;
     for (int g = 0; g < n_slots; ++g) hcase_index[g] = -1;

@@ -288,8 +288,9 @@ int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases,
  * of esr_batch_solve. esr_batch_results (valid once *n_done == n_cases)
  * fills results[n_cases] and, when final_states is non-NULL, final_states[i]
  * (NULL entries skipped), then releases the batch. esr_batch_cancel
- * abandons a pending batch: running cases stop and their slots go inactive.
- * A failing poll cancels the batch itself. */
+ * abandons a pending batch: running cases stop and their slots go inactive
+ * (without a pending batch it does nothing). A failing poll cancels the
+ * batch itself. */
 int esr_batch_submit(esr_solver* solver, const esr_case* cases, int32_t n_cases,
                      const double* const* init_fields, int32_t want_states);
 int esr_batch_poll(esr_solver* solver, int32_t* n_done);
