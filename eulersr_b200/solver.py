@@ -217,6 +217,8 @@ class Solver:
         are all float32 go through the float32 entry point (half the bytes);
         pinned host arrays copy fastest."""
         n = len(slots)
+        if len(cases) != n or (W_inits is not None and len(W_inits) != n):
+            raise ValueError("set_cases: slots, cases and W_inits must have the same length")
         sl = np.ascontiguousarray(slots, dtype=np.int32)
         carr = self._case_array(cases)
         given = [W for W in (W_inits or []) if W is not None]
@@ -265,6 +267,8 @@ class Solver:
         ncell = self._cells_of_slots(sl)
         if out is None:
             out = [np.empty((int(k), 4), dtype=dtype) for k in ncell]
+        if len(out) != n:
+            raise ValueError("get_states: one output array per slot")
         f32 = out[0].dtype == np.float32 if n else False
         want = np.float32 if f32 else np.float64
         addr = np.zeros(n, dtype=np.uintp)
