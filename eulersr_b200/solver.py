@@ -373,15 +373,7 @@ class Solver:
         n = len(cases)
         carr = (F.Case * n)(*[c.to_c() for c in cases])
         res = (F.Result * n)()
-        keep = []
-        init_arr = None
-        if init_fields is not None:
-            init_arr = (F._f64p * n)()
-            for i, f in enumerate(init_fields):
-                if f is not None:
-                    a = F.f64(f)
-                    keep.append(a)
-                    init_arr[i] = F.ptr(a, C.c_double)
+        init_arr, keep = self._init_array(cases, init_fields)
         fin_arr = None
         states = None
         if want_states:
@@ -390,21 +382,32 @@ class Solver:
         F.check(F.lib().esr_batch_solve(self.handle, carr, n, init_arr, fin_arr, res))
         return [r.as_dict() for r in res], states
 
+    def _init_array(self, cases, init_fields):
+        """Pointer array of the cases' float64 warm fields (None: freestream),
+        each checked against its mesh's (n_cells, 4); the arrays to keep alive."""
+        if init_fields is None:
+            return None, []
+        n = len(cases)
+        if len(init_fields) != n:
+            raise ValueError("one init field (or None) per case")
+        arr, keep = (F._f64p * n)(), []
+        for i, (c, f) in enumerate(zip(cases, init_fields)):
+            if f is None:
+                continue
+            a = F.f64(f)
+            if a.shape != (self.meshes[c.mesh].n_cells, 4):
+                raise ValueError(f"init field {i} has shape {a.shape}, expected ({self.meshes[c.mesh].n_cells}, 4)")
+            keep.append(a)
+            arr[i] = F.ptr(a, C.c_double)
+        return arr, keep
+
     def batch_submit(self, cases, init_fields=None, want_states=False):
         """Start the batch of ``batch_solve`` and return at once; the fields
         are copied before this returns. Until ``batch_results`` or
         ``batch_cancel`` the batch owns the slots."""
         n = len(cases)
         carr = (F.Case * n)(*[c.to_c() for c in cases])
-        keep = []
-        init_arr = None
-        if init_fields is not None:
-            init_arr = (F._f64p * n)()
-            for i, f in enumerate(init_fields):
-                if f is not None:
-                    a = F.f64(f)
-                    keep.append(a)
-                    init_arr[i] = F.ptr(a, C.c_double)
+        init_arr, keep = self._init_array(cases, init_fields)
         F.check(F.lib().esr_batch_submit(self.handle, carr, n, init_arr, int(bool(want_states))))
         self._pending = ([self.meshes[c.mesh].n_cells for c in cases], bool(want_states))
 
