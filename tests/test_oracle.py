@@ -175,3 +175,76 @@ def test_c_port_matches_numpy_oracle(diamond02):
     assert rel_err(Wc, W) <= 1e-12
     c32 = CpuCase(diamond02, 2.5, 5.0, np.float32)
     assert rel_err(c32.srk2(c32.W0, 20), W) <= 1e-5
+
+
+def test_rusanov_consistency_and_antisymmetry():
+    """The Rusanov branch of getFlux: F(U, U, n) is the physical flux and
+    F(L, R, n) = -F(R, L, -n)."""
+    W = _states(200, 11)
+    rng = np.random.default_rng(12)
+    th = rng.uniform(0, 2 * np.pi, 200)
+    n = np.column_stack([np.cos(th), np.sin(th)])
+    one = np.ones((200, 1))
+    F = O.get_flux(W[:, None], W[:, None], n[:, None], one, flux='rusanov')
+    H = O.get_flux(W[:, None], W[:, None], n[:, None], one, flux='hllc')
+    assert np.allclose(F, H, rtol=1e-12, atol=1e-12)
+    WR = _states(200, 13)
+    Fa = O.get_flux(W[:, None], WR[:, None], n[:, None], one, flux='rusanov')
+    Fb = O.get_flux(WR[:, None], W[:, None], -n[:, None], one, flux='rusanov')
+    assert np.allclose(Fa, -Fb, rtol=1e-10, atol=1e-10)
+
+
+def test_slip_wall_ghost_reflects_the_normal_velocity(diamond02):
+    """helper.py:196-204: at a wall slot the ghost keeps density, pressure and
+    tangential velocity and reverses the normal velocity."""
+    om = oracle_mesh(diamond02, np.float64)
+    n = diamond02.n_cells
+    W = np.repeat(_states(n, 21)[:, None, :], 3, axis=1)
+    G = O.bc_state(W.copy(), W, om, inlet=O.get_conserved(np.array([1.0, 2.0, 0.0, 1.0])))
+    wall = diamond02.face_markers[diamond02.face_connectivity] == 2
+    assert wall.sum() > 10
+    P, Pg = O.get_primitive(W[wall]), O.get_primitive(G[wall])
+    nrm = om.normals[wall]
+    un, ung = (P[:, 1:3] * nrm).sum(1), (Pg[:, 1:3] * nrm).sum(1)
+    t = np.column_stack([-nrm[:, 1], nrm[:, 0]])
+    assert np.allclose(ung, -un, atol=1e-12)
+    assert np.allclose((Pg[:, 1:3] * t).sum(1), (P[:, 1:3] * t).sum(1), atol=1e-12)
+    assert np.allclose(Pg[:, [0, 3]], P[:, [0, 3]], rtol=1e-12)
+    # inflow slots take the inlet state, outflow slots copy the cell
+    mk = diamond02.face_markers[diamond02.face_connectivity]
+    assert np.allclose(G[mk == 3], O.get_conserved(np.array([1.0, 2.0, 0.0, 1.0])))
+    assert np.array_equal(G[mk == 4], W[mk == 4])
+
+
+def test_sponge_vanishes_at_freestream_and_in_the_core(diamond02):
+    """helper.py:262-295: sigma >= 0 and zero outside the bands of 0.2 Ly along
+    the top and bottom; the source is zero where the state is the inlet's."""
+    om = oracle_mesh(diamond02, np.float64)
+    W, inlet = O.initialize(diamond02.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=2.0, aoa=0.0,
+                                                    case='diamond'), np.float64)
+    assert np.abs(O.sponge_source(W, om, inlet)).max() == 0.0
+    Wp = W * 1.1
+    S = O.sponge_source(Wp, om, inlet)
+    y = om.barycenter[:, 1]
+    y0, y1 = om.points[:, 1].min(), om.points[:, 1].max()
+    core = np.minimum(y - y0, y1 - y) >= 0.2 * (y1 - y0)
+    assert np.abs(S[core]).max() == 0.0
+    sigma = S[:, 0] / (inlet[0] - Wp[:, 0])
+    assert (sigma >= 0).all() and sigma.max() > 0
+
+
+def test_global_dt_is_the_minimum_local_dt(diamond02):
+    om = oracle_mesh(diamond02, np.float64)
+    W = _states(diamond02.n_cells, 31)
+    assert O.get_dt(W, om, CFL=0.6) == O.get_local_dt(W, om, CFL=0.6).min()
+
+
+def test_every_time_scheme_preserves_freestream_without_body():
+    m = _box_mesh()
+    om = oracle_mesh(m, np.float64)
+    W, inlet = O.initialize(m.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=1.5, aoa=10.0,
+                                            case='diamond'), np.float64)
+    dt = O.get_dt(W, om, CFL=0.5)
+    for name, fn in O.TIME_SCHEMES.items():
+        Wn = fn(W, om, dt, inlet)
+        assert np.allclose(Wn, W, rtol=0, atol=1e-12), name
