@@ -248,3 +248,38 @@ def test_every_time_scheme_preserves_freestream_without_body():
     for name, fn in O.TIME_SCHEMES.items():
         Wn = fn(W, om, dt, inlet)
         assert np.allclose(Wn, W, rtol=0, atol=1e-12), name
+
+
+def test_mlp_oracle_gradients_match_finite_differences():
+    """The MLP oracle's exact (float64) backward against central differences
+    of its loss, on sampled weights and biases of every layer: the oracle the
+    BF16 GPU gradients are held to is itself right."""
+    from oracle import mlp_oracle as MO
+    rng = np.random.default_rng(7)
+    P = {"W0": rng.standard_normal((256, 128)) * 0.1, "b0": rng.standard_normal(256) * 0.1}
+    for l in (1, 2, 3):
+        P[f"W{l}"] = rng.standard_normal((256, 256)) * 0.06
+        P[f"b{l}"] = rng.standard_normal(256) * 0.1
+    P["W4"], P["b4"] = rng.standard_normal((4, 256)) * 0.1, rng.standard_normal(4) * 0.1
+    X = np.zeros((16, 128))
+    X[:, :13] = rng.standard_normal((16, 13))
+    base, tgt = rng.standard_normal((16, 4)), rng.standard_normal((16, 4))
+    w, inv_den = 1 + 4 * rng.random(16), np.array([1.3, 0.7, 2.0, 1.1])
+
+    def loss(params):
+        y, _ = MO.forward(params, X, base, bf16=False)
+        return MO.loss_and_grad(y, tgt, w, inv_den)[0]
+
+    y, acts = MO.forward(P, X, base, bf16=False)
+    _, dy = MO.loss_and_grad(y, tgt, w, inv_den)
+    g = MO.backward(P, acts, dy, bf16=False)
+    h = 1e-6
+    for k in ("W0", "b0", "W1", "b2", "W3", "b3", "W4", "b4"):
+        for _ in range(4):
+            idx = tuple(rng.integers(0, s) for s in P[k].shape)
+            Pp = {kk: v.copy() for kk, v in P.items()}
+            Pm = {kk: v.copy() for kk, v in P.items()}
+            Pp[k][idx] += h
+            Pm[k][idx] -= h
+            fd = (loss(Pp) - loss(Pm)) / (2 * h)
+            assert abs(fd - g[k][idx]) <= 1e-6 * max(1e-3, abs(fd)), (k, idx, fd, g[k][idx])
