@@ -283,3 +283,16 @@ def test_mlp_oracle_gradients_match_finite_differences():
             Pm[k][idx] -= h
             fd = (loss(Pp) - loss(Pm)) / (2 * h)
             assert abs(fd - g[k][idx]) <= 1e-6 * max(1e-3, abs(fd)), (k, idx, fd, g[k][idx])
+
+
+def test_mlp_loss_is_the_shock_weighted_relative_mse():
+    """With the batch's own denominators, the oracle's loss is loss.py:20-23's
+    shock_weighted_rel_mse: mean over variables of
+    mean_rows(w (pred - target)^2) / (mean_rows(target^2) + 1e-8)."""
+    from oracle import mlp_oracle as MO
+    rng = np.random.default_rng(9)
+    y, t = rng.standard_normal((50, 4)), rng.standard_normal((50, 4)) * [1.0, 2.0, 0.5, 3.0]
+    w = 1 + 4 * rng.random(50)
+    ref = ((w[:, None] * (y - t) ** 2).mean(0) / ((t ** 2).mean(0) + 1e-8)).mean()
+    L, _ = MO.loss_and_grad(y, t, w, 1.0 / ((t ** 2).mean(0) + 1e-8))
+    assert L == pytest.approx(ref, rel=1e-13)
