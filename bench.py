@@ -165,24 +165,25 @@ def dist_setup():
     return world, rank, local
 
 
-def allreduce_max(x: float, world: int) -> float:
+def _allreduce(x: float, world: int, op: str) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def allreduce_max(x: float, world: int) -> float:
+    """Max over ranks (the job's time is its slowest rank's)."""
+    return _allreduce(x, world, "max")
 
 
 def allreduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """Sum over ranks (work done by the whole job)."""
+    return _allreduce(x, world, "sum")
 
 
 def barrier(world):

@@ -51,3 +51,38 @@ def test_config_blocks(monkeypatch):
 def test_diamond_single_case_settings():
     assert bench.diamond_case(0.1)[:4] == (2.5, 5.0, 0.8, "density_l2")
     assert bench.diamond_case(0.025)[:4] == (2.0, 0.0, 0.6, "reference")
+
+
+def _rank_main(rank, world, port, q):
+    import os
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        bench.barrier(world)
+        t = bench.allreduce_max(1.5 + rank, world)
+        s = bench.allreduce_sum(10.0 * (rank + 1), world)
+        q.put((rank, t, s))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_reductions_over_two_ranks():
+    """The job time is the max over ranks and the work the sum, as bench.py
+    reduces them under torchrun (gloo here, NCCL on GPUs)."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out == [(0, 2.5, 30.0), (1, 2.5, 30.0)]
