@@ -119,14 +119,14 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def cpu_oracle_sample(mesh, mach, aoa, seconds=12.0):
+def cpu_oracle_sample(mesh, mach, aoa, seconds=12.0, dtype=np.float32):
     """Time the oracle's SRK2 step on one case of the workload mesh on the
     host: the C/OpenMP restatement on every host thread (the NumPy oracle,
     one thread, when the C build is unavailable). Returns (cell-updates/s,
     steps, seconds, threads, kind)."""
     try:
         from oracle.cport import CpuCase, threads
-        cc = CpuCase(mesh, float(mach), float(aoa), np.float32)
+        cc = CpuCase(mesh, float(mach), float(aoa), dtype)
         W = cc.srk2(cc.W0, 2)               # warm-up (thread pool, caches)
         n, t0 = 0, time.perf_counter()
         step = 5
@@ -139,9 +139,9 @@ def cpu_oracle_sample(mesh, mach, aoa, seconds=12.0):
         pass
     from oracle import euler_oracle as O
     om = O.build_oracle_mesh(mesh.points, mesh.tris, mesh.neighbors, mesh.faces, mesh.face_markers,
-                             mesh.face_connectivity, dtype=np.float32, metadata=mesh.metadata)
+                             mesh.face_connectivity, dtype=dtype, metadata=mesh.metadata)
     cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=float(mach), aoa=float(aoa), case=mesh.metadata['case'])
-    W, inlet = O.initialize(mesh.n_cells, cfg, np.float32)
+    W, inlet = O.initialize(mesh.n_cells, cfg, dtype)
     dt = O.get_dt(W, om, CFL=0.6)
     W = O.time_step_srk2(W, om, dt, inlet)   # warm-up
     n, t0 = 0, time.perf_counter()
@@ -195,31 +195,42 @@ def barrier(world):
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
+    dtype, prec = np.float32, "f32"
     if args.workload == "ragged":
         meshes, per = ragged_workload()
         cfg_mesh, mesh = (meshes, per), meshes[-1]
         mach = np.array([m for p in per for m, _ in p])
         aoa = np.array([a for p in per for _, a in p])
+        config = workload_config(args, cfg_mesh)
+    elif args.workload == "diamond":
+        mesh = get_mesh("diamond", args.h)
+        m_d, a_d, cfl = diamond_case(args.h)[:3]
+        mach, aoa = np.array([m_d]), np.array([a_d])
+        if args.precision == "f64":
+            dtype, prec = np.float64, "f64"
+        config = {"workload": f"diamond h={args.h} ({mesh.n_cells} cells), one case M={m_d} alpha={a_d} CFL {cfl}, "
+                              f"SRK2 steps of the case", "cells": mesh.n_cells}
     else:
         mesh = get_mesh("naca0012", args.h)
-        cfg_mesh = mesh
         mach, aoa = batch_cases(args.cases)
+        config = workload_config(args, mesh)
     ncores = os.cpu_count() or 1
     vals = []
     per_step = max(3.0, 40.0 / max(1, args.steps + args.warmup))
     for i in range(args.warmup + args.steps):
-        v, n, el, thr, kind = cpu_oracle_sample(mesh, mach[i % len(mach)], aoa[i % len(aoa)], seconds=per_step)
+        v, n, el, thr, kind = cpu_oracle_sample(mesh, mach[i % len(mach)], aoa[i % len(aoa)], seconds=per_step,
+                                                dtype=dtype)
         if i >= args.warmup:
             vals.append((v, n, el))
     value = float(np.mean([v for v, _, _ in vals]))
-    sample = (f"{kind} (the reference's JAX CPU path needs JAX, not installed), float32, one case of the "
-              f"workload mesh ({mesh.n_cells} cells) per step, {vals[-1][1]} SRK2 steps in {vals[-1][2]:.1f} s "
-              f"on {thr} threads")
+    sample = (f"{kind} (the reference's JAX CPU path needs JAX, not installed), {np.dtype(dtype).name}, one case "
+              f"of the workload mesh ({mesh.n_cells} cells) per step, {vals[-1][1]} SRK2 steps in "
+              f"{vals[-1][2]:.1f} s on {thr} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean([e for _, _, e in vals]) * 1e3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": prec,
             "data": "synthetic (seeded Mach/alpha draws, freestream start)",
-            "config": workload_config(args, cfg_mesh),
+            "config": config,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": f"host has {ncores} cores"}
