@@ -326,9 +326,10 @@ def run_single(args, world, rank, local):
                 "note": "one case: the state is L2-resident and the launches are latency-bound"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, n, el, thr_, kind = cpu_oracle_sample(mesh, mach, aoa, seconds=12.0)
+        cdt = np.float64 if prec == "f64" else np.float32
+        v, n, el, thr_, kind = cpu_oracle_sample(mesh, mach, aoa, seconds=12.0, dtype=cdt)
         cpu = {"value": v, "unit": UNIT, "cores": thr_, "kind": "port",
-               "sample": f"{kind}, float32, {n} SRK2 steps of the case on the {N}-cell mesh ({el:.1f} s)"}
+               "sample": f"{kind}, {np.dtype(cdt).name}, {n} SRK2 steps of the case on the {N}-cell mesh ({el:.1f} s)"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
