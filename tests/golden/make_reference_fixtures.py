@@ -9,8 +9,9 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
 * ``utils/aero.py:28-72,85-110`` build_wall_cache + aero_coeffs (CL, CD);
 * ``euler/graph.py:5-108`` export_graph on the golden diamond mesh with one
   seeded snapshot, written by the reference itself as ``reference_graph.npz``;
-* ``euler/config.py:24-30,82-103`` the default configuration and the output
-  naming (h tag, condition tag, snapshot name) into ``reference_config.json``.
+* ``euler/config.py:24-62,82-103`` the default configuration, the command
+  line's configurations for a few argument lists and the output naming (h
+  tag, condition tag, snapshot name) into ``reference_config.json``.
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -63,8 +64,18 @@ def main(ref_root: str) -> Path:
         names.append(dict(case=case, Mach=m_c, aoa=a_c, t=t, h=h, h_tag=ref_config.format_h(mesh_h),
                           condition=ref_config.format_condition_tag(cfg),
                           snapshot=ref_config.format_snapshot_name(cfg, t)))
-    (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names}, indent=1,
-                                                           sort_keys=True) + "\n")
+    cli = []
+    saved = sys.argv
+    for argv in (["--case", "naca0012", "--mach", "0.8", "--aoa", "-2.5"],
+                 ["--time-scheme", "SSP_RK2", "--reconstruction", "muscl", "--quiet"],
+                 ["--flux", "Rusanov", "--reconstruction", "constant", "--time-scheme", "EE",
+                  "--stationarity-threshold", "1e-5", "--stationarity-check-every", "0",
+                  "--stationarity-patience", "3", "--mesh-path", "m.npy"]):
+        sys.argv = ["main.py", *argv]
+        cli.append({"argv": argv, "cfg": ref_config.build_config_from_cli(base)})
+    sys.argv = saved
+    (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names, "cli": cli},
+                                                           indent=1, sort_keys=True) + "\n")
     out = HERE / "reference_utils.npz"
     np.savez_compressed(out, graph_snapshot=snap, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
                         aero_prim=prim, aero_mach=np.float64(mach), aero_cl=np.float64(ac["CL"]),

@@ -81,3 +81,15 @@ def test_config_defaults_and_output_names_match_reference():
         assert Cfg.format_h(mesh) == r["h_tag"]
         assert Cfg.format_condition_tag(cfg) == r["condition"]
         assert Cfg.format_snapshot_name(cfg, r["t"]) == r["snapshot"]
+
+
+def test_cli_configurations_match_reference():
+    """euler/config.py:32-62: the configuration the command line builds, for
+    the same argument lists, key by key (the package adds --precision)."""
+    import json
+    from eulersr_b200 import config as Cfg
+    ref = json.loads((GOLDEN / "reference_config.json").read_text())
+    for case in ref["cli"]:
+        ours = Cfg.build_config_from_cli(Cfg.load_default_config(), case["argv"])
+        for k, v in case["cfg"].items():
+            assert ours.get(k) == v, (case["argv"], k, ours.get(k), v)
