@@ -11,7 +11,11 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   seeded snapshot, written by the reference itself as ``reference_graph.npz``;
 * ``euler/config.py:24-62,82-103`` the default configuration, the command
   line's configurations for a few argument lists and the output naming (h
-  tag, condition tag, snapshot name) into ``reference_config.json``.
+  tag, condition tag, snapshot name) into ``reference_config.json``;
+* ``euler/utils.py:147-191`` build_run_summary and export_run_summary (the
+  module imports matplotlib, which is not installed, so these two functions
+  are taken from its source alone and run with NumPy), their summaries and
+  the written file's name and text into ``reference_summary.json``.
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -76,10 +80,42 @@ def main(ref_root: str) -> Path:
     sys.argv = saved
     (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names, "cli": cli},
                                                            indent=1, sort_keys=True) + "\n")
+    summaries = _summaries(Path(ref_root) / "euler" / "utils.py")
+    (HERE / "reference_summary.json").write_text(json.dumps(summaries, indent=1, sort_keys=True) + "\n")
     out = HERE / "reference_utils.npz"
     np.savez_compressed(out, graph_snapshot=snap, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
                         aero_prim=prim, aero_mach=np.float64(mach), aero_cl=np.float64(ac["CL"]),
                         aero_cd=np.float64(ac["CD"]))
+    return out
+
+
+def _summaries(utils_py: Path) -> list:
+    """Run the reference's two summary functions, compiled from their source
+    text, on a few argument sets; the file export goes to a scratch folder
+    beside this script that is removed afterwards."""
+    import ast
+    import shutil
+    tree = ast.parse(utils_py.read_text())
+    keep = [n for n in tree.body if isinstance(n, ast.FunctionDef)
+            and n.name in ("build_run_summary", "export_run_summary")]
+    ns = {"np": np, "json": json, "Path": Path}
+    exec(compile(ast.Module(body=keep, type_ignores=[]), str(utils_py), "exec"), ns)
+    mesh = type("M", (), {"metadata": {"h": 0.025}, "tris": np.zeros((1234, 3), np.int32)})()
+    cfg = dict(case="naca0012", Mach=0.8, aoa=-2.5, time_scheme="SRK2", flux="HLLC", reconstruction="MUSCL",
+               mesh_path="m.npy", stationarity_threshold=1e-5, stationarity_check_every=25)
+    calls = [dict(cd=0.0123, cl=-0.2, delta_s=1.5e-3, wall_time_s=2.25),
+             dict(cd=0.0123, cl=-0.2, delta_s=1.5e-3, wall_time_s=2.25, stationarity_rel=3e-6, converged=True,
+                  stopping_step=4200, compile_time_s=0.0, solve_time_s=2.25, stationarity_patience=3,
+                  engineering_converged=False, engineering_stopping_step=5000, engineering_target_cd=0.0125,
+                  engineering_target_cl=-0.21)]
+    out = []
+    scratch = HERE / "_summary_scratch"
+    for kw in calls:
+        summ = ns["build_run_summary"](cfg, mesh, **kw)
+        ns["export_run_summary"]({"res": scratch}, summ, "AOA-2.50_M0.80_HLLC_MUSCL_SRK2_t1.00", verbose=False)
+        f = scratch / "summary_AOA-2.50_M0.80_HLLC_MUSCL_SRK2_t1.00.json"
+        out.append({"kwargs": kw, "summary": summ, "file": f.name, "text": f.read_text()})
+    shutil.rmtree(scratch)
     return out
 
 

@@ -93,3 +93,19 @@ def test_cli_configurations_match_reference():
         ours = Cfg.build_config_from_cli(Cfg.load_default_config(), case["argv"])
         for k, v in case["cfg"].items():
             assert ours.get(k) == v, (case["argv"], k, ours.get(k), v)
+
+
+def test_run_summary_matches_reference(tmp_path):
+    """euler/utils.py:147-191: the summary dictionary (keys, order, values)
+    and the JSON file the reference writes for it, byte for byte."""
+    import json
+    from eulersr_b200 import main as M
+    ref = json.loads((GOLDEN / "reference_summary.json").read_text())
+    mesh = type("M", (), {"metadata": {"h": 0.025}, "tris": np.zeros((1234, 3), np.int32), "n_cells": 1234})()
+    cfg = dict(case="naca0012", Mach=0.8, aoa=-2.5, time_scheme="SRK2", flux="HLLC", reconstruction="MUSCL",
+               mesh_path="m.npy", stationarity_threshold=1e-5, stationarity_check_every=25)
+    for r in ref:
+        summ = M.build_run_summary(cfg, mesh, **r["kwargs"])
+        assert summ == r["summary"]
+        M.export_run_summary({"res": tmp_path}, summ, "AOA-2.50_M0.80_HLLC_MUSCL_SRK2_t1.00", verbose=False)
+        assert (tmp_path / r["file"]).read_text() == r["text"]
