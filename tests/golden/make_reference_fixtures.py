@@ -15,7 +15,11 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
 * ``euler/utils.py:147-191`` build_run_summary and export_run_summary (the
   module imports matplotlib, which is not installed, so these two functions
   are taken from its source alone and run with NumPy), their summaries and
-  the written file's name and text into ``reference_summary.json``.
+  the written file's name and text into ``reference_summary.json``;
+* ``euler/postproc/theory_validation_diamond.py:44-175`` the shock-expansion
+  panel states of the diamond (same treatment: the gas-dynamics functions
+  taken from the source, run with NumPy and SciPy) for a set of Mach numbers
+  and incidences into ``reference_theory.json``.
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -80,12 +84,42 @@ def main(ref_root: str) -> Path:
     sys.argv = saved
     (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names, "cli": cli},
                                                            indent=1, sort_keys=True) + "\n")
+    theory = _theory(Path(ref_root) / "euler" / "postproc" / "theory_validation_diamond.py")
+    (HERE / "reference_theory.json").write_text(json.dumps(theory, indent=1, sort_keys=True) + "\n")
     summaries = _summaries(Path(ref_root) / "euler" / "utils.py")
     (HERE / "reference_summary.json").write_text(json.dumps(summaries, indent=1, sort_keys=True) + "\n")
     out = HERE / "reference_utils.npz"
     np.savez_compressed(out, graph_snapshot=snap, idw_dist=dist, idw_w=w, wall_query=query, wall_dist=wd, wall_normal=wn,
                         aero_prim=prim, aero_mach=np.float64(mach), aero_cl=np.float64(ac["CL"]),
                         aero_cd=np.float64(ac["CD"]))
+    return out
+
+
+def _theory(src: Path) -> list:
+    """Panel states (Mach, pressure ratio to freestream, Cp, shock angle,
+    attached) of the reference's diamond_panels for several (M, alpha)."""
+    import ast
+    import dataclasses
+    from scipy.optimize import brentq
+    names = {"prandtl_meyer", "inverse_prandtl_meyer", "_theta_of_beta", "theta_max", "oblique_shock_beta",
+             "PanelState", "_apply_deflection", "diamond_panels", "all_attached"}
+    tree = ast.parse(src.read_text())
+    keep = [n for n in tree.body if isinstance(n, (ast.FunctionDef, ast.ClassDef)) and n.name in names]
+    import types
+    mod = types.ModuleType("reference_theory")     # dataclass() looks its module up in sys.modules
+    mod.__dict__.update(np=np, brentq=brentq, dataclass=dataclasses.dataclass, GAMMA=1.4)
+    sys.modules[mod.__name__] = mod
+    try:
+        exec(compile(ast.Module(body=keep, type_ignores=[]), str(src), "exec"), mod.__dict__)
+    finally:
+        del sys.modules[mod.__name__]
+    ns = mod.__dict__
+    out = []
+    for mach, aoa in ((1.5, 0.0), (2.0, 0.0), (2.0, 3.0), (2.5, 5.0), (3.0, -2.0), (1.05, 0.0)):
+        panels = ns["diamond_panels"](mach, aoa, 5.0)
+        out.append({"mach": mach, "aoa": aoa, "attached": bool(ns["all_attached"](panels)),
+                    "panels": {k: {"M": p.M, "p_ratio": p.p_ratio_freestream, "Cp": p.Cp, "beta_deg": p.beta_deg,
+                                   "attached": p.attached, "regime": p.regime} for k, p in panels.items()}})
     return out
 
 

@@ -109,3 +109,27 @@ def test_run_summary_matches_reference(tmp_path):
         assert summ == r["summary"]
         M.export_run_summary({"res": tmp_path}, summ, "AOA-2.50_M0.80_HLLC_MUSCL_SRK2_t1.00", verbose=False)
         assert (tmp_path / r["file"]).read_text() == r["text"]
+
+
+def test_diamond_panels_match_reference_theory():
+    """The shock-expansion states of the diamond's four faces (Mach, pressure
+    ratio, Cp, shock angle, attached or detached) against the reference's own
+    diamond_panels (euler/postproc/theory_validation_diamond.py:44-175)."""
+    import json
+    from eulersr_b200 import theory_validation as TV
+    ref = json.loads((GOLDEN / "reference_theory.json").read_text())
+    for r in ref:
+        ours = TV.diamond_panels(r["mach"], r["aoa"], 5.0)
+        assert TV.all_attached(ours) == r["attached"], (r["mach"], r["aoa"])
+        if not r["attached"]:
+            continue
+        for name, p in r["panels"].items():
+            q = ours[name]
+            assert q.regime == p["regime"], name
+            assert q.M == pytest.approx(p["M"], rel=1e-8), (r["mach"], r["aoa"], name)
+            assert q.p_ratio_freestream == pytest.approx(p["p_ratio"], rel=1e-8), name
+            assert q.Cp == pytest.approx(p["Cp"], rel=1e-8, abs=1e-12), name
+            if p["beta_deg"] is None:
+                assert q.beta_deg is None, name
+            else:
+                assert q.beta_deg == pytest.approx(p["beta_deg"], abs=1e-6), name
