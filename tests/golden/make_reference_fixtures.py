@@ -19,7 +19,11 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
 * ``euler/postproc/theory_validation_diamond.py:44-175`` the shock-expansion
   panel states of the diamond (same treatment: the gas-dynamics functions
   taken from the source, run with NumPy and SciPy) for a set of Mach numbers
-  and incidences into ``reference_theory.json``.
+  and incidences, and its campaign helpers (``:237-342,609-621``: plateau
+  values, shock-angle measurement, log-log order fit) and the mesh-convergence
+  helpers (``mesh_convergence_diamond.py:106-161``: profile error, GCI) on
+  seeded inputs, into ``reference_theory.json`` (the helpers' array inputs
+  in ``reference_theory_inputs.npz``).
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -102,9 +106,18 @@ def _theory(src: Path) -> list:
     import dataclasses
     from scipy.optimize import brentq
     names = {"prandtl_meyer", "inverse_prandtl_meyer", "_theta_of_beta", "theta_max", "oblique_shock_beta",
-             "PanelState", "_apply_deflection", "diamond_panels", "all_attached"}
+             "PanelState", "_apply_deflection", "diamond_panels", "all_attached", "_panel_of", "_plateau_value",
+             "_panel_masks", "_measure_shock_angle", "fit_order", "richardson_gci", "_relative_profile_error",
+             "SHOCK_WINDOW_X", "SHOCK_WINDOW_Y_FACTOR", "SHOCK_TOP_PCT", "H_GCI"}
+
+    def wanted(n):
+        if isinstance(n, (ast.FunctionDef, ast.ClassDef)):
+            return n.name in names
+        return (isinstance(n, ast.Assign) and len(n.targets) == 1 and isinstance(n.targets[0], ast.Name)
+                and n.targets[0].id in names)
     tree = ast.parse(src.read_text())
-    keep = [n for n in tree.body if isinstance(n, (ast.FunctionDef, ast.ClassDef)) and n.name in names]
+    conv = ast.parse((src.parent / "mesh_convergence_diamond.py").read_text())
+    keep = [n for n in conv.body if wanted(n)] + [n for n in tree.body if wanted(n)]
     import types
     mod = types.ModuleType("reference_theory")     # dataclass() looks its module up in sys.modules
     mod.__dict__.update(np=np, brentq=brentq, dataclass=dataclasses.dataclass, GAMMA=1.4)
@@ -114,10 +127,41 @@ def _theory(src: Path) -> list:
     finally:
         del sys.modules[mod.__name__]
     ns = mod.__dict__
-    out = []
+    out = {"panels": [], "helpers": {}}
+    rng = np.random.default_rng(17)
+    # plateau values on a synthetic two-sided wall profile around (1.5, 2.0)
+    x = np.sort(rng.uniform(1.0, 2.0, 80))
+    y = 2.0 + np.where(np.arange(80) % 2 == 0, 1.0, -1.0) * 0.05 * (1 - np.abs(x - 1.5) / 0.5)
+    prof = {"x": x, "y": y, "p": rng.uniform(0.5, 2.0, 80), "mach": rng.uniform(1.0, 3.0, 80)}
+    masks = ns["_panel_masks"](prof, 1.5, 2.0)
+    arrays = {f"profile_{k}": v for k, v in prof.items()}
+    out["helpers"]["plateau_p"] = ns["_plateau_value"](prof, masks, "p", lambda p: (p - 1.0) / 2.8)
+    out["helpers"]["plateau_mach"] = ns["_plateau_value"](prof, masks, "mach", lambda m: m)
+    # shock angle from a gradient ridge through the leading edge at 40 degrees, jittered
+    pos = np.column_stack([rng.uniform(0.6, 1.5, 2000), rng.uniform(1.7, 2.3, 2000)])
+    dist = np.abs(np.sin(np.radians(40.0)) * (pos[:, 0] - 1.0) - np.cos(np.radians(40.0)) * (pos[:, 1] - 2.0))
+    grad = np.zeros((2000, 4, 2))
+    grad[:, 3, 0] = np.exp(-(dist / 0.01) ** 2) + 0.01 * rng.random(2000)
+    bundle = {"node_pos": pos, "primitives_grad": grad}
+    arrays.update(shock_node_pos=pos, shock_grad_p=grad[:, 3, :])
+    out["helpers"]["shock"] = {"upper": ns["_measure_shock_angle"](bundle, None, 1.5, 2.0, 1.0, 0.0875, 0.0, "upper"),
+                               "lower": ns["_measure_shock_angle"](bundle, None, 1.5, 2.0, 1.0, 0.0875, 0.0, "lower")}
+    rows = [{"h": h, "e": 0.3 * h ** 1.7 * (1 + 0.05 * rng.standard_normal())} for h in (0.2, 0.1, 0.05, 0.025, 0.0125)]
+    p_ord, r2, npts = ns["fit_order"](rows, "e")
+    out["helpers"]["fit"] = {"rows": rows, "p": p_ord, "r2": r2, "n": npts}
+    vals = {h: 0.05 + 0.3 * h ** 1.8 + 0.01 * h ** 3 for h in ns["H_GCI"]}
+    out["helpers"]["gci"] = {"values": {str(h): v for h, v in vals.items()}, "chain": ns["H_GCI"],
+                             "triplets": ns["richardson_gci"](vals)}
+    s_ref = np.linspace(0, 2, 50)
+    ref_p = {"s": s_ref, "mach": 1.5 + 0.3 * np.sin(3 * s_ref)}
+    cur_p = {"s": np.linspace(0.05, 1.9, 37), "mach": 1.5 + 0.31 * np.sin(3 * np.linspace(0.05, 1.9, 37))}
+    arrays.update(perr_ref_s=ref_p["s"], perr_ref_mach=ref_p["mach"], perr_cur_s=cur_p["s"],
+                  perr_cur_mach=cur_p["mach"])
+    out["helpers"]["profile_error"] = ns["_relative_profile_error"](ref_p, cur_p)
+    np.savez_compressed(HERE / "reference_theory_inputs.npz", **arrays)
     for mach, aoa in ((1.5, 0.0), (2.0, 0.0), (2.0, 3.0), (2.5, 5.0), (3.0, -2.0), (1.05, 0.0)):
         panels = ns["diamond_panels"](mach, aoa, 5.0)
-        out.append({"mach": mach, "aoa": aoa, "attached": bool(ns["all_attached"](panels)),
+        out["panels"].append({"mach": mach, "aoa": aoa, "attached": bool(ns["all_attached"](panels)),
                     "panels": {k: {"M": p.M, "p_ratio": p.p_ratio_freestream, "Cp": p.Cp, "beta_deg": p.beta_deg,
                                    "attached": p.attached, "regime": p.regime} for k, p in panels.items()}})
     return out

@@ -117,7 +117,7 @@ def test_diamond_panels_match_reference_theory():
     diamond_panels (euler/postproc/theory_validation_diamond.py:44-175)."""
     import json
     from eulersr_b200 import theory_validation as TV
-    ref = json.loads((GOLDEN / "reference_theory.json").read_text())
+    ref = json.loads((GOLDEN / "reference_theory.json").read_text())["panels"]
     for r in ref:
         ours = TV.diamond_panels(r["mach"], r["aoa"], 5.0)
         assert TV.all_attached(ours) == r["attached"], (r["mach"], r["aoa"])
@@ -133,3 +133,38 @@ def test_diamond_panels_match_reference_theory():
                 assert q.beta_deg is None, name
             else:
                 assert q.beta_deg == pytest.approx(p["beta_deg"], abs=1e-6), name
+
+
+def test_campaign_helpers_match_reference():
+    """The validation campaigns' helpers against the reference's own on the
+    same inputs: per-face plateau values of a wall profile, the leading-edge
+    shock angle from a |grad p| field, the log-log order fit
+    (theory_validation_diamond.py:237-342,609-621), the GCI triplets and the
+    wall-profile error (mesh_convergence_diamond.py:106-161)."""
+    import json
+    from eulersr_b200 import mesh_convergence as MC
+    from eulersr_b200 import theory_validation as TV
+    h = json.loads((GOLDEN / "reference_theory.json").read_text())["helpers"]
+    a = np.load(GOLDEN / "reference_theory_inputs.npz")
+    prof = {k: a[f"profile_{k}"] for k in ("x", "y", "p", "mach")}
+    masks = TV.panel_masks(prof, 1.5, 2.0)
+    assert TV.plateau_value(prof, masks, "p", lambda p: (p - 1.0) / 2.8) == pytest.approx(h["plateau_p"], rel=1e-14)
+    assert TV.plateau_value(prof, masks, "mach", lambda m: m) == pytest.approx(h["plateau_mach"], rel=1e-14)
+    for side in ("upper", "lower"):
+        got = TV.measure_shock_angle(a["shock_node_pos"], a["shock_grad_p"], 1.5, 2.0, 1.0, 0.0875, 0.0, side)
+        assert got == pytest.approx(h["shock"][side], abs=1e-9), side
+    p, r2, n = TV.fit_order(h["fit"]["rows"], "e")
+    assert (p, r2, n) == (pytest.approx(h["fit"]["p"], rel=1e-12), pytest.approx(h["fit"]["r2"], rel=1e-12),
+                          h["fit"]["n"])
+    vals = {float(k): v for k, v in h["gci"]["values"].items()}
+    ours = MC.richardson_gci(vals, h["gci"]["chain"])
+    assert len(ours) == len(h["gci"]["triplets"])
+    for o, r in zip(ours, h["gci"]["triplets"]):
+        for k in ("h_coarse", "h_mid", "h_fine"):
+            assert o[k] == r[k]
+        for k in ("p_obs", "extrap", "gci_fine_pct"):
+            assert o[k] == pytest.approx(r[k], rel=1e-12), k
+    err = MC.relative_profile_error({"s": a["perr_ref_s"], "mach": a["perr_ref_mach"]},
+                                    {"s": a["perr_cur_s"], "mach": a["perr_cur_mach"]})
+    assert err == pytest.approx(h["profile_error"], rel=1e-12)
+
