@@ -32,11 +32,13 @@ def _freestream_values(mach, aoa_deg, gamma, rho_inf, p_inf, dtype_str):
     rounded in the dtype), cached: a batch re-submits the same cases."""
     dtype = np.dtype(dtype_str)
     c_inf = (gamma * p_inf / rho_inf) ** 0.5
-    a = math.radians(aoa_deg)
+    # as euler/main.py:28-41 computes it in the run's precision: the angle,
+    # its cosine and sine in `dtype`; Python-float constants ((gamma - 1)
+    # formed in double and rounded once)
+    a = np.deg2rad(np.asarray(aoa_deg, dtype=dtype))
     prim = np.asarray([rho_inf, mach * c_inf * np.cos(a), mach * c_inf * np.sin(a), p_inf], dtype=dtype)
-    t = prim.dtype.type
     rho, u, v, p = prim
-    E = p / ((t(gamma) - 1) * t(1.0) ** 2) + t(0.5) * rho * (u ** 2 + v ** 2)
+    E = p / ((gamma - 1) * 1.0 ** 2) + 0.5 * rho * (u ** 2 + v ** 2)
     return tuple(float(x) for x in np.asarray([rho, rho * u, rho * v, E], dtype=dtype))
 
 

@@ -101,19 +101,19 @@ def build_oracle_mesh(points, tris, neighbors, faces, face_markers, face_connect
 
 def get_conserved(P, gamma=1.4, M=1.0):
     """helper.py:25-35."""
-    dt = P.dtype.type
+    # constants stay Python floats, as in the reference: (gamma - 1) is formed
+    # in double precision and rounded once to the array's type
     rho, u, v, p = P[..., 0], P[..., 1], P[..., 2], P[..., 3]
-    E = p / ((dt(gamma) - 1) * dt(M) ** 2) + dt(0.5) * rho * (u ** 2 + v ** 2)
+    E = p / ((gamma - 1) * M ** 2) + 0.5 * rho * (u ** 2 + v ** 2)
     return np.stack([rho, rho * u, rho * v, E], axis=-1)
 
 
 def get_primitive(W, gamma=1.4, M=1.0):
     """helper.py:37-46."""
-    dt = W.dtype.type
     rho = W[..., 0]
     u = W[..., 1] / rho
     v = W[..., 2] / rho
-    p = (W[..., 3] - dt(0.5) * rho * (u ** 2 + v ** 2)) * dt(M) ** 2 * (dt(gamma) - 1)
+    p = (W[..., 3] - 0.5 * rho * (u ** 2 + v ** 2)) * M ** 2 * (gamma - 1)
     return np.stack([rho, u, v, p], axis=-1)
 
 
@@ -449,7 +449,9 @@ def initialize(n_cells, cfg, dtype=np.float64):
     rho_inf, p_inf, gamma, mach = cfg['rho_inf'], cfg['p_inf'], cfg['gamma'], cfg['Mach']
     c_inf = (gamma * p_inf / rho_inf) ** 0.5
     aoa = float(cfg.get('aoa', 0.0)) if str(cfg.get('case', '')).lower() in [c.lower() for c in AOA_CASES] else 0.0
-    a = math.radians(aoa)
+    # the angle and its sine and cosine in the run's precision, Mach and c_inf
+    # as Python floats (jnp.deg2rad(jnp.asarray(aoa)) under float32 JAX)
+    a = np.deg2rad(np.asarray(aoa, dtype=dtype))
     prim0 = np.asarray([rho_inf, mach * c_inf * np.cos(a), mach * c_inf * np.sin(a), p_inf], dtype=dtype)
     W = get_conserved(np.tile(prim0[None, :], (n_cells, 1)), gamma, 1.0)
     inlet = get_conserved(prim0[None], gamma, 1.0)[0]
@@ -486,13 +488,12 @@ def force_coefficients(W, mesh: OracleMesh, rho_inf, U_inf, L_ref, marker=None):
 
 def total_entropy(W, mesh: OracleMesh, gamma=1.4):
     """helper.py:48-55,312-315."""
-    dt = W.dtype.type
     rho = W[..., 0]
     u = W[..., 1] / rho
     v = W[..., 2] / rho
-    p = (W[..., 3] - dt(0.5) * rho * (u ** 2 + v ** 2)) * (dt(gamma) - 1)
-    s = np.log(p / rho ** dt(gamma))
-    return np.sum(rho * s * mesh.area / (dt(gamma) - 1), axis=-1)
+    p = (W[..., 3] - 0.5 * rho * (u ** 2 + v ** 2)) * (gamma - 1)
+    s = np.log(p / rho ** gamma)
+    return np.sum(rho * s * mesh.area / (gamma - 1), axis=-1)
 
 
 # ----------------------------------------------------------------------------

@@ -16,6 +16,12 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   module imports matplotlib, which is not installed, so these two functions
   are taken from its source alone and run with NumPy), their summaries and
   the written file's name and text into ``reference_summary.json``;
+* the reference's own solver source (``reference_solver_run.py``: mesh
+  geometry, initialize, dt, boundary states, LSQ gradient, limiter, MUSCL,
+  HLLC, sponge, residual, SRK2) with NumPy standing in for jax.numpy: 20 SRK2
+  steps of the supersonic diamond (M 2.5, alpha 5) and the transonic NACA0012
+  (M 0.8, alpha 1.25) golden meshes in float32 and float64, with their dt,
+  into ``reference_solver.npz``;
 * ``euler/postproc/theory_validation_diamond.py:44-175`` the shock-expansion
   panel states of the diamond (same treatment: the gas-dynamics functions
   taken from the source, run with NumPy and SciPy) for a set of Mach numbers
@@ -88,6 +94,16 @@ def main(ref_root: str) -> Path:
     sys.argv = saved
     (HERE / "reference_config.json").write_text(json.dumps({"default": base, "names": names, "cli": cli},
                                                            indent=1, sort_keys=True) + "\n")
+    sys.path.insert(0, str(HERE))
+    import reference_solver_run as RS
+    solver = {}
+    for tag, name, m_s, a_s in (("diamond", "diamond_h0.2", 2.5, 5.0), ("naca", "naca0012_h0.2", 0.8, 1.25)):
+        m = Mesh.load(HERE / f"{name}.npz")
+        for dname, dtp in (("f32", np.float32), ("f64", np.float64)):
+            W, dt_ = RS.run(ref_root, m, m_s, a_s, 20, dtp, ref_config._AOA_CASES_LC)
+            solver[f"{tag}_{dname}_W20"] = W
+            solver[f"{tag}_{dname}_dt"] = np.asarray(dt_, dtype=dtp)
+    np.savez_compressed(HERE / "reference_solver.npz", **solver)
     theory = _theory(Path(ref_root) / "euler" / "postproc" / "theory_validation_diamond.py")
     (HERE / "reference_theory.json").write_text(json.dumps(theory, indent=1, sort_keys=True) + "\n")
     summaries = _summaries(Path(ref_root) / "euler" / "utils.py")

@@ -1,0 +1,155 @@
+"""Run EulerSR's own solver source on a golden mesh with NumPy in place of
+jax.numpy (JAX is not installed), for the fixture ``reference_solver.npz``.
+
+The functions are compiled from the reference's source text (no module of the
+reference is imported, so none of its plotting or meshing dependencies is
+needed): the mesh geometry methods of ``euler/jax_fvm/src/mesh.py:223-264``,
+the helpers of ``euler/jax_fvm/src/helper.py`` (conversions, dt, LSQ
+gradient, boundary states, sponge), the solver of
+``euler/jax_fvm/src/euler_solver.py`` (limiter, MUSCL, reconstruction, HLLC,
+getFlux, residual, SRK2) and ``initialize`` of ``euler/main.py:28-41``.
+What stands in for JAX:
+
+* ``jnp``: NumPy, with array results given an ``.at[...].set()`` that
+  returns an updated copy, and, in single precision, new float arrays made
+  float32 as JAX does without ``JAX_ENABLE_X64``;
+* ``jax.jit``: the identity; ``jax.lax.cond``: a Python branch;
+  ``jax.vmap``: a loop over the leading axis.
+
+Used by ``make_reference_fixtures.py``.
+"""
+from __future__ import annotations
+
+import ast
+import functools
+import types
+from pathlib import Path
+
+import numpy as np
+
+
+class _JArr(np.ndarray):
+    @property
+    def at(self):
+        return _At(self)
+
+
+class _At:
+    def __init__(self, a):
+        self.a = a
+
+    def __getitem__(self, idx):
+        return _AtIdx(self.a, idx)
+
+
+class _AtIdx:
+    def __init__(self, a, idx):
+        self.a, self.idx = a, idx
+
+    def set(self, v):
+        c = np.array(self.a, copy=True).view(_JArr)
+        c[self.idx] = v
+        return c
+
+
+def _wrap(x):
+    if isinstance(x, np.ndarray) and not isinstance(x, _JArr):
+        return x.view(_JArr)
+    return x
+
+
+class _NumpyAsJnp:
+    def __init__(self, mod, float32):
+        self._mod, self._f32 = mod, float32
+
+    def __getattr__(self, name):
+        if name == "linalg":
+            return _NumpyAsJnp(np.linalg, self._f32)
+        attr = getattr(self._mod, name)
+        if isinstance(attr, type) or not callable(attr):
+            return attr
+        make = name in ("asarray", "array", "zeros", "ones", "full", "arange", "linspace")
+
+        def call(*a, **k):
+            out = attr(*a, **k)
+            if make and self._f32 and "dtype" not in k and isinstance(out, np.ndarray) and out.dtype == np.float64:
+                out = out.astype(np.float32)
+            return _wrap(out)
+        return call
+
+
+def _vmap(f):
+    def g(*args):
+        return _wrap(np.stack([f(*[a[i] for a in args]) for i in range(args[0].shape[0])]))
+    return g
+
+
+def _jax(jnp):
+    jit = lambda f=None, **kw: f if f is not None else (lambda g: g)   # noqa: E731
+    lax = types.SimpleNamespace(cond=lambda p, t, f, operand=None: t(operand) if bool(p) else f(operand))
+    return types.SimpleNamespace(jit=jit, lax=lax, vmap=_vmap, numpy=jnp)
+
+
+def _defs(path: Path, names, cls=None):
+    tree = ast.parse(path.read_text())
+    body = tree.body
+    if cls is not None:
+        body = next(n for n in body if isinstance(n, ast.ClassDef) and n.name == cls).body
+    found = [n for n in body if isinstance(n, ast.FunctionDef) and n.name in names]
+    assert {n.name for n in found} == set(names), set(names) - {n.name for n in found}
+    return found
+
+
+def _compile(nodes, ns, filename):
+    exec(compile(ast.Module(body=nodes, type_ignores=[]), filename, "exec"), ns)
+    return ns
+
+
+def run(ref_root, mesh, mach, aoa, steps, dtype, aoa_cases):
+    """(W after `steps` SRK2 steps, dt) of the reference code on `mesh`
+    (an object with points, tris, faces, face_markers, neighbors, metadata)."""
+    src = Path(ref_root) / "euler"
+    f32 = dtype == np.float32
+    jnp = _NumpyAsJnp(np, f32)
+    jax = _jax(jnp)
+    base = {"jnp": jnp, "jax": jax, "np": np, "partial": functools.partial}
+
+    # geometry: the reference Mesh's own methods on a bare object
+    geo = _compile(_defs(src / "jax_fvm" / "src" / "mesh.py",
+                         ["getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"],
+                         cls="Mesh"), dict(base), "mesh.py")
+    M = types.SimpleNamespace()
+    M.points = _wrap(np.asarray(mesh.points, dtype=dtype))
+    M.tris = np.asarray(mesh.tris, dtype=np.int32)
+    M.faces = np.asarray(mesh.faces, dtype=np.int32)
+    for meth in ("getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"):
+        geo[meth](M)
+    M.neighbors = np.asarray(mesh.neighbors, dtype=np.int32)
+    M.face_markers = np.asarray(mesh.face_markers, dtype=np.int32)
+    M.face_connectivity_opposite = np.arange(M.faces.shape[0])
+    M.metadata = dict(mesh.metadata)
+    M.inlet_subsonic = jnp.array([1.0, 1., 0.0, 1.0])
+
+    helper_names = ["get_dt", "getConserved", "getPrimitive", "getgradientLSQ", "BC_outflow", "BC_inflow",
+                    "BC_subsonic_inlet", "BC_slipwall", "_mesh_metadata", "BC_state", "get_sponge_source"]
+    hns = _compile(_defs(src / "jax_fvm" / "src" / "helper.py", helper_names), dict(base), "helper.py")
+    helper = types.SimpleNamespace(**{k: hns[k] for k in helper_names})
+    solver_names = ["venkatakrishnan", "getlimiting", "MUSCL", "get_reconstruction_mode", "get_flux_type",
+                    "build_reconstruction", "build_flux", "apply_face_surfaces", "Rusanov", "HLLC", "getFlux",
+                    "residual", "time_step_RK2_SSP"]
+    sns = _compile(_defs(src / "jax_fvm" / "src" / "euler_solver.py", solver_names),
+                   dict(base, helper=helper), "euler_solver.py")
+    mns = _compile(_defs(src / "main.py", ["initialize"]),
+                   dict(base, helper=helper, _AOA_CASES_LC=tuple(aoa_cases)), "main.py")
+
+    cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa, case=mesh.metadata["case"], CFL=0.6)
+    if 0.6 < cfg["Mach"] < 1.1 and cfg["CFL"] > 0.45:     # euler/main.py:117-120
+        cfg["CFL"] = 0.45
+    W, inlet = mns["initialize"](M, cfg)
+    if steps == 0:
+        return np.asarray(W), float(helper.get_dt(W, M, CFL=cfg["CFL"], gamma=cfg["gamma"], M=1.0))
+    dt = helper.get_dt(W, M, CFL=cfg["CFL"], gamma=cfg["gamma"], M=1.0)
+    kw = dict(gamma=cfg["gamma"], M=1.0, reconstruction="MUSCL", flux="HLLC", value=inlet, entropy=False)
+    for _ in range(steps):
+        W = sns["time_step_RK2_SSP"](W, M, dt, **kw)
+    return np.asarray(W), float(dt)

@@ -168,3 +168,42 @@ def test_campaign_helpers_match_reference():
                                     {"s": a["perr_cur_s"], "mach": a["perr_cur_mach"]})
     assert err == pytest.approx(h["profile_error"], rel=1e-12)
 
+
+
+@pytest.mark.parametrize("tag,name,mach,aoa", [("diamond", "diamond_h0.2", 2.5, 5.0),
+                                               ("naca", "naca0012_h0.2", 0.8, 1.25)])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_oracle_bitwise_equals_reference_solver_source(tag, name, mach, aoa, prec):
+    """20 SRK2 steps of the oracle equal, bit for bit, those of EulerSR's own
+    solver source (geometry, initialize, dt, boundary states, LSQ gradient,
+    Venkatakrishnan limiter, MUSCL, HLLC, sponge, SSP-RK2) run with NumPy in
+    place of jax.numpy (tests/golden/reference_solver_run.py), in float32 and
+    float64, supersonic diamond and transonic NACA0012."""
+    from conftest import oracle_mesh
+    from oracle import euler_oracle as O
+    ref = np.load(GOLDEN / "reference_solver.npz")
+    dtype = np.float32 if prec == "f32" else np.float64
+    mesh = load_mesh(name)
+    om = oracle_mesh(mesh, dtype)
+    W, inlet = O.initialize(mesh.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa,
+                                               case=mesh.metadata["case"]), dtype)
+    dt = O.get_dt(W, om, CFL=0.45 if 0.6 < mach < 1.1 else 0.6)
+    assert dt == ref[f"{tag}_{prec}_dt"]
+    for _ in range(20):
+        W = O.time_step_srk2(W, om, dt, inlet)
+    assert W.dtype == ref[f"{tag}_{prec}_W20"].dtype
+    assert np.array_equal(W, ref[f"{tag}_{prec}_W20"])
+
+
+def test_freestream_equals_reference_initial_state():
+    """The package's freestream state (what the solver fills a slot with) is
+    the reference's initialize() state bit for bit, float32 and float64."""
+    from eulersr_b200.solver import freestream
+    ref = np.load(GOLDEN / "reference_solver.npz")
+    from oracle import euler_oracle as O
+    for dtype in (np.float32, np.float64):
+        for mach, aoa in ((2.5, 5.0), (0.8, 1.25), (1.7, -3.3)):
+            W, _ = O.initialize(3, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa, case="diamond"),
+                                dtype)
+            assert np.array_equal(freestream(mach, aoa, dtype=dtype), W[0])
+    assert ref["diamond_f32_W20"].dtype == np.float32
