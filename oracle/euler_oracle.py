@@ -5,16 +5,19 @@ only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of
 ``bench.py`` use it, and only to check the CUDA results (or, in bench.py,
 as the timed CPU baseline), never as the thing measured or shipped.
 
-Parity status: **unpinned** against the reference itself. The reference runs on
-JAX 0.4.38 (``pyproject.toml:14``), which is not installed here or on the GPU
-hosts, and the reference ships no tests, fixtures or golden vectors. This
-module therefore restates the reference source line by line (citations below
-are ``path:line`` inside the EulerSR checkout) and is pinned instead by
-known-answer properties (freestream preservation, HLLC consistency, LSQ
-exactness on linear fields) and by the analytic diamond shock-expansion theory.
-Where the reference runs without JAX (its NumPy utilities), it is pinned
-directly: ``idw_weights`` below equals ``utils/metrics.py:9-14`` on the golden
-vectors of ``tests/golden/reference_utils.npz``.
+Parity status: **pinned to the reference's own solver source**, executed
+with NumPy in place of jax.numpy. JAX 0.4.38 (``pyproject.toml:14``) is not
+installed here or on the GPU hosts and the reference ships no tests or golden
+vectors, so ``tests/golden/reference_solver_run.py`` compiles the reference's
+geometry, initialize, dt, boundary-state, gradient, limiter, MUSCL, HLLC,
+sponge, residual and SSP-RK2 functions from their source text and runs them
+on the golden meshes; this module reproduces those runs bit for bit in
+float32 and float64 (``tests/test_reference_fixtures.py``). What stays
+unpinned is JAX's own arithmetic (XLA's fusions and its float32 LU solve)
+against NumPy's. Known-answer properties (freestream preservation, HLLC
+consistency, LSQ exactness on linear fields) and the analytic diamond
+shock-expansion theory check it further. The reference's NumPy utilities
+pin ``idw_weights`` below (``utils/metrics.py:9-14``) directly.
 
 All arithmetic is done in the dtype of the input arrays (float32 or float64),
 as the reference does under ``JAX_ENABLE_X64`` false / true. Quirks that are

@@ -1,9 +1,10 @@
 """Known-answer properties of the oracle (CPU only).
 
-The reference has no tests or golden vectors and cannot run here (JAX is
-absent), so the restatement is pinned by properties every correct
-implementation of euler_solver.py / helper.py satisfies, plus a committed
-regression fixture of the oracle itself.
+The reference has no tests or golden vectors and JAX is absent here; the
+oracle is pinned bit for bit to the reference's own solver source run with
+NumPy (tests/test_reference_fixtures.py), and these tests add properties
+every correct implementation of euler_solver.py / helper.py satisfies, plus a
+committed regression fixture of the oracle itself.
 """
 import numpy as np
 import pytest
