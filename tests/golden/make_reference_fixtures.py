@@ -21,7 +21,10 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   HLLC, sponge, residual, SRK2) with NumPy standing in for jax.numpy: 20 SRK2
   steps of the supersonic diamond (M 2.5, alpha 5) and the transonic NACA0012
   (M 0.8, alpha 1.25) golden meshes in float32 and float64, with their dt,
-  into ``reference_solver.npz``;
+  into ``reference_solver.npz``; and ``euler/main.py:43-270`` itself (the
+  stepping loop with the stationarity rule, the engineering criterion and
+  the stop bookkeeping, exports off) on three configurations, final states
+  and stop records into ``reference_runs.npz``;
 * ``euler/postproc/theory_validation_diamond.py:44-175`` the shock-expansion
   panel states of the diamond (same treatment: the gas-dynamics functions
   taken from the source, run with NumPy and SciPy) for a set of Mach numbers
@@ -104,6 +107,28 @@ def main(ref_root: str) -> Path:
             solver[f"{tag}_{dname}_W20"] = W
             solver[f"{tag}_{dname}_dt"] = np.asarray(dt_, dtype=dtp)
     np.savez_compressed(HERE / "reference_solver.npz", **solver)
+    runs, cfgs = {}, {}
+    base = ref_config.load_default_config()
+    eng = dict(engineering_target_cd=0.1235, engineering_target_cl=0.0635, engineering_cd_tol=0.3,
+               engineering_cl_tol=0.3, engineering_patience=2)
+    for tag, name, extra, precs in (
+            ("diamond", "diamond_h0.2", dict(case="diamond", Mach=2.5, aoa=5.0, tf=0.5, stationarity_threshold=2e-3,
+                                             stationarity_check_every=10, stationarity_patience=2), ("f32", "f64")),
+            ("naca_eng", "naca0012_h0.2", dict(case="naca0012", Mach=0.8, aoa=1.25, tf=0.3, stationarity_threshold=2e-4,
+                                               stationarity_check_every=7, stationarity_patience=3, **eng), ("f32", "f64")),
+            ("naca_cap", "naca0012_h0.2", dict(case="naca0012", Mach=0.8, aoa=1.25, tf=0.3, stationarity_threshold=5e-5,
+                                               stationarity_check_every=7, stationarity_patience=3, **eng), ("f64",))):
+        m = Mesh.load(HERE / f"{name}.npz")
+        cfg = dict(base, **extra)
+        cfgs[tag] = {k: v for k, v in cfg.items() if k != "export"}
+        for prec in precs:
+            W, carry = RS.run_main(ref_root, m, dict(cfg), np.float32 if prec == "f32" else np.float64,
+                                   ref_config._AOA_CASES_LC, ref_config._KNOWN_CASES_LC, ref_config.format_snapshot_name)
+            runs[f"{tag}_{prec}_W"] = W
+            runs[f"{tag}_{prec}_stop"] = np.array([bool(carry[4]), int(carry[6]), bool(carry[9]), int(carry[12])],
+                                                  dtype=np.int64)
+    runs["cfgs_json"] = np.array(json.dumps(cfgs, sort_keys=True))
+    np.savez_compressed(HERE / "reference_runs.npz", **runs)
     theory = _theory(Path(ref_root) / "euler" / "postproc" / "theory_validation_diamond.py")
     (HERE / "reference_theory.json").write_text(json.dumps(theory, indent=1, sort_keys=True) + "\n")
     summaries = _summaries(Path(ref_root) / "euler" / "utils.py")

@@ -84,10 +84,34 @@ def _vmap(f):
     return g
 
 
+class _Jitted:
+    """jax.jit: calls the function; .lower(x).compile() gives it back."""
+
+    def __init__(self, f, **kw):
+        self.f = f
+
+    def __call__(self, *a, **k):
+        return self.f(*a, **k)
+
+    def lower(self, *a, **k):
+        return types.SimpleNamespace(compile=lambda: self.f)
+
+
+def _jit(f=None, **kw):
+    return _Jitted(f, **kw) if f is not None else (lambda g: _Jitted(g, **kw))
+
+
+def _scan(body, carry, xs, length=None):
+    """jax.lax.scan as a loop (no per-step outputs are used here)."""
+    for _ in range(length):
+        carry, _ = body(carry, None)
+    return carry, None
+
+
 def _jax(jnp):
-    jit = lambda f=None, **kw: f if f is not None else (lambda g: g)   # noqa: E731
-    lax = types.SimpleNamespace(cond=lambda p, t, f, operand=None: t(operand) if bool(p) else f(operand))
-    return types.SimpleNamespace(jit=jit, lax=lax, vmap=_vmap, numpy=jnp)
+    lax = types.SimpleNamespace(cond=lambda p, t, f, operand=None: t(operand) if bool(p) else f(operand),
+                                scan=_scan)
+    return types.SimpleNamespace(jit=_jit, lax=lax, vmap=_vmap, numpy=jnp, block_until_ready=lambda x: x)
 
 
 def _defs(path: Path, names, cls=None):
@@ -103,6 +127,63 @@ def _defs(path: Path, names, cls=None):
 def _compile(nodes, ns, filename):
     exec(compile(ast.Module(body=nodes, type_ignores=[]), filename, "exec"), ns)
     return ns
+
+
+def _setup(ref_root, mesh, dtype, aoa_cases, known_cases=(), format_snapshot_name=None):
+    src = Path(ref_root) / "euler"
+    f32 = dtype == np.float32
+    jnp = _NumpyAsJnp(np, f32)
+    jax = _jax(jnp)
+    base = {"jnp": jnp, "jax": jax, "np": np, "partial": functools.partial}
+    geo = _compile(_defs(src / "jax_fvm" / "src" / "mesh.py",
+                         ["getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"],
+                         cls="Mesh"), dict(base), "mesh.py")
+    M = types.SimpleNamespace()
+    M.points = _wrap(np.asarray(mesh.points, dtype=dtype))
+    M.tris = np.asarray(mesh.tris, dtype=np.int32)
+    M.faces = np.asarray(mesh.faces, dtype=np.int32)
+    for meth in ("getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"):
+        geo[meth](M)
+    M.neighbors = np.asarray(mesh.neighbors, dtype=np.int32)
+    M.face_markers = np.asarray(mesh.face_markers, dtype=np.int32)
+    M.face_connectivity_opposite = np.arange(M.faces.shape[0])
+    M.metadata = dict(mesh.metadata)
+    M.inlet_subsonic = jnp.array([1.0, 1., 0.0, 1.0])
+    helper_names = ["get_dt", "getConserved", "getPrimitive", "getgradientLSQ", "BC_outflow", "BC_inflow",
+                    "BC_subsonic_inlet", "BC_slipwall", "_mesh_metadata", "BC_state", "get_sponge_source"]
+    hns = _compile(_defs(src / "jax_fvm" / "src" / "helper.py", helper_names), dict(base), "helper.py")
+    helper = types.SimpleNamespace(**{k: hns[k] for k in helper_names})
+    solver_names = ["venkatakrishnan", "getlimiting", "MUSCL", "get_reconstruction_mode", "get_flux_type",
+                    "build_reconstruction", "build_flux", "apply_face_surfaces", "Rusanov", "HLLC", "getFlux",
+                    "residual", "time_step_Euler", "time_step_RK2_SSP", "time_step_RK2", "time_step_RK4"]
+    sns = _compile(_defs(src / "jax_fvm" / "src" / "euler_solver.py", solver_names),
+                   dict(base, helper=helper), "euler_solver.py")
+    euler = types.SimpleNamespace(**{k: sns[k] for k in solver_names})
+    import time as _time
+    mns = _compile(_defs(src / "main.py", ["initialize", "run"]),
+                   dict(base, helper=helper, euler=euler, time=_time, _AOA_CASES_LC=tuple(aoa_cases),
+                        _KNOWN_CASES_LC=tuple(known_cases), format_snapshot_name=format_snapshot_name),
+                   "main.py")
+    return M, helper, sns, mns
+
+
+def run_main(ref_root, mesh, cfg, dtype, aoa_cases, known_cases, format_snapshot_name):
+    """euler/main.py:43-270 itself (stop rule, engineering criterion, final
+    probe) with all exports off; returns (W, final carry of the loop)."""
+    M, helper, sns, mns = _setup(ref_root, mesh, dtype, aoa_cases, known_cases, format_snapshot_name)
+    W, inlet = mns["initialize"](M, cfg)
+    captured = {}
+    scan0 = mns["jax"].lax.scan
+
+    def scan(body, carry, xs, length=None):
+        out = scan0(body, carry, xs, length=length)
+        captured["carry"] = out[0]
+        return out
+    mns["jax"].lax.scan = scan
+    cfg = dict(cfg, export=dict(results=False, figures=False, graph=False, summary=False, bundle=False, n_snaps=1),
+               verbose=False)
+    W = mns["run"](W, M, inlet, cfg, {})
+    return np.asarray(W), captured["carry"]
 
 
 def run(ref_root, mesh, mach, aoa, steps, dtype, aoa_cases):
