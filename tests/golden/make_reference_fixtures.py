@@ -21,7 +21,9 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   HLLC, sponge, residual, SRK2) with NumPy standing in for jax.numpy: 20 SRK2
   steps of the supersonic diamond (M 2.5, alpha 5) and the transonic NACA0012
   (M 0.8, alpha 1.25) golden meshes in float32 and float64, with their dt,
-  into ``reference_solver.npz``; and ``euler/main.py:43-270`` itself (the
+  CD, CL and entropy created, plus 10 steps of the diamond with the Rusanov
+  flux, constant reconstruction, explicit Euler and RK2, into
+  ``reference_solver.npz``; and ``euler/main.py:43-270`` itself (the
   stepping loop with the stationarity rule, the engineering criterion and
   the stop bookkeeping, exports off) on three configurations, final states
   and stop records into ``reference_runs.npz``;
@@ -103,9 +105,17 @@ def main(ref_root: str) -> Path:
     for tag, name, m_s, a_s in (("diamond", "diamond_h0.2", 2.5, 5.0), ("naca", "naca0012_h0.2", 0.8, 1.25)):
         m = Mesh.load(HERE / f"{name}.npz")
         for dname, dtp in (("f32", np.float32), ("f64", np.float64)):
-            W, dt_ = RS.run(ref_root, m, m_s, a_s, 20, dtp, ref_config._AOA_CASES_LC)
+            W, dt_, cd, cl, ds = RS.run(ref_root, m, m_s, a_s, 20, dtp, ref_config._AOA_CASES_LC, diagnostics=True)
             solver[f"{tag}_{dname}_W20"] = W
             solver[f"{tag}_{dname}_dt"] = np.asarray(dt_, dtype=dtp)
+            solver[f"{tag}_{dname}_cd_cl_dS"] = np.array([cd, cl, ds])
+    dmesh = Mesh.load(HERE / "diamond_h0.2.npz")
+    for flux, rec, sch in (("Rusanov", "MUSCL", "SRK2"), ("HLLC", "constant", "SRK2"), ("HLLC", "MUSCL", "EE"),
+                           ("HLLC", "MUSCL", "RK2")):
+        for dname, dtp in (("f32", np.float32), ("f64", np.float64)):
+            W, _ = RS.run(ref_root, dmesh, 2.5, 5.0, 10, dtp, ref_config._AOA_CASES_LC, flux=flux,
+                          reconstruction=rec, scheme=sch)
+            solver[f"variant_{flux}_{rec}_{sch}_{dname}_W10"] = W
     np.savez_compressed(HERE / "reference_solver.npz", **solver)
     runs, cfgs = {}, {}
     base = ref_config.load_default_config()

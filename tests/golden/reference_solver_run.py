@@ -80,7 +80,10 @@ class _NumpyAsJnp:
 
 def _vmap(f):
     def g(*args):
-        return _wrap(np.stack([f(*[a[i] for a in args]) for i in range(args[0].shape[0])]))
+        outs = [f(*[a[i] for a in args]) for i in range(args[0].shape[0])]
+        if outs and isinstance(outs[0], tuple):
+            return tuple(_wrap(np.stack([o[j] for o in outs])) for j in range(len(outs[0])))
+        return _wrap(np.stack(outs))
     return g
 
 
@@ -150,7 +153,9 @@ def _setup(ref_root, mesh, dtype, aoa_cases, known_cases=(), format_snapshot_nam
     M.metadata = dict(mesh.metadata)
     M.inlet_subsonic = jnp.array([1.0, 1., 0.0, 1.0])
     helper_names = ["get_dt", "getConserved", "getPrimitive", "getgradientLSQ", "BC_outflow", "BC_inflow",
-                    "BC_subsonic_inlet", "BC_slipwall", "_mesh_metadata", "BC_state", "get_sponge_source"]
+                    "BC_subsonic_inlet", "BC_slipwall", "_mesh_metadata", "BC_state", "get_sponge_source",
+                    "get_drag_coefficient", "get_lift_coefficient", "get_specific_entropy", "get_total_entropy",
+                    "get_entropy_creation"]
     hns = _compile(_defs(src / "jax_fvm" / "src" / "helper.py", helper_names), dict(base), "helper.py")
     helper = types.SimpleNamespace(**{k: hns[k] for k in helper_names})
     solver_names = ["venkatakrishnan", "getlimiting", "MUSCL", "get_reconstruction_mode", "get_flux_type",
@@ -186,51 +191,28 @@ def run_main(ref_root, mesh, cfg, dtype, aoa_cases, known_cases, format_snapshot
     return np.asarray(W), captured["carry"]
 
 
-def run(ref_root, mesh, mach, aoa, steps, dtype, aoa_cases):
-    """(W after `steps` SRK2 steps, dt) of the reference code on `mesh`
-    (an object with points, tris, faces, face_markers, neighbors, metadata)."""
-    src = Path(ref_root) / "euler"
-    f32 = dtype == np.float32
-    jnp = _NumpyAsJnp(np, f32)
-    jax = _jax(jnp)
-    base = {"jnp": jnp, "jax": jax, "np": np, "partial": functools.partial}
-
-    # geometry: the reference Mesh's own methods on a bare object
-    geo = _compile(_defs(src / "jax_fvm" / "src" / "mesh.py",
-                         ["getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"],
-                         cls="Mesh"), dict(base), "mesh.py")
-    M = types.SimpleNamespace()
-    M.points = _wrap(np.asarray(mesh.points, dtype=dtype))
-    M.tris = np.asarray(mesh.tris, dtype=np.int32)
-    M.faces = np.asarray(mesh.faces, dtype=np.int32)
-    for meth in ("getCenterTriangles", "getNormals", "getArea", "getSurface", "get_face_connectivity"):
-        geo[meth](M)
-    M.neighbors = np.asarray(mesh.neighbors, dtype=np.int32)
-    M.face_markers = np.asarray(mesh.face_markers, dtype=np.int32)
-    M.face_connectivity_opposite = np.arange(M.faces.shape[0])
-    M.metadata = dict(mesh.metadata)
-    M.inlet_subsonic = jnp.array([1.0, 1., 0.0, 1.0])
-
-    helper_names = ["get_dt", "getConserved", "getPrimitive", "getgradientLSQ", "BC_outflow", "BC_inflow",
-                    "BC_subsonic_inlet", "BC_slipwall", "_mesh_metadata", "BC_state", "get_sponge_source"]
-    hns = _compile(_defs(src / "jax_fvm" / "src" / "helper.py", helper_names), dict(base), "helper.py")
-    helper = types.SimpleNamespace(**{k: hns[k] for k in helper_names})
-    solver_names = ["venkatakrishnan", "getlimiting", "MUSCL", "get_reconstruction_mode", "get_flux_type",
-                    "build_reconstruction", "build_flux", "apply_face_surfaces", "Rusanov", "HLLC", "getFlux",
-                    "residual", "time_step_RK2_SSP"]
-    sns = _compile(_defs(src / "jax_fvm" / "src" / "euler_solver.py", solver_names),
-                   dict(base, helper=helper), "euler_solver.py")
-    mns = _compile(_defs(src / "main.py", ["initialize"]),
-                   dict(base, helper=helper, _AOA_CASES_LC=tuple(aoa_cases)), "main.py")
-
+def run(ref_root, mesh, mach, aoa, steps, dtype, aoa_cases, flux="HLLC", reconstruction="MUSCL",
+        scheme="SRK2", diagnostics=False):
+    """(W after `steps` steps of `scheme`, dt) of the reference code on `mesh`
+    (an object with points, tris, faces, face_markers, neighbors, metadata);
+    with diagnostics, also the reference's CD, CL (helper.py:366-415) and the
+    entropy created since the start (helper.py:312-320) of the final state."""
+    M, helper, sns, mns = _setup(ref_root, mesh, dtype, aoa_cases)
     cfg = dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa, case=mesh.metadata["case"], CFL=0.6)
     if 0.6 < cfg["Mach"] < 1.1 and cfg["CFL"] > 0.45:     # euler/main.py:117-120
         cfg["CFL"] = 0.45
-    W, inlet = mns["initialize"](M, cfg)
-    if steps == 0:
-        return np.asarray(W), float(helper.get_dt(W, M, CFL=cfg["CFL"], gamma=cfg["gamma"], M=1.0))
-    dt = helper.get_dt(W, M, CFL=cfg["CFL"], gamma=cfg["gamma"], M=1.0)
-    kw = dict(gamma=cfg["gamma"], M=1.0, reconstruction="MUSCL", flux="HLLC", value=inlet, entropy=False)
+    W0, inlet = mns["initialize"](M, cfg)
+    dt = helper.get_dt(W0, M, CFL=cfg["CFL"], gamma=cfg["gamma"], M=1.0)
+    fn = {"EE": sns["time_step_Euler"], "RK2": sns["time_step_RK2"], "SRK2": sns["time_step_RK2_SSP"]}[scheme]
+    kw = dict(gamma=cfg["gamma"], M=1.0, reconstruction=reconstruction, flux=flux, value=inlet, entropy=False)
+    W = W0
     for _ in range(steps):
-        W = sns["time_step_RK2_SSP"](W, M, dt, **kw)
-    return np.asarray(W), float(dt)
+        W = fn(W, M, dt, **kw)
+    if not diagnostics:
+        return np.asarray(W), float(dt)
+    u_inf = mach * float(np.sqrt(1.4 * 1.0 / 1.0))
+    L = mesh.metadata["obstacle_length"]
+    cd = helper.get_drag_coefficient(W=W, mesh=M, rho_inf=1.0, U_inf=u_inf, L_ref=L)
+    cl = helper.get_lift_coefficient(W=W, mesh=M, rho_inf=1.0, U_inf=u_inf, L_ref=L)
+    ds = helper.get_entropy_creation(W0, W, M, gamma=1.4)
+    return np.asarray(W), float(dt), float(cd), float(cl), float(ds)

@@ -193,6 +193,34 @@ def test_oracle_bitwise_equals_reference_solver_source(tag, name, mach, aoa, pre
         W = O.time_step_srk2(W, om, dt, inlet)
     assert W.dtype == ref[f"{tag}_{prec}_W20"].dtype
     assert np.array_equal(W, ref[f"{tag}_{prec}_W20"])
+    # the reference's CD, CL (helper.py:366-415) and entropy created (:312-320)
+    W0, _ = O.initialize(mesh.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=mach, aoa=aoa,
+                                            case=mesh.metadata["case"]), dtype)
+    cd, cl = O.force_coefficients(W, om, 1.0, mach * 1.4 ** 0.5, mesh.metadata["obstacle_length"])
+    ds = O.total_entropy(W, om) - O.total_entropy(W0, om)
+    assert [cd, cl, float(ds)] == ref[f"{tag}_{prec}_cd_cl_dS"].tolist()
+
+
+@pytest.mark.parametrize("flux,rec,scheme", [("Rusanov", "MUSCL", "SRK2"), ("HLLC", "constant", "SRK2"),
+                                             ("HLLC", "MUSCL", "EE"), ("HLLC", "MUSCL", "RK2")])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_oracle_scheme_variants_equal_reference_source(flux, rec, scheme, prec):
+    """The Rusanov flux, constant reconstruction, explicit Euler and RK2 of the
+    oracle against the reference's own functions (euler_solver.py:201-244,
+    106-122, 630-654), 10 steps of the diamond, bit for bit."""
+    from conftest import oracle_mesh
+    from oracle import euler_oracle as O
+    ref = np.load(GOLDEN / "reference_solver.npz")
+    dtype = np.float32 if prec == "f32" else np.float64
+    mesh = load_mesh("diamond_h0.2")
+    om = oracle_mesh(mesh, dtype)
+    W, inlet = O.initialize(mesh.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=2.5, aoa=5.0,
+                                               case="diamond"), dtype)
+    dt = O.get_dt(W, om, CFL=0.6)
+    fn = O.TIME_SCHEMES[scheme]
+    for _ in range(10):
+        W = fn(W, om, dt, inlet, reconstruction=rec.lower(), flux=flux.lower())
+    assert np.array_equal(W, ref[f"variant_{flux}_{rec}_{scheme}_{prec}_W10"])
 
 
 def test_freestream_equals_reference_initial_state():
