@@ -1,4 +1,6 @@
-"""CUDA kernels vs the NumPy oracle on the same meshes and inputs.
+"""CUDA kernels vs the NumPy oracle on the same meshes and inputs (the oracle
+equals the reference's own solver source bit for bit, tests/
+test_reference_fixtures.py), and directly vs that source's golden output.
 
 Tolerances: float64 kernels vs float64 oracle 1e-12 (field-scaled relative,
 after 100 SRK2 steps); float32 kernels vs float32 oracle 1e-5 after 100 steps;
@@ -375,3 +377,18 @@ def test_per_case_threshold(diamond02):
         r1 = one.run()[0]
         assert (r1['stopping_step'], r1['status']) == (r['stopping_step'], r['status']), (t, r1, r)
     assert res[1]['stopping_step'] > res[0]['stopping_step'] > res[2]['stopping_step']
+
+
+@pytest.mark.parametrize("tag,name,mach,aoa,prec,tol", [("diamond", "diamond_h0.2", 2.5, 5.0, "f64", 1e-12),
+                                                        ("naca", "naca0012_h0.2", 0.8, 1.25, "f64", 1e-12),
+                                                        ("diamond", "diamond_h0.2", 2.5, 5.0, "f32", 1e-5)])
+def test_cuda_against_reference_solver_source(tag, name, mach, aoa, prec, tol):
+    """The CUDA path against EulerSR's own solver source run with NumPy for
+    jax.numpy (tests/golden/reference_solver.npz, made by
+    tests/golden/make_reference_fixtures.py): 20 SRK2 steps and the dt."""
+    from conftest import GOLDEN, load_mesh
+    ref = np.load(GOLDEN / "reference_solver.npz")
+    Wg, dtg, _ = _gpu_steps(load_mesh(name), prec, mach, aoa, 20)
+    dt_ref = float(ref[f"{tag}_{prec}_dt"])
+    assert abs(dtg - dt_ref) <= (1e-14 if prec == "f64" else 2e-6) * dt_ref
+    assert rel_err(Wg, ref[f"{tag}_{prec}_W20"]) <= tol
