@@ -804,12 +804,26 @@ struct SolverT : SolverBase {
     hcase_index[slot] = -1;
     return ESR_OK;
   }
+  // A caller's device state buffer is read or written by a kernel as 4-value
+  // vectors, so it must be memory of this solver's GPU (or managed memory)
+  // aligned for them; a host address or another GPU's memory is an argument
+  // error here, before any launch.
+  int check_state_ptr(const void* p, const char* what) {
+    cudaPointerAttributes a{};
+    ESR_CUDA(cudaPointerGetAttributes(&a, p));
+    const bool dev = (a.type == cudaMemoryTypeDevice && a.device == device) || a.type == cudaMemoryTypeManaged;
+    if (!dev) return fail(ESR_ERR_ARG, std::string(what) + ": not device memory of the solver's GPU");
+    if ((uintptr_t)p % alignof(V) != 0)
+      return fail(ESR_ERR_ARG, std::string(what) + ": state must be aligned to " + std::to_string(alignof(V)) + " bytes");
+    return ESR_OK;
+  }
   int set_state(int slot, const double* Wh, bool device_src) {
     int m, b;
     ESR_TRY(mesh_of_slot(slot, m, b));
     MeshDev& md = *meshes[m];
     const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
     if (device_src) {
+      ESR_TRY(check_state_ptr(Wh, "set_state_device"));
       k_copy_in_device<T><<<nb, tb, 0, stream>>>((const V*)Wh, md.inv.p, N, W.p, Wref.p, md.off, md.B, b);
     } else {
       if (stage_rows.n < (size_t)4 * N) ESR_TRY(stage_rows.alloc((size_t)4 * N));
@@ -826,6 +840,7 @@ struct SolverT : SolverBase {
     MeshDev& md = *meshes[m];
     const int N = md.hm->n_cells, tb = 256, nb = (N + tb - 1) / tb;
     if (device_dst) {
+      ESR_TRY(check_state_ptr(Wh, "get_state_device"));
       k_copy_out_device<T><<<nb, tb, 0, stream>>>(W.p, md.inv.p, N, md.off, md.B, b, (V*)Wh);
       ++launches;
       ESR_CUDA(cudaGetLastError());

@@ -28,7 +28,13 @@ ROW_TILE = 128  # the GEMM tiles rows by 128
 
 
 def _p(t):
-    return C.c_void_p(t.data_ptr()) if t is not None else None
+    """Device address of a CUDA tensor for a kernel argument. A tensor in host
+    memory is refused here: the kernels would dereference its address."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError(f"expected a CUDA tensor, got one on {t.device}")
+    return C.c_void_p(t.data_ptr())
 
 
 def _stream():
@@ -41,6 +47,8 @@ class MLP:
               ("W3", (H, H)), ("b3", (H,)), ("W4", (N_OUT, H)), ("b4", (N_OUT,))]
 
     def __init__(self, device="cuda", seed=0, n_features=13, gemm="tcgen05"):
+        if torch.device(device).type != "cuda":
+            raise ValueError(f"the MLP runs on the library's CUDA kernels; device must be a CUDA device, not {device!r}")
         self.L = F.lib()
         # the 256-wide layers: tcgen05 kernel, or the mma.sync kernel kept as its cross-check
         self.gemm = {"tcgen05": self.L.esr_gemm_bf16, "mma_sync": self.L.esr_gemm_bf16_mma_sync}[gemm]

@@ -39,7 +39,13 @@ def draw_cases(n_train, n_eval, seed=3):
 
 
 def _p(t):
-    return C.c_void_p(t.data_ptr()) if t is not None else None
+    """Device address of a CUDA tensor for a kernel argument. A tensor in host
+    memory is refused here: the kernels would dereference its address."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError(f"expected a CUDA tensor, got one on {t.device}")
+    return C.c_void_p(t.data_ptr())
 
 
 def _stream():
@@ -68,6 +74,8 @@ class WarmStart:
     """IDW (+ MLP) prediction of an HR initial field from an LR solution."""
 
     def __init__(self, pair: MeshPair, mu=None, sig=None, mlp: MLP | None = None, device="cuda"):
+        if torch.device(device).type != "cuda":
+            raise ValueError(f"the warm start runs on the library's CUDA kernels; device must be a CUDA device, not {device!r}")
         self.pair = pair
         self.L = F.lib()
         self.device = device

@@ -218,7 +218,9 @@ int esr_get_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, floa
  * reset and dt recomputed from W, as esr_set_case with W_init does. */
 int esr_set_state(esr_solver* solver, int32_t slot, const double* W);
 int esr_get_state(esr_solver* solver, int32_t slot, double* W);
-/* device-resident float32/float64 state of a slot in the caller's cell order */
+/* device-resident float32/float64 state of a slot in the caller's cell order;
+ * d_W must be memory of the solver's GPU (or managed memory) aligned to 16
+ * bytes, else ESR_ERR_ARG before any launch */
 int esr_set_state_device(esr_solver* solver, int32_t slot, const void* d_W);
 int esr_get_state_device(esr_solver* solver, int32_t slot, void* d_W);
 int esr_compute_dt(esr_solver* solver, double* dt_per_slot);

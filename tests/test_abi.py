@@ -138,3 +138,26 @@ def test_ctypes_signatures_match_header_prototypes():
     for name, (_, args) in F._SIGS.items():
         assert name in protos, name
         assert len(args) == protos[name], (name, len(args), protos[name])
+
+
+def test_no_cpu_fallback(diamond02):
+    """The product path has no CPU fallback: on a machine without a usable GPU
+    the solver fails with ESR_ERR_CUDA and the CUDA error text, and the warm
+    start wrappers refuse host tensors and host devices before any launch."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    from eulersr_b200.solver import Solver
+    from eulersr_b200.warmstart import mlp as mlp_mod, pipeline
+    if not torch.cuda.is_available():
+        with pytest.raises(F.EsrError) as e:
+            Solver(diamond02, 2, precision="f32")
+        assert e.value.code == F.ESR_ERR_CUDA
+        assert "cuda" in str(e.value).lower()
+    for wrap in (mlp_mod._p, pipeline._p):
+        assert wrap(None) is None
+        with pytest.raises(ValueError, match="CUDA tensor"):
+            wrap(torch.zeros(4))
+    with pytest.raises(ValueError, match="CUDA device"):
+        mlp_mod.MLP(device="cpu")
+    with pytest.raises(ValueError, match="CUDA device"):
+        pipeline.WarmStart(None, device="cpu")
