@@ -161,3 +161,76 @@ def test_no_cpu_fallback(diamond02):
         mlp_mod.MLP(device="cpu")
     with pytest.raises(ValueError, match="CUDA device"):
         pipeline.WarmStart(None, device="cpu")
+
+
+def _single_triangle(points=((0.0, 0.0), (1.0, 0.0), (0.0, 1.0)), markers=(3, 4, 2)):
+    from eulersr_b200.mesh import Mesh
+    return Mesh.from_arrays(np.array(points), [[0, 1, 2]], [[-1, -1, -1]], [[0, 1], [1, 2], [2, 0]], list(markers),
+                            [[0, 1, 2]], dict(case="diamond"))
+
+
+def test_mesh_edge_cases(diamond02):
+    """Smallest and malformed meshes: one triangle whose three faces are all
+    boundary faces prepares; an empty mesh, a degenerate triangle, an
+    interior marker on a boundary edge and a neighbour that does not share
+    the face are argument errors on the host, as are null arguments."""
+    from eulersr_b200 import _ffi as F
+    from eulersr_b200.mesh import Mesh
+    from eulersr_b200.solver import DeviceMesh
+    one = DeviceMesh(_single_triangle())
+    assert one.n_cells == 1 and one.info.n_boundary_slots == 3 and one.info.n_wall_faces == 1
+    assert list(one.permutation()) == [0]
+
+    def rejects(mesh, text):
+        with pytest.raises(F.EsrError) as e:
+            DeviceMesh(mesh)
+        assert e.value.code == F.ESR_ERR_ARG and text in str(e.value), str(e.value)
+
+    rejects(_single_triangle(points=((0.0, 0.0), (1.0, 0.0), (2.0, 0.0))), "degenerate")
+    rejects(_single_triangle(markers=(0, 4, 2)), "interior face marker")
+    empty = Mesh.__new__(Mesh)
+    empty.__dict__.update(diamond02.__dict__)
+    empty.tris = np.zeros((0, 3), np.int32)
+    empty.neighbors = np.zeros((0, 3), np.int32)
+    empty.face_connectivity = np.zeros((0, 3), np.int32)
+    rejects(empty, "empty mesh")
+    # a neighbour that exists but does not list the shared face
+    nb = diamond02.neighbors.copy()
+    c = int(np.argmax((nb >= 0).all(axis=1)))
+    far = next(j for j in range(diamond02.n_cells) if j != c and j not in set(nb[c].tolist())
+               and c not in set(nb[j].tolist()))
+    nb[c, 0] = far
+    bad = Mesh.__new__(Mesh)
+    bad.__dict__.update(diamond02.__dict__)
+    bad.neighbors = nb
+    rejects(bad, "does not list the shared face")
+    L = F.lib()
+    assert L.esr_mesh_create(None, None) == F.ESR_ERR_ARG
+    assert b"null" in L.esr_last_error()
+
+
+@pytest.mark.parametrize("field,value,text", [("precision", 2, "unknown precision"), ("flux", 7, "Unknown flux type"),
+                                              ("reconstruction", 5, "Unknown reconstruction scheme"),
+                                              ("time_scheme", 3, "unknown time scheme"), ("dt_mode", -1, "unknown dt mode"),
+                                              ("stop_rule", 3, "unknown stop rule"), ("gamma", 1.0, "gamma must be > 1"),
+                                              ("slots", 0, "slots_per_mesh must be > 0")])
+def test_solver_create_checks_arguments_first(diamond02, field, value, text):
+    """esr_solver_create checks every argument before it touches a device, so
+    a bad one is ESR_ERR_ARG with the reference's message on any machine."""
+    from eulersr_b200 import _ffi as F
+    from eulersr_b200.solver import DeviceMesh
+    L = F.lib()
+    dm = DeviceMesh(diamond02)
+    p = F.Params(precision=0, flux=0, reconstruction=0, time_scheme=0, dt_mode=0, stop_rule=0, gamma=1.4,
+                 threshold=1e-6, check_every=10, patience=3, device=0, use_graphs=1, block_size=0)
+    slots = (C.c_int32 * 1)(4)
+    if field == "slots":
+        slots[0] = value
+    else:
+        setattr(p, field, value)
+    meshes = (C.c_void_p * 1)(dm.handle.value)
+    h = C.c_void_p()
+    assert L.esr_solver_create(meshes, slots, 1, C.byref(p), C.byref(h)) == F.ESR_ERR_ARG
+    assert text in L.esr_last_error().decode()
+    assert not h.value
+    assert L.esr_solver_create(None, slots, 1, C.byref(p), C.byref(h)) == F.ESR_ERR_ARG
