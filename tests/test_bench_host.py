@@ -86,3 +86,12 @@ def test_bench_reductions_over_two_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert out == [(0, 2.5, 30.0), (1, 2.5, 30.0)]
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    """Under torchrun the reference arm's other ranks exit 0 at once: no mesh,
+    no CPU work, no JSON line."""
+    made = _fake_meshes(monkeypatch)
+    args = types.SimpleNamespace(workload="naca", h=0.025, cases=256, steps=3, warmup=3, precision="f32")
+    assert bench.run_reference(args, 2, 1) == 0
+    assert made == [] and capsys.readouterr().out == ""
