@@ -86,7 +86,8 @@ struct SolverT : SolverBase {
   int block = 128;
 
   struct MeshDev {
-    const HostMesh* hm;
+    HostMesh own;            // the solver's copy: the caller may destroy its mesh
+    const HostMesh* hm = nullptr;
     DevBuf<T> geo;
     DevBuf<int4> nbr;
     DevBuf<int> wall_cell;
@@ -200,7 +201,8 @@ struct SolverT : SolverBase {
     int max_cells = 0;
     for (int m = 0; m < nm; ++m) {
       auto md = std::make_unique<MeshDev>();
-      md->hm = &ms[m]->hm;
+      md->own = ms[m]->hm;
+      md->hm = &md->own;
       md->B = slots[m];
       md->case0 = case0;
       md->off = off;

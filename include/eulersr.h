@@ -187,7 +187,9 @@ int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info);
 int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm);
 
 /* A solver holds `n_meshes` meshes and slots_per_mesh[m] concurrent case
- * slots on mesh m; all slots advance together in one launch per kernel. */
+ * slots on mesh m; all slots advance together in one launch per kernel. It
+ * keeps its own copy of each mesh, so a mesh may be destroyed once the
+ * solvers made from it exist. */
 int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_mesh, int32_t n_meshes,
                       const esr_params* params, esr_solver** out);
 int esr_solver_destroy(esr_solver* solver);
