@@ -159,6 +159,7 @@ _SIGS = {
     "esr_rel_change_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_idw_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                 C.c_void_p, C.c_void_p]),
+    "esr_idw_status": (C.c_int, [C.POINTER(C.c_int32)]),
 }
 
 

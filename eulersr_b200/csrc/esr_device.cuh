@@ -9,7 +9,8 @@
 //              per cell and case, cases of one mesh innermost so a warp of a
 //              batched mesh walks 32 cases of the same cell: every geometry
 //              load is a broadcast and every branch on boundary type uniform)
-//   geometry   per mesh, structure of arrays geo[field * stride + cell]
+//   geometry   per mesh, one record of G_COUNT values per cell
+//              (geo[cell * G_COUNT + field], esr_layout.h), read as float4/double4 groups
 //   K1 recon   cell + 3 neighbour primitives, LSQ gradient, Venkatakrishnan
 //              limiter, the 3 MUSCL face states of the cell -> FV[k][item]
 //   K2 flux    per cell: the 3 face fluxes (HLLC or Rusanov) from its own
@@ -1251,17 +1252,29 @@ __global__ void k_copy_out_device(const V4<T>* __restrict__ W, const int* __rest
 
 // ------------------------------------------------------------------- IDW
 // eval/core.py:135-142 with utils/metrics.py:9-14: weights from float64
-// distances, float32 weighted sum over the k neighbours in order.
-static __global__ void k_idw(const float* __restrict__ src, int n_vars, const int* __restrict__ idx,
-                      const float* __restrict__ dist, int n_dst, int k, float* __restrict__ out) {
+// distances, float32 weighted sum over the k neighbours in order. A
+// neighbour index outside [0, n_src) is never read: the row becomes NaN and
+// *bad is set (the host reads it with esr_idw_status).
+__device__ int g_idw_bad = 0;
+
+static __global__ void k_idw(const float* __restrict__ src, int n_src, int n_vars, const int* __restrict__ idx,
+                             const float* __restrict__ dist, int n_dst, int k, float* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_dst) return;
   double wsum = 0.0;
   double w[16];
+  bool in_range = true;
   for (int j = 0; j < k; ++j) {
+    const int q = idx[(size_t)i * k + j];
+    in_range = in_range && q >= 0 && q < n_src;
     const double d = (double)dist[(size_t)i * k + j];
     w[j] = 1.0 / (d * d + 1e-12);
     wsum += w[j];
+  }
+  if (!in_range) {
+    atomicExch(&g_idw_bad, 1);
+    for (int v = 0; v < n_vars; ++v) out[(size_t)i * n_vars + v] = __int_as_float(0x7fc00000);
+    return;
   }
   for (int v = 0; v < n_vars; ++v) {
     float acc = 0.0f;

@@ -1658,9 +1658,20 @@ int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars, const int32
   if (k < 1 || k > 16) return fail(ESR_ERR_ARG, "idw: k must be in [1, 16]");
   if (n_dst == 0) return ESR_OK;
   const int tb = 128, nb = (n_dst + tb - 1) / tb;
-  esr::k_idw<<<nb, tb, 0, (cudaStream_t)stream>>>(d_src, n_vars, d_idx, d_dist, n_dst, k, d_out);
+  esr::k_idw<<<nb, tb, 0, (cudaStream_t)stream>>>(d_src, n_src, n_vars, d_idx, d_dist, n_dst, k, d_out);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? ESR_OK : fail(ESR_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int esr_idw_status(int32_t* bad) {
+  if (!bad) return fail(ESR_ERR_ARG, "idw_status: null output");
+  int v = 0;
+  const int zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, esr::g_idw_bad, sizeof(int));
+  if (e == cudaSuccess && v) e = cudaMemcpyToSymbol(esr::g_idw_bad, &zero, sizeof(int));
+  if (e != cudaSuccess) return fail(ESR_ERR_CUDA, std::string("idw_status: ") + cudaGetErrorString(e));
+  *bad = v;
+  return ESR_OK;
 }
 
 }  // extern "C"

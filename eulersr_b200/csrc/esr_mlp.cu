@@ -478,7 +478,9 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
   const int k_begin = blockIdx.z * K_split;
   const int KT = K_split / BK;
 
+  __shared__ int s_abort;   // set when a pipeline wait gave up: the tile is not written
   if (tid == 0) {
+    s_abort = 0;
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(empty + 8 * s, 1);
       mbar_init(full + 8 * s, 1);
@@ -511,10 +513,14 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
         else for (int g = 0; g < BN / 64; ++g) tma_load_2d(b + g * 8192, &tmB, n_blk + 64 * g, k0, bar);
       };
       constexpr uint32_t idesc = instr_desc<A_T, B_T, BN>();
-      for (int p = 0; p < STAGES && p < KT; ++p) produce(p, p);
-      for (int kt = 0; kt < KT; ++kt) {
+      int issued = 0;      // K-blocks whose loads have been issued
+      int landed = 0;      // K-blocks whose loads are known to have landed
+      bool ok = true;
+      for (int p = 0; p < STAGES && p < KT; ++p) { produce(p, p); issued = p + 1; }
+      for (int kt = 0; kt < KT && ok; ++kt) {
         const int s = kt % STAGES;
-        mbar_wait(full + 8 * s, (kt / STAGES) & 1);
+        if (!mbar_wait(full + 8 * s, (kt / STAGES) & 1)) { ok = false; break; }
+        landed = kt + 1;
         tc_fence_after();
         const uint32_t a = tiles + s * STAGE_BYTES, b = a + A_BYTES;
 #pragma unroll
@@ -528,18 +534,40 @@ __global__ void __launch_bounds__(THREADS) k_gemm_tc(int M, int N, int K_split, 
         const int nxt = kt - 1 + STAGES;
         if (kt >= 1 && nxt < KT) {
           const int ps = (kt - 1) % STAGES;
-          mbar_wait(empty + 8 * ps, ((kt - 1) / STAGES) & 1);
+          if (!mbar_wait(empty + 8 * ps, ((kt - 1) / STAGES) & 1)) { ok = false; break; }
           produce(nxt, ps);
+          issued = nxt + 1;
         }
       }
-      umma_commit(done);   // its one phase completes when every MMA of the tile has
+      if (!ok) {
+        // A wait gave up: nothing more is issued. Loads already issued may
+        // still be landing in shared memory; give each a bounded wait before
+        // the block can exit (each stage has at most one load outstanding).
+        for (int j = landed; j < issued; ++j) mbar_wait(full + 8 * (j % STAGES), (j / STAGES) & 1);
+        s_abort = 1;
+      }
+      umma_commit(done);   // its one phase completes when every MMA issued so far has
     }
     __syncwarp();
   }
   // The other warps reach this wait while the mainloop is still running. A
   // stage barrier cannot serve here: waiting on parity 1 of a barrier still in
   // its first phase returns at once. `done` completes exactly once.
-  mbar_wait(done, 0);
+  const bool done_ok = mbar_wait(done, 0);
+  if (!done_ok) atomicOr(&s_abort, 1);
+  __syncthreads();
+  if (s_abort) {
+    // The tile is not complete: write nothing. The accumulator is released
+    // once the MMAs issued have finished (one more bounded wait), so the
+    // block holds no tensor memory when it returns; the host sees the flag.
+    if (warp == 0) {
+      if (!done_ok) mbar_wait(done, 0);
+      __syncwarp();
+      tc_fence_after();
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(BN));
+    }
+    return;
+  }
   tc_fence_after();
 
   // Accumulators -> shared memory (the pipeline buffers are free now), 128

@@ -84,6 +84,25 @@ __global__ void k_relchange_final(const double2* __restrict__ part, int nb, doub
   *out = sqrt(s0) / (sqrt(s1) + 1e-16);
 }
 
+// A kernel of this file reads `p` (or writes it): it must be memory of the
+// current GPU, or managed memory, aligned to `align` bytes. A host address or
+// another GPU's memory is an argument error here, before any launch.
+int check_device_ptr(const void* p, int dev, size_t align, const char* what) {
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // the failed query must not surface as a later launch's error
+    return noalloc_fail(ESR_ERR_ARG, std::string("rel_change_noalloc: ") + what + ": not a device address (" +
+                                         cudaGetErrorString(e) + ")");
+  }
+  const bool ok = (a.type == cudaMemoryTypeDevice && a.device == dev) || a.type == cudaMemoryTypeManaged;
+  if (!ok) return noalloc_fail(ESR_ERR_ARG, std::string("rel_change_noalloc: ") + what + ": not device memory of the current GPU");
+  if ((uintptr_t)p % align)
+    return noalloc_fail(ESR_ERR_ARG, std::string("rel_change_noalloc: ") + what + " must be " + std::to_string(align) +
+                                         "-byte aligned");
+  return ESR_OK;
+}
+
 // device address of the partials array for the current device (set-up on first use)
 int partials_for_current_device(double2** out) {
   int dev = 0;
@@ -115,11 +134,17 @@ int esr_rel_change_noalloc(const void* d_A, const void* d_B, int64_t n_rows, int
   if (n_rows > kNoAllocMaxRows)
     return noalloc_fail(ESR_ERR_ARG, "rel_change_noalloc: n_rows " + std::to_string(n_rows) + " exceeds the maximum " +
                                          std::to_string(kNoAllocMaxRows) + " of the fixed scratch array");
-  const size_t align = 16;
-  if (((uintptr_t)d_A % align) || ((uintptr_t)d_B % align))
-    return noalloc_fail(ESR_ERR_ARG, "rel_change_noalloc: inputs must be 16-byte aligned");
+  int dev = 0;
+  cudaError_t ge = cudaGetDevice(&dev);
+  if (ge != cudaSuccess) return noalloc_fail(ESR_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ge));
+  // the rows are read as 4-value vectors (16-byte loads), the result written as one double
+  const size_t row_align = 16;
+  int rc = check_device_ptr(d_A, dev, row_align, "d_A");
+  if (rc == ESR_OK) rc = check_device_ptr(d_B, dev, row_align, "d_B");
+  if (rc == ESR_OK) rc = check_device_ptr(d_out, dev, alignof(double), "d_out");
+  if (rc != ESR_OK) return rc;
   double2* part = nullptr;
-  int rc = partials_for_current_device(&part);
+  rc = partials_for_current_device(&part);
   if (rc != ESR_OK) return rc;
   const int nb = (int)((n_rows + kNoAllocRowsPerBlock - 1) / kNoAllocRowsPerBlock);
   cudaStream_t st = (cudaStream_t)stream;

@@ -303,8 +303,10 @@ int esr_batch_cancel(esr_solver* solver);
 
 /* Relative change ||A - B||_F / (||B||_F + 1e-16) of two device fields of
  * n_rows x 4 values (float4 rows for ESR_PREC_F32, double4 rows for
- * ESR_PREC_F64, 16-byte aligned), written to the device double *d_out on
- * `stream`. No counterpart in the reference: it is the allocation-free form
+ * ESR_PREC_F64), written to the device double *d_out on `stream`. d_A and
+ * d_B must be memory of the current GPU (or managed memory) aligned to 16
+ * bytes, d_out the same aligned to 8 bytes; anything else (a host address,
+ * another GPU's memory) is ESR_ERR_ARG before any launch. No counterpart in the reference: it is the allocation-free form
  * of the solver's stop-rule norm, for callers that cannot allocate device
  * memory when they need it (a host allocator that owns the whole device
  * budget, a pre-sized arena that forbids allocation after start-up). Its
@@ -317,10 +319,15 @@ int esr_rel_change_noalloc(const void* d_A, const void* d_B, int64_t n_rows, int
                            double* d_out, void* stream);
 
 /* IDW (k neighbours, weights 1/(d^2+1e-12) normalised) of a source field onto
- * target points; all pointers are device pointers, float32, row-major. */
+ * target points; all pointers are device pointers, float32, row-major. A
+ * neighbour index outside [0, n_src) is never read: that target row is set
+ * to NaN and the library's IDW error flag is raised. */
 int esr_idw_apply(const float* d_src, int32_t n_src, int32_t n_vars,
                   const int32_t* d_idx, const float* d_dist, int32_t n_dst, int32_t k,
                   float* d_out, void* stream);
+/* Synchronous: 1 in *bad when an esr_idw_apply since the last call met an
+ * out-of-range neighbour index, then clears the flag. */
+int esr_idw_status(int32_t* bad);
 
 /* ---- learned warm start: BF16 training/inference kernels of the residual
  * MLP that corrects the IDW interpolation (replaces the DAM/AMNet forward of

@@ -1,6 +1,6 @@
 """Throughput of the warm-start MLP kernels on the GPU.
 
-    python -m eulersr_b200.warmstart.mlp_bench [--rows 32768] [--reps 20]
+    python mlp_bench.py [--rows 32768] [--reps 20]
 
 Times, with CUDA events on the current stream after warm-up, for the tcgen05
 GEMM and the mma.sync GEMM it replaced: one 256-wide forward layer
@@ -15,12 +15,16 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import sys
 from pathlib import Path
 
 import torch
 
-from .. import _ffi as F
-from .mlp import H, K_IN, MLP
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from eulersr_b200 import _ffi as F  # noqa: E402
+from eulersr_b200.warmstart.mlp import H, K_IN, MLP  # noqa: E402
 
 
 def _time(fn, reps):
@@ -54,7 +58,7 @@ def main(argv=None):
     p = lambda t: C.c_void_p(t.data_ptr())
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     peak = None
-    pk = Path(__file__).resolve().parents[2] / "MEASURED_PEAKS.json"
+    pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
         peak = float(json.loads(pk.read_text())["bf16_tflops"])
     out = {"rows": rows, "peak_bf16_tflops": peak}

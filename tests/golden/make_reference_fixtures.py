@@ -38,7 +38,7 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
 
 Run from the repository root with the reference checkout as the argument:
 
-    python tests/golden/make_reference_fixtures.py /root/reference
+    python tests/golden/make_reference_fixtures.py <path of the EulerSR checkout>
 """
 from __future__ import annotations
 
@@ -249,4 +249,6 @@ def _summaries(utils_py: Path) -> list:
 
 
 if __name__ == "__main__":
-    print(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_reference_fixtures.py <path of the EulerSR checkout>")
+    print(main(sys.argv[1]))

@@ -91,6 +91,39 @@ def test_idw_kernel_matches_formula():
     torch.cuda.synchronize()
     ref = O.idw_predict(src, idx, dist)
     assert np.max(np.abs(out.cpu().numpy() - ref)) <= 2e-6 * max(1.0, np.abs(ref).max())
+    bad = C.c_int32(7)
+    F.check(F.lib().esr_idw_status(C.byref(bad)))
+    assert bad.value == 0
+
+
+def test_idw_kernel_refuses_out_of_range_indices():
+    """A neighbour index outside [0, n_src) is never dereferenced: its row
+    comes out NaN, the other rows are unchanged, and the status flag reports
+    it once (reading it clears it)."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    from oracle import euler_oracle as O
+    rng = np.random.default_rng(1)
+    src = rng.standard_normal((50, 4)).astype(np.float32)
+    idx = rng.integers(0, 50, (64, 6)).astype(np.int32)
+    idx[5, 2] = 50          # one past the end
+    idx[9, 0] = -1          # negative
+    dist = rng.uniform(1e-3, 0.5, (64, 6)).astype(np.float32)
+    ds, di, dd = (torch.from_numpy(a).cuda() for a in (src, idx, dist))
+    out = torch.empty((64, 4), dtype=torch.float32, device="cuda")
+    F.check(F.lib().esr_idw_apply(C.c_void_p(ds.data_ptr()), 50, 4, C.c_void_p(di.data_ptr()),
+                                  C.c_void_p(dd.data_ptr()), 64, 6, C.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.isnan(got[[5, 9]]).all()
+    good = np.setdiff1d(np.arange(64), [5, 9])
+    ref = O.idw_predict(src, idx[good], dist[good])
+    assert np.max(np.abs(got[good] - ref)) <= 2e-6 * max(1.0, np.abs(ref).max())
+    bad = C.c_int32(0)
+    F.check(F.lib().esr_idw_status(C.byref(bad)))
+    assert bad.value == 1
+    F.check(F.lib().esr_idw_status(C.byref(bad)))
+    assert bad.value == 0
 
 
 def test_feature_and_decode_kernels_match_formula():

@@ -60,3 +60,30 @@ def test_rel_change_noalloc_rejects_oversize():
                                   C.c_void_p(out.data_ptr()), None)
     assert rc == F.ESR_ERR_ARG
     assert b"exceeds the maximum" in L.esr_last_error()
+
+
+def test_rel_change_noalloc_rejects_host_and_misaligned_pointers():
+    """Addresses its kernels could not read are refused before any launch:
+    plain and pinned host memory, and device rows or an output that are not
+    aligned for the vector loads and the double store."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    L = F.lib()
+    dev = torch.zeros((64, 4), dtype=torch.float32, device='cuda')
+    out = torch.zeros(4, dtype=torch.float64, device='cuda')
+    host = np.zeros((64, 4), dtype=np.float32)
+    pinned = torch.zeros((64, 4), dtype=torch.float32, pin_memory=True)
+    vp = lambda a: C.c_void_p(a)
+    cases = [
+        (host.ctypes.data, dev.data_ptr(), out.data_ptr(), b"d_A"),
+        (dev.data_ptr(), pinned.data_ptr(), out.data_ptr(), b"d_B"),
+        (dev.data_ptr(), dev.data_ptr(), host.ctypes.data, b"d_out"),
+        (dev.data_ptr() + 4, dev.data_ptr(), out.data_ptr(), b"aligned"),
+        (dev.data_ptr(), dev.data_ptr(), out.data_ptr() + 4, b"aligned"),
+    ]
+    for a, b, o, what in cases:
+        rc = L.esr_rel_change_noalloc(vp(a), vp(b), 16, 0, vp(o), None)
+        assert rc == F.ESR_ERR_ARG, (what, rc)
+        assert what in L.esr_last_error(), L.esr_last_error()
+    torch.cuda.synchronize()
+    assert float(out.abs().sum().item()) == 0.0      # nothing was launched
