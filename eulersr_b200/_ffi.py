@@ -24,6 +24,7 @@ RECON = {"muscl": 0, "second_order": 0, "2nd_order": 0, "constant": 1, "first_or
 TIME = {"SRK2": 0, "SSP_RK2": 0, "EE": 1, "RK2": 2}
 DT_MODE = {"global": 0, "local": 1}
 STOP_RULE = {"reference": 0, "density_l2": 1, "engineering": 2}
+FIDELITY = {"fast": 0, "reference": 1}
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
@@ -48,7 +49,7 @@ class Params(C.Structure):
                 ("time_scheme", C.c_int32), ("dt_mode", C.c_int32), ("stop_rule", C.c_int32),
                 ("gamma", C.c_double), ("threshold", C.c_double), ("check_every", C.c_int32),
                 ("patience", C.c_int32), ("device", C.c_int32), ("use_graphs", C.c_int32),
-                ("block_size", C.c_int32), ("reserved", C.c_int32)]
+                ("block_size", C.c_int32), ("fidelity", C.c_int32)]
 
 
 class Case(C.Structure):
@@ -107,6 +108,7 @@ _SIGS = {
     "esr_mesh_destroy": (C.c_int, [C.c_void_p]),
     "esr_mesh_get_info": (C.c_int, [C.c_void_p, C.POINTER(MeshInfo)]),
     "esr_mesh_get_permutation": (C.c_int, [C.c_void_p, _i32p]),
+    "esr_mesh_get_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_solver_create": (C.c_int, [C.POINTER(C.c_void_p), _i32p, C.c_int32, C.POINTER(Params), C.POINTER(C.c_void_p)]),
     "esr_solver_destroy": (C.c_int, [C.c_void_p]),
     "esr_solver_num_slots": (C.c_int, [C.c_void_p, _i32p]),

@@ -47,6 +47,7 @@ struct Seg {                 // one mesh and its B case slots
   const T* wall_nx;          // owner's outward unit normal
   const T* wall_ny;
   const T* wall_ds;          // face length
+  const LsqRef* lsq;         // per-cell least-squares data (reference-fidelity float32 only)
   int n_wall;
   int b_shift;               // item / B = (umulhi(item, b_magic) + item) >> b_shift
   unsigned b_magic;
@@ -84,13 +85,17 @@ __device__ __forceinline__ void block_origin(const BlockMap<T>& bm, Seg<T>& s, i
   }
 }
 
-// Precision policy. float64 kernels keep IEEE division and the reference's
-// exact operation sequence (the faithful twin). float32 kernels use the
-// approximate divide (div.approx, <= 2 ulp) and reciprocal-multiplies; their
-// results stay within the float32 parity tolerance of the oracle.
-template <typename T> __device__ __forceinline__ T dv(T a, T b) { return a / b; }
-template <> __device__ __forceinline__ float dv<float>(float a, float b) { return __fdividef(a, b); }
-template <typename T> constexpr bool kFast = sizeof(T) == 4;
+// Precision policy. FAST = false keeps IEEE division and the reference's
+// exact operation sequence: every float64 kernel, and the float32 kernels of
+// the reference-fidelity mode (compiled without FMA contraction in their own
+// translation unit, esr_faithful.cu). FAST float32 kernels (the default) use
+// the approximate divide (div.approx, <= 2 ulp) and reciprocal-multiplies.
+template <typename T, bool FAST> constexpr bool kFastPath = FAST && sizeof(T) == 4;
+template <typename T, bool FAST = (sizeof(T) == 4)>
+__device__ __forceinline__ T dv(T a, T b) {
+  if constexpr (kFastPath<T, FAST>) return __fdividef(a, b);
+  else return a / b;
+}
 
 // Resident 256-thread blocks per SM the float32 cell kernels are compiled for
 // (register caps 65536 / (256 x n)); float64 kernels take what they need.
@@ -101,7 +106,7 @@ template <typename T> constexpr bool kFast = sizeof(T) == 4;
 #define ESR_K1_MINB_LOCAL 4
 #endif
 #ifndef ESR_K2_MINB
-#define ESR_K2_MINB 4   // 5 is 9 % faster but rounds float32 to 1.04e-5 of the oracle's float32 on the diamond test
+#define ESR_K2_MINB 5   // 48 registers: 7-9 % faster than 4 blocks (62 registers), no spills
 #endif
 
 template <typename T>
@@ -126,11 +131,11 @@ struct Cases {               // per global slot
 
 // ----------------------------------------------------------- conversions
 // helper.py:37-46 getPrimitive (M = 1)
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ void prim(const V4<T>& W, T gm1, T half, T P[4]) {
   T r = W.x;
   T u, v;
-  if constexpr (kFast<T>) {
+  if constexpr (kFastPath<T, FAST>) {
     const T ri = __fdividef(1.0f, r);
     u = W.y * ri;
     v = W.z * ri;
@@ -142,50 +147,50 @@ __device__ __forceinline__ void prim(const V4<T>& W, T gm1, T half, T P[4]) {
   P[3] = (W.w - half * r * (u * u + v * v)) * gm1;
 }
 // helper.py:25-35 getConserved (M = 1)
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ V4<T> cons(const T P[4], T gm1, T inv_gm1, T half) {
   T r = P[0], u = P[1], v = P[2];
-  const T e = kFast<T> ? P[3] * inv_gm1 : P[3] / gm1;
+  const T e = kFastPath<T, FAST> ? P[3] * inv_gm1 : P[3] / gm1;
   return mk4<T>(r, r * u, r * v, e + half * r * (u * u + v * v));
 }
 
 // helper.py:196-204 slip wall ghost (gamma 1.4, background value 0)
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ V4<T> wall_ghost(const V4<T>& Wc, T nx, T ny, const Consts<T>& k) {
   T P[4];
-  prim<T>(Wc, k.gm1_14, k.half, P);
+  prim<T, FAST>(Wc, k.gm1_14, k.half, P);
   T vn = P[1] * nx + P[2] * ny;
   T Q[4] = {P[0], P[1] - T(2) * vn * nx, P[2] - T(2) * vn * ny, P[3]};
-  return cons<T>(Q, k.gm1_14, k.inv_gm1_14, k.half);
+  return cons<T, FAST>(Q, k.gm1_14, k.inv_gm1_14, k.half);
 }
 // helper.py:179-194 subsonic inlet ghost: rho,u,v imposed, p from the cell (gamma 1.4)
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ V4<T> subsonic_ghost(const V4<T>& Wc, const Consts<T>& k) {
   T P[4];
-  prim<T>(Wc, k.gm1_14, k.half, P);
+  prim<T, FAST>(Wc, k.gm1_14, k.half, P);
   T Q[4] = {k.sub_rho, k.sub_u, k.sub_v, P[3]};
-  return cons<T>(Q, k.gm1_14, k.inv_gm1_14, k.half);
+  return cons<T, FAST>(Q, k.gm1_14, k.inv_gm1_14, k.half);
 }
 // helper.py:233-256 BC_state for one boundary slot (conserved ghost)
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ V4<T> ghost_cons(int kind, const V4<T>& Wc, T nx, T ny, const V4<T>& inlet,
                                             const Consts<T>& k) {
-  if (kind == K_WALL) return wall_ghost<T>(Wc, nx, ny, k);
+  if (kind == K_WALL) return wall_ghost<T, FAST>(Wc, nx, ny, k);
   if (kind == K_INLET) return inlet;
-  if (kind == K_SUBSONIC) return subsonic_ghost<T>(Wc, k);
+  if (kind == K_SUBSONIC) return subsonic_ghost<T, FAST>(Wc, k);
   return Wc;  // outlet
 }
 
 // euler_solver.py:36-39 Venkatakrishnan with K = 0
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ T venkat(T a, T b, T eps) {
-  return dv<T>(a * a + T(2) * a * b, a * a + T(2) * b * b + a * b + eps);
+  return dv<T, FAST>(a * a + T(2) * a * b, a * a + T(2) * b * b + a * b + eps);
 }
 
 // ------------------------------------------------------------------ fluxes
 // euler_solver.py:376-420 getFlux with the HLLC dissipation of :273-374;
 // returns Fc - (Fc - F_HLLC) exactly as the reference assembles it.
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
                                      T nx, T ny, const Consts<T>& k, T F[4]) {
   const T rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
@@ -195,8 +200,8 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const T tx = -ny, ty = nx;
   const T utL = uL * tx + vL * ty;
   const T utR = uR * tx + vR * ty;
-  const T aL = sqrt(fabs(dv<T>(k.gamma * pL, rL)));
-  const T aR = sqrt(fabs(dv<T>(k.gamma * pR, rR)));
+  const T aL = sqrt(fabs(dv<T, FAST>(k.gamma * pL, rL)));
+  const T aR = sqrt(fabs(dv<T, FAST>(k.gamma * pR, rR)));
   T SL = fmin(unL - aL, unR - aR);
   T SR = fmax(unL + aL, unR + aR);
   if (SL == SR) SL = SL - k.ss_eps;
@@ -204,7 +209,7 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const T EL = WL.w, ER = WR.w;
   T den = rL * (SL - unL) - rR * (SR - unR);
   if (den == T(0)) den = k.den_eps;
-  const T Ss = dv<T>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
+  const T Ss = dv<T, FAST>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
   const T PsL = pL + rL * (SL - unL) * (Ss - unL);
   const T PsR = pR + rR * (SR - unR) * (Ss - unR);
   const T Ps = k.half * (PsL + PsR);
@@ -215,7 +220,7 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   const bool left = c1 || c2;
   const T rK = left ? rL : rR, unK = left ? unL : unR, SK = left ? SL : SR;
   const T EK = left ? EL : ER, pK = left ? pL : pR, utK = left ? utL : utR;
-  if constexpr (kFast<T>) {
+  if constexpr (kFastPath<T, FAST>) {
     // float32: the HLLC flux itself (the central-flux identity F = Fc - (Fc - H)
     // is exact in real arithmetic) and only the physical flux of the selected side
     const T uK = left ? uL : uR, vK = left ? vL : vR;
@@ -297,15 +302,15 @@ __device__ __forceinline__ void hllc_fast(const T PL[4], const T PR[4], T nx, T 
 }
 
 // euler_solver.py:203-240 Rusanov (plain branch) inside getFlux
-template <typename T>
+template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
                                         T nx, T ny, const Consts<T>& k, T F[4]) {
   const T unL = PL[1] * nx + PL[2] * ny;
   const T unR = PR[1] * nx + PR[2] * ny;
   const T FL0 = PL[0] * unL, FL1 = PL[0] * PL[1] * unL + PL[3] * nx, FL2 = PL[0] * PL[2] * unL + PL[3] * ny, FL3 = (WL.w + PL[3]) * unL;
   const T FR0 = PR[0] * unR, FR1 = PR[0] * PR[1] * unR + PR[3] * nx, FR2 = PR[0] * PR[2] * unR + PR[3] * ny, FR3 = (WR.w + PR[3]) * unR;
-  const T CL = sqrt(fabs(dv<T>(k.gamma * PL[3], PL[0]))) + fabs(unL);
-  const T CR = sqrt(fabs(dv<T>(k.gamma * PR[3], PR[0]))) + fabs(unR);
+  const T CL = sqrt(fabs(dv<T, FAST>(k.gamma * PL[3], PL[0]))) + fabs(unL);
+  const T CR = sqrt(fabs(dv<T, FAST>(k.gamma * PR[3], PR[0]))) + fabs(unR);
   const T C = fmax(CR, CL);
   F[0] = k.half * (FL0 + FR0) - k.half * C * (WR.x - WL.x);
   F[1] = k.half * (FL1 + FR1) - k.half * C * (WR.y - WL.y);
@@ -334,8 +339,8 @@ __device__ __forceinline__ void geo_groups(const Seg<T>& s, int c, int g0, T out
 // own MUSCL face states (euler_solver.py:69-98). Writes FV[k][item] (primitive).
 // With LOCALDT it also writes the per-cell CFL time step of the state.
 // MUSCL=false only computes the local dt (constant reconstruction needs no face states).
-template <typename T, bool MUSCL, bool LOCALDT>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_LOCAL : ESR_K1_MINB) : 1) k_recon(const BlockMap<T> bm,
+template <typename T, bool FAST, bool MUSCL, bool LOCALDT>
+__global__ void __launch_bounds__(256, kFastPath<T, FAST> ? (LOCALDT ? ESR_K1_MINB_LOCAL : ESR_K1_MINB) : 1) k_recon(const BlockMap<T> bm,
                                                const V4<T>* __restrict__ W, V4<T>* __restrict__ FV,
                                                long long total, Cases<T> cs, Consts<T> kc, int pos,
                                                T* __restrict__ dt_local) {
@@ -351,7 +356,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
   const long long gi = s.off + item;
   const V4<T> Wc = W[gi];
   T Pc[4];
-  prim<T>(Wc, kc.gm1, kc.half, Pc);
+  prim<T, FAST>(Wc, kc.gm1, kc.half, Pc);
   if (LOCALDT) {
     T gn[12];
     geo_groups<T, 3>(s, c, 0, gn);
@@ -375,19 +380,43 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
     const int kind = slot_kind(nb.w, k);
     V4<T> Wk;
     if (kind == K_INTERIOR) Wk = W[s.off + (long long)nbk[k] * s.B + b];
-    else Wk = ghost_cons<T>(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc);
-    prim<T>(Wk, kc.gm1, kc.half, Pk[k]);
+    else Wk = ghost_cons<T, FAST>(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc);
+    prim<T, FAST>(Wk, kc.gm1, kc.half, Pk[k]);
   }
   T gx[4], gy[4];
   T gc[12];   // LSQ coefficients and face offsets (groups 3-5)
   geo_groups<T, 3>(s, c, 3, gc);
-  const T c0x = gc[G_C0X - 12], c0y = gc[G_C0Y - 12], c1x = gc[G_C1X - 12], c1y = gc[G_C1Y - 12];
-  const T c2x = gc[G_C2X - 12], c2y = gc[G_C2Y - 12];
+  if constexpr (!FAST && sizeof(T) == 4) {
+    // helper.py:136-153 per call, in the reference's float32 rounding:
+    // b = sum_k (w_k dW_k) dx_k summed k = 0, 1, 2 in turn, then the 2x2
+    // solve with partial pivoting in float64 rounded to float32 (what
+    // numpy.linalg.solve computes for float32 operands)
+    const LsqRef L = s.lsq[c];
+    const double a00 = L.a[0], a01 = L.a[1], a10 = L.a[2], a11 = L.a[3];
+    const bool sw = fabs(a10) > fabs(a00);
+    const double p00 = sw ? a10 : a00, p01 = sw ? a11 : a01, p10 = sw ? a00 : a10, p11 = sw ? a01 : a11;
+    const double l = p10 * (1.0 / p00), u11 = p11 - l * p01;
 #pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
-    gx[v] = c0x * d0 + c1x * d1 + c2x * d2;
-    gy[v] = c0y * d0 + c1y * d1 + c2y * d2;
+    for (int v = 0; v < 4; ++v) {
+      const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
+      const T x0 = L.w[0] * d0, x1 = L.w[1] * d1, x2 = L.w[2] * d2;
+      const T bx = (x0 * L.dx[0] + x1 * L.dx[2]) + x2 * L.dx[4];
+      const T by = (x0 * L.dx[1] + x1 * L.dx[3]) + x2 * L.dx[5];
+      const double q0 = sw ? by : bx, q1 = sw ? bx : by;
+      const double s1 = (q1 - l * q0) / u11;
+      const double s0 = (q0 - p01 * s1) / p00;
+      gx[v] = (T)s0;
+      gy[v] = (T)s1;
+    }
+  } else {
+    const T c0x = gc[G_C0X - 12], c0y = gc[G_C0Y - 12], c1x = gc[G_C1X - 12], c1y = gc[G_C1Y - 12];
+    const T c2x = gc[G_C2X - 12], c2y = gc[G_C2Y - 12];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const T d0 = Pk[0][v] - Pc[v], d1 = Pk[1][v] - Pc[v], d2 = Pk[2][v] - Pc[v];
+      gx[v] = c0x * d0 + c1x * d1 + c2x * d2;
+      gy[v] = c0y * d0 + c1y * d1 + c2y * d2;
+    }
   }
   const T fx[3] = {gc[G_F0X - 12], gc[G_F1X - 12], gc[G_F2X - 12]};
   const T fy[3] = {gc[G_F0Y - 12], gc[G_F1Y - 12], gc[G_F2Y - 12]};
@@ -403,8 +432,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LOCALDT ? ESR_K1_MINB_L
       const T d = fx[k] * gx[v] + fy[k] * gy[v];
       D[k][v] = d;
       T p = T(1);
-      if (d > kc.eps_lim) p = venkat<T>(mx - Pc[v], d, kc.venk_eps);
-      else if (d < -kc.eps_lim) p = venkat<T>(mn - Pc[v], d, kc.venk_eps);
+      if (d > kc.eps_lim) p = venkat<T, FAST>(mx - Pc[v], d, kc.venk_eps);
+      else if (d < -kc.eps_lim) p = venkat<T, FAST>(mn - Pc[v], d, kc.venk_eps);
       ph = (k == 0) ? p : fmin(ph, p);
     }
     phi[v] = ph;
@@ -461,8 +490,8 @@ enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
 
 // euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
 // then the stage update of :630-653.
-template <typename T, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(const BlockMap<T> bm,
+template <typename T, bool FAST, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
+__global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_flux(const BlockMap<T> bm,
                                               const V4<T>* __restrict__ Win, const V4<T>* __restrict__ Wbase,
                                               V4<T>* __restrict__ Wout, const V4<T>* __restrict__ FV,
                                               long long total, Cases<T> cs, Consts<T> kc, int pos,
@@ -498,36 +527,36 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
         const V4<T> fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)nbk[k] * s.B + b];
         qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
       } else {
-        prim<T>(ghost_cons<T>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+        prim<T, FAST>(ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
       }
-      if constexpr (kFast<T>) {
+      if constexpr (kFastPath<T, FAST>) {
         // float32: the face primitives are used as reconstructed (the
         // reference converts them to conserved and back, a rounding-level
         // step); HLLC forms the conserved state of the selected side itself
 #pragma unroll
         for (int v = 0; v < 4; ++v) { PL[v] = qL[v]; PR[v] = qR[v]; }
         if (FLUX != 0) {
-          WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
-          WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
+          WL = cons<T, FAST>(qL, kc.gm1, kc.inv_gm1, kc.half);
+          WR = cons<T, FAST>(qR, kc.gm1, kc.inv_gm1, kc.half);
         }
       } else {
-        WL = cons<T>(qL, kc.gm1, kc.inv_gm1, kc.half);
-        WR = cons<T>(qR, kc.gm1, kc.inv_gm1, kc.half);
-        prim<T>(WL, kc.gm1, kc.half, PL);
-        prim<T>(WR, kc.gm1, kc.half, PR);
+        WL = cons<T, FAST>(qL, kc.gm1, kc.inv_gm1, kc.half);
+        WR = cons<T, FAST>(qR, kc.gm1, kc.inv_gm1, kc.half);
+        prim<T, FAST>(WL, kc.gm1, kc.half, PL);
+        prim<T, FAST>(WR, kc.gm1, kc.half, PR);
       }
     } else {
       WL = Wc;
-      WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T>(kind, Wc, nx, ny, inlet, kc);
-      prim<T>(WL, kc.gm1, kc.half, PL);
-      prim<T>(WR, kc.gm1, kc.half, PR);
+      WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc);
+      prim<T, FAST>(WL, kc.gm1, kc.half, PL);
+      prim<T, FAST>(WR, kc.gm1, kc.half, PR);
     }
     T F[4];
     if (FLUX == 0) {
-      if constexpr (kFast<T> && MUSCL) hllc_fast<T>(PL, PR, nx, ny, kc, F);
-      else hllc<T>(WL, PL, WR, PR, nx, ny, kc, F);
+      if constexpr (kFastPath<T, FAST> && MUSCL) hllc_fast<T>(PL, PR, nx, ny, kc, F);
+      else hllc<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
     } else {
-      rusanov<T>(WL, PL, WR, PR, nx, ny, kc, F);
+      rusanov<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
     }
     const T sk = gk[G_S0 + k];
     if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
@@ -535,10 +564,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? ESR_K2_MINB : 1) k_flux(
   }
   const T area = gk[G_AREA];
   const T sig = cs.strength[g] * gk[G_BLEND3];
-  const T R0 = dv<T>(acc[0], area) - sig * (inlet.x - Wc.x);
-  const T R1 = dv<T>(acc[1], area) - sig * (inlet.y - Wc.y);
-  const T R2 = dv<T>(acc[2], area) - sig * (inlet.z - Wc.z);
-  const T R3 = dv<T>(acc[3], area) - sig * (inlet.w - Wc.w);
+  const T R0 = dv<T, FAST>(acc[0], area) - sig * (inlet.x - Wc.x);
+  const T R1 = dv<T, FAST>(acc[1], area) - sig * (inlet.y - Wc.y);
+  const T R2 = dv<T, FAST>(acc[2], area) - sig * (inlet.z - Wc.z);
+  const T R3 = dv<T, FAST>(acc[3], area) - sig * (inlet.w - Wc.w);
   const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
   // density residual of the state the step starts from (density-L2 stop rule)
   if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
@@ -585,7 +614,7 @@ struct CaseMap {             // global slot -> (segment, slot)
 // (euler/main.py:150-152); RED_DTMIN: min_i area/sum_k (c+|u.n|) s
 // (helper.py:8-18); RED_ENTROPY: sum rho log(p/rho^g) area/(g-1)
 // (helper.py:48-55,312-315); RED_DIFF: sum |A - B|^2, sum |B|^2 (probe).
-template <typename T, int OP>
+template <typename T, int OP, bool FAST = (sizeof(T) == 4)>
 __global__ void __launch_bounds__(256) k_case_reduce(const Seg<T>* __restrict__ segs, CaseMap cm,
                                                      const V4<T>* __restrict__ W, V4<T>* __restrict__ Wref,
                                                      const int* __restrict__ due, int chunk_cells,
@@ -611,7 +640,7 @@ __global__ void __launch_bounds__(256) k_case_reduce(const Seg<T>* __restrict__ 
       if (OP == RED_NORM) Wref[gi] = w;
     } else if (OP == RED_DTMIN) {
       T P[4];
-      prim<T>(w, kc.gm1, kc.half, P);
+      prim<T, FAST>(w, kc.gm1, kc.half, P);
       const T cel = sqrt(fabs(kc.gamma * P[3] / P[0]));
       T lam = T(0);
 #pragma unroll

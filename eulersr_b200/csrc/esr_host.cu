@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "esr_device.cuh"
+#include "esr_faithful.h"
 #include "esr_internal.h"
 
 namespace {
@@ -92,6 +93,7 @@ struct SolverT : SolverBase {
     DevBuf<int4> nbr;
     DevBuf<int> wall_cell;
     DevBuf<T> wall_nx, wall_ny, wall_ds;
+    DevBuf<LsqRef> lsq;  // reference-fidelity float32: per-call least-squares data
     DevBuf<int> inv;  // caller cell -> solver cell
     int B = 0, case0 = 0;
     long long off = 0;
@@ -176,6 +178,9 @@ struct SolverT : SolverBase {
   CaseMap cmap() { return CaseMap{d_case_seg.p, d_case_slot.p}; }
   Seg<T> hseg0{};   // host copy of the first segment (one-mesh block map)
   BlockMap<T> bmap() { return BlockMap<T>{d_segs.p, d_blk.p, hseg0, meshes.size() == 1 ? 1 : 0}; }
+  // float32 with esr_params.fidelity = ESR_FIDELITY_REFERENCE: the kernels of esr_faithful.cu
+  bool faithful() const { return sizeof(T) == 4 && P.fidelity == ESR_FIDELITY_REFERENCE; }
+  static constexpr bool kF = sizeof(T) == 4;   // FAST flag of the kernels this file instantiates
 
   int init(const esr_mesh* const* ms, const int32_t* slots, int nm, const esr_params* p) {
     P = *p;
@@ -236,15 +241,27 @@ struct SolverT : SolverBase {
       MeshDev& md = *meshes[m];
       const HostMesh& hm = *md.hm;
       const int N = hm.n_cells;
+      // geometry records: float64 rounded once (fast), or formed as the
+      // reference forms them in the run's precision (reference fidelity)
+      const bool ref = P.fidelity == ESR_FIDELITY_REFERENCE;
       std::vector<T> g(hm.geo.size());
-      for (size_t i = 0; i < g.size(); ++i) g[i] = (T)hm.geo[i];
+      for (size_t i = 0; i < g.size(); ++i)
+        g[i] = ref ? (sizeof(T) == 4 ? (T)hm.geo_ref32[i] : (T)hm.geo_ref64[i]) : (T)hm.geo[i];
       ESR_TRY(md.geo.alloc(g.size()));
       ESR_CUDA(cudaMemcpy(md.geo.p, g.data(), g.size() * sizeof(T), cudaMemcpyHostToDevice));
+      if (faithful()) {
+        ESR_TRY(md.lsq.alloc(N));
+        ESR_CUDA(cudaMemcpy(md.lsq.p, hm.lsq_ref32.data(), (size_t)N * sizeof(LsqRef), cudaMemcpyHostToDevice));
+      }
       ESR_TRY(md.nbr.alloc(N));
       ESR_CUDA(cudaMemcpy(md.nbr.p, hm.nbr.data(), (size_t)N * sizeof(int4), cudaMemcpyHostToDevice));
       const int nw = (int)hm.wall_cell.size();
       std::vector<T> wx(nw), wy(nw), wd(nw);
-      for (int i = 0; i < nw; ++i) { wx[i] = (T)hm.wall_n[2 * i]; wy[i] = (T)hm.wall_n[2 * i + 1]; wd[i] = (T)hm.wall_ds[i]; }
+      for (int i = 0; i < nw; ++i) {
+        if (!ref) { wx[i] = (T)hm.wall_n[2 * i]; wy[i] = (T)hm.wall_n[2 * i + 1]; wd[i] = (T)hm.wall_ds[i]; }
+        else if (sizeof(T) == 4) { wx[i] = (T)hm.wall_n_ref32[2 * i]; wy[i] = (T)hm.wall_n_ref32[2 * i + 1]; wd[i] = (T)hm.wall_ds_ref32[i]; }
+        else { wx[i] = (T)hm.wall_n_ref64[2 * i]; wy[i] = (T)hm.wall_n_ref64[2 * i + 1]; wd[i] = (T)hm.wall_ds_ref64[i]; }
+      }
       ESR_TRY(md.wall_cell.alloc(std::max(nw, 1)));
       ESR_TRY(md.wall_nx.alloc(std::max(nw, 1)));
       ESR_TRY(md.wall_ny.alloc(std::max(nw, 1)));
@@ -261,6 +278,7 @@ struct SolverT : SolverBase {
       s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = G_COUNT; s.off = md.off;
       s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
       s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
+      s.lsq = md.lsq.p;
       ESR_TRY(set_divider(s));
       hsegs.push_back(s);
       for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
@@ -413,8 +431,8 @@ struct SolverT : SolverBase {
   template <int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
   void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
     tap_begin(1);
-    k_flux<T, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(bmap(), win, wbase, wout, FV.p,
-                                                                        total, cs, kc, pos, dt_local.p, res.p);
+    k_flux<T, kF, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(bmap(), win, wbase, wout, FV.p,
+                                                                            total, cs, kc, pos, dt_local.p, res.p);
     tap_end();
     ++launches;
   }
@@ -423,24 +441,55 @@ struct SolverT : SolverBase {
     const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
     const bool local = P.dt_mode == ESR_DT_LOCAL;
     const bool rus = P.flux == ESR_FLUX_RUSANOV;
+    if constexpr (sizeof(T) == 4) {
+      if (faithful()) {
+        tap_begin(1);
+        faithful_flux(STAGE, bmap(), win, wbase, wout, FV.p, total, cs, kc, pos, dt_local.p, res.p, rus, muscl, local,
+                      n_blk, block, stream);
+        tap_end();
+        ++launches;
+        return;
+      }
+    }
 #define ESR_FLUX_CASE(F, M, L) if (rus == (F == 1) && muscl == M && local == L) { launch_flux<F, M, STAGE, L>(win, wbase, wout, cs, pos); return; }
     ESR_FLUX_CASE(0, true, false) ESR_FLUX_CASE(0, true, true) ESR_FLUX_CASE(0, false, false) ESR_FLUX_CASE(0, false, true)
     ESR_FLUX_CASE(1, true, false) ESR_FLUX_CASE(1, true, true) ESR_FLUX_CASE(1, false, false) ESR_FLUX_CASE(1, false, true)
 #undef ESR_FLUX_CASE
   }
   void recon(const V* w, const Cases<T>& cs, int pos, bool write_dt) {
-    if (P.reconstruction != ESR_RECON_MUSCL) {
-      if (write_dt) {  // constant reconstruction still needs the local dt
-        k_recon<T, false, true><<<n_blk, block, 0, stream>>>(bmap(), w, nullptr, 0, cs, kc, pos, dt_local.p);
+    const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
+    if (!muscl && !write_dt) return;   // constant reconstruction needs K1 only for the local dt
+    if constexpr (sizeof(T) == 4) {
+      if (faithful()) {
+        tap_begin(0);
+        faithful_recon(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p, muscl, write_dt, n_blk, block, stream);
+        tap_end();
         ++launches;
+        return;
       }
+    }
+    if (!muscl) {
+      k_recon<T, kF, false, true><<<n_blk, block, 0, stream>>>(bmap(), w, nullptr, 0, cs, kc, pos, dt_local.p);
+      ++launches;
       return;
     }
     tap_begin(0);
-    if (write_dt) k_recon<T, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
-    else k_recon<T, true, false><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    if (write_dt) k_recon<T, kF, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    else k_recon<T, kF, true, false><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
     tap_end();
     ++launches;
+  }
+  // per-case minimum CFL step partials of the slots flagged in `flags`
+  void dtmin_reduce(const int* flags) {
+    dim3 grid(n_chunks, n_slots);
+    if constexpr (sizeof(T) == 4) {
+      if (faithful()) {
+        faithful_dtmin(grid, kReduceThreads, d_segs.p, cmap(), W.p, flags, kReduceCells, partial.p, n_chunks, kc, stream);
+        return;
+      }
+    }
+    k_case_reduce<T, RED_DTMIN><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, flags,
+                                                                     kReduceCells, partial.p, n_chunks, kc);
   }
   // one time step of every live slot, step index `pos` inside the chunk
   void step_kernels(const Cases<T>& cs, int pos) {
@@ -674,9 +723,7 @@ struct SolverT : SolverBase {
   }
   // dt + N for every slot flagged in `fill` (one reduction launch for all)
   int finish_fill() {
-    dim3 grid(n_chunks, n_slots);
-    k_case_reduce<T, RED_DTMIN><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, fill.p, kReduceCells,
-                                                                     partial.p, n_chunks, kc);
+    dtmin_reduce(fill.p);
     const int tb = 128, nb = (n_slots + tb - 1) / tb;
     k_dt_finish<T><<<nb, tb, 0, stream>>>(fill.p, n_slots, partial.p, n_chunks, cfl.p, tf.p, max_steps.p, dt.p, ctl(),
                                           P.dt_mode == ESR_DT_LOCAL);
@@ -1080,9 +1127,7 @@ struct SolverT : SolverBase {
     if (with_states) k_retire_states<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), q, W.p, inv_ptrs.p);
     k_assign<T><<<(int)(meshes.size() + 31) / 32, 32, 0, stream>>>(d_segs.p, (int)meshes.size(), q, sp, ctl(), fill.p);
     k_fill_slots<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), q, fill.p, perm_ptrs.p, W.p, Wref.p);
-    dim3 grid(n_chunks, n_slots);
-    k_case_reduce<T, RED_DTMIN><<<grid, kReduceThreads, 0, stream>>>(d_segs.p, cmap(), W.p, nullptr, fill.p, kReduceCells,
-                                                                     partial.p, n_chunks, kc);
+    dtmin_reduce(fill.p);
     k_dt_finish<T><<<nb, tb, 0, stream>>>(fill.p, n_slots, partial.p, n_chunks, cfl.p, tf.p, max_steps.p, dt.p, ctl(),
                                           P.dt_mode == ESR_DT_LOCAL);
     k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, fill.p, eng_track.p);
@@ -1443,6 +1488,31 @@ int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm) {
   return ESR_OK;
 }
 
+int esr_mesh_get_geometry(const esr_mesh* mesh, int32_t fidelity, int32_t precision, double* geo, double* lsq) {
+  if (!mesh || !geo) return fail(ESR_ERR_ARG, "mesh_get_geometry: null argument");
+  if (fidelity != ESR_FIDELITY_FAST && fidelity != ESR_FIDELITY_REFERENCE) return fail(ESR_ERR_ARG, "unknown fidelity");
+  if (precision != ESR_PREC_F32 && precision != ESR_PREC_F64) return fail(ESR_ERR_ARG, "unknown precision");
+  const HostMesh& hm = mesh->hm;
+  const bool ref = fidelity == ESR_FIDELITY_REFERENCE;
+  for (int c = 0; c < hm.n_cells; ++c) {
+    const size_t i = (size_t)hm.inv[c] * G_COUNT;
+    for (int f = 0; f < G_COUNT; ++f) {
+      double v;
+      if (!ref) v = precision == ESR_PREC_F32 ? (double)(float)hm.geo[i + f] : hm.geo[i + f];
+      else v = precision == ESR_PREC_F32 ? (double)hm.geo_ref32[i + f] : hm.geo_ref64[i + f];
+      geo[(size_t)c * G_COUNT + f] = v;
+    }
+    if (lsq && ref && precision == ESR_PREC_F32) {
+      const LsqRef& L = hm.lsq_ref32[hm.inv[c]];
+      double* o = lsq + (size_t)c * 13;
+      for (int k = 0; k < 3; ++k) o[k] = L.w[k];
+      for (int k = 0; k < 6; ++k) o[3 + k] = L.dx[k];
+      for (int k = 0; k < 4; ++k) o[9 + k] = L.a[k];
+    }
+  }
+  return ESR_OK;
+}
+
 int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_mesh, int32_t n_meshes,
                       const esr_params* params, esr_solver** out) {
   ESR_GUARD_BEGIN
@@ -1460,6 +1530,7 @@ int esr_solver_create(const esr_mesh* const* meshes, const int32_t* slots_per_me
   if (p.stop_rule != ESR_STOP_REFERENCE && p.stop_rule != ESR_STOP_DENSITY_L2 && p.stop_rule != ESR_STOP_ENGINEERING)
     return fail(ESR_ERR_ARG, "unknown stop rule");
   if (!(p.gamma > 1.0)) return fail(ESR_ERR_ARG, "gamma must be > 1");
+  if (p.fidelity != ESR_FIDELITY_FAST && p.fidelity != ESR_FIDELITY_REFERENCE) return fail(ESR_ERR_ARG, "unknown fidelity");
   auto s = std::make_unique<esr_solver>();
   s->precision = p.precision;
   int rc;

@@ -14,6 +14,15 @@ struct HostMesh {
   std::vector<int> perm;          // new -> old
   std::vector<int> inv;           // old -> new
   std::vector<double> geo;        // n_cells records of G_COUNT values, renumbered
+  // The same records formed as the reference forms them on every call, in
+  // its operation order, from the points rounded to the run's precision
+  // (esr_params.fidelity = ESR_FIDELITY_REFERENCE); float32 adds the
+  // per-call least-squares data.
+  std::vector<float> geo_ref32;
+  std::vector<LsqRef> lsq_ref32;
+  std::vector<double> geo_ref64;
+  std::vector<float> wall_n_ref32, wall_ds_ref32;
+  std::vector<double> wall_n_ref64, wall_ds_ref64;
   std::vector<int> nbr;           // 4 x n_cells (x,y,z neighbours, w packed)
   std::vector<int> wall_cell;     // renumbered owner cell of each force face
   std::vector<double> wall_n;     // (nx, ny) per force face

@@ -17,6 +17,19 @@ enum GeoField {
 };
 static_assert(G_COUNT == 24, "geometry groups of 4");
 
+// Per-cell least-squares data of the reference-fidelity float32 path, which
+// forms the gradient per call as helper.py:136-153 does: offsets dx_k
+// (neighbour barycentre or twice the face offset), weights 1/|dx_k|^2 and the
+// 2x2 matrix A = sum_k w_k dx_k dx_k^T, all rounded as the reference's
+// float32 arithmetic rounds them.
+struct LsqRef {
+  float w[3];
+  float dx[6];      // dx_k = (dx[2k], dx[2k+1])
+  float a[4];       // a00, a01, a10, a11
+  float pad[3];
+};
+static_assert(sizeof(LsqRef) == 64, "one 64-byte record per cell");
+
 // slot kinds (face markers of euler/jax_fvm/src/mesh.py:47-52)
 enum SlotKind { K_INTERIOR = 0, K_WALL = 2, K_INLET = 3, K_OUTLET = 4, K_SUBSONIC = 5 };
 

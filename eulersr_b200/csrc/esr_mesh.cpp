@@ -65,6 +65,121 @@ std::vector<int> rcm_order(int n, const std::vector<int>& nbr) {
   return order;
 }
 
+// The geometry records as the reference forms them on every call, in its
+// operation order and in precision R (float for a float32 run, whose points
+// are float32 there): barycentre ((p0 + p1) + p2) / 3 and face midpoint
+// (pa + pb) / 2 (jnp.mean), normal (dy, -dx) / sqrt(dx dx + dy dy) and area
+// |0.5 ((y1-y0)(x2-x0) - (x1-x0)(y2-y0))| (mesh.py:223-240), face offsets
+// midpoint - barycentre (euler_solver.py:49,74,79), least-squares offsets
+// (neighbour barycentre - own, or 2 (midpoint - own) on a boundary face),
+// weights 1 / |dx|^2 and A = sum_k (w_k dx_k) dx_k^T summed k = 0, 1, 2 in
+// turn (helper.py:136-150), sponge blend^3 with width 0.2 (y_max - y_min)
+// (helper.py:262-295). The LSQ coefficients of the fast path are derived
+// from these offsets in float64. Requires hm.perm / hm.inv / hm.nbr.
+template <typename R>
+static void reference_geometry(const esr_mesh_desc& d, const std::vector<int>& walls, HostMesh& hm,
+                               std::vector<R>& geo, std::vector<LsqRef>* lsq, std::vector<R>& wall_n,
+                               std::vector<R>& wall_ds) {
+  const int N = d.n_cells, F = d.n_faces, P = d.n_points;
+  std::vector<R> px(P), py(P);
+  for (int p = 0; p < P; ++p) { px[p] = (R)d.points[2 * p]; py[p] = (R)d.points[2 * p + 1]; }
+  std::vector<R> bx(N), by(N), area(N), nrm(6 * N), fmx(F), fmy(F), flen(F);
+  for (int c = 0; c < N; ++c) {
+    const int* t = d.tris + 3 * c;
+    bx[c] = ((px[t[0]] + px[t[1]]) + px[t[2]]) / (R)3;
+    by[c] = ((py[t[0]] + py[t[1]]) + py[t[2]]) / (R)3;
+    const R cr = (py[t[1]] - py[t[0]]) * (px[t[2]] - px[t[0]]) - (px[t[1]] - px[t[0]]) * (py[t[2]] - py[t[0]]);
+    area[c] = std::fabs((R)0.5 * cr);
+    for (int k = 0; k < 3; ++k) {
+      const R dx = px[t[(k + 1) % 3]] - px[t[k]], dy = py[t[(k + 1) % 3]] - py[t[k]];
+      const R ln = std::sqrt(dx * dx + dy * dy);
+      nrm[6 * c + 2 * k] = dy / ln;
+      nrm[6 * c + 2 * k + 1] = (-dx) / ln;
+    }
+  }
+  for (int f = 0; f < F; ++f) {
+    const int a = d.faces[2 * f], b = d.faces[2 * f + 1];
+    fmx[f] = (px[a] + px[b]) / (R)2;
+    fmy[f] = (py[a] + py[b]) / (R)2;
+    const R dx = px[b] - px[a], dy = py[b] - py[a];
+    flen[f] = std::sqrt(dx * dx + dy * dy);
+  }
+  R ymin = py[0], ymax = py[0];
+  for (int p = 1; p < P; ++p) { ymin = std::min(ymin, py[p]); ymax = std::max(ymax, py[p]); }
+  const R Ly = ymax - ymin;
+  const R width = d.sponge_width > 0 ? (R)d.sponge_width : (R)0.2 * Ly;
+  geo.assign((size_t)G_COUNT * N, (R)0);
+  if (lsq) lsq->assign(N, LsqRef{});
+  for (int i = 0; i < N; ++i) {
+    const int c = hm.perm[i];
+    R* g = geo.data() + (size_t)i * G_COUNT;
+    R dxk[3][2], w[3];
+    for (int k = 0; k < 3; ++k) {
+      const int f = d.face_connectivity[3 * c + k];
+      const int j = d.neighbors[3 * c + k];
+      const R ox = fmx[f] - bx[c], oy = fmy[f] - by[c];
+      g[G_F0X + 2 * k] = ox;
+      g[G_F0Y + 2 * k] = oy;
+      g[G_N0X + 2 * k] = nrm[6 * c + 2 * k];
+      g[G_N0Y + 2 * k] = nrm[6 * c + 2 * k + 1];
+      g[G_S0 + k] = flen[f];
+      if (d.face_markers[f] > 0) { dxk[k][0] = (R)2 * ox; dxk[k][1] = (R)2 * oy; }
+      else { dxk[k][0] = bx[j] - bx[c]; dxk[k][1] = by[j] - by[c]; }
+      const R ln = std::sqrt(dxk[k][0] * dxk[k][0] + dxk[k][1] * dxk[k][1]);
+      w[k] = (R)1 / (ln * ln);
+    }
+    // A in the reference's order, then the fast path's c_k = w_k A^-1 dx_k in float64
+    R a[4];
+    for (int r = 0; r < 2; ++r)
+      for (int q = 0; q < 2; ++q) {
+        R acc = (w[0] * dxk[0][r]) * dxk[0][q];
+        acc = acc + (w[1] * dxk[1][r]) * dxk[1][q];
+        acc = acc + (w[2] * dxk[2][r]) * dxk[2][q];
+        a[2 * r + q] = acc;
+      }
+    const double A00 = a[0], A01 = a[1], A10 = a[2], A11 = a[3];
+    const double det = A00 * A11 - A01 * A10;
+    for (int k = 0; k < 3; ++k) {
+      const double wx = (double)w[k] * (double)dxk[k][0], wy = (double)w[k] * (double)dxk[k][1];
+      g[G_C0X + 2 * k] = (R)((A11 * wx - A01 * wy) / det);
+      g[G_C0Y + 2 * k] = (R)((-A10 * wx + A00 * wy) / det);
+    }
+    g[G_AREA] = area[c];
+    R bl = 0;
+    if (d.sponge) {
+      const R y = by[c];
+      const R dist = std::min(y - ymin, ymax - y);
+      bl = std::min((R)1, std::max((R)0, (width - dist) / width));
+      bl = std::pow(bl, (R)3);
+    }
+    g[G_BLEND3] = bl;
+    if (lsq) {
+      LsqRef& L = (*lsq)[i];
+      for (int k = 0; k < 3; ++k) {
+        L.w[k] = (float)w[k];
+        L.dx[2 * k] = (float)dxk[k][0];
+        L.dx[2 * k + 1] = (float)dxk[k][1];
+      }
+      for (int q = 0; q < 4; ++q) L.a[q] = (float)a[q];
+    }
+  }
+  // force faces: the first slot listing each face, as prepare_mesh picks it
+  const int fm = d.force_marker > 0 ? d.force_marker : 2;
+  std::vector<int> first(F, -1);
+  for (int t = 0; t < 3 * N; ++t)
+    if (first[d.face_connectivity[t]] < 0) first[d.face_connectivity[t]] = t;
+  wall_n.clear();
+  wall_ds.clear();
+  for (int f = 0; f < F; ++f) {
+    if (d.face_markers[f] != fm || first[f] < 0) continue;
+    const int c = first[f] / 3, k = first[f] % 3;
+    wall_n.push_back(nrm[6 * c + 2 * k]);
+    wall_n.push_back(nrm[6 * c + 2 * k + 1]);
+    wall_ds.push_back(flen[f]);
+  }
+  (void)walls;
+}
+
 int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err) {
   const int N = d.n_cells, F = d.n_faces, P = d.n_points;
   if (N <= 0 || F <= 0 || P <= 0 || !d.points || !d.tris || !d.neighbors || !d.faces || !d.face_markers ||
@@ -227,6 +342,8 @@ int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err) {
     hm.wall_ds.push_back(flen[f]);
   }
   for (int k = 0; k < 4; ++k) hm.inlet_subsonic[k] = d.inlet_subsonic[k];
+  reference_geometry<float>(d, walls, hm, hm.geo_ref32, &hm.lsq_ref32, hm.wall_n_ref32, hm.wall_ds_ref32);
+  reference_geometry<double>(d, walls, hm, hm.geo_ref64, nullptr, hm.wall_n_ref64, hm.wall_ds_ref64);
   return ESR_OK;
 }
 

@@ -139,6 +139,22 @@ class DeviceMesh:
         F.check(F.lib().esr_mesh_get_permutation(self.handle, F.ptr(perm, C.c_int32)))
         return perm
 
+    def geometry(self, fidelity='fast', precision='f32'):
+        """The per-cell records the kernels read (caller's cell order): a dict
+        of normals (n,3,2), face lengths (n,3), area, blend3, lsq coefficients
+        (n,3,2), face offsets (n,3,2) and, for reference fidelity in float32,
+        the per-call least-squares data w (n,3), dx (n,3,2), A (n,2,2)."""
+        n = self.n_cells
+        geo = np.empty((n, 24), dtype=np.float64)
+        lsq = np.empty((n, 13), dtype=np.float64)
+        F.check(F.lib().esr_mesh_get_geometry(self.handle, F.FIDELITY[fidelity], F.PREC[precision],
+                                              F.ptr(geo, C.c_double), F.ptr(lsq, C.c_double)))
+        out = dict(normals=geo[:, 0:6].reshape(n, 3, 2), surface=geo[:, 6:9], area=geo[:, 9], blend3=geo[:, 10],
+                   lsq_coef=geo[:, 12:18].reshape(n, 3, 2), face_offset=geo[:, 18:24].reshape(n, 3, 2))
+        if fidelity == 'reference' and precision == 'f32':
+            out.update(w=lsq[:, 0:3], dx=lsq[:, 3:9].reshape(n, 3, 2), A=lsq[:, 9:13].reshape(n, 2, 2))
+        return out
+
     def close(self):
         if getattr(self, 'handle', None):
             F.lib().esr_mesh_destroy(self.handle)
@@ -157,7 +173,7 @@ class Solver:
 
     def __init__(self, meshes, slots, precision='f32', flux='hllc', reconstruction='muscl', time_scheme='SRK2',
                  dt_mode='global', stop_rule='reference', gamma=1.4, threshold=1e-6, check_every=25, patience=1,
-                 device=0, use_graphs=True, block_size=0):
+                 device=0, use_graphs=True, block_size=0, fidelity='fast'):
         L = F.lib()
         if isinstance(meshes, (DeviceMesh, Mesh)):
             meshes = [meshes]
@@ -185,6 +201,10 @@ class Solver:
         p.device = int(device)
         p.use_graphs = int(bool(use_graphs))
         p.block_size = int(block_size)
+        try:
+            p.fidelity = F.FIDELITY[str(fidelity).lower()]
+        except KeyError:
+            raise ValueError(f"unknown fidelity '{fidelity}': expected 'fast' or 'reference'") from None
         self.params = p
         self.precision = 'f64' if p.precision == 1 else 'f32'
         self.dtype = np.float64 if p.precision == 1 else np.float32

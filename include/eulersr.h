@@ -80,6 +80,14 @@ extern "C" {
 #define ESR_STOP_DENSITY_L2 1  /* RMS over cells of the density residual */
 #define ESR_STOP_ENGINEERING 2 /* stop when the engineering criterion (force coefficients
                                 * within tolerance of given targets) is confirmed */
+#define ESR_FIDELITY_FAST 0      /* geometry formed in float64 and rounded once; float32 kernels
+                                  * with approximate division and the direct HLLC flux */
+#define ESR_FIDELITY_REFERENCE 1 /* the reference's rounding: geometry formed in the run's
+                                  * precision in its operation order (mesh.py:223-240,
+                                  * euler_solver.py:49,74,79, helper.py:136-150), the
+                                  * least-squares gradient solved per call (helper.py:136-153)
+                                  * and float32 kernels with IEEE division, the central-flux
+                                  * identity and no fused multiply-add */
 
 /* Mesh description; all host arrays are owned by the caller and copied. */
 typedef struct esr_mesh_desc {
@@ -125,7 +133,7 @@ typedef struct esr_params {
     int32_t device;           /* CUDA device ordinal */
     int32_t use_graphs;       /* 1: capture step chunks in CUDA graphs */
     int32_t block_size;       /* threads per block for the cell kernels: 64, 128, 256, or 0 = autotuned */
-    int32_t reserved;
+    int32_t fidelity;         /* ESR_FIDELITY_* (0: fast) */
 } esr_params;
 
 /* One (Mach, alpha) case. inlet = conserved freestream (euler/main.py:39). */
@@ -185,6 +193,15 @@ int esr_mesh_destroy(esr_mesh* mesh);
 int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info);
 /* new-to-old cell permutation chosen by the renumbering (n_cells entries) */
 int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm);
+/* The per-cell geometry the kernels read, in the caller's cell order, for a
+ * fidelity (ESR_FIDELITY_*) and precision (ESR_PREC_*): geo receives
+ * n_cells x 24 values (normals n_kx, n_ky of the three edges, face lengths,
+ * area, sponge blend^3, pad, least-squares coefficients c_kx, c_ky, face
+ * offsets f_kx, f_ky); lsq, when not NULL and the pair is reference
+ * fidelity in float32, receives n_cells x 13 values (weights w_k, offsets
+ * dx_k, the 2x2 matrix a00 a01 a10 a11 of the per-call solve). Inspection
+ * only (mesh.py:223-260 computes the same quantities). */
+int esr_mesh_get_geometry(const esr_mesh* mesh, int32_t fidelity, int32_t precision, double* geo, double* lsq);
 
 /* A solver holds `n_meshes` meshes and slots_per_mesh[m] concurrent case
  * slots on mesh m; all slots advance together in one launch per kernel. It

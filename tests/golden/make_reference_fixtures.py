@@ -23,7 +23,10 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   (M 0.8, alpha 1.25) golden meshes in float32 and float64, with their dt,
   CD, CL and entropy created, plus 10 steps of the diamond with the Rusanov
   flux, constant reconstruction, explicit Euler and RK2, into
-  ``reference_solver.npz``; and ``euler/main.py:43-270`` itself (the
+  ``reference_solver.npz``; the same 20 steps on the HR diamond of the
+  north-star workload (h = 0.025 by the package's mesher, 19,384 cells,
+  M 2.0, alpha 0) in float32 and float64 into ``reference_solver_hr.npz``
+  (``--hr-only`` writes just that one); and ``euler/main.py:43-270`` itself (the
   stepping loop with the stationarity rule, the engineering criterion and
   the stop bookkeeping, exports off) on three configurations, final states
   and stop records into ``reference_runs.npz``;
@@ -248,7 +251,42 @@ def _summaries(utils_py: Path) -> list:
     return out
 
 
+def mesh_digest(mesh) -> str:
+    """sha256 of the mesh arrays the solver reads (the fixture's mesh identity)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in (mesh.points, mesh.tris, mesh.neighbors, mesh.faces, mesh.face_markers, mesh.face_connectivity):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def hr_fixture(ref_root: str) -> Path:
+    """The reference's own solver source on the HR diamond of the north-star
+    workload (h = 0.025, made by the package's mesher: 19,384 cells), M 2.0,
+    alpha 0, CFL 0.6: 20 SRK2 steps in float32 and float64 with their dt,
+    into ``reference_solver_hr.npz`` with the mesh's digest."""
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(HERE))
+    sys.dont_write_bytecode = True
+    import reference_solver_run as RS
+    from eulersr_b200.meshing.generate import cached_mesh
+    sys.path.insert(0, str(Path(ref_root) / "euler"))
+    import config as ref_config
+    mesh = cached_mesh("diamond", 0.025)
+    out = {"mesh_sha256": np.asarray(mesh_digest(mesh)), "n_cells": np.asarray(mesh.n_cells)}
+    for dname, dtp in (("f32", np.float32), ("f64", np.float64)):
+        W, dt_ = RS.run(ref_root, mesh, 2.0, 0.0, 20, dtp, ref_config._AOA_CASES_LC)
+        out[f"{dname}_W20"] = W
+        out[f"{dname}_dt"] = np.asarray(dt_, dtype=dtp)
+    path = HERE / "reference_solver_hr.npz"
+    np.savez_compressed(path, **out)
+    return path
+
+
 if __name__ == "__main__":
-    if len(sys.argv) != 2:
-        sys.exit("usage: python tests/golden/make_reference_fixtures.py <path of the EulerSR checkout>")
-    print(main(sys.argv[1]))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if len(args) != 1:
+        sys.exit("usage: python tests/golden/make_reference_fixtures.py <path of the EulerSR checkout> [--hr-only]")
+    if "--hr-only" not in sys.argv:
+        print(main(args[0]))
+    print(hr_fixture(args[0]))

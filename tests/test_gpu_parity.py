@@ -45,13 +45,15 @@ def _gpu_steps(mesh, prec, mach, aoa, steps, cfl=0.6, flux='hllc', recon='muscl'
     return W, dt, s
 
 
-@pytest.mark.parametrize("prec,tol", [("f64", TOL64), ("f32", TOL32)])
-def test_srk2_100_steps_diamond(diamond02, prec, tol):
+@pytest.mark.parametrize("prec,fidelity,tol", [("f64", "fast", TOL64), ("f32", "fast", TOL32),
+                                               ("f32", "reference", TOL32)])
+def test_srk2_100_steps_diamond(diamond02, prec, fidelity, tol):
     dtype = np.float64 if prec == 'f64' else np.float32
     Wo, dto, _, _ = _oracle_steps(diamond02, dtype, 2.5, 5.0, 100)
-    Wg, dtg, _ = _gpu_steps(diamond02, prec, 2.5, 5.0, 100)
+    Wg, dtg, _ = _gpu_steps(diamond02, prec, 2.5, 5.0, 100, fidelity=fidelity)
     dt_tol = 1e-14 if prec == 'f64' else 2e-6
     assert abs(dtg - float(dto)) <= dt_tol * float(dto)
+    print(f"diamond h=0.2 {prec} {fidelity}: {rel_err(Wg, Wo):.3e} after 100 steps")
     assert rel_err(Wg, Wo) <= tol, rel_err(Wg, Wo)
 
 
@@ -379,16 +381,24 @@ def test_per_case_threshold(diamond02):
     assert res[1]['stopping_step'] > res[0]['stopping_step'] > res[2]['stopping_step']
 
 
-@pytest.mark.parametrize("tag,name,mach,aoa,prec,tol", [("diamond", "diamond_h0.2", 2.5, 5.0, "f64", 1e-12),
-                                                        ("naca", "naca0012_h0.2", 0.8, 1.25, "f64", 1e-12),
-                                                        ("diamond", "diamond_h0.2", 2.5, 5.0, "f32", 1e-5)])
-def test_cuda_against_reference_solver_source(tag, name, mach, aoa, prec, tol):
+@pytest.mark.parametrize("tag,name,mach,aoa,prec,fidelity,tol", [
+    ("diamond", "diamond_h0.2", 2.5, 5.0, "f64", "fast", 1e-12),
+    ("naca", "naca0012_h0.2", 0.8, 1.25, "f64", "fast", 1e-12),
+    ("diamond", "diamond_h0.2", 2.5, 5.0, "f32", "fast", 1e-5),
+    ("diamond", "diamond_h0.2", 2.5, 5.0, "f32", "reference", 1e-5),
+    ("naca", "naca0012_h0.2", 0.8, 1.25, "f32", "reference", 1e-5)])
+def test_cuda_against_reference_solver_source(tag, name, mach, aoa, prec, fidelity, tol):
     """The CUDA path against EulerSR's own solver source run with NumPy for
     jax.numpy (tests/golden/reference_solver.npz, made by
-    tests/golden/make_reference_fixtures.py): 20 SRK2 steps and the dt."""
+    tests/golden/make_reference_fixtures.py): 20 SRK2 steps and the dt. With
+    the reference fidelity the float32 dt is the reference's bit for bit."""
     from conftest import GOLDEN, load_mesh
     ref = np.load(GOLDEN / "reference_solver.npz")
-    Wg, dtg, _ = _gpu_steps(load_mesh(name), prec, mach, aoa, 20)
+    Wg, dtg, _ = _gpu_steps(load_mesh(name), prec, mach, aoa, 20, fidelity=fidelity)
     dt_ref = float(ref[f"{tag}_{prec}_dt"])
+    if fidelity == "reference":
+        assert dtg == dt_ref
     assert abs(dtg - dt_ref) <= (1e-14 if prec == "f64" else 2e-6) * dt_ref
-    assert rel_err(Wg, ref[f"{tag}_{prec}_W20"]) <= tol
+    err = rel_err(Wg, ref[f"{tag}_{prec}_W20"])
+    print(f"{name} {prec} {fidelity}: {err:.3e} after 20 steps")
+    assert err <= tol

@@ -265,3 +265,27 @@ def test_oracle_run_equals_reference_main_loop(tag, name, prec):
     else:   # untracked: the reference reports None (euler/main.py:225-226)
         assert r.eng_converged is None and r.eng_stopping_step is None
     assert np.array_equal(r.W, ref[f"{tag}_{prec}_W"])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_oracle_bitwise_equals_reference_solver_source_hr(prec):
+    """The same pin at the north-star's HR size: 20 SRK2 steps on the diamond
+    h = 0.025 (19,384 cells, the package's mesher; the fixture records the
+    mesh's digest), M 2.0, alpha 0, equal bit for bit to the reference's own
+    source run with NumPy (tests/golden/reference_solver_hr.npz)."""
+    from conftest import oracle_mesh
+    from golden.make_reference_fixtures import mesh_digest
+    from eulersr_b200.meshing.generate import cached_mesh
+    from oracle import euler_oracle as O
+    ref = np.load(GOLDEN / "reference_solver_hr.npz")
+    mesh = cached_mesh("diamond", 0.025)
+    assert str(ref["mesh_sha256"]) == mesh_digest(mesh)
+    dtype = np.float32 if prec == "f32" else np.float64
+    om = oracle_mesh(mesh, dtype)
+    W, inlet = O.initialize(mesh.n_cells, dict(rho_inf=1.0, p_inf=1.0, gamma=1.4, Mach=2.0, aoa=0.0,
+                                               case="diamond"), dtype)
+    dt = O.get_dt(W, om, CFL=0.6)
+    assert dt == ref[f"{prec}_dt"]
+    for _ in range(20):
+        W = O.time_step_srk2(W, om, dt, inlet)
+    assert np.array_equal(W, ref[f"{prec}_W20"])
