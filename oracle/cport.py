@@ -84,6 +84,21 @@ class CpuCase:
             raise MemoryError("esr_cpu_srk2: allocation failed")
         return W
 
+    def srk2_local(self, W, nsteps, cfl):
+        """nsteps SRK2 steps with the per-cell CFL step (oracle time_step_srk2_local)."""
+        W = np.ascontiguousarray(W, dtype=self.dtype).copy()
+        L = lib()
+        f = L.esr_cpu_srk2_local_f64 if self.dtype == np.float64 else L.esr_cpu_srk2_local_f32
+        ct = C.c_double if self.dtype == np.float64 else C.c_float
+        p = lambda a, t=ct: a.ctypes.data_as(C.POINTER(t))
+        n = self.area.shape[0]
+        inl = np.ascontiguousarray(self.inlet, dtype=self.dtype)
+        rc = f(n, p(self.nbr, C.c_int32), p(self.kind, C.c_int32), p(self.nrm), p(self.s), p(self.dxf), p(self.dxl),
+               p(self.dxn), p(self.area), p(self.sigma), ct(self.gamma), p(inl), ct(cfl), int(nsteps), p(W))
+        if rc != 0:
+            raise MemoryError("esr_cpu_srk2_local: allocation failed")
+        return W
+
 
 def threads() -> int:
     return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))

@@ -219,3 +219,46 @@ int FN(esr_cpu_srk2)(int n, const int* nbr, const int* kind, const R* nrm, const
   free(W1); free(Pc); free(G); free(ph); free(Res);
   return 0;
 }
+
+/* nsteps SRK2 steps with the per-cell CFL step of the state at the start of
+ * each step (the local-time-step option: dt_c = cfl * area_c / sum_k
+ * (c + |u.n_k|) s_k, helper.py:8-18 per cell), as oracle/euler_oracle.py
+ * time_step_srk2_local */
+int FN(esr_cpu_srk2_local)(int n, const int* nbr, const int* kind, const R* nrm, const R* s, const R* dxf,
+                           const R* dxl, const R* dxn, const R* area, const R* sigma, R gamma, const R* inlet, R cfl,
+                           int nsteps, R* W) {
+  Mesh m = {n, nbr, kind, nrm, s, dxf, dxl, dxn, area, sigma, gamma, (R)(gamma - 1.0),
+            sizeof(R) == 8 ? (R)1e-12 : (R)1e-7, {inlet[0], inlet[1], inlet[2], inlet[3]}};
+  R* W1 = (R*)malloc(sizeof(R) * 4 * n);
+  R* Pc = (R*)malloc(sizeof(R) * 4 * n);
+  R* G = (R*)malloc(sizeof(R) * 8 * n);
+  R* ph = (R*)malloc(sizeof(R) * 4 * n);
+  R* Res = (R*)malloc(sizeof(R) * 4 * n);
+  R* dt = (R*)malloc(sizeof(R) * n);
+  if (!W1 || !Pc || !G || !ph || !Res || !dt) {
+    free(W1); free(Pc); free(G); free(ph); free(Res); free(dt);
+    return 1;
+  }
+  for (int it = 0; it < nsteps; ++it) {
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < n; ++c) {
+      R P[4];
+      prim(W + 4 * c, m.gm1, P);
+      const R cel = sqrt(fabs(gamma * P[3] / P[0]));
+      R lam = 0;
+      for (int k = 0; k < 3; ++k) {
+        const R un = P[1] * nrm[6 * c + 2 * k] + P[2] * nrm[6 * c + 2 * k + 1];
+        lam += (cel + fabs(un)) * s[3 * c + k];
+      }
+      dt[c] = area[c] / lam * cfl;
+    }
+    residual(&m, W, Pc, G, ph, Res);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < 4 * n; ++i) W1[i] = W[i] - dt[i / 4] * Res[i];
+    residual(&m, W1, Pc, G, ph, Res);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < 4 * n; ++i) W[i] = (R)0.5 * (W[i] + W1[i] - dt[i / 4] * Res[i]);
+  }
+  free(W1); free(Pc); free(G); free(ph); free(Res); free(dt);
+  return 0;
+}

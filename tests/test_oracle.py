@@ -178,6 +178,18 @@ def test_c_port_matches_numpy_oracle(diamond02):
     assert rel_err(c32.srk2(c32.W0, 20), W) <= 1e-5
 
 
+def test_c_port_local_dt_matches_numpy_oracle(diamond02):
+    """The C restatement's local-CFL SRK2 (the converged-cases CPU baseline
+    runs it) agrees with the oracle's time_step_srk2_local."""
+    from oracle.cport import CpuCase
+    cc = CpuCase(diamond02, 0.85, 2.0, np.float64)
+    Wc = cc.srk2_local(cc.W0, 20, 0.45)
+    W = cc.W0
+    for _ in range(20):
+        W = O.time_step_srk2_local(W, cc.om, 0.45, cc.inlet)
+    assert rel_err(Wc, W) <= 1e-12
+
+
 def test_rusanov_consistency_and_antisymmetry():
     """The Rusanov branch of getFlux: F(U, U, n) is the physical flux and
     F(L, R, n) = -F(R, L, -n)."""
