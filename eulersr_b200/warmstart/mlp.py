@@ -53,6 +53,7 @@ class MLP:
         # the 256-wide layers: tcgen05 kernel, or the mma.sync kernel kept as its cross-check
         self.gemm = {"tcgen05": self.L.esr_gemm_bf16, "mma_sync": self.L.esr_gemm_bf16_mma_sync}[gemm]
         self.device = device
+        self.launches = 0          # library kernels launched by forward()
         self.n_features = n_features
         self.offsets = {}
         off = 0
@@ -122,6 +123,7 @@ class MLP:
         y = self._buf(f"{tag}y", (rows, N_OUT), torch.float32)
         F.check(self.L.esr_mlp_head_fwd(_p(h[3]), rows, H, _p(self.view("W4")), _p(self.view("b4")),
                                         _p(base) if base is not None else None, _p(y), st))
+        self.launches += 5
         if keep:
             return y, dict(X=X, h=h, z=z)
         return y

@@ -52,9 +52,9 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def pressure_gradients(mesh, dm, states, machs, aoas):
+def pressure_gradients(mesh, dm, states, machs, aoas, device=0):
     """LSQ pressure gradient of each state, from the library's gradient kernel."""
-    s = Solver(dm, 1, precision="f64")
+    s = Solver(dm, 1, precision="f64", device=device)
     out = []
     for W, m, a in zip(states, machs, aoas):
         s.set_case(0, FlowCase(mach=float(m), aoa_deg=float(a), tf=1.0), W_init=W)
@@ -84,6 +84,7 @@ class WarmStart:
         self.sig = torch.tensor(sig if sig is not None else [1.0, 1.0, 1.0, 1.0], dtype=torch.float32, device=device)
         self.n_hr = pair.hr.n_cells
         self.rows = ((self.n_hr + ROW_TILE - 1) // ROW_TILE) * ROW_TILE
+        self.launches = 0          # library kernels launched by inputs() and predict_state()
         self.idx = torch.from_numpy(pair.knn_idx).to(device)
         self.dist = torch.from_numpy(pair.knn_dist).to(device)
         self.stat = torch.from_numpy(pair.static5).to(device)
@@ -102,6 +103,7 @@ class WarmStart:
         base = torch.zeros((self.rows, 4), dtype=torch.float32, device=self.device)
         F.check(self.L.esr_mlp_features(_p(self.stat), _p(idw), _p(idg), self.n_hr, (mach - MACH_MID) / MACH_SCALE,
                                         aoa / AOA_SCALE, _p(self.mu), _p(self.sig), K_IN, _p(X), _p(base), st))
+        self.launches += 3
         return X, base
 
     def predict_state(self, lr_prim, lr_gradp, mach, aoa, use_mlp=True, gamma=1.4):
@@ -111,6 +113,7 @@ class WarmStart:
         W = torch.empty((self.n_hr, 4), dtype=torch.float64, device=self.device)
         F.check(self.L.esr_mlp_decode(_p(pred), self.n_hr, _p(self.mu), _p(self.sig), gamma, 0.05, 0.05, _p(W),
                                       _stream()))
+        self.launches += 1
         return W.cpu().numpy()
 
 

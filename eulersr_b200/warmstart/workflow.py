@@ -1,0 +1,217 @@
+"""The warm-start workflow as one reusable object (evaluation and bench).
+
+Converged HR cases per second at a CD accuracy, for four ways of reaching a
+converged HR field of each (Mach, alpha) case:
+
+* ``mlp``    LR solve of every case -> LR pressure gradients -> IDW (k=6, p=2)
+             + residual MLP on the GPU -> HR solve from that prediction
+             (eval/convergence_case.py:106-140: the whole pipeline is timed);
+* ``idw``    the same without the MLP;
+* ``cold``   HR solve from freestream, ``slots`` cases at a time with
+             retire/refill;
+* ``single`` HR solve from freestream one case at a time (one slot), the
+             plain single-case solve.
+
+Every HR solve runs the local CFL step and ends a case once its CD has stayed
+within ``cd_tol`` of that case's reference CD for ``patience`` checks
+``check_every`` steps apart, or at ``max_steps``. A case counts as converged
+when the rule stopped it, its reference is steady and the CD it stopped at is
+within ``cd_tol`` of the reference. The reference CD of a case comes from a
+long float64 solve of the same kernels (``truth``): ``ref_steps`` steps, then
+``confirm_steps`` more; a reference whose CD still moves by more than 0.1 %
+marks the case unsteady (a failure for every start).
+
+Solvers are created once and reused, so a timed pass contains no solver
+set-up, autotuning or mesh upload.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from ..meshing.generate import cached_mesh
+from ..solver import DeviceMesh, FlowCase, Solver
+from .features import MeshPair
+from .mlp import MLP
+from .pipeline import WarmStart, build_training_set, draw_cases, eval_loss, pressure_gradients, primitives, train
+
+
+@dataclass
+class PassResult:
+    start: str
+    results: list
+    converged: int
+    seconds: float                 # device timeline of the pass (CUDA events, device synchronised)
+    wall_s: float
+    parts_s: dict = field(default_factory=dict)
+    iterations: list = field(default_factory=list)
+    states: list | None = None
+
+    @property
+    def cases_per_s(self) -> float:
+        return self.converged / self.seconds if self.seconds > 0 else 0.0
+
+
+def _device_timed(fn):
+    """Run fn() between two CUDA events recorded after a device-wide
+    synchronisation (the events bracket every stream's work); returns
+    (fn(), device seconds, wall seconds)."""
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    e1.record()
+    e1.synchronize()
+    return out, e0.elapsed_time(e1) * 1e-3, time.perf_counter() - t0
+
+
+class WarmStartWorkflow:
+    def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=6000, max_steps=12000,
+                 check_every=25, patience=8, cd_tol=0.005, device=0):
+        self.hr, self.lr = cached_mesh(geom, h_hr), cached_mesh(geom, h_lr)
+        self.pair = MeshPair.build(self.hr, self.lr)
+        self.dm_hr, self.dm_lr = DeviceMesh(self.hr), DeviceMesh(self.lr)
+        self.slots, self.lr_steps, self.max_steps = slots, lr_steps, max_steps
+        self.check_every, self.patience, self.cd_tol = check_every, patience, cd_tol
+        self.device = device
+        self.ws = WarmStart(self.pair, device=f"cuda:{device}")
+        self._solvers = {}
+        self.train_info = {}
+
+    # --------------------------------------------------------------- solvers
+    def _solver(self, key, dm, slots, **kw):
+        s = self._solvers.get(key)
+        if s is None:
+            s = Solver(dm, slots, device=self.device, **kw)
+            self._solvers[key] = s
+        return s
+
+    def _hr_solver(self, slots):
+        return self._solver(("hr", slots), self.dm_hr, slots, precision="f32", dt_mode="local",
+                            stop_rule="engineering", threshold=1e-30, check_every=self.check_every,
+                            patience=self.patience)
+
+    def _lr_solver(self, slots):
+        return self._solver(("lr", slots), self.dm_lr, slots, precision="f32", dt_mode="local", stop_rule="reference",
+                            threshold=1e-30, check_every=self.check_every, patience=self.patience)
+
+    def _grad_solver(self):
+        return self._solver(("grad",), self.dm_lr, 1, precision="f64")
+
+    def _cases(self, machs, aoas, targets=None, max_steps=None, dtype=np.float32):
+        out = []
+        for i, (m, a) in enumerate(zip(machs, aoas)):
+            kw = {}
+            if targets is not None:
+                kw = dict(eng_target_cd=float(targets[i]), eng_target_cl=0.0, eng_cd_tol=self.cd_tol,
+                          eng_cl_tol=1e12, eng_patience=self.patience)
+            out.append(FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9,
+                                max_steps=int(max_steps or self.max_steps), dtype=dtype, **kw))
+        return out
+
+    def close(self):
+        for s in self._solvers.values():
+            s.close()
+        self._solvers.clear()
+
+    def kernel_launches(self) -> int:
+        """Library kernels launched so far by this workflow's solvers and its
+        IDW, feature, MLP and decode calls."""
+        return sum(s.kernel_launches() for s in self._solvers.values()) + self.ws.launches + (
+            self.ws.mlp.launches if self.ws.mlp is not None else 0)
+
+    # ----------------------------------------------------------------- set-up
+    def lr_solutions(self, machs, aoas):
+        """LR fields of every case (fixed lr_steps) and their LSQ pressure gradients."""
+        s = self._lr_solver(len(machs))
+        _, states = s.batch_solve(self._cases(machs, aoas, max_steps=self.lr_steps), want_states=True)
+        g = self._grad_solver()
+        grads = []
+        for W, m, a in zip(states, machs, aoas):
+            g.set_case(0, FlowCase(mach=float(m), aoa_deg=float(a), tf=1.0), W_init=W)
+            grads.append(g.gradients(0)[:, 3, :].astype(np.float32))
+        return states, grads
+
+    def prepare(self, n_train=256, seed=3, target_steps=12000, train_steps=2000, batch=32768):
+        """Training pairs from the batched solver (LR and HR solves of
+        n_train cases drawn from default_rng(seed)), then the MLP trained by
+        the library's BF16 kernels."""
+        t0 = time.perf_counter()
+        (mt, at), _ = draw_cases(n_train, 0, seed=seed)
+        lr_states, lr_gp = self.lr_solutions(mt, at)
+        self._solvers.pop(("lr", n_train)).close()
+        hs = Solver(self.dm_hr, n_train, device=self.device, precision="f32", dt_mode="local",
+                    stop_rule="reference", threshold=1e-30, check_every=self.check_every)
+        _, hr_states = hs.batch_solve(self._cases(mt, at, max_steps=target_steps), want_states=True)
+        hs.close()
+        hr_gp = pressure_gradients(self.hr, self.dm_hr, hr_states, mt, at, device=self.device)
+        data, mu, sig = build_training_set(self.ws, lr_states, lr_gp, hr_states, hr_gp, mt, at)
+        del hr_states
+        mlp = MLP(device=f"cuda:{self.device}", seed=0)
+        self.ws.mlp = mlp
+        loss_idw = eval_loss(None, data)
+        hist, t_train = train(mlp, data, steps=train_steps, batch=batch)
+        self.train_info = {"n_train": n_train, "rows": int(data.X.shape[0]), "target_steps": target_steps,
+                           "train_steps": train_steps, "loss_idw": loss_idw, "loss_mlp": eval_loss(mlp, data),
+                           "train_s": t_train, "setup_s": time.perf_counter() - t0}
+        del data
+        torch.cuda.empty_cache()
+        return self.train_info
+
+    def truth(self, machs, aoas, ref_steps=30000, confirm_steps=5000):
+        """Reference CD of every case from a long float64 solve of the same
+        kernels, and whether it is steady (CD moved by <= 0.1 % over the
+        confirming steps)."""
+        s = Solver(self.dm_hr, len(machs), precision="f64", dt_mode="local", stop_rule="reference",
+                   threshold=1e-30, check_every=self.check_every, device=self.device)
+        ra, states = s.batch_solve(self._cases(machs, aoas, max_steps=ref_steps, dtype=np.float64),
+                                   want_states=True)
+        rb, _ = s.batch_solve(self._cases(machs, aoas, max_steps=confirm_steps, dtype=np.float64),
+                              init_fields=states)
+        s.close()
+        cd_a = np.array([r["cd"] for r in ra])
+        cd = np.array([r["cd"] for r in rb])
+        steady = np.abs(cd - cd_a) <= 1e-3 * np.abs(cd)
+        return cd, steady
+
+    # ------------------------------------------------------------- one pass
+    def _score(self, start, res, truth, steady, seconds, wall, parts):
+        st = np.array([r["status"] == 2 for r in res])
+        cd = np.array([r["cd"] for r in res])
+        ok = st & steady & (np.abs(cd - truth) <= self.cd_tol * np.abs(truth))
+        return PassResult(start, res, int(ok.sum()), seconds, wall, parts,
+                          [int(r["stopping_step"]) for r in res])
+
+    def solve(self, machs, aoas, truth, steady, start="mlp", want_states=False):
+        """One timed pass of `start` over the cases (see the module docstring)."""
+        parts = {}
+
+        def run():
+            if start in ("cold", "single"):
+                s = self._hr_solver(1 if start == "single" else min(self.slots, len(machs)))
+                t = time.perf_counter()
+                res, states = s.batch_solve(self._cases(machs, aoas, truth), want_states=want_states)
+                parts["hr_solve_s"] = time.perf_counter() - t
+                return res, states
+            t = time.perf_counter()
+            lr_states, lr_gp = self.lr_solutions(machs, aoas)
+            parts["lr_solve_s"] = time.perf_counter() - t
+            t = time.perf_counter()
+            inits = [self.ws.predict_state(primitives(W).astype(np.float32), g, m, a, use_mlp=(start == "mlp"))
+                     for W, g, m, a in zip(lr_states, lr_gp, machs, aoas)]
+            parts["inference_s"] = time.perf_counter() - t
+            s = self._hr_solver(min(self.slots, len(machs)))
+            t = time.perf_counter()
+            res, states = s.batch_solve(self._cases(machs, aoas, truth), init_fields=inits, want_states=want_states)
+            parts["hr_solve_s"] = time.perf_counter() - t
+            return res, states
+
+        (res, states), sec, wall = _device_timed(run)
+        out = self._score(start, res, truth, steady, sec, wall, parts)
+        out.states = states
+        return out

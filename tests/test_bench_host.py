@@ -95,3 +95,46 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = types.SimpleNamespace(workload="naca", h=0.025, cases=256, steps=3, warmup=3, precision="f32")
     assert bench.run_reference(args, 2, 1) == 0
     assert made == [] and capsys.readouterr().out == ""
+
+
+def test_warm_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    made = _fake_meshes(monkeypatch)
+    args = types.SimpleNamespace(workload="warm", steps=3, warmup=3)
+    assert bench.run_reference_warm(args, 2, 1) == 0
+    assert made == [] and capsys.readouterr().out == ""
+
+
+def test_warm_cases_are_the_held_out_draws_sharded_by_cost():
+    """The held-out cases follow the training draws of default_rng(3); under
+    two ranks the product's cost-balanced scheduler deals 2 x n_eval draws
+    without overlap and with balanced estimated cost."""
+    from eulersr_b200.parallel import case_cost
+    from eulersr_b200.warmstart.pipeline import draw_cases
+    args = types.SimpleNamespace(n_train=16, n_eval=8)
+    idx, me, ae = bench.warm_cases(args, 1, 0)
+    _, (me1, ae1) = draw_cases(16, 8, seed=3)
+    assert list(idx) == list(range(8)) and np.array_equal(me, me1) and np.array_equal(ae, ae1)
+    i0, m0, _ = bench.warm_cases(args, 2, 0)
+    i1, m1, _ = bench.warm_cases(args, 2, 1)
+    assert len(i0) + len(i1) == 16 and not (set(i0) & set(i1))
+    c0, c1 = case_cost(m0).sum(), case_cost(m1).sum()
+    assert abs(c0 - c1) <= case_cost(np.r_[m0, m1]).max()
+
+
+def test_cpu_converged_sample_rule(diamond02):
+    """The host arm's stop rule: a case stops once its CD stayed within the
+    tolerance of its reference for `patience` checks; an unreachable
+    reference runs to the cap and does not count."""
+    from oracle import euler_oracle as O
+    from oracle.cport import CpuCase
+    cc = CpuCase(diamond02, 2.5, 5.0, np.float32)
+    W = cc.srk2_local(cc.W0, 100, 0.6)
+    cd100 = float(O.force_coefficients(W.astype(np.float64), cc.om, 1.0, 2.5 * 1.4 ** 0.5,
+                                       diamond02.metadata.get("obstacle_length", 1.0))[0])
+    n, t, recs, thr = bench.cpu_converged_sample(
+        [{"mach": 2.5, "aoa": 5.0, "cd": cd100 * 10, "steady": True}], 1e9, diamond02, patience=2, max_steps=100)
+    assert n == 0 and recs[0]["steps"] == 100 and not recs[0]["converged"]
+    n, t, recs, thr = bench.cpu_converged_sample(
+        [{"mach": 2.5, "aoa": 5.0, "cd": cd100, "steady": True}], 1e9, diamond02, cd_tol=0.2, patience=2,
+        max_steps=400)
+    assert recs[0]["steps"] <= 400 and thr >= 1
