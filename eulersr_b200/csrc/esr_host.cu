@@ -1488,6 +1488,14 @@ int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm) {
   return ESR_OK;
 }
 
+int esr_mesh_get_patches(const esr_mesh* mesh, int32_t* n_patches, int32_t* start) {
+  if (!mesh || !n_patches) return fail(ESR_ERR_ARG, "mesh_get_patches: null argument");
+  const auto& ps = mesh->hm.patch_start;
+  *n_patches = (int32_t)ps.size() - 1;
+  if (start) std::memcpy(start, ps.data(), ps.size() * sizeof(int32_t));
+  return ESR_OK;
+}
+
 int esr_mesh_get_geometry(const esr_mesh* mesh, int32_t fidelity, int32_t precision, double* geo, double* lsq) {
   if (!mesh || !geo) return fail(ESR_ERR_ARG, "mesh_get_geometry: null argument");
   if (fidelity != ESR_FIDELITY_FAST && fidelity != ESR_FIDELITY_REFERENCE) return fail(ESR_ERR_ARG, "unknown fidelity");

@@ -12,6 +12,7 @@ struct HostMesh {
   int n_cells = 0, n_faces = 0, n_boundary_slots = 0;
   double y_min = 0, y_max = 0;
   std::vector<int> perm;          // new -> old
+  std::vector<int> patch_start;   // cells of patch p: [patch_start[p], patch_start[p+1]) in the new order
   std::vector<int> inv;           // old -> new
   std::vector<double> geo;        // n_cells records of G_COUNT values, renumbered
   // The same records formed as the reference forms them on every call, in
@@ -34,6 +35,8 @@ int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err);
 // records `msg` as the calling thread's esr_last_error() and returns `code`
 int report_error(int code, const std::string& msg);
 std::vector<int> rcm_order(int n, const std::vector<int>& nbr);
+std::vector<int> patch_order(int n, const std::vector<int>& nbr, const std::vector<int>& seed,
+                             std::vector<int>& patch_start);
 
 }  // namespace esr
 

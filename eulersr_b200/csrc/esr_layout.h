@@ -30,6 +30,10 @@ struct LsqRef {
 };
 static_assert(sizeof(LsqRef) == 64, "one 64-byte record per cell");
 
+// cells per patch of the renumbering: the face-flux kernel of batched float32
+// solves exchanges the fluxes of a patch's inner faces in shared memory
+constexpr int kPatchCells = 32;
+
 // slot kinds (face markers of euler/jax_fvm/src/mesh.py:47-52)
 enum SlotKind { K_INTERIOR = 0, K_WALL = 2, K_INLET = 3, K_OUTLET = 4, K_SUBSONIC = 5 };
 

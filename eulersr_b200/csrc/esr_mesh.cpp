@@ -180,6 +180,55 @@ static void reference_geometry(const esr_mesh_desc& d, const std::vector<int>& w
   (void)walls;
 }
 
+// Compact patches of at most kPatchCells cells, in the order of `seed`
+// (reverse Cuthill-McKee): each patch grows from the first unassigned cell
+// by adding, among the unassigned neighbours of the patch, the one with the
+// most neighbours already inside it (ties: earliest in `seed`), so that most
+// faces of a patch join two of its own cells. Cells are numbered patch by
+// patch; patch_start[p] is the first cell of patch p (n_patches + 1 entries).
+std::vector<int> patch_order(int n, const std::vector<int>& nbr, const std::vector<int>& seed,
+                             std::vector<int>& patch_start) {
+  std::vector<int> rank(n), owner(n, -1), order;
+  for (int i = 0; i < n; ++i) rank[seed[i]] = i;
+  order.reserve(n);
+  patch_start.assign(1, 0);
+  std::vector<int> members, cand, links(n, 0);
+  for (int s0 : seed) {
+    if (owner[s0] >= 0) continue;
+    const int p = (int)patch_start.size() - 1;
+    members.assign(1, s0);
+    owner[s0] = p;
+    cand.clear();
+    auto add_nbrs = [&](int c) {
+      for (int k = 0; k < 3; ++k) {
+        const int j = nbr[3 * c + k];
+        if (j < 0 || owner[j] >= 0) continue;
+        if (links[j]++ == 0) cand.push_back(j);
+      }
+    };
+    add_nbrs(s0);
+    while ((int)members.size() < kPatchCells && !cand.empty()) {
+      int best = -1;
+      for (int i = 0; i < (int)cand.size(); ++i) {
+        const int j = cand[i];
+        if (best < 0 || links[j] > links[cand[best]] || (links[j] == links[cand[best]] && rank[j] < rank[cand[best]]))
+          best = i;
+      }
+      const int c = cand[best];
+      cand[best] = cand.back();
+      cand.pop_back();
+      links[c] = 0;
+      owner[c] = p;
+      members.push_back(c);
+      add_nbrs(c);
+    }
+    for (int j : cand) links[j] = 0;
+    for (int c : members) order.push_back(c);
+    patch_start.push_back((int)order.size());
+  }
+  return order;
+}
+
 int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err) {
   const int N = d.n_cells, F = d.n_faces, P = d.n_points;
   if (N <= 0 || F <= 0 || P <= 0 || !d.points || !d.tris || !d.neighbors || !d.faces || !d.face_markers ||
@@ -201,8 +250,13 @@ int prepare_mesh(const esr_mesh_desc& d, HostMesh& hm, std::string& err) {
   // renumbering: perm[new] = old
   std::vector<int> nb_old(d.neighbors, d.neighbors + 3 * N);
   hm.perm.resize(N);
-  if (d.renumber) hm.perm = rcm_order(N, nb_old);
-  else std::iota(hm.perm.begin(), hm.perm.end(), 0);
+  if (d.renumber) hm.perm = patch_order(N, nb_old, rcm_order(N, nb_old), hm.patch_start);
+  else {
+    std::iota(hm.perm.begin(), hm.perm.end(), 0);
+    hm.patch_start.clear();   // consecutive cells in patches of kPatchCells
+    for (int c = 0; c < N; c += kPatchCells) hm.patch_start.push_back(c);
+    hm.patch_start.push_back(N);
+  }
   if ((int)hm.perm.size() != N) { err = "mesh: renumbering lost cells"; return ESR_ERR_ARG; }
   hm.inv.assign(N, -1);
   for (int i = 0; i < N; ++i) hm.inv[hm.perm[i]] = i;

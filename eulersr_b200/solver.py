@@ -139,6 +139,14 @@ class DeviceMesh:
         F.check(F.lib().esr_mesh_get_permutation(self.handle, F.ptr(perm, C.c_int32)))
         return perm
 
+    def patches(self) -> np.ndarray:
+        """First new cell of every patch of the renumbering, plus n_cells."""
+        n = C.c_int32()
+        F.check(F.lib().esr_mesh_get_patches(self.handle, C.byref(n), None))
+        start = np.empty(n.value + 1, dtype=np.int32)
+        F.check(F.lib().esr_mesh_get_patches(self.handle, C.byref(n), F.ptr(start, C.c_int32)))
+        return start
+
     def geometry(self, fidelity='fast', precision='f32'):
         """The per-cell records the kernels read (caller's cell order): a dict
         of normals (n,3,2), face lengths (n,3), area, blend3, lsq coefficients

@@ -193,6 +193,11 @@ int esr_mesh_destroy(esr_mesh* mesh);
 int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info);
 /* new-to-old cell permutation chosen by the renumbering (n_cells entries) */
 int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm);
+/* The renumbering's patches (at most 32 cells each; the face-flux kernel of
+ * batched float32 solves exchanges the fluxes of a patch's inner faces in
+ * shared memory): *n_patches, and when start is not NULL the first new cell
+ * of every patch plus n_cells (n_patches + 1 entries). */
+int esr_mesh_get_patches(const esr_mesh* mesh, int32_t* n_patches, int32_t* start);
 /* The per-cell geometry the kernels read, in the caller's cell order, for a
  * fidelity (ESR_FIDELITY_*) and precision (ESR_PREC_*): geo receives
  * n_cells x 24 values (normals n_kx, n_ky of the three edges, face lengths,
