@@ -16,8 +16,7 @@ workload (25,049 cells), transonic M 0.8, alpha 1.25 (CFL 0.45).
 * converged force coefficients: the float32 run (reference fidelity) stopped
   by the reference rule (threshold 1e-5, checked every 25 steps) against the
   float64 build of the same kernels advanced the same number of steps:
-  CD within 1e-4 relative, CL within 1e-4 of CD's magnitude (CL is ~0 at
-  alpha 0).
+  CD within 1e-4 relative, CL within 1e-5 absolute (CL is ~0 at alpha 0).
 
 Why the float32 bar needs the reference's rounding: on the HR diamond the
 reference's own float32 field moves by ~1.5e-5 after 100 steps when its state
@@ -134,4 +133,6 @@ def test_hr_diamond_converged_forces_f32_vs_f64(hr_meshes):
     print(f"HR diamond converged in {n} steps: float32 CD {r['cd']:.7f} CL {r['cl']:.2e}, "
           f"float64 CD {cd[0]:.7f} CL {cl[0]:.2e}")
     assert abs(r["cd"] - cd[0]) <= 1e-4 * abs(cd[0])
-    assert abs(r["cl"] - cl[0]) <= 1e-4 * abs(cd[0])
+    # CL is zero by symmetry at alpha 0 (the mesh leaves ~3e-4): relative
+    # error means nothing there, so it is held to 1e-5 absolute
+    assert abs(r["cl"] - cl[0]) <= 1e-5
