@@ -605,7 +605,8 @@ def run_warm(args, world, rank, local):
     torch.cuda.set_device(local)
     t_setup = time.perf_counter()
     wf = WarmStartWorkflow(slots=args.slots, max_steps=args.max_steps, device=local)
-    info = wf.prepare(n_train=args.n_train, target_steps=args.target_steps, train_steps=args.train_steps)
+    info = {} if args.make_truth else wf.prepare(n_train=args.n_train, target_steps=args.target_steps,
+                                                 train_steps=args.train_steps)
     idx, me, ae = warm_cases(args, world, rank)
     t0 = time.perf_counter()
     truth, steady = wf.truth(me, ae)

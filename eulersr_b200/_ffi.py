@@ -80,14 +80,18 @@ class KernelTimes(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+BLOCK_PATCHES = -1
+
+
 class Tuning(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("n_candidates", C.c_int32), ("candidates", C.c_int32 * 4),
-                ("step_ms", C.c_double * 4)]
+                ("k2_patches", C.c_int32), ("reserved", C.c_int32), ("step_ms", C.c_double * 4)]
 
     def as_dict(self):
         n = int(self.n_candidates)
-        return {"block_size": int(self.block_size),
-                "step_ms": {int(self.candidates[i]): float(self.step_ms[i]) for i in range(n)}}
+        name = lambda c: "patches" if c == BLOCK_PATCHES else int(c)
+        return {"block_size": int(self.block_size), "k2_patches": bool(self.k2_patches),
+                "step_ms": {name(self.candidates[i]): float(self.step_ms[i]) for i in range(n)}}
 
 
 class EsrError(RuntimeError):

@@ -48,6 +48,8 @@ struct Seg {                 // one mesh and its B case slots
   const T* wall_ny;
   const T* wall_ds;          // face length
   const LsqRef* lsq;         // per-cell least-squares data (reference-fidelity float32 only)
+  const int* patch_start;    // first cell of every patch of the renumbering (+ n_cells)
+  int n_patches;
   int n_wall;
   int b_shift;               // item / B = (umulhi(item, b_magic) + item) >> b_shift
   unsigned b_magic;
@@ -553,8 +555,18 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
     }
     T F[4];
     if (FLUX == 0) {
-      if constexpr (kFastPath<T, FAST> && MUSCL) hllc_fast<T>(PL, PR, nx, ny, kc, F);
-      else hllc<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
+      if constexpr (kFastPath<T, FAST> && MUSCL) {
+        // the face's canonical flux: evaluated from its owner (the lower
+        // cell), negated on the other side, as the patch kernel forms it
+        if (kind == K_INTERIOR && nbk[k] < c) {
+          hllc_fast<T>(PR, PL, -nx, -ny, kc, F);
+          F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
+        } else {
+          hllc_fast<T>(PL, PR, nx, ny, kc, F);
+        }
+      } else {
+        hllc<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
+      }
     } else {
       rusanov<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
     }
@@ -584,6 +596,119 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
                kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
   }
   Wout[gi] = o;
+}
+
+// ----------------------------------------------------- K2 by patches (float32)
+// The face-flux form of K2 for batched float32 HLLC + MUSCL solves: one block
+// per (patch of <= kPatchCells cells, group of 32 case slots), one warp per
+// cell at a time with its lanes over the 32 slots. Phase 1 evaluates every
+// face of the patch's cells once: an inner face (both cells in the patch) by
+// its owner, the lower cell, which stores F and -F in shared memory for both
+// cells; a face to a cell outside the patch and a boundary face by the cell
+// itself (the canonical flux, from the owner's side). Phase 2 forms each
+// cell's residual sum_k s_k F_k in slot order from shared memory (a
+// deterministic cell-owned sum, no atomics), then the sponge and the stage
+// update as k_flux. The fluxes equal k_flux's bit for bit.
+constexpr int kPatchWarps = 8;
+
+template <int STAGE, bool LOCALDT>
+__global__ void __launch_bounds__(32 * kPatchWarps, 4) k_flux_patch(const Seg<float>* __restrict__ segs,
+                                                                  const int4* __restrict__ pblk,
+                                                                  const float4* __restrict__ Win,
+                                                                  const float4* __restrict__ Wbase,
+                                                                  float4* __restrict__ Wout,
+                                                                  const float4* __restrict__ FV, long long total,
+                                                                  Cases<float> cs, Consts<float> kc, int pos,
+                                                                  const float* __restrict__ dt_local,
+                                                                  float* __restrict__ res_out) {
+  __shared__ float4 G[kPatchCells][3][32];   // signed face fluxes of the patch's cells (48 KB)
+  const int4 pb = pblk[blockIdx.x];          // segment, patch, first slot
+  const Seg<float> s = segs[pb.x];
+  const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int b = pb.z + lane;
+  const bool in_seg = b < s.B;
+  const int g = s.case0 + (in_seg ? b : 0);
+  const bool live = in_seg && cs.active[g] && cs.step[g] + pos < cs.nmax[g];
+  if (!__syncthreads_or(live)) return;        // every slot of the group idle
+  const bool warp_live = __any_sync(0xffffffffu, live);
+  const float4 inlet = cs.inlet[g];
+  if (warp_live) {
+    for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
+      const int c = c0 + lc;
+      const long long gi = s.off + (long long)c * s.B + b;
+      const int4 nb = __ldg(s.nbr + c);
+      const int nbk[3] = {nb.x, nb.y, nb.z};
+      float gk[12];
+      geo_groups<float, 3>(s, c, 0, gk);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int kind = slot_kind(nb.w, k);
+        const float nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
+        const int j = nbk[k];
+        const bool inner = kind == K_INTERIOR && j >= c0 && j < c1;
+        if (inner && j < c) continue;   // the owner, inside the patch, stores this one
+        float qL[4] = {0.f, 0.f, 0.f, 0.f}, qR[4] = {0.f, 0.f, 0.f, 0.f};
+        if (in_seg) {
+          const float4 fl = FV[(long long)k * total + gi];
+          qL[0] = fl.x; qL[1] = fl.y; qL[2] = fl.z; qL[3] = fl.w;
+          if (kind == K_INTERIOR) {
+            const float4 fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)j * s.B + b];
+            qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
+          } else {
+            prim<float>(ghost_cons<float>(kind, Win[gi], nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+          }
+        }
+        float F[4];
+        if (kind == K_INTERIOR && j < c) {     // owner outside the patch: its side, negated
+          hllc_fast<float>(qR, qL, -nx, -ny, kc, F);
+          F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
+        } else {
+          hllc_fast<float>(qL, qR, nx, ny, kc, F);
+        }
+        G[lc][k][lane] = make_float4(F[0], F[1], F[2], F[3]);
+        if (inner) G[j - c0][slot_opp(nb.w, k)][lane] = make_float4(-F[0], -F[1], -F[2], -F[3]);
+      }
+    }
+  }
+  __syncthreads();
+  if (!live) return;
+  for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
+    const int c = c0 + lc;
+    const long long gi = s.off + (long long)c * s.B + b;
+    const float4 Wc = Win[gi];
+    float gk[12];
+    geo_groups<float, 3>(s, c, 0, gk);
+    float acc[4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 f = G[lc][k][lane];
+      const float sk = gk[G_S0 + k];
+      if (k == 0) { acc[0] = sk * f.x; acc[1] = sk * f.y; acc[2] = sk * f.z; acc[3] = sk * f.w; }
+      else { acc[0] = acc[0] + sk * f.x; acc[1] = acc[1] + sk * f.y; acc[2] = acc[2] + sk * f.z; acc[3] = acc[3] + sk * f.w; }
+    }
+    const float area = gk[G_AREA];
+    const float sig = cs.strength[g] * gk[G_BLEND3];
+    const float R0 = dv<float>(acc[0], area) - sig * (inlet.x - Wc.x);
+    const float R1 = dv<float>(acc[1], area) - sig * (inlet.y - Wc.y);
+    const float R2 = dv<float>(acc[2], area) - sig * (inlet.z - Wc.z);
+    const float R3 = dv<float>(acc[3], area) - sig * (inlet.w - Wc.w);
+    const float dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+    if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
+    float4 o;
+    if (STAGE == ST_FIRST) {
+      o = make_float4(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
+    } else if (STAGE == ST_SRK2_SECOND) {
+      const float4 W0 = Wbase[gi];
+      o = make_float4(kc.half * (W0.x + Wc.x - dt * R0), kc.half * (W0.y + Wc.y - dt * R1),
+                      kc.half * (W0.z + Wc.z - dt * R2), kc.half * (W0.w + Wc.w - dt * R3));
+    } else {
+      const float4 W0 = Wbase[gi];
+      o = make_float4(kc.half * (W0.x - dt * R0 + Wc.x), kc.half * (W0.y - dt * R1 + Wc.y),
+                      kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
+    }
+    Wout[gi] = o;
+  }
 }
 
 // copy a stage result back into the state for live slots (explicit Euler)

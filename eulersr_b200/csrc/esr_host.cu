@@ -94,6 +94,7 @@ struct SolverT : SolverBase {
     DevBuf<int> wall_cell;
     DevBuf<T> wall_nx, wall_ny, wall_ds;
     DevBuf<LsqRef> lsq;  // reference-fidelity float32: per-call least-squares data
+    DevBuf<int> patch;   // first cell of every patch (+ n_cells)
     DevBuf<int> inv;  // caller cell -> solver cell
     int B = 0, case0 = 0;
     long long off = 0;
@@ -106,6 +107,9 @@ struct SolverT : SolverBase {
   DevBuf<Seg<T>> d_segs;
   DevBuf<int2> d_blk;
   int n_blk = 0;
+  DevBuf<int4> d_pblk;   // K2 by patches: (mesh segment, patch, first slot) per block
+  int n_pblk = 0;
+  bool use_patch = false;
   DevBuf<int> d_case_seg, d_case_slot, d_ncells;
 
   DevBuf<V> W, Wa, Wref, FV, Wp;   // Wp: probe step output (batch solves)
@@ -181,6 +185,10 @@ struct SolverT : SolverBase {
   // float32 with esr_params.fidelity = ESR_FIDELITY_REFERENCE: the kernels of esr_faithful.cu
   bool faithful() const { return sizeof(T) == 4 && P.fidelity == ESR_FIDELITY_REFERENCE; }
   static constexpr bool kF = sizeof(T) == 4;   // FAST flag of the kernels this file instantiates
+  // K2 by patches applies to float32 fast-fidelity HLLC + MUSCL solves
+  bool patch_eligible() const {
+    return sizeof(T) == 4 && !faithful() && P.flux == ESR_FLUX_HLLC && P.reconstruction == ESR_RECON_MUSCL;
+  }
 
   int init(const esr_mesh* const* ms, const int32_t* slots, int nm, const esr_params* p) {
     P = *p;
@@ -229,11 +237,15 @@ struct SolverT : SolverBase {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     block = p->block_size > 0 ? p->block_size : 0;
-    if (block == 0) {   // starting point; measured below
+    if (p->block_size == ESR_BLOCK_PATCHES) {
+      block = 128;
+      use_patch = patch_eligible();
+    } else if (block == 0) {   // starting point; measured below
       block = 256;
       while (block > 64 && (total + block - 1) / block < 2 * sms) block /= 2;
     }
-    if (block != 64 && block != 128 && block != 256) return fail(ESR_ERR_ARG, "solver: block_size must be 0, 64, 128 or 256");
+    if (block != 64 && block != 128 && block != 256)
+      return fail(ESR_ERR_ARG, "solver: block_size must be 0, 64, 128, 256 or ESR_BLOCK_PATCHES");
     // upload meshes
     std::vector<Seg<T>> hsegs;
     std::vector<int> hseg_of(n_slots), hslot_of(n_slots), hnc(n_slots);
@@ -274,11 +286,16 @@ struct SolverT : SolverBase {
       }
       ESR_TRY(md.inv.alloc(N));
       ESR_CUDA(cudaMemcpy(md.inv.p, hm.inv.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+      ESR_TRY(md.patch.alloc(hm.patch_start.size()));
+      ESR_CUDA(cudaMemcpy(md.patch.p, hm.patch_start.data(), hm.patch_start.size() * sizeof(int),
+                          cudaMemcpyHostToDevice));
       Seg<T> s{};
       s.n_cells = N; s.B = md.B; s.case0 = md.case0; s.geo_stride = G_COUNT; s.off = md.off;
       s.nbr = md.nbr.p; s.geo = md.geo.p; s.wall_cell = md.wall_cell.p; s.wall_nx = md.wall_nx.p;
       s.wall_ny = md.wall_ny.p; s.wall_ds = md.wall_ds.p; s.n_wall = nw;
       s.lsq = md.lsq.p;
+      s.patch_start = md.patch.p;
+      s.n_patches = (int)hm.patch_start.size() - 1;
       ESR_TRY(set_divider(s));
       hsegs.push_back(s);
       for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
@@ -287,6 +304,7 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
     hseg0 = hsegs[0];
     ESR_TRY(build_blocks(block));
+    ESR_TRY(build_patch_blocks());
     ESR_TRY(d_case_seg.alloc(n_slots));
     ESR_TRY(d_case_slot.alloc(n_slots));
     ESR_TRY(d_ncells.alloc(n_slots));
@@ -367,6 +385,20 @@ struct SolverT : SolverBase {
     return ESR_OK;
   }
 
+  // block table of K2 by patches: every patch of every mesh x groups of 32 slots
+  int build_patch_blocks() {
+    std::vector<int4> h;
+    for (int m = 0; m < (int)meshes.size(); ++m) {
+      const int np = (int)meshes[m]->hm->patch_start.size() - 1;
+      for (int p = 0; p < np; ++p)
+        for (int b0 = 0; b0 < meshes[m]->B; b0 += 32) h.push_back(make_int4(m, p, b0, 0));
+    }
+    ESR_TRY(d_pblk.alloc(h.size()));
+    if (!h.empty()) ESR_CUDA(cudaMemcpy(d_pblk.p, h.data(), h.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    n_pblk = (int)h.size();
+    return ESR_OK;
+  }
+
   // Autotuner: time one full step of every slot (the solver's own meshes,
   // scheme and slot counts; a uniform finite state, all slots live) for each
   // block size and keep the fastest. Results do not depend on the choice:
@@ -401,9 +433,26 @@ struct SolverT : SolverBase {
       tuning.step_ms[i] = ms / 3.0;
       if (ms / 3.0 < best) { best = ms / 3.0; best_blk = cand[i]; }
     }
+    // K2 by patches, with K1 at the best block size
+    if (patch_eligible()) {
+      ESR_TRY(build_blocks(best_blk));
+      use_patch = true;
+      step_kernels(cs, 0);
+      ESR_CUDA(cudaEventRecord(ev0, stream));
+      for (int r = 0; r < 3; ++r) step_kernels(cs, 0);
+      ESR_CUDA(cudaEventRecord(ev1, stream));
+      ESR_CUDA(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev0, ev1);
+      tuning.candidates[3] = ESR_BLOCK_PATCHES;
+      tuning.step_ms[3] = ms / 3.0;
+      tuning.n_candidates = 4;
+      use_patch = ms / 3.0 < best;
+    }
     launches = before;
     ESR_TRY(build_blocks(best_blk));
     tuning.block_size = best_blk;
+    tuning.k2_patches = use_patch ? 1 : 0;
     ESR_CUDA(cudaMemsetAsync(W.p, 0, total * sizeof(V), stream));
     ESR_CUDA(cudaMemsetAsync(Wa.p, 0, total * sizeof(V), stream));
     ESR_CUDA(cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream));
@@ -416,6 +465,7 @@ struct SolverT : SolverBase {
   int get_tuning(esr_tuning* out) {
     *out = tuning;
     if (out->block_size == 0) out->block_size = block;   // given, not measured
+    out->k2_patches = use_patch ? 1 : 0;
     return ESR_OK;
   }
 
@@ -446,6 +496,18 @@ struct SolverT : SolverBase {
         tap_begin(1);
         faithful_flux(STAGE, bmap(), win, wbase, wout, FV.p, total, cs, kc, pos, dt_local.p, res.p, rus, muscl, local,
                       n_blk, block, stream);
+        tap_end();
+        ++launches;
+        return;
+      }
+      if (use_patch && n_pblk > 0) {   // eligible by construction: HLLC + MUSCL, fast fidelity
+        tap_begin(1);
+        if (local)
+          k_flux_patch<STAGE, true><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, win, wbase, wout, FV.p,
+                                                                             total, cs, kc, pos, dt_local.p, res.p);
+        else
+          k_flux_patch<STAGE, false><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, win, wbase, wout, FV.p,
+                                                                              total, cs, kc, pos, dt_local.p, res.p);
         tap_end();
         ++launches;
         return;

@@ -208,7 +208,7 @@ class Solver:
         p.patience = max(1, int(patience))
         p.device = int(device)
         p.use_graphs = int(bool(use_graphs))
-        p.block_size = int(block_size)
+        p.block_size = F.BLOCK_PATCHES if block_size == "patches" else int(block_size)
         try:
             p.fidelity = F.FIDELITY[str(fidelity).lower()]
         except KeyError:

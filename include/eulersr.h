@@ -80,6 +80,10 @@ extern "C" {
 #define ESR_STOP_DENSITY_L2 1  /* RMS over cells of the density residual */
 #define ESR_STOP_ENGINEERING 2 /* stop when the engineering criterion (force coefficients
                                 * within tolerance of given targets) is confirmed */
+#define ESR_BLOCK_PATCHES (-1)  /* esr_params.block_size: K2 by patches of <= 32 cells, each inner
+                                  * face's flux evaluated once and exchanged in shared memory
+                                  * (float32 fast fidelity, HLLC + MUSCL; the fluxes are bitwise
+                                  * those of the per-cell K2) */
 #define ESR_FIDELITY_FAST 0      /* geometry formed in float64 and rounded once; float32 kernels
                                   * with approximate division and the direct HLLC flux */
 #define ESR_FIDELITY_REFERENCE 1 /* the reference's rounding: geometry formed in the run's
@@ -132,7 +136,8 @@ typedef struct esr_params {
     int32_t patience;         /* consecutive checks under the threshold (>= 1) */
     int32_t device;           /* CUDA device ordinal */
     int32_t use_graphs;       /* 1: capture step chunks in CUDA graphs */
-    int32_t block_size;       /* threads per block for the cell kernels: 64, 128, 256, or 0 = autotuned */
+    int32_t block_size;       /* threads per block for the cell kernels: 64, 128, 256, 0 = autotuned,
+                               * or ESR_BLOCK_PATCHES: cell kernels at 128 with K2 formed by patches */
     int32_t fidelity;         /* ESR_FIDELITY_* (0: fast) */
 } esr_params;
 
@@ -282,12 +287,18 @@ typedef struct esr_kernel_times {
 int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out);
 
 /* The autotuner's record: with esr_params.block_size = 0 the solver times one
- * full step of all its slots for each candidate block size at creation and
- * keeps the fastest (no reference counterpart: XLA picks launch shapes). */
+ * full step of all its slots for each candidate at creation and keeps the
+ * fastest (no reference counterpart: XLA picks launch shapes). Candidates:
+ * the cell kernels at 64, 128 and 256 threads per block, then, where
+ * eligible (float32 fast fidelity, HLLC + MUSCL), K2 by patches with the
+ * best of those for K1 (ESR_BLOCK_PATCHES). Results do not depend on the
+ * choice. */
 typedef struct esr_tuning {
-    int32_t block_size;       /* threads per block in use */
+    int32_t block_size;       /* threads per block of the cell kernels in use */
     int32_t n_candidates;     /* 0 when block_size was given */
     int32_t candidates[4];
+    int32_t k2_patches;       /* 1: K2 runs by patches */
+    int32_t reserved;
     double step_ms[4];        /* device ms of one step per candidate */
 } esr_tuning;
 int esr_solver_tuning(const esr_solver* solver, esr_tuning* out);

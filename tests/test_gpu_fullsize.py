@@ -78,15 +78,16 @@ def test_full_mesh_f32_fast_fidelity_accuracy(naca_hr):
 
 def test_full_batch_slots_equal_single_solves(naca_hr):
     """The bench's batch: 256 cases, Mach ~ U[0.7, 3] and alpha on the 0.5-degree
-    grid from default_rng(1); a 50-step chunk of the whole batch leaves every
-    sampled slot bitwise equal to the same case advanced alone."""
+    grid from default_rng(1); a 50-step chunk of the whole batch (K2 by
+    patches) leaves every sampled slot bitwise equal to the same case advanced
+    alone (per-cell K2)."""
     from eulersr_b200.solver import DeviceMesh, FlowCase, Solver
     rng = np.random.default_rng(1)
     mach = rng.uniform(0.7, 3.0, 256)
     aoa = rng.choice(np.arange(-5, 5.01, 0.5), 256)
     cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, dtype=np.float32) for m, a in zip(mach, aoa)]
     dm = DeviceMesh(naca_hr)
-    s = Solver(dm, 256, precision="f32")
+    s = Solver(dm, 256, precision="f32", block_size="patches")   # K2 by patches; the single solves per cell
     s.set_cases(list(range(256)), cases)
     s.step(50)
     states = s.get_states(list(range(256)), dtype=np.float32)

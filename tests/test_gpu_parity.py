@@ -146,12 +146,14 @@ def test_maxstep_cap(diamond02):
     assert r['steps'] == r['n_max'] == int(np.float32(0.05) / np.float32(r['dt'])) + 1
 
 
-@pytest.mark.parametrize("precision", ["f32", "f64"])
-def test_batch_equals_single(diamond02, naca02, precision):
+@pytest.mark.parametrize("precision,block", [("f32", 0), ("f32", "patches"), ("f64", 0)])
+def test_batch_equals_single(diamond02, naca02, precision, block):
     """Every case solved inside a ragged two-mesh batch, with the queue
     retiring and refilling slots on the device, is bitwise identical to the
     same case solved alone: state, stop step, status and force coefficients.
-    Case 4 starts from a warm field and case 1 tracks the engineering rule."""
+    Case 4 starts from a warm field and case 1 tracks the engineering rule.
+    With block='patches' the batch's K2 runs by patches (face fluxes once per
+    inner face) while the single solves run the per-cell K2."""
     from eulersr_b200.solver import Solver, FlowCase
     dt_ = np.float32 if precision == 'f32' else np.float64
     meshes = [diamond02, naca02]
@@ -165,11 +167,11 @@ def test_batch_equals_single(diamond02, naca02, precision):
     warm.step(30)
     init = [None] * len(cases)
     init[4] = warm.get_state(0)
-    s = Solver(meshes, [2, 1], precision=precision, threshold=1e-5, check_every=10)
+    s = Solver(meshes, [2, 1], precision=precision, threshold=1e-5, check_every=10, block_size=block)
     res, states = s.batch_solve(cases, init_fields=init, want_states=True)
     assert sorted(r['case_index'] for r in res) == list(range(len(cases)))
     for i, c in enumerate(cases):
-        one = Solver(meshes[c.mesh], 1, precision=precision, threshold=1e-5, check_every=10)
+        one = Solver(meshes[c.mesh], 1, precision=precision, threshold=1e-5, check_every=10, block_size=128)
         c1 = FlowCase(mach=c.mach, aoa_deg=c.aoa_deg, cfl=0.6, tf=0.4, dtype=dt_)
         if i == 1:
             for k, v in eng.items():
@@ -238,19 +240,27 @@ def test_batch_submit_poll_results(diamond02, naca02):
 
 
 def test_autotuner_and_block_invariance(naca02):
-    """The autotuner times every candidate block size and keeps the fastest;
-    the state after 30 steps is bitwise the same whatever the block size."""
+    """The autotuner times every candidate (cell kernels at 64, 128 and 256
+    threads, and K2 by patches) and keeps the fastest; the state after 30 steps
+    is bitwise the same whatever the choice: K2 by patches evaluates each inner
+    face once and the per-cell K2 the same canonical flux from the face's
+    owner."""
     from eulersr_b200.solver import Solver, FlowCase
     states = []
-    for bs in (0, 64, 128, 256):
+    for bs in (0, 64, 128, 256, "patches"):
         s = Solver(naca02, 3, precision='f32', block_size=bs)
         t = s.tuning()
         if bs == 0:
-            assert sorted(t['step_ms']) == [64, 128, 256]
+            assert sorted(t['step_ms'], key=str) == [128, 256, 64, "patches"]
             assert all(v > 0 for v in t['step_ms'].values())
-            assert t['block_size'] == min(t['step_ms'], key=t['step_ms'].get)
+            best = min(t['step_ms'], key=t['step_ms'].get)
+            assert t['k2_patches'] == (best == "patches")
+            if best != "patches":
+                assert t['block_size'] == best
+        elif bs == "patches":
+            assert t['k2_patches'] and t['block_size'] == 128 and t['step_ms'] == {}
         else:
-            assert t['block_size'] == bs and t['step_ms'] == {}
+            assert t['block_size'] == bs and not t['k2_patches'] and t['step_ms'] == {}
         for g, (m, a) in enumerate([(0.8, 1.0), (2.0, -3.0), (1.3, 2.5)]):
             s.set_case(g, FlowCase(mach=m, aoa_deg=a, tf=1.0, dtype=np.float32))
         s.step(30)
