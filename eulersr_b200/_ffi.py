@@ -114,6 +114,10 @@ _SIGS = {
     "esr_mesh_get_permutation": (C.c_int, [C.c_void_p, _i32p]),
     "esr_mesh_get_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_mesh_get_patches": (C.c_int, [C.c_void_p, _i32p, C.c_void_p]),
+    "esr_stage_cases_f32": (C.c_int, [C.c_void_p, C.c_int32, _i32p, C.c_void_p, C.c_void_p]),
+    "esr_apply_staged": (C.c_int, [C.c_void_p]),
+    "esr_fetch_states_f32": (C.c_int, [C.c_void_p, C.c_int32, _i32p, C.c_void_p]),
+    "esr_wait_transfers": (C.c_int, [C.c_void_p]),
     "esr_solver_create": (C.c_int, [C.POINTER(C.c_void_p), _i32p, C.c_int32, C.POINTER(Params), C.POINTER(C.c_void_p)]),
     "esr_solver_destroy": (C.c_int, [C.c_void_p]),
     "esr_solver_num_slots": (C.c_int, [C.c_void_p, _i32p]),

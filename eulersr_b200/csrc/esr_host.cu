@@ -61,6 +61,22 @@ struct DevBuf {
   }
 };
 
+// page-locked host memory owned by the solver (tables of the overlapped copies)
+template <typename T>
+struct PinnedBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~PinnedBuf() { if (p) cudaFreeHost(p); }
+  int reserve(size_t count) {
+    if (count <= n) return ESR_OK;
+    if (p) { cudaFreeHost(p); p = nullptr; n = 0; }
+    cudaError_t e = cudaMallocHost(&p, count * sizeof(T));
+    if (e != cudaSuccess) { p = nullptr; return fail(ESR_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e)); }
+    n = count;
+    return ESR_OK;
+  }
+};
+
 constexpr int kChunkMax = 64;       // steps per captured chunk (upper bound)
 constexpr int kReduceThreads = 256;
 constexpr int kReduceCells = 2048;  // cells per reduction block
@@ -158,8 +174,12 @@ struct SolverT : SolverBase {
     }
     if (g_run) cudaGraphExecDestroy(g_run);
     if (g_plain) cudaGraphExecDestroy(g_plain);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : {ev_in_ready, ev_in_consumed, ev_out_ready, ev_out_done})
+      if (e) cudaEventDestroy(e);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -799,6 +819,153 @@ struct SolverT : SolverBase {
   DevBuf<double> stage_many;            // host rows of set_cases / get_states
   DevBuf<SlotInit<T>> d_init;
   DevBuf<SlotCopy<T>> d_jobs;
+
+  // ------------------------------ overlapped transfers (float32 host fields)
+  // The next cases' fields go up on a copy stream while the current chunk
+  // runs (stage_in), are placed by one launch on the solver's stream
+  // (apply_staged); final fields are gathered on the solver's stream and go
+  // down on the copy stream while the next chunk runs (fetch_states). Events
+  // order the two streams: a staging buffer is rewritten only after the
+  // launches that read it have run.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_in_ready = nullptr, ev_in_consumed = nullptr, ev_out_ready = nullptr, ev_out_done = nullptr;
+  DevBuf<float> st_in, st_out;
+  DevBuf<SlotInit<T>> st_init;
+  DevBuf<SlotCopy<T>> st_jobs_in, st_jobs_out;
+  PinnedBuf<SlotInit<T>> h_init;
+  PinnedBuf<SlotCopy<T>> h_jobs_in, h_jobs_out;
+  int staged_n = 0, staged_max = 0;
+  std::vector<int> staged_slots;
+  int transfer_setup() {
+    if (copy_stream) return ESR_OK;
+    ESR_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_in_ready, &ev_in_consumed, &ev_out_ready, &ev_out_done})
+      ESR_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return ESR_OK;
+  }
+  int stage_in(int n, const int32_t* slots, const esr_case* cs, const float* const* W_init) {
+    if (n <= 0 || !slots || !cs || !W_init) return fail(ESR_ERR_ARG, "stage_cases: bad arguments");
+    ESR_TRY(transfer_setup());
+    std::vector<char> seen(n_slots, 0);
+    long long rows = 0;
+    int max_n = 0;
+    // everything is checked before the staging buffers change
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      if (seen[slots[i]]) return fail(ESR_ERR_ARG, "stage_cases: a slot is listed twice");
+      seen[slots[i]] = 1;
+      if (!W_init[i]) return fail(ESR_ERR_ARG, "stage_cases: null field");
+      if (!(cs[i].tf > 0) && cs[i].max_steps <= 0) return fail(ESR_ERR_ARG, "stage_cases: tf must be > 0");
+      if (!(cs[i].cfl > 0)) return fail(ESR_ERR_ARG, "stage_cases: cfl must be > 0");
+      rows += meshes[m]->hm->n_cells;
+      max_n = std::max(max_n, meshes[m]->hm->n_cells);
+    }
+    // the previous staging's copies have finished: its host tables are free
+    ESR_CUDA(cudaEventSynchronize(ev_in_ready));
+    ESR_TRY(h_init.reserve(n));
+    ESR_TRY(h_jobs_in.reserve(n));
+    if (st_in.n < (size_t)4 * rows) ESR_TRY(st_in.alloc((size_t)4 * rows));
+    if (st_init.n < (size_t)n) ESR_TRY(st_init.alloc(n));
+    if (st_jobs_in.n < (size_t)n) ESR_TRY(st_jobs_in.alloc(n));
+    long long row = 0;
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      mesh_of_slot(slots[i], m, b);
+      esr_case c = cs[i];
+      c.mesh = m;
+      SlotInit<T>& x = h_init.p[i];
+      x = SlotInit<T>{};
+      x.slot = slots[i];
+      case_params(c, x.inlet, x.strength, x.qref, x.eng_t, x.eng_track, x.eng_pat);
+      x.cfl = c.cfl;
+      x.tf = c.tf;
+      x.thr = c.threshold;
+      x.max_steps = c.max_steps;
+      MeshDev& md = *meshes[m];
+      h_jobs_in.p[i] = SlotCopy<T>{row, md.inv.p, md.off, md.hm->n_cells, md.B, b, 0, x.inlet};
+      row += md.hm->n_cells;
+    }
+    // the device staging is rewritten once the last placement has read it
+    ESR_CUDA(cudaStreamWaitEvent(copy_stream, ev_in_consumed, 0));
+    ESR_CUDA(cudaMemcpyAsync(st_init.p, h_init.p, n * sizeof(SlotInit<T>), cudaMemcpyHostToDevice, copy_stream));
+    ESR_CUDA(cudaMemcpyAsync(st_jobs_in.p, h_jobs_in.p, n * sizeof(SlotCopy<T>), cudaMemcpyHostToDevice, copy_stream));
+    for (int i = 0; i < n; ++i)
+      ESR_CUDA(cudaMemcpyAsync(st_in.p + 4 * h_jobs_in.p[i].stage_row, W_init[i],
+                               (size_t)4 * h_jobs_in.p[i].n_cells * sizeof(float), cudaMemcpyHostToDevice,
+                               copy_stream));
+    ESR_CUDA(cudaEventRecord(ev_in_ready, copy_stream));
+    staged_n = n;
+    staged_max = max_n;
+    staged_slots.assign(slots, slots + n);
+    return ESR_OK;
+  }
+  int apply_staged() {
+    if (staged_n <= 0) return fail(ESR_ERR_STATE, "apply_staged: nothing staged");
+    ESR_CUDA(cudaStreamWaitEvent(stream, ev_in_ready, 0));
+    ESR_CUDA(cudaMemsetAsync(fill.p, 0, n_slots * sizeof(int), stream));
+    SlotParams<T> sp{dt.p, inlet.p, strength.p, cfl.p, tf.p, max_steps.p, qref.p, eng_track.p, eng_patience.p, eng_t.p, thr.p};
+    k_init_slots<T><<<(staged_n + 127) / 128, 128, 0, stream>>>(st_init.p, staged_n, sp, ctl(), fill.p);
+    ++launches;
+    for (int j0 = 0; j0 < staged_n; j0 += 65535) {
+      const int nj = std::min(65535, staged_n - j0);
+      k_scatter_slots<T, float><<<dim3((staged_max + 255) / 256, nj), 256, 0, stream>>>(st_in.p, st_jobs_in.p + j0, W.p,
+                                                                                        Wref.p);
+      ++launches;
+    }
+    ESR_TRY(finish_fill());
+    ESR_CUDA(cudaEventRecord(ev_in_consumed, stream));
+    for (int g : staged_slots) hcase_index[g] = g;
+    staged_n = 0;
+    return ESR_OK;
+  }
+  int fetch_states(int n, const int32_t* slots, float* const* out) {
+    if (n <= 0 || !slots || !out) return fail(ESR_ERR_ARG, "fetch_states: bad arguments");
+    ESR_TRY(transfer_setup());
+    long long rows = 0;
+    int max_n = 0;
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      ESR_TRY(mesh_of_slot(slots[i], m, b));
+      if (!out[i]) return fail(ESR_ERR_ARG, "fetch_states: null output");
+      rows += meshes[m]->hm->n_cells;
+      max_n = std::max(max_n, meshes[m]->hm->n_cells);
+    }
+    // the previous download has finished: the gather staging and its table are free
+    ESR_CUDA(cudaEventSynchronize(ev_out_done));
+    ESR_TRY(h_jobs_out.reserve(n));
+    if (st_out.n < (size_t)4 * rows) ESR_TRY(st_out.alloc((size_t)4 * rows));
+    if (st_jobs_out.n < (size_t)n) ESR_TRY(st_jobs_out.alloc(n));
+    long long row = 0;
+    for (int i = 0; i < n; ++i) {
+      int m, b;
+      mesh_of_slot(slots[i], m, b);
+      MeshDev& md = *meshes[m];
+      h_jobs_out.p[i] = SlotCopy<T>{row, md.inv.p, md.off, md.hm->n_cells, md.B, b, 0, V{}};
+      row += md.hm->n_cells;
+    }
+    ESR_CUDA(cudaMemcpyAsync(st_jobs_out.p, h_jobs_out.p, n * sizeof(SlotCopy<T>), cudaMemcpyHostToDevice, stream));
+    for (int j0 = 0; j0 < n; j0 += 65535) {
+      const int nj = std::min(65535, n - j0);
+      k_gather_slots<T, float><<<dim3((max_n + 255) / 256, nj), 256, 0, stream>>>(W.p, st_jobs_out.p + j0, st_out.p);
+      ++launches;
+    }
+    ESR_CUDA(cudaEventRecord(ev_out_ready, stream));
+    ESR_CUDA(cudaStreamWaitEvent(copy_stream, ev_out_ready, 0));
+    for (int i = 0; i < n; ++i)
+      ESR_CUDA(cudaMemcpyAsync(out[i], st_out.p + 4 * h_jobs_out.p[i].stage_row,
+                               (size_t)4 * h_jobs_out.p[i].n_cells * sizeof(float), cudaMemcpyDeviceToHost,
+                               copy_stream));
+    ESR_CUDA(cudaEventRecord(ev_out_done, copy_stream));
+    ESR_CUDA(cudaGetLastError());
+    return ESR_OK;
+  }
+  int wait_transfers() {
+    if (!copy_stream) return ESR_OK;
+    ESR_CUDA(cudaEventSynchronize(ev_in_ready));
+    ESR_CUDA(cudaEventSynchronize(ev_out_done));
+    return ESR_OK;
+  }
   // Upload the slot table and launch fn(table, grid) once per 65,535 slots
   // (the grid's y limit); grid.x covers the largest mesh. The caller
   // synchronises the stream before the host table goes.
@@ -1663,6 +1830,27 @@ int esr_set_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const
 int esr_get_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out) {
   ESR_GUARD_BEGIN
   return dispatch(solver, [&](auto& s) { return s.get_states(n, slots, out); });
+  ESR_GUARD_END
+}
+int esr_stage_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                        const float* const* W_init) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.stage_in(n, slots, cases, W_init); });
+  ESR_GUARD_END
+}
+int esr_apply_staged(esr_solver* solver) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.apply_staged(); });
+  ESR_GUARD_END
+}
+int esr_fetch_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out) {
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.fetch_states(n, slots, out); });
+  ESR_GUARD_END
+}
+int esr_wait_transfers(esr_solver* solver) {
+  ESR_GUARD_BEGIN
+  return dispatch_any(solver, [&](auto& s) { return s.wait_transfers(); });
   ESR_GUARD_END
 }
 int esr_clear_slot(esr_solver* solver, int32_t slot) {

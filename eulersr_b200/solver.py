@@ -310,6 +310,50 @@ class Solver:
         F.check(fn(self.handle, n, F.ptr(sl, C.c_int32), addr.ctypes.data))
         return out
 
+    # ----------------------------------------------- overlapped transfers
+    def stage_cases(self, slots, cases, fields):
+        """Start uploading float32 fields (C-contiguous (n_cells, 4), pinned
+        memory overlaps) for ``cases`` on ``slots`` and return; the arrays
+        must stay unchanged until ``wait_transfers`` or the next stage_cases.
+        ``apply_staged`` places them."""
+        n = len(slots)
+        if len(cases) != n or len(fields) != n:
+            raise ValueError("stage_cases: slots, cases and fields must have the same length")
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        ncell = self._cells_of_slots(sl)
+        addr = np.zeros(n, dtype=np.uintp)
+        for i, W in enumerate(fields):
+            if W.dtype != np.float32 or W.shape != (ncell[i], 4) or not W.flags.c_contiguous:
+                raise ValueError("stage_cases: fields must be C-contiguous float32 (n_cells, 4) arrays")
+            addr[i] = W.ctypes.data
+        self._staged = (sl, fields)        # kept alive while the copy runs
+        F.check(F.lib().esr_stage_cases_f32(self.handle, n, F.ptr(sl, C.c_int32), self._case_array(cases),
+                                            addr.ctypes.data))
+
+    def apply_staged(self):
+        F.check(F.lib().esr_apply_staged(self.handle))
+
+    def fetch_states(self, slots, out):
+        """Gather the slots' fields after everything issued so far and start
+        copying them into ``out`` (float32, C-contiguous (n_cells, 4)); returns
+        at once. ``wait_transfers`` waits for the copy."""
+        n = len(slots)
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        ncell = self._cells_of_slots(sl)
+        if len(out) != n:
+            raise ValueError("fetch_states: one output array per slot")
+        addr = np.zeros(n, dtype=np.uintp)
+        for i, o in enumerate(out):
+            if o.dtype != np.float32 or o.shape != (ncell[i], 4) or not o.flags.c_contiguous:
+                raise ValueError("fetch_states: outputs must be C-contiguous float32 (n_cells, 4) arrays")
+            addr[i] = o.ctypes.data
+        self._fetching = (sl, out)
+        F.check(F.lib().esr_fetch_states_f32(self.handle, n, F.ptr(sl, C.c_int32), addr.ctypes.data))
+        return out
+
+    def wait_transfers(self):
+        F.check(F.lib().esr_wait_transfers(self.handle))
+
     def set_state(self, slot: int, W):
         W = F.f64(W)
         if W.shape != (self._n_cells(slot), 4):

@@ -243,6 +243,25 @@ int esr_get_states(esr_solver* solver, int32_t n, const int32_t* slots, double* 
 int esr_set_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
                       const float* const* W_init);
 int esr_get_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out);
+/* The same moves overlapped with the solver's work, for pipelines that feed
+ * one batch while the previous one runs (the upload of the next cases and
+ * the download of the last fields run on a copy stream of the solver):
+ * esr_stage_cases_f32 checks the cases and starts copying their float32
+ * fields (host memory; page-locked copies overlap) and returns; the fields
+ * must stay unchanged until the copy ends (esr_wait_transfers, or the next
+ * esr_stage_cases_f32). esr_apply_staged places the staged cases in their
+ * slots on the solver's stream (as esr_set_cases_f32 would) without waiting
+ * for them. esr_fetch_states_f32 gathers the slots' fields on the solver's
+ * stream (after everything issued before it) and starts copying them into
+ * out[i], returning at once; esr_wait_transfers waits for every staged and
+ * fetched copy. Results equal esr_set_cases_f32 / esr_get_states_f32 bit for
+ * bit. (Same calls as esr_set_cases / esr_get_state, euler/main.py:28-41 and
+ * the grid loop's np.asarray(W), issued ahead.) */
+int esr_stage_cases_f32(esr_solver* solver, int32_t n, const int32_t* slots, const esr_case* cases,
+                        const float* const* W_init);
+int esr_apply_staged(esr_solver* solver);
+int esr_fetch_states_f32(esr_solver* solver, int32_t n, const int32_t* slots, float* const* out);
+int esr_wait_transfers(esr_solver* solver);
 /* Slot `slot` restarts from state W (caller's cell order): stop-rule counters
  * reset and dt recomputed from W, as esr_set_case with W_init does. */
 int esr_set_state(esr_solver* solver, int32_t slot, const double* W);
