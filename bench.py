@@ -753,7 +753,7 @@ def main():
     ap.add_argument("--workload", default="warm", choices=["warm", "naca", "ragged", "diamond"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"], help="diamond workload only")
     ap.add_argument("--n-train", type=int, default=256, help="warm workload: training cases")
-    ap.add_argument("--n-eval", type=int, default=64, help="warm workload: held-out cases per GPU")
+    ap.add_argument("--n-eval", type=int, default=128, help="warm workload: held-out cases per GPU")
     ap.add_argument("--slots", type=int, default=32, help="warm workload: HR case slots")
     ap.add_argument("--max-steps", type=int, default=12000, help="warm workload: step cap of an HR solve")
     ap.add_argument("--target-steps", type=int, default=12000, help="warm workload: steps of a training target")

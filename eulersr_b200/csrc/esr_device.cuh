@@ -258,51 +258,6 @@ __device__ __forceinline__ void hllc(const V4<T>& WL, const T PL[4], const V4<T>
   }
 }
 
-// float32 HLLC from the face primitives alone: the same arithmetic as the
-// fast branch of hllc() with the conserved variables formed only for the side
-// the wave fan selects (bitwise the same flux).
-template <typename T>
-__device__ __forceinline__ void hllc_fast(const T PL[4], const T PR[4], T nx, T ny, const Consts<T>& k, T F[4]) {
-  const T rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
-  const T rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
-  const T unL = uL * nx + vL * ny;
-  const T unR = uR * nx + vR * ny;
-  const T tx = -ny, ty = nx;
-  const T aL = sqrt(fabs(dv<T>(k.gamma * pL, rL)));
-  const T aR = sqrt(fabs(dv<T>(k.gamma * pR, rR)));
-  T SL = fmin(unL - aL, unR - aR);
-  T SR = fmax(unL + aL, unR + aR);
-  if (SL == SR) SL = SL - k.ss_eps;
-  if (SL == SR) SR = SR + k.ss_eps;
-  T den = rL * (SL - unL) - rR * (SR - unR);
-  if (den == T(0)) den = k.den_eps;
-  const T Ss = dv<T>(pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR), den);
-  const T PsL = pL + rL * (SL - unL) * (Ss - unL);
-  const T PsR = pR + rR * (SR - unR) * (Ss - unR);
-  const T Ps = k.half * (PsL + PsR);
-  const bool c1 = SL >= T(0);
-  const bool c2 = (SL <= T(0)) && (Ss >= T(0));
-  const bool c3 = (Ss <= T(0)) && (SR >= T(0));
-  const bool left = c1 || c2;
-  const T rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
-  const T unK = left ? unL : unR, SK = left ? SL : SR;
-  const T EK = pK * k.inv_gm1 + k.half * rK * (uK * uK + vK * vK);   // cons() of the selected side
-  const T FK0 = rK * unK, FK1 = rK * uK * unK + pK * nx, FK2 = rK * vK * unK + pK * ny, FK3 = (EK + pK) * unK;
-  if (left ? !c1 : c3) {
-    const T utK = uK * tx + vK * ty;
-    const T inv = __fdividef(1.0f, SK - Ss);
-    const T rs = rK * (SK - unK) * inv;
-    const T Us3 = ((SK - unK) * EK - pK * unK + Ps * Ss) * inv;
-    const T Us1 = rs * (Ss * nx + utK * tx), Us2 = rs * (Ss * ny + utK * ty);
-    F[0] = FK0 + SK * (rs - rK);
-    F[1] = FK1 + SK * (Us1 - rK * uK);
-    F[2] = FK2 + SK * (Us2 - rK * vK);
-    F[3] = FK3 + SK * (Us3 - EK);
-  } else {
-    F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
-  }
-}
-
 // euler_solver.py:203-240 Rusanov (plain branch) inside getFlux
 template <typename T, bool FAST = (sizeof(T) == 4)>
 __device__ __forceinline__ void rusanov(const V4<T>& WL, const T PL[4], const V4<T>& WR, const T PR[4],
@@ -490,6 +445,126 @@ __global__ void k_grad_export(const Seg<T>* __restrict__ segs, int seg, int b, c
 // ----------------------------------------------------------------- K2 flux
 enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
 
+// ---- the fast float32 face flux and cell update with every rounding written
+// out (__fmul_rn / __fadd_rn / __fsub_rn / __fmaf_rn are never fused or
+// split by the compiler), so the per-cell K2 and K2 by patches, which reach
+// the same faces from different code, round every face flux and every cell
+// update identically: a case's result does not depend on which K2 ran.
+namespace xr {
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// helper.py:37-46 (M = 1)
+__device__ __forceinline__ void prim(const float4& W, float gm1, float half, float P[4]) {
+  const float r = W.x, ri = __fdividef(1.0f, r);
+  const float u = mul(W.y, ri), v = mul(W.z, ri);
+  P[0] = r; P[1] = u; P[2] = v;
+  P[3] = mul(sub(W.w, mul(mul(half, r), fma(u, u, mul(v, v)))), gm1);
+}
+// helper.py:25-35 (M = 1)
+__device__ __forceinline__ float4 cons(const float P[4], float inv_gm1, float half) {
+  const float r = P[0], u = P[1], v = P[2];
+  return make_float4(r, mul(r, u), mul(r, v), fma(mul(half, r), fma(u, u, mul(v, v)), mul(P[3], inv_gm1)));
+}
+// helper.py:233-256 boundary states, as primitives of the ghost (gamma 1.4)
+__device__ __forceinline__ void ghost_prim(int kind, const float4& Wc, float nx, float ny, const float4& inlet,
+                                           const Consts<float>& k, float Q[4]) {
+  float P[4];
+  if (kind == K_INLET) { prim(inlet, k.gm1, k.half, Q); return; }
+  if (kind != K_WALL && kind != K_SUBSONIC) { prim(Wc, k.gm1, k.half, Q); return; }   // outlet
+  prim(Wc, k.gm1_14, k.half, P);
+  float G[4];
+  if (kind == K_WALL) {       // helper.py:196-204
+    const float t = mul(2.0f, fma(P[1], nx, mul(P[2], ny)));
+    G[0] = P[0]; G[1] = sub(P[1], mul(t, nx)); G[2] = sub(P[2], mul(t, ny)); G[3] = P[3];
+  } else {                    // helper.py:179-194
+    G[0] = k.sub_rho; G[1] = k.sub_u; G[2] = k.sub_v; G[3] = P[3];
+  }
+  prim(cons(G, k.inv_gm1_14, k.half), k.gm1, k.half, Q);
+}
+// euler_solver.py:273-374 HLLC flux from the face primitives, the conserved
+// variables formed only for the side the wave fan selects
+__device__ __forceinline__ void hllc(const float PL[4], const float PR[4], float nx, float ny,
+                                     const Consts<float>& k, float F[4]) {
+  const float rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
+  const float rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
+  const float unL = fma(uL, nx, mul(vL, ny)), unR = fma(uR, nx, mul(vR, ny));
+  const float tx = -ny, ty = nx;
+  const float aL = sqrtf(fabsf(__fdividef(mul(k.gamma, pL), rL)));
+  const float aR = sqrtf(fabsf(__fdividef(mul(k.gamma, pR), rR)));
+  float SL = fminf(sub(unL, aL), sub(unR, aR));
+  float SR = fmaxf(add(unL, aL), add(unR, aR));
+  if (SL == SR) SL = sub(SL, k.ss_eps);
+  if (SL == SR) SR = add(SR, k.ss_eps);
+  const float dL = sub(SL, unL), dR = sub(SR, unR);
+  float den = sub(mul(rL, dL), mul(rR, dR));
+  if (den == 0.0f) den = k.den_eps;
+  const float Ss = __fdividef(sub(fma(mul(rL, unL), dL, sub(pR, pL)), mul(mul(rR, unR), dR)), den);
+  const float PsL = fma(mul(rL, dL), sub(Ss, unL), pL);
+  const float PsR = fma(mul(rR, dR), sub(Ss, unR), pR);
+  const float Ps = mul(k.half, add(PsL, PsR));
+  const bool c1 = SL >= 0.0f;
+  const bool c2 = (SL <= 0.0f) && (Ss >= 0.0f);
+  const bool c3 = (Ss <= 0.0f) && (SR >= 0.0f);
+  const bool left = c1 || c2;
+  const float rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
+  const float unK = left ? unL : unR, SK = left ? SL : SR, dK = left ? dL : dR;
+  const float EK = fma(mul(k.half, rK), fma(uK, uK, mul(vK, vK)), mul(pK, k.inv_gm1));
+  const float ruK = mul(rK, uK), rvK = mul(rK, vK);
+  const float FK0 = mul(rK, unK), FK1 = fma(pK, nx, mul(ruK, unK)), FK2 = fma(pK, ny, mul(rvK, unK));
+  const float FK3 = mul(add(EK, pK), unK);
+  if (left ? !c1 : c3) {
+    const float inv = __fdividef(1.0f, sub(SK, Ss));
+    const float rs = mul(mul(rK, dK), inv);
+    const float Us3 = mul(fma(Ps, Ss, sub(mul(dK, EK), mul(pK, unK))), inv);
+    const float utK = fma(uK, tx, mul(vK, ty));
+    const float Us1 = mul(rs, fma(Ss, nx, mul(utK, tx))), Us2 = mul(rs, fma(Ss, ny, mul(utK, ty)));
+    F[0] = fma(SK, sub(rs, rK), FK0);
+    F[1] = fma(SK, sub(Us1, ruK), FK1);
+    F[2] = fma(SK, sub(Us2, rvK), FK2);
+    F[3] = fma(SK, sub(Us3, EK), FK3);
+  } else {
+    F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
+  }
+}
+// the canonical flux of a face through the cell's edge of outward normal n:
+// evaluated from the face's owner (the lower cell), negated on the other side
+__device__ __forceinline__ void face_flux(const float qOwn[4], const float qOther[4], float nx, float ny,
+                                          bool other_owns, const Consts<float>& k, float F[4]) {
+  if (other_owns) {
+    hllc(qOther, qOwn, -nx, -ny, k, F);
+    F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
+  } else {
+    hllc(qOwn, qOther, nx, ny, k, F);
+  }
+}
+// sum_k s_k F_k in slot order: face k's term added to acc
+__device__ __forceinline__ void accumulate(int k, float sk, const float F[4], float acc[4]) {
+  if (k == 0) { acc[0] = mul(sk, F[0]); acc[1] = mul(sk, F[1]); acc[2] = mul(sk, F[2]); acc[3] = mul(sk, F[3]); }
+  else { acc[0] = fma(sk, F[0], acc[0]); acc[1] = fma(sk, F[1], acc[1]); acc[2] = fma(sk, F[2], acc[2]); acc[3] = fma(sk, F[3], acc[3]); }
+}
+// euler_solver.py:602-643: residual acc / area - sponge and the stage update
+template <int STAGE>
+__device__ __forceinline__ float4 cell_update(const float acc[4], float area, float sig, const float4& inlet,
+                                              const float4& Wc, const float4& W0, float dt, float half,
+                                              float* R0_out) {
+  const float R0 = sub(__fdividef(acc[0], area), mul(sig, sub(inlet.x, Wc.x)));
+  const float R1 = sub(__fdividef(acc[1], area), mul(sig, sub(inlet.y, Wc.y)));
+  const float R2 = sub(__fdividef(acc[2], area), mul(sig, sub(inlet.z, Wc.z)));
+  const float R3 = sub(__fdividef(acc[3], area), mul(sig, sub(inlet.w, Wc.w)));
+  *R0_out = R0;
+  const float m = -dt;
+  if (STAGE == ST_FIRST) return make_float4(fma(m, R0, Wc.x), fma(m, R1, Wc.y), fma(m, R2, Wc.z), fma(m, R3, Wc.w));
+  if (STAGE == ST_SRK2_SECOND)
+    return make_float4(mul(half, fma(m, R0, add(W0.x, Wc.x))), mul(half, fma(m, R1, add(W0.y, Wc.y))),
+                       mul(half, fma(m, R2, add(W0.z, Wc.z))), mul(half, fma(m, R3, add(W0.w, Wc.w))));
+  return make_float4(mul(half, add(fma(m, R0, W0.x), Wc.x)), mul(half, add(fma(m, R1, W0.y), Wc.y)),
+                     mul(half, add(fma(m, R2, W0.z), Wc.z)), mul(half, add(fma(m, R3, W0.w), Wc.w)));
+}
+}  // namespace xr
+
 // euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
 // then the stage update of :630-653.
 template <typename T, bool FAST, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
@@ -514,88 +589,107 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
   const V4<T> inlet = cs.inlet[g];
   T gk[12];   // normals, face lengths, area, blend (groups 0-2)
   geo_groups<T, 3>(s, c, 0, gk);
-  T acc[4];
+  if constexpr (kFastPath<T, FAST> && MUSCL && FLUX == 0) {
+    // fast float32 HLLC + MUSCL: canonical face fluxes and the cell update
+    // rounded exactly as K2 by patches rounds them
+    float acc[4];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const int kind = slot_kind(nb.w, k);
-    const T nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
-    V4<T> WL, WR;
-    T PL[4], PR[4];
-    if (MUSCL) {
-      const V4<T> fl = FV[(long long)k * total + gi];
-      T qL[4] = {fl.x, fl.y, fl.z, fl.w};
-      T qR[4];
+    for (int k = 0; k < 3; ++k) {
+      const int kind = slot_kind(nb.w, k);
+      const float nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
+      const float4 fl = FV[(long long)k * total + gi];
+      const float qL[4] = {fl.x, fl.y, fl.z, fl.w};
+      float qR[4];
       if (kind == K_INTERIOR) {
-        const V4<T> fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)nbk[k] * s.B + b];
+        const float4 fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)nbk[k] * s.B + b];
         qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
       } else {
-        prim<T, FAST>(ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+        xr::ghost_prim(kind, Wc, nx, ny, inlet, kc, qR);
       }
-      if constexpr (kFastPath<T, FAST>) {
-        // float32: the face primitives are used as reconstructed (the
-        // reference converts them to conserved and back, a rounding-level
-        // step); HLLC forms the conserved state of the selected side itself
-#pragma unroll
-        for (int v = 0; v < 4; ++v) { PL[v] = qL[v]; PR[v] = qR[v]; }
-        if (FLUX != 0) {
+      float F[4];
+      xr::face_flux(qL, qR, nx, ny, kind == K_INTERIOR && nbk[k] < c, kc, F);
+      xr::accumulate(k, gk[G_S0 + k], F, acc);
+    }
+    const float sig = xr::mul(cs.strength[g], gk[G_BLEND3]);
+    const float dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+    const float4 W0 = (STAGE == ST_FIRST) ? Wc : Wbase[gi];
+    float R0;
+    const float4 o = xr::cell_update<STAGE>(acc, gk[G_AREA], sig, inlet, Wc, W0, dt, kc.half, &R0);
+    if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
+    Wout[gi] = o;
+  } else {
+    T acc[4];
+  #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int kind = slot_kind(nb.w, k);
+      const T nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
+      V4<T> WL, WR;
+      T PL[4], PR[4];
+      if (MUSCL) {
+        const V4<T> fl = FV[(long long)k * total + gi];
+        T qL[4] = {fl.x, fl.y, fl.z, fl.w};
+        T qR[4];
+        if (kind == K_INTERIOR) {
+          const V4<T> fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)nbk[k] * s.B + b];
+          qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
+        } else {
+          prim<T, FAST>(ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+        }
+        if constexpr (kFastPath<T, FAST>) {
+          // float32: the face primitives are used as reconstructed (the
+          // reference converts them to conserved and back, a rounding-level
+          // step); HLLC forms the conserved state of the selected side itself
+  #pragma unroll
+          for (int v = 0; v < 4; ++v) { PL[v] = qL[v]; PR[v] = qR[v]; }
+          if (FLUX != 0) {
+            WL = cons<T, FAST>(qL, kc.gm1, kc.inv_gm1, kc.half);
+            WR = cons<T, FAST>(qR, kc.gm1, kc.inv_gm1, kc.half);
+          }
+        } else {
           WL = cons<T, FAST>(qL, kc.gm1, kc.inv_gm1, kc.half);
           WR = cons<T, FAST>(qR, kc.gm1, kc.inv_gm1, kc.half);
+          prim<T, FAST>(WL, kc.gm1, kc.half, PL);
+          prim<T, FAST>(WR, kc.gm1, kc.half, PR);
         }
       } else {
-        WL = cons<T, FAST>(qL, kc.gm1, kc.inv_gm1, kc.half);
-        WR = cons<T, FAST>(qR, kc.gm1, kc.inv_gm1, kc.half);
+        WL = Wc;
+        WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc);
         prim<T, FAST>(WL, kc.gm1, kc.half, PL);
         prim<T, FAST>(WR, kc.gm1, kc.half, PR);
       }
-    } else {
-      WL = Wc;
-      WR = (kind == K_INTERIOR) ? Win[s.off + (long long)nbk[k] * s.B + b] : ghost_cons<T, FAST>(kind, Wc, nx, ny, inlet, kc);
-      prim<T, FAST>(WL, kc.gm1, kc.half, PL);
-      prim<T, FAST>(WR, kc.gm1, kc.half, PR);
-    }
-    T F[4];
-    if (FLUX == 0) {
-      if constexpr (kFastPath<T, FAST> && MUSCL) {
-        // the face's canonical flux: evaluated from its owner (the lower
-        // cell), negated on the other side, as the patch kernel forms it
-        if (kind == K_INTERIOR && nbk[k] < c) {
-          hllc_fast<T>(PR, PL, -nx, -ny, kc, F);
-          F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
-        } else {
-          hllc_fast<T>(PL, PR, nx, ny, kc, F);
-        }
-      } else {
+      T F[4];
+      if (FLUX == 0) {
         hllc<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
+      } else {
+        rusanov<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
       }
-    } else {
-      rusanov<T, FAST>(WL, PL, WR, PR, nx, ny, kc, F);
+      const T sk = gk[G_S0 + k];
+      if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
+      else { acc[0] = acc[0] + sk * F[0]; acc[1] = acc[1] + sk * F[1]; acc[2] = acc[2] + sk * F[2]; acc[3] = acc[3] + sk * F[3]; }
     }
-    const T sk = gk[G_S0 + k];
-    if (k == 0) { acc[0] = sk * F[0]; acc[1] = sk * F[1]; acc[2] = sk * F[2]; acc[3] = sk * F[3]; }
-    else { acc[0] = acc[0] + sk * F[0]; acc[1] = acc[1] + sk * F[1]; acc[2] = acc[2] + sk * F[2]; acc[3] = acc[3] + sk * F[3]; }
+    const T area = gk[G_AREA];
+    const T sig = cs.strength[g] * gk[G_BLEND3];
+    const T R0 = dv<T, FAST>(acc[0], area) - sig * (inlet.x - Wc.x);
+    const T R1 = dv<T, FAST>(acc[1], area) - sig * (inlet.y - Wc.y);
+    const T R2 = dv<T, FAST>(acc[2], area) - sig * (inlet.z - Wc.z);
+    const T R3 = dv<T, FAST>(acc[3], area) - sig * (inlet.w - Wc.w);
+    const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+    // density residual of the state the step starts from (density-L2 stop rule)
+    if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
+    V4<T> o;
+    if (STAGE == ST_FIRST) {
+      o = mk4<T>(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
+    } else if (STAGE == ST_SRK2_SECOND) {
+      const V4<T> W0 = Wbase[gi];
+      o = mk4<T>(kc.half * (W0.x + Wc.x - dt * R0), kc.half * (W0.y + Wc.y - dt * R1),
+                 kc.half * (W0.z + Wc.z - dt * R2), kc.half * (W0.w + Wc.w - dt * R3));
+    } else {
+      const V4<T> W0 = Wbase[gi];
+      o = mk4<T>(kc.half * (W0.x - dt * R0 + Wc.x), kc.half * (W0.y - dt * R1 + Wc.y),
+                 kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
+    }
+    Wout[gi] = o;
   }
-  const T area = gk[G_AREA];
-  const T sig = cs.strength[g] * gk[G_BLEND3];
-  const T R0 = dv<T, FAST>(acc[0], area) - sig * (inlet.x - Wc.x);
-  const T R1 = dv<T, FAST>(acc[1], area) - sig * (inlet.y - Wc.y);
-  const T R2 = dv<T, FAST>(acc[2], area) - sig * (inlet.z - Wc.z);
-  const T R3 = dv<T, FAST>(acc[3], area) - sig * (inlet.w - Wc.w);
-  const T dt = LOCALDT ? dt_local[gi] : cs.dt[g];
-  // density residual of the state the step starts from (density-L2 stop rule)
-  if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
-  V4<T> o;
-  if (STAGE == ST_FIRST) {
-    o = mk4<T>(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
-  } else if (STAGE == ST_SRK2_SECOND) {
-    const V4<T> W0 = Wbase[gi];
-    o = mk4<T>(kc.half * (W0.x + Wc.x - dt * R0), kc.half * (W0.y + Wc.y - dt * R1),
-               kc.half * (W0.z + Wc.z - dt * R2), kc.half * (W0.w + Wc.w - dt * R3));
-  } else {
-    const V4<T> W0 = Wbase[gi];
-    o = mk4<T>(kc.half * (W0.x - dt * R0 + Wc.x), kc.half * (W0.y - dt * R1 + Wc.y),
-               kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
-  }
-  Wout[gi] = o;
 }
 
 // ----------------------------------------------------- K2 by patches (float32)
@@ -656,16 +750,11 @@ __global__ void __launch_bounds__(32 * kPatchWarps, 4) k_flux_patch(const Seg<fl
             const float4 fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)j * s.B + b];
             qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
           } else {
-            prim<float>(ghost_cons<float>(kind, Win[gi], nx, ny, inlet, kc), kc.gm1, kc.half, qR);
+            xr::ghost_prim(kind, Win[gi], nx, ny, inlet, kc, qR);
           }
         }
         float F[4];
-        if (kind == K_INTERIOR && j < c) {     // owner outside the patch: its side, negated
-          hllc_fast<float>(qR, qL, -nx, -ny, kc, F);
-          F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
-        } else {
-          hllc_fast<float>(qL, qR, nx, ny, kc, F);
-        }
+        xr::face_flux(qL, qR, nx, ny, kind == K_INTERIOR && j < c, kc, F);   // owner outside: its side, negated
         G[lc][k][lane] = make_float4(F[0], F[1], F[2], F[3]);
         if (inner) G[j - c0][slot_opp(nb.w, k)][lane] = make_float4(-F[0], -F[1], -F[2], -F[3]);
       }
@@ -683,30 +772,15 @@ __global__ void __launch_bounds__(32 * kPatchWarps, 4) k_flux_patch(const Seg<fl
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const float4 f = G[lc][k][lane];
-      const float sk = gk[G_S0 + k];
-      if (k == 0) { acc[0] = sk * f.x; acc[1] = sk * f.y; acc[2] = sk * f.z; acc[3] = sk * f.w; }
-      else { acc[0] = acc[0] + sk * f.x; acc[1] = acc[1] + sk * f.y; acc[2] = acc[2] + sk * f.z; acc[3] = acc[3] + sk * f.w; }
+      const float F[4] = {f.x, f.y, f.z, f.w};
+      xr::accumulate(k, gk[G_S0 + k], F, acc);
     }
-    const float area = gk[G_AREA];
-    const float sig = cs.strength[g] * gk[G_BLEND3];
-    const float R0 = dv<float>(acc[0], area) - sig * (inlet.x - Wc.x);
-    const float R1 = dv<float>(acc[1], area) - sig * (inlet.y - Wc.y);
-    const float R2 = dv<float>(acc[2], area) - sig * (inlet.z - Wc.z);
-    const float R3 = dv<float>(acc[3], area) - sig * (inlet.w - Wc.w);
+    const float sig = xr::mul(cs.strength[g], gk[G_BLEND3]);
     const float dt = LOCALDT ? dt_local[gi] : cs.dt[g];
+    const float4 W0 = (STAGE == ST_FIRST) ? Wc : Wbase[gi];
+    float R0;
+    const float4 o = xr::cell_update<STAGE>(acc, gk[G_AREA], sig, inlet, Wc, W0, dt, kc.half, &R0);
     if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
-    float4 o;
-    if (STAGE == ST_FIRST) {
-      o = make_float4(Wc.x - dt * R0, Wc.y - dt * R1, Wc.z - dt * R2, Wc.w - dt * R3);
-    } else if (STAGE == ST_SRK2_SECOND) {
-      const float4 W0 = Wbase[gi];
-      o = make_float4(kc.half * (W0.x + Wc.x - dt * R0), kc.half * (W0.y + Wc.y - dt * R1),
-                      kc.half * (W0.z + Wc.z - dt * R2), kc.half * (W0.w + Wc.w - dt * R3));
-    } else {
-      const float4 W0 = Wbase[gi];
-      o = make_float4(kc.half * (W0.x - dt * R0 + Wc.x), kc.half * (W0.y - dt * R1 + Wc.y),
-                      kc.half * (W0.z - dt * R2 + Wc.z), kc.half * (W0.w - dt * R3 + Wc.w));
-    }
     Wout[gi] = o;
   }
 }
