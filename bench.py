@@ -366,7 +366,7 @@ def run_throughput(args, world, rank, local, report=True):
         cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=1e9, dtype=np.float32)
                  for k, p in enumerate(per) for m, a in p]
         s = Solver([DeviceMesh(m) for m in meshes], [len(p) for p in per], precision="f32",
-                   device=local if world > 1 else 0)
+                   device=local if world > 1 else 0, block_size=args.block)
         mesh = (meshes, per)
         items = sum(m.n_cells * len(p) for m, p in zip(meshes, per))
         B, N = len(cases), items / len(cases)       # N: mean cells per case
@@ -381,7 +381,8 @@ def run_throughput(args, world, rank, local, report=True):
         mach, aoa = mach_all[mine], aoa_all[mine]
         cases = [FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9, dtype=np.float32)
                  for m, a in zip(mach, aoa)]
-        s = Solver(DeviceMesh(mesh), len(cases), precision="f32", device=local if world > 1 else 0)
+        s = Solver(DeviceMesh(mesh), len(cases), precision="f32", device=local if world > 1 else 0,
+                   block_size=args.block)
         B, N = len(cases), mesh.n_cells
         cpu_mesh = mesh
         shard_note = "parallel.shard_cases (cost-balanced LPT)"
@@ -759,7 +760,9 @@ def main():
     ap.add_argument("--target-steps", type=int, default=12000, help="warm workload: steps of a training target")
     ap.add_argument("--train-steps", type=int, default=2000, help="warm workload: MLP training steps")
     ap.add_argument("--make-truth", action="store_true", help="write the held-out cases' reference CDs and exit")
+    ap.add_argument("--block", default="0", help="throughput workloads: 0 (autotuned), 64, 128, 256 or patches")
     args = ap.parse_args()
+    args.block = args.block if args.block == "patches" else int(args.block)
     args.warmup = max(3, args.warmup)
 
     if args.impl == "reference":
