@@ -138,3 +138,50 @@ def test_cpu_converged_sample_rule(diamond02):
         [{"mach": 2.5, "aoa": 5.0, "cd": cd100, "steady": True}], 1e9, diamond02, cd_tol=0.2, patience=2,
         max_steps=400)
     assert recs[0]["steps"] <= 400 and thr >= 1
+
+
+def _shard_rank_main(rank, world, port, q):
+    import os
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from eulersr_b200.parallel import case_cost
+        args = types.SimpleNamespace(n_train=32, n_eval=16)
+        idx, me, ae = bench.warm_cases(args, world, rank)
+        n = bench.allreduce_sum(float(len(idx)), world)
+        cmax = bench.allreduce_max(float(case_cost(me).sum()), world)
+        csum = bench.allreduce_sum(float(case_cost(me).sum()), world)
+        got = [None] * world
+        dist.all_gather_object(got, sorted(int(i) for i in idx))
+        q.put((rank, n, cmax, csum, got))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_warm_shards_over_two_gloo_ranks():
+    """Under two ranks (gloo here, NCCL on GPUs) the held-out draws are dealt
+    by the cost-balanced scheduler: every draw to exactly one rank, the
+    slowest rank's estimated cost within one case of the mean."""
+    import multiprocessing as mp
+    import socket
+    from eulersr_b200.parallel import case_cost
+    from eulersr_b200.warmstart.pipeline import draw_cases
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, n, cmax, csum, got), _ = out
+    assert n == 32
+    assert sorted(got[0] + got[1]) == list(range(32))
+    _, (me, _) = draw_cases(32, 32, seed=3)
+    assert cmax - csum / 2 <= case_cost(me).max()
