@@ -49,6 +49,8 @@ struct Seg {                 // one mesh and its B case slots
   const T* wall_ds;          // face length
   const LsqRef* lsq;         // per-cell least-squares data (reference-fidelity float32 only)
   const int* patch_start;    // first cell of every patch of the renumbering (+ n_cells)
+  const int4* live;          // (A, magic, shift, -): slots 0..A-1 may hold running cases (A = B
+                             // until a batch's queue is empty and its running cases are packed)
   int n_patches;
   int n_wall;
   int b_shift;               // item / B = (umulhi(item, b_magic) + item) >> b_shift
@@ -61,6 +63,25 @@ struct Seg {                 // one mesh and its B case slots
 template <typename T>
 __device__ __forceinline__ int cell_of(const Seg<T>& s, int item) {
   return (int)((__umulhi((unsigned)item, s.b_magic) + (unsigned)item) >> s.b_shift);
+}
+
+// cell and slot of thread item `item` of segment s: items walk (cell, slot)
+// over the first A slots of every cell, A = live slots (B until a batch's
+// queue drains and compaction packs its running cases into slots 0..A-1),
+// so once few cases remain the work lands on few warps with full lanes
+template <typename T>
+__device__ __forceinline__ bool item_slot(const Seg<T>& s, int item, int& c, int& b) {
+  const int4 L = *s.live;
+  if (L.x == s.B) {
+    if (item >= s.n_cells * s.B) return false;
+    c = cell_of(s, item);
+    b = item - c * s.B;
+  } else {
+    if (item >= s.n_cells * L.x) return false;
+    c = (int)divide((unsigned)item, Divider{(unsigned)L.y, L.z});
+    b = item - c * L.x;
+  }
+  return true;
 }
 
 // Which segment and first item a block of the cell kernels covers. A
@@ -304,13 +325,11 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? (LOCALDT ? ESR_K1_MI
   Seg<T> s;
   int first;
   block_origin(bm, s, first);
-  const int item = first + threadIdx.x;
-  if (item >= s.n_cells * s.B) return;
-  const int c = cell_of(s, item);
-  const int b = item - c * s.B;
+  int c, b;
+  if (!item_slot(s, first + threadIdx.x, c, b)) return;
   const int g = s.case0 + b;
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
-  const long long gi = s.off + item;
+  const long long gi = s.off + (long long)c * s.B + b;
   const V4<T> Wc = W[gi];
   T Pc[4];
   prim<T, FAST>(Wc, kc.gm1, kc.half, Pc);
@@ -576,13 +595,11 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
   Seg<T> s;
   int first;
   block_origin(bm, s, first);
-  const int item = first + threadIdx.x;
-  if (item >= s.n_cells * s.B) return;
-  const int c = cell_of(s, item);
-  const int b = item - c * s.B;
+  int c, b;
+  if (!item_slot(s, first + threadIdx.x, c, b)) return;
   const int g = s.case0 + b;
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
-  const long long gi = s.off + item;
+  const long long gi = s.off + (long long)c * s.B + b;
   const V4<T> Wc = Win[gi];
   const int4 nb = __ldg(s.nbr + c);
   const int nbk[3] = {nb.x, nb.y, nb.z};
@@ -703,10 +720,13 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
 // cell's residual sum_k s_k F_k in slot order from shared memory (a
 // deterministic cell-owned sum, no atomics), then the sponge and the stage
 // update as k_flux. The fluxes equal k_flux's bit for bit.
+#ifndef ESR_PATCH_MINB
+#define ESR_PATCH_MINB 4
+#endif
 constexpr int kPatchWarps = 8;
 
 template <int STAGE, bool LOCALDT>
-__global__ void __launch_bounds__(32 * kPatchWarps, 4) k_flux_patch(const Seg<float>* __restrict__ segs,
+__global__ void __launch_bounds__(32 * kPatchWarps, ESR_PATCH_MINB) k_flux_patch(const Seg<float>* __restrict__ segs,
                                                                   const int4* __restrict__ pblk,
                                                                   const float4* __restrict__ Win,
                                                                   const float4* __restrict__ Wbase,
@@ -1280,12 +1300,21 @@ __global__ void k_init_slots(const SlotInit<T>* __restrict__ si, int n, SlotPara
 // once in the step kernels. One thread per mesh pairs the lowest free slot
 // with the highest running one; move_src[dst] = src, -1 elsewhere.
 template <typename T>
-__global__ void k_compact_plan(const Seg<T>* __restrict__ segs, int n_segs, Queue<T> q, int* __restrict__ move_src) {
+__global__ void k_compact_plan(const Seg<T>* __restrict__ segs, int n_segs, Queue<T> q, int* __restrict__ move_src,
+                               int4* __restrict__ live) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n_segs) return;
   const Seg<T> s = segs[m];
   for (int b = 0; b < s.B; ++b) move_src[s.case0 + b] = -1;
-  if (q.qhead[m] < q.qoff[m + 1] - q.qoff[m]) return;   // cases still queued: no slot is free
+  if (q.qhead[m] < q.qoff[m + 1] - q.qoff[m]) {   // cases still queued: no slot is free
+    live[m] = make_int4(s.B, (int)s.b_magic, s.b_shift, 0);
+    return;
+  }
+  // after the moves the running cases fill slots 0..A-1: the step kernels walk those alone
+  int running = 0;
+  for (int b = 0; b < s.B; ++b) running += q.slot_case[s.case0 + b] >= 0;
+  const Divider d = make_divider((unsigned)max(running, 1));
+  live[m] = make_int4(running, (int)d.magic, d.shift, 0);
   int lo = 0, hi = s.B - 1;
   for (;;) {
     while (lo < hi && q.slot_case[s.case0 + lo] >= 0) ++lo;

@@ -123,6 +123,8 @@ struct SolverT : SolverBase {
   DevBuf<Seg<T>> d_segs;
   DevBuf<int2> d_blk;
   int n_blk = 0;
+  DevBuf<int4> d_live;   // per mesh segment: live slots (A, divider of A)
+  std::vector<int4> h_live_full;   // A = B for every segment
   DevBuf<int4> d_pblk;   // K2 by patches: (mesh segment, patch, first slot) per block
   int n_pblk = 0;
   bool use_patch = false;
@@ -317,9 +319,13 @@ struct SolverT : SolverBase {
       s.patch_start = md.patch.p;
       s.n_patches = (int)hm.patch_start.size() - 1;
       ESR_TRY(set_divider(s));
+      h_live_full.push_back(make_int4(s.B, (int)s.b_magic, s.b_shift, 0));
       hsegs.push_back(s);
       for (int b = 0; b < md.B; ++b) { hseg_of[md.case0 + b] = m; hslot_of[md.case0 + b] = b; hnc[md.case0 + b] = N; }
     }
+    ESR_TRY(d_live.alloc(hsegs.size()));
+    ESR_CUDA(cudaMemcpy(d_live.p, h_live_full.data(), hsegs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    for (size_t m = 0; m < hsegs.size(); ++m) hsegs[m].live = d_live.p + m;
     ESR_TRY(d_segs.alloc(hsegs.size()));
     ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
     hseg0 = hsegs[0];
@@ -376,17 +382,13 @@ struct SolverT : SolverBase {
   // l = ceil(log2 B), m = floor(2^32 (2^l - B) / B) + 1 (exact for n < 2^31)
   static int set_divider(Seg<T>& s) {
     const uint32_t d = (uint32_t)s.B;
-    int l = 0;
-    while ((1ull << l) < d) ++l;
-    const uint64_t m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
-    if (m > 0xFFFFFFFFull) return fail(ESR_ERR_ARG, "solver: slot count has no 32-bit divider");
-    s.b_magic = (uint32_t)m;
-    s.b_shift = l;
+    const Divider v = make_divider(d);
+    s.b_magic = v.magic;
+    s.b_shift = v.shift;
     const uint64_t items = (uint64_t)s.n_cells * d;
     if (items >= (1ull << 31)) return fail(ESR_ERR_ARG, "solver: cells x slots of one mesh must stay below 2^31");
     for (uint64_t n : {uint64_t(0), uint64_t(d - 1), uint64_t(d), items - 1, items / 2 + 1}) {
-      const uint32_t q = (uint32_t)((((n * s.b_magic) >> 32) + n) >> l);
-      if (n < items && q != n / d) return fail(ESR_ERR_STATE, "solver: item divider check failed");
+      if (n < items && divide((uint32_t)n, v) != n / d) return fail(ESR_ERR_STATE, "solver: item divider check failed");
     }
     return ESR_OK;
   }
@@ -1362,7 +1364,8 @@ struct SolverT : SolverBase {
     k_forces<T><<<n_slots, 256, 0, stream>>>(d_segs.p, cmap(), W.p, qref.p, forces.p, kc, fill.p, eng_track.p);
     k_eng_init<<<nb, tb, 0, stream>>>(ctl(), fill.p, n_slots);
     // pack running cases into the lowest slots once a mesh's queue is empty
-    k_compact_plan<T><<<(int)(meshes.size() + 31) / 32, 32, 0, stream>>>(d_segs.p, (int)meshes.size(), q, move_src.p);
+    k_compact_plan<T><<<(int)(meshes.size() + 31) / 32, 32, 0, stream>>>(d_segs.p, (int)meshes.size(), q, move_src.p,
+                                                                         d_live.p);
     k_compact_items<T><<<g2, 256, 0, stream>>>(d_segs.p, cmap(), move_src.p, W.p, Wref.p);
     k_compact_slots<T><<<nb, tb, 0, stream>>>(move_src.p, n_slots, q, sp, ctl(), forces.p);
     launches += with_states ? 15 : 14;
@@ -1395,6 +1398,8 @@ struct SolverT : SolverBase {
     if (!pend) return ESR_OK;   // nothing pending: nothing changes
     int rc = ESR_OK;
     if (clear_slots && pend->n > 0) cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream);
+    // every slot is a step kernel's again
+    cudaMemcpyAsync(d_live.p, h_live_full.data(), h_live_full.size() * sizeof(int4), cudaMemcpyHostToDevice, stream);
     // nothing of the batch may still run when its buffers are freed
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch_cancel: ") + cudaGetErrorString(e));
@@ -1514,6 +1519,8 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemsetAsync(B.retiring.p, 0, n_slots * sizeof(int), stream));
     ESR_CUDA(cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream));
     ESR_CUDA(cudaMemsetAsync(status.p, 0, n_slots * sizeof(int), stream));
+    ESR_CUDA(cudaMemcpyAsync(d_live.p, h_live_full.data(), h_live_full.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                             stream));
     for (DevBuf<int>* b : {&B.r_status, &B.r_stop, &B.r_steps, &B.r_nmax, &B.r_eng_conv, &B.r_eng_stop})
       ESR_TRY(b->alloc(n));
     for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time, &B.r_probe}) ESR_TRY(b->alloc(n));

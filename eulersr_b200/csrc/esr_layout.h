@@ -32,7 +32,34 @@ static_assert(sizeof(LsqRef) == 64, "one 64-byte record per cell");
 
 // cells per patch of the renumbering: the face-flux kernel of batched float32
 // solves exchanges the fluxes of a patch's inner faces in shared memory
-constexpr int kPatchCells = 32;
+// (kPatchCells x 3 x 32 lanes x 16 B per block)
+#ifndef ESR_PATCH_CELLS
+#define ESR_PATCH_CELLS 32
+#endif
+constexpr int kPatchCells = ESR_PATCH_CELLS;
+
+// n / d without an integer divide for 0 <= n < 2^31: q = (umulhi(n, magic) +
+// n) >> shift with shift = ceil(log2 d), magic = floor(2^32 (2^shift - d) / d)
+// + 1 (d >= 1; magic < 2^32 because 2^(shift-1) < d)
+struct Divider {
+  unsigned magic;
+  int shift;
+};
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline Divider make_divider(unsigned d) {
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  const unsigned long long m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+  return Divider{(unsigned)m, l};
+}
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline unsigned divide(unsigned n, Divider v) {
+  return (unsigned)((((unsigned long long)n * v.magic >> 32) + n) >> v.shift);
+}
 
 // slot kinds (face markers of euler/jax_fvm/src/mesh.py:47-52)
 enum SlotKind { K_INTERIOR = 0, K_WALL = 2, K_INLET = 3, K_OUTLET = 4, K_SUBSONIC = 5 };
