@@ -675,6 +675,23 @@ def run_warm(args, world, rank, local):
         base[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
         base[start + "_detail"] = {"converged": r.converged, "seconds": r.seconds,
                                    "median_iterations": float(np.median(r.iterations)), "parts_s": r.parts_s}
+    # by case class: the cases whose reference settles, alone (the cases that
+    # never settle cost every start the whole step cap)
+    cls = {}
+    keep = np.nonzero(steady)[0]
+    if len(keep):
+        for start in ("mlp", "single"):
+            flush.add_(1.0)
+            barrier(world)
+            r = wf.solve(me[keep], ae[keep], truth[keep], steady[keep], start)
+            cls[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
+    steps_warm = np.array([x["steps"] for x in passes[-1].results])
+    capped = steps_warm >= args.max_steps
+    by_class = {"steady_cases": int(steady.sum()), "unsteady_cases": int((~steady).sum()),
+                "warm_capped_cases": int(capped.sum()),
+                "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
+                "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
+                "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
     # end to end: the pipeline with every case's final HR field read into host memory
     flush.add_(1.0)
     barrier(world)
@@ -729,7 +746,8 @@ def run_warm(args, world, rank, local):
                     "warm_passes": [{"converged": p.converged, "seconds": p.seconds, "parts_s": p.parts_s}
                                     for p in passes[:3]],
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
-                    "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")}},
+                    "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
+                    "by_case_class": by_class},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",

@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
 // deterministic cell-owned sum, no atomics), then the sponge and the stage
 // update as k_flux. The fluxes equal k_flux's bit for bit.
 #ifndef ESR_PATCH_MINB
-#define ESR_PATCH_MINB 4
+#define ESR_PATCH_MINB 5
 #endif
 constexpr int kPatchWarps = 8;
 

@@ -34,7 +34,7 @@ static_assert(sizeof(LsqRef) == 64, "one 64-byte record per cell");
 // solves exchanges the fluxes of a patch's inner faces in shared memory
 // (kPatchCells x 3 x 32 lanes x 16 B per block)
 #ifndef ESR_PATCH_CELLS
-#define ESR_PATCH_CELLS 32
+#define ESR_PATCH_CELLS 24
 #endif
 constexpr int kPatchCells = ESR_PATCH_CELLS;
 

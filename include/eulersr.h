@@ -80,7 +80,7 @@ extern "C" {
 #define ESR_STOP_DENSITY_L2 1  /* RMS over cells of the density residual */
 #define ESR_STOP_ENGINEERING 2 /* stop when the engineering criterion (force coefficients
                                 * within tolerance of given targets) is confirmed */
-#define ESR_BLOCK_PATCHES (-1)  /* esr_params.block_size: K2 by patches of <= 32 cells, each inner
+#define ESR_BLOCK_PATCHES (-1)  /* esr_params.block_size: K2 by patches of <= 24 cells, each inner
                                   * face's flux evaluated once and exchanged in shared memory
                                   * (float32 fast fidelity, HLLC + MUSCL; the fluxes are bitwise
                                   * those of the per-cell K2) */
@@ -198,7 +198,7 @@ int esr_mesh_destroy(esr_mesh* mesh);
 int esr_mesh_get_info(const esr_mesh* mesh, esr_mesh_info* info);
 /* new-to-old cell permutation chosen by the renumbering (n_cells entries) */
 int esr_mesh_get_permutation(const esr_mesh* mesh, int32_t* perm);
-/* The renumbering's patches (at most 32 cells each; the face-flux kernel of
+/* The renumbering's patches (at most 24 cells each; the face-flux kernel of
  * batched float32 solves exchanges the fluxes of a patch's inner faces in
  * shared memory): *n_patches, and when start is not NULL the first new cell
  * of every patch plus n_cells (n_patches + 1 entries). */
