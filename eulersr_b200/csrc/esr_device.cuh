@@ -723,7 +723,10 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
 #ifndef ESR_PATCH_MINB
 #define ESR_PATCH_MINB 5
 #endif
-constexpr int kPatchWarps = 8;
+#ifndef ESR_PATCH_WARPS
+#define ESR_PATCH_WARPS 8
+#endif
+constexpr int kPatchWarps = ESR_PATCH_WARPS;
 
 template <int STAGE, bool LOCALDT>
 __global__ void __launch_bounds__(32 * kPatchWarps, ESR_PATCH_MINB) k_flux_patch(const Seg<float>* __restrict__ segs,
