@@ -692,6 +692,14 @@ def run_warm(args, world, rank, local):
                 "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
                 "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
                 "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
+    # a stream of batches, as a campaign runs them: the next batch's LR solve
+    # and prediction overlap this batch's HR solve
+    flush.add_(1.0)
+    barrier(world)
+    sp, s_sec, s_wall = wf.solve_stream([(me, ae)] * args.steps, [truth] * args.steps, [steady] * args.steps)
+    streamed = {"batches": args.steps, "seconds": s_sec, "wall_s": s_wall,
+                "value": allreduce_sum(float(sum(p.converged for p in sp)), world) / allreduce_max(s_sec, world),
+                "parts_s": [p.parts_s for p in sp[:3]]}
     # end to end: the pipeline with every case's final HR field read into host memory
     flush.add_(1.0)
     barrier(world)
@@ -747,7 +755,7 @@ def run_warm(args, world, rank, local):
                                     for p in passes[:3]],
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
-                    "by_case_class": by_class},
+                    "by_case_class": by_class, "warm_mlp_streamed": streamed},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",

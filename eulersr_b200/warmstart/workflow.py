@@ -179,6 +179,56 @@ class WarmStartWorkflow:
         steady = np.abs(cd - cd_a) <= 1e-3 * np.abs(cd)
         return cd, steady
 
+    # ----------------------------------------------------------- the stream
+    def warm_fields(self, machs, aoas, use_mlp=True):
+        """LR solve, LR pressure gradients and the IDW (+ MLP) prediction of
+        every case: the conserved HR warm fields (float64, HR cell order)."""
+        lr_states, lr_gp = self.lr_solutions(machs, aoas)
+        return [self.ws.predict_state(primitives(W).astype(np.float32), g, m, a, use_mlp=use_mlp)
+                for W, g, m, a in zip(lr_states, lr_gp, machs, aoas)]
+
+    def solve_stream(self, batches, truth_of, steady_of, use_mlp=True):
+        """Warm-started solves of a stream of case batches, as a campaign
+        runs them: batch k+1's LR solve and prediction run while batch k's HR
+        solve does (the HR batch is driven from a second host thread; each
+        solver has its own stream, so the GPU runs both). batches: list of
+        (machs, aoas); truth_of / steady_of: per-batch reference CDs and
+        steady flags. Returns (per-batch PassResult, device seconds of the
+        whole stream, wall seconds)."""
+        import threading
+        out = [None] * len(batches)
+        s = self._hr_solver(min(self.slots, max(len(b[0]) for b in batches)))
+
+        def hr(k, inits, box):
+            try:
+                torch.cuda.set_device(self.device)     # a new host thread starts on device 0
+                m, a = batches[k]
+                t = time.perf_counter()
+                res, _ = s.batch_solve(self._cases(m, a, truth_of[k]), init_fields=inits)
+                box["res"], box["s"] = res, time.perf_counter() - t
+            except BaseException as e:   # re-raised in the caller's thread
+                box["err"] = e
+
+        def run():
+            inits = self.warm_fields(*batches[0], use_mlp=use_mlp)
+            for k in range(len(batches)):
+                box = {}
+                th = threading.Thread(target=hr, args=(k, inits, box))
+                th.start()
+                t = time.perf_counter()
+                nxt = self.warm_fields(*batches[k + 1], use_mlp=use_mlp) if k + 1 < len(batches) else None
+                lr_s = time.perf_counter() - t
+                th.join()
+                if "err" in box:
+                    raise box["err"]
+                out[k] = self._score("mlp" if use_mlp else "idw", box["res"], truth_of[k], steady_of[k], 0.0, 0.0,
+                                     {"hr_solve_s": box["s"], "next_lr_and_prediction_s": lr_s})
+                inits = nxt
+            return out
+
+        _, sec, wall = _device_timed(run)
+        return out, sec, wall
+
     # ------------------------------------------------------------- one pass
     def _score(self, start, res, truth, steady, seconds, wall, parts):
         st = np.array([r["status"] == 2 for r in res])

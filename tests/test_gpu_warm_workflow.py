@@ -1,0 +1,35 @@
+"""The warm-start workflow on the GPU: a stream of batches, whose next LR
+solve and prediction run beside the current HR solve, gives every case the
+result the one-batch-at-a-time pass gives it (eval/convergence_case.py:106-140
+times the same pipeline one case set at a time)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def wf():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    from eulersr_b200.warmstart.workflow import WarmStartWorkflow
+    w = WarmStartWorkflow(slots=4, lr_steps=800, max_steps=1500)
+    w.prepare(n_train=8, target_steps=500, train_steps=20, batch=4096)
+    yield w
+    w.close()
+
+
+def test_streamed_batches_equal_one_pass_each(wf):
+    b1 = (np.array([0.50, 0.60, 0.70, 0.55, 0.65]), np.array([0.0, 1.0, 2.0, -1.0, 0.5]))
+    b2 = (np.array([0.58, 0.68, 0.52]), np.array([1.5, -0.5, 2.5]))
+    t1, s1 = wf.truth(*b1, ref_steps=2500, confirm_steps=500)
+    t2, s2 = wf.truth(*b2, ref_steps=2500, confirm_steps=500)
+    passes = [wf.solve(*b1, t1, s1, "mlp"), wf.solve(*b2, t2, s2, "mlp")]
+    streamed, sec, wall = wf.solve_stream([b1, b2], [t1, t2], [s1, s2])
+    assert sec > 0 and wall > 0
+    for p, q in zip(passes, streamed):
+        assert [r["stopping_step"] for r in p.results] == [r["stopping_step"] for r in q.results]
+        assert [r["cd"] for r in p.results] == [r["cd"] for r in q.results]
+        assert [r["status"] for r in p.results] == [r["status"] for r in q.results]
+        assert p.converged == q.converged
