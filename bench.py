@@ -692,6 +692,16 @@ def run_warm(args, world, rank, local):
                 "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
                 "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
                 "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
+    # the same warm pass with the HR cases queued in submission order
+    flush.add_(1.0)
+    barrier(world)
+    wf.schedule = "fifo"
+    try:
+        r = wf.solve(me, ae, truth, steady, "mlp")
+    finally:
+        wf.schedule = "lr_longest_first"
+    fifo = {"value": allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world),
+            "converged": r.converged, "seconds": r.seconds, "parts_s": r.parts_s}
     # a stream of batches, as a campaign runs them: the next batch's LR solve
     # and prediction overlap this batch's HR solve
     flush.add_(1.0)
@@ -746,7 +756,9 @@ def run_warm(args, world, rank, local):
                            "reference_cd": f"float64 solves of the same kernels, 30,000 + 5,000 steps ({truth_s:.1f} s)",
                            "steady_cases": int(steady.sum()), "truth_check": truth_check,
                            "l2": "256 MB buffer overwritten between passes", "setup_s": setup_s,
-                           "sharding": "parallel.shard_cases (cost-balanced LPT)"},
+                           "sharding": "parallel.shard_cases (cost-balanced LPT)",
+                           "hr_queue": "warm starts: cases queued by the LR solve's last relative change, "
+                                       "largest first (WarmStartWorkflow.hr_order); cold starts: submission order"},
                 "converged_cases_per_s": {
                     "warm_mlp_batched": value, "warm_idw_batched": base["idw"], "plain_batched": base["cold"],
                     "plain_single_case": base["single"], "ratio_warm_vs_plain_single_case": ratio["single"],
@@ -755,7 +767,8 @@ def run_warm(args, world, rank, local):
                                     for p in passes[:3]],
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
-                    "by_case_class": by_class, "warm_mlp_streamed": streamed},
+                    "by_case_class": by_class, "warm_mlp_streamed": streamed,
+                    "warm_mlp_fifo_queue": fifo},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",

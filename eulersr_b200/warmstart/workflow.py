@@ -72,13 +72,16 @@ def _device_timed(fn):
 
 class WarmStartWorkflow:
     def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=6000, max_steps=12000,
-                 check_every=25, patience=8, cd_tol=0.005, device=0):
+                 check_every=25, patience=8, cd_tol=0.005, device=0, schedule="lr_longest_first"):
         self.hr, self.lr = cached_mesh(geom, h_hr), cached_mesh(geom, h_lr)
         self.pair = MeshPair.build(self.hr, self.lr)
         self.dm_hr, self.dm_lr = DeviceMesh(self.hr), DeviceMesh(self.lr)
         self.slots, self.lr_steps, self.max_steps = slots, lr_steps, max_steps
         self.check_every, self.patience, self.cd_tol = check_every, patience, cd_tol
         self.device = device
+        if schedule not in ("lr_longest_first", "fifo"):
+            raise ValueError("schedule must be 'lr_longest_first' or 'fifo'")
+        self.schedule = schedule
         self.ws = WarmStart(self.pair, device=f"cuda:{device}")
         self._solvers = {}
         self.train_info = {}
@@ -126,16 +129,46 @@ class WarmStartWorkflow:
             self.ws.mlp.launches if self.ws.mlp is not None else 0)
 
     # ----------------------------------------------------------------- set-up
-    def lr_solutions(self, machs, aoas):
-        """LR fields of every case (fixed lr_steps) and their LSQ pressure gradients."""
+    def lr_solutions(self, machs, aoas, with_results=False):
+        """LR fields of every case (fixed lr_steps) and their LSQ pressure
+        gradients (and the LR solve's per-case results)."""
         s = self._lr_solver(len(machs))
-        _, states = s.batch_solve(self._cases(machs, aoas, max_steps=self.lr_steps), want_states=True)
+        res, states = s.batch_solve(self._cases(machs, aoas, max_steps=self.lr_steps), want_states=True)
         g = self._grad_solver()
         grads = []
         for W, m, a in zip(states, machs, aoas):
             g.set_case(0, FlowCase(mach=float(m), aoa_deg=float(a), tf=1.0), W_init=W)
             grads.append(g.gradients(0)[:, 3, :].astype(np.float32))
-        return states, grads
+        return (states, grads, res) if with_results else (states, grads)
+
+    def hr_order(self, lr_results):
+        """Queue order of the HR cases: with ``schedule='lr_longest_first'``
+        the cases whose LR field still moved most at the end of the LR solve
+        (largest last relative change) first, since the cases that settle
+        slowest at LR are the ones that run longest at HR; a long case that
+        starts early runs beside the short ones instead of alone at the end.
+        ``'fifo'``: submission order. The order changes no case's result
+        (every case's steps are independent of its slot), only the time."""
+        n = len(lr_results)
+        if self.schedule == "fifo":
+            return np.arange(n)
+        key = np.array([r["last_rel"] for r in lr_results], dtype=np.float64)
+        key = np.where(np.isfinite(key), key, np.inf)
+        return np.argsort(-key, kind="stable")
+
+    def _hr_batch(self, s, machs, aoas, truth, inits, order, want_states=False):
+        """HR batch solve with the cases queued in `order`; results (and
+        states) returned in the callers' case order."""
+        order = np.asarray(order)
+        cases = self._cases(np.asarray(machs)[order], np.asarray(aoas)[order], np.asarray(truth)[order])
+        init_q = None if inits is None else [inits[i] for i in order]
+        res_q, st_q = s.batch_solve(cases, init_fields=init_q, want_states=want_states)
+        res, states = [None] * len(order), (None if st_q is None else [None] * len(order))
+        for j, i in enumerate(order):
+            res[i] = res_q[j]
+            if st_q is not None:
+                states[i] = st_q[j]
+        return res, states
 
     def prepare(self, n_train=256, seed=3, target_steps=12000, train_steps=2000, batch=32768):
         """Training pairs from the batched solver (LR and HR solves of
@@ -180,12 +213,18 @@ class WarmStartWorkflow:
         return cd, steady
 
     # ----------------------------------------------------------- the stream
-    def warm_fields(self, machs, aoas, use_mlp=True):
+    def warm_fields(self, machs, aoas, use_mlp=True, parts=None):
         """LR solve, LR pressure gradients and the IDW (+ MLP) prediction of
-        every case: the conserved HR warm fields (float64, HR cell order)."""
-        lr_states, lr_gp = self.lr_solutions(machs, aoas)
-        return [self.ws.predict_state(primitives(W).astype(np.float32), g, m, a, use_mlp=use_mlp)
-                for W, g, m, a in zip(lr_states, lr_gp, machs, aoas)]
+        every case: the conserved HR warm fields (float64, HR cell order) and
+        the HR queue order (``hr_order``)."""
+        t = time.perf_counter()
+        lr_states, lr_gp, lr_res = self.lr_solutions(machs, aoas, with_results=True)
+        t1 = time.perf_counter()
+        inits = [self.ws.predict_state(primitives(W).astype(np.float32), g, m, a, use_mlp=use_mlp)
+                 for W, g, m, a in zip(lr_states, lr_gp, machs, aoas)]
+        if parts is not None:
+            parts["lr_solve_s"], parts["inference_s"] = t1 - t, time.perf_counter() - t1
+        return inits, self.hr_order(lr_res)
 
     def solve_stream(self, batches, truth_of, steady_of, use_mlp=True):
         """Warm-started solves of a stream of case batches, as a campaign
@@ -199,21 +238,21 @@ class WarmStartWorkflow:
         out = [None] * len(batches)
         s = self._hr_solver(min(self.slots, max(len(b[0]) for b in batches)))
 
-        def hr(k, inits, box):
+        def hr(k, warm, box):
             try:
                 torch.cuda.set_device(self.device)     # a new host thread starts on device 0
                 m, a = batches[k]
                 t = time.perf_counter()
-                res, _ = s.batch_solve(self._cases(m, a, truth_of[k]), init_fields=inits)
-                box["res"], box["s"] = res, time.perf_counter() - t
+                box["res"], _ = self._hr_batch(s, m, a, truth_of[k], *warm)
+                box["s"] = time.perf_counter() - t
             except BaseException as e:   # re-raised in the caller's thread
                 box["err"] = e
 
         def run():
-            inits = self.warm_fields(*batches[0], use_mlp=use_mlp)
+            warm = self.warm_fields(*batches[0], use_mlp=use_mlp)
             for k in range(len(batches)):
                 box = {}
-                th = threading.Thread(target=hr, args=(k, inits, box))
+                th = threading.Thread(target=hr, args=(k, warm, box))
                 th.start()
                 t = time.perf_counter()
                 nxt = self.warm_fields(*batches[k + 1], use_mlp=use_mlp) if k + 1 < len(batches) else None
@@ -223,7 +262,7 @@ class WarmStartWorkflow:
                     raise box["err"]
                 out[k] = self._score("mlp" if use_mlp else "idw", box["res"], truth_of[k], steady_of[k], 0.0, 0.0,
                                      {"hr_solve_s": box["s"], "next_lr_and_prediction_s": lr_s})
-                inits = nxt
+                warm = nxt
             return out
 
         _, sec, wall = _device_timed(run)
@@ -248,16 +287,10 @@ class WarmStartWorkflow:
                 res, states = s.batch_solve(self._cases(machs, aoas, truth), want_states=want_states)
                 parts["hr_solve_s"] = time.perf_counter() - t
                 return res, states
-            t = time.perf_counter()
-            lr_states, lr_gp = self.lr_solutions(machs, aoas)
-            parts["lr_solve_s"] = time.perf_counter() - t
-            t = time.perf_counter()
-            inits = [self.ws.predict_state(primitives(W).astype(np.float32), g, m, a, use_mlp=(start == "mlp"))
-                     for W, g, m, a in zip(lr_states, lr_gp, machs, aoas)]
-            parts["inference_s"] = time.perf_counter() - t
+            inits, order = self.warm_fields(machs, aoas, use_mlp=(start == "mlp"), parts=parts)
             s = self._hr_solver(min(self.slots, len(machs)))
             t = time.perf_counter()
-            res, states = s.batch_solve(self._cases(machs, aoas, truth), init_fields=inits, want_states=want_states)
+            res, states = self._hr_batch(s, machs, aoas, truth, inits, order, want_states)
             parts["hr_solve_s"] = time.perf_counter() - t
             return res, states
 
