@@ -83,15 +83,31 @@ class KernelTimes(C.Structure):
 BLOCK_PATCHES = -1
 
 
+TUNING_MAX_VARIANTS = 12
+
+
+class TuningVariant(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("k2_patches", C.c_int32), ("k1_minb", C.c_int32),
+                ("k2_minb", C.c_int32), ("step_ms", C.c_double)]
+
+    def as_dict(self):
+        return {"block_size": int(self.block_size), "k2_patches": bool(self.k2_patches),
+                "k1_minb": int(self.k1_minb), "k2_minb": int(self.k2_minb), "step_ms": float(self.step_ms)}
+
+
 class Tuning(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("n_candidates", C.c_int32), ("candidates", C.c_int32 * 4),
-                ("k2_patches", C.c_int32), ("reserved", C.c_int32), ("step_ms", C.c_double * 4)]
+                ("k2_patches", C.c_int32), ("cached", C.c_int32), ("step_ms", C.c_double * 4),
+                ("k1_minb", C.c_int32), ("k2_minb", C.c_int32), ("n_variants", C.c_int32),
+                ("reserved", C.c_int32), ("variants", TuningVariant * TUNING_MAX_VARIANTS)]
 
     def as_dict(self):
         n = int(self.n_candidates)
         name = lambda c: "patches" if c == BLOCK_PATCHES else int(c)
         return {"block_size": int(self.block_size), "k2_patches": bool(self.k2_patches),
-                "step_ms": {name(self.candidates[i]): float(self.step_ms[i]) for i in range(n)}}
+                "k1_minb": int(self.k1_minb), "k2_minb": int(self.k2_minb), "cached": bool(self.cached),
+                "step_ms": {name(self.candidates[i]): float(self.step_ms[i]) for i in range(n)},
+                "variants": [self.variants[i].as_dict() for i in range(int(self.n_variants))]}
 
 
 class EsrError(RuntimeError):
@@ -140,6 +156,7 @@ _SIGS = {
     "esr_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "esr_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "esr_solver_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "esr_solver_set_shape": (C.c_int, [C.c_void_p, C.POINTER(TuningVariant)]),
     "esr_set_cases": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(Case), C.c_void_p]),
     "esr_get_states": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "esr_set_cases_f32": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(Case), C.c_void_p]),

@@ -131,6 +131,16 @@ __device__ __forceinline__ T dv(T a, T b) {
 #ifndef ESR_K2_MINB
 #define ESR_K2_MINB 5   // 48 registers: 7-9 % faster than 4 blocks (62 registers), no spills
 #endif
+// The autotuner's second register budget of each fast float32 kernel; a
+// kernel's MINB template argument of 0 means the default above.
+#ifndef ESR_K1_MINB_ALT
+#define ESR_K1_MINB_ALT 6
+#endif
+#ifndef ESR_K2_MINB_ALT
+#define ESR_K2_MINB_ALT 4
+#endif
+template <typename T, bool FAST, int MINB, int DEF>
+constexpr int kMinBlocks = kFastPath<T, FAST> ? (MINB ? MINB : DEF) : 1;
 
 template <typename T>
 struct Consts {
@@ -317,8 +327,8 @@ __device__ __forceinline__ void geo_groups(const Seg<T>& s, int c, int g0, T out
 // own MUSCL face states (euler_solver.py:69-98). Writes FV[k][item] (primitive).
 // With LOCALDT it also writes the per-cell CFL time step of the state.
 // MUSCL=false only computes the local dt (constant reconstruction needs no face states).
-template <typename T, bool FAST, bool MUSCL, bool LOCALDT>
-__global__ void __launch_bounds__(256, kFastPath<T, FAST> ? (LOCALDT ? ESR_K1_MINB_LOCAL : ESR_K1_MINB) : 1) k_recon(const BlockMap<T> bm,
+template <typename T, bool FAST, bool MUSCL, bool LOCALDT, int MINB = 0>
+__global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, LOCALDT ? ESR_K1_MINB_LOCAL : ESR_K1_MINB>)) k_recon(const BlockMap<T> bm,
                                                const V4<T>* __restrict__ W, V4<T>* __restrict__ FV,
                                                long long total, Cases<T> cs, Consts<T> kc, int pos,
                                                T* __restrict__ dt_local) {
@@ -586,8 +596,8 @@ __device__ __forceinline__ float4 cell_update(const float acc[4], float area, fl
 
 // euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
 // then the stage update of :630-653.
-template <typename T, bool FAST, int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
-__global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_flux(const BlockMap<T> bm,
+template <typename T, bool FAST, int FLUX, bool MUSCL, int STAGE, bool LOCALDT, int MINB = 0>
+__global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, ESR_K2_MINB>)) k_flux(const BlockMap<T> bm,
                                               const V4<T>* __restrict__ Win, const V4<T>* __restrict__ Wbase,
                                               V4<T>* __restrict__ Wout, const V4<T>* __restrict__ FV,
                                               long long total, Cases<T> cs, Consts<T> kc, int pos,
@@ -723,13 +733,16 @@ __global__ void __launch_bounds__(256, kFastPath<T, FAST> ? ESR_K2_MINB : 1) k_f
 #ifndef ESR_PATCH_MINB
 #define ESR_PATCH_MINB 5
 #endif
+#ifndef ESR_PATCH_MINB_ALT
+#define ESR_PATCH_MINB_ALT 6
+#endif
 #ifndef ESR_PATCH_WARPS
 #define ESR_PATCH_WARPS 8
 #endif
 constexpr int kPatchWarps = ESR_PATCH_WARPS;
 
-template <int STAGE, bool LOCALDT>
-__global__ void __launch_bounds__(32 * kPatchWarps, ESR_PATCH_MINB) k_flux_patch(const Seg<float>* __restrict__ segs,
+template <int STAGE, bool LOCALDT, int MINB = ESR_PATCH_MINB>
+__global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg<float>* __restrict__ segs,
                                                                   const int4* __restrict__ pblk,
                                                                   const float4* __restrict__ Win,
                                                                   const float4* __restrict__ Wbase,
@@ -738,7 +751,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, ESR_PATCH_MINB) k_flux_patch
                                                                   Cases<float> cs, Consts<float> kc, int pos,
                                                                   const float* __restrict__ dt_local,
                                                                   float* __restrict__ res_out) {
-  __shared__ float4 G[kPatchCells][3][32];   // signed face fluxes of the patch's cells (48 KB)
+  __shared__ float4 G[kPatchCells][3][32];   // signed face fluxes of the patch's cells (1.5 KB per cell)
   const int4 pb = pblk[blockIdx.x];          // segment, patch, first slot
   const Seg<float> s = segs[pb.x];
   const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];

@@ -14,7 +14,9 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -128,6 +130,8 @@ struct SolverT : SolverBase {
   DevBuf<int4> d_pblk;   // K2 by patches: (mesh segment, patch, first slot) per block
   int n_pblk = 0;
   bool use_patch = false;
+  // second register budget of each fast float32 kernel (autotuned)
+  bool k1_alt = false, k2_alt = false, kp_alt = false;
   DevBuf<int> d_case_seg, d_case_slot, d_ncells;
 
   DevBuf<V> W, Wa, Wref, FV, Wp;   // Wp: probe step output (batch solves)
@@ -423,10 +427,82 @@ struct SolverT : SolverBase {
 
   // Autotuner: time one full step of every slot (the solver's own meshes,
   // scheme and slot counts; a uniform finite state, all slots live) for each
-  // block size and keep the fastest. Results do not depend on the choice:
-  // every item is computed the same way whatever block it falls in.
+  // launch shape and keep the fastest. Shapes: the cell kernels at 64, 128
+  // and 256 threads per block; at the best of those, K2's second register
+  // budget, K2 by patches at both budgets, then K1's second budget with the
+  // best K2. Results do not depend on the choice: every item is computed the
+  // same way whatever block and kernel form it falls in. The choice is kept
+  // per process for each solver shape (device, precision, scheme, meshes'
+  // cells and slots), so a second solver of the same shape skips the timing.
+  struct TuneChoice {
+    int block = 256;
+    bool patches = false, k1 = false, k2 = false, kp = false;
+  };
+  struct TuneEntry {
+    TuneChoice choice;
+    esr_tuning record;
+  };
+  static std::mutex& tune_mutex() { static std::mutex m; return m; }
+  static std::map<std::string, TuneEntry>& tune_cache() { static std::map<std::string, TuneEntry> c; return c; }
+  std::string tune_key() const {
+    std::string k = std::to_string(device) + "/" + std::to_string(sizeof(T)) + "/" + std::to_string(P.fidelity) + "/" +
+                    std::to_string(P.flux) + "/" + std::to_string(P.reconstruction) + "/" +
+                    std::to_string(P.time_scheme) + "/" + std::to_string(P.dt_mode);
+    for (const auto& m : meshes) k += "/" + std::to_string(m->hm->n_cells) + "x" + std::to_string(m->B);
+    return k;
+  }
+  bool fast_float() const { return sizeof(T) == 4 && !faithful(); }
+  int k1_minb_of(const TuneChoice& c) const {
+    if (!fast_float() || P.reconstruction != ESR_RECON_MUSCL) return 0;
+    return c.k1 ? ESR_K1_MINB_ALT : ESR_K1_MINB;
+  }
+  int k2_minb_of(const TuneChoice& c) const {
+    if (!fast_float()) return 0;
+    if (c.patches) return c.kp ? ESR_PATCH_MINB_ALT : ESR_PATCH_MINB;
+    return c.k2 ? ESR_K2_MINB_ALT : ESR_K2_MINB;
+  }
+  int apply_choice(const TuneChoice& c) {
+    ESR_TRY(build_blocks(c.block));
+    use_patch = c.patches && patch_eligible();
+    k1_alt = c.k1;
+    k2_alt = c.k2;
+    kp_alt = c.kp;
+    return ESR_OK;
+  }
+  int time_choice(const TuneChoice& c, const Cases<T>& cs, double& ms) {
+    ESR_TRY(apply_choice(c));
+    step_kernels(cs, 0);   // warm-up
+    ESR_CUDA(cudaEventRecord(ev0, stream));
+    for (int r = 0; r < 3; ++r) step_kernels(cs, 0);
+    ESR_CUDA(cudaEventRecord(ev1, stream));
+    ESR_CUDA(cudaEventSynchronize(ev1));
+    float t = 0.f;
+    ESR_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+    ms = t / 3.0;
+    if (tuning.n_variants < ESR_TUNING_MAX_VARIANTS) {
+      esr_tuning_variant& v = tuning.variants[tuning.n_variants++];
+      v.block_size = c.block;
+      v.k2_patches = c.patches ? 1 : 0;
+      v.k1_minb = k1_minb_of(c);
+      v.k2_minb = k2_minb_of(c);
+      v.step_ms = ms;
+    }
+    return ESR_OK;
+  }
   esr_tuning tuning{};
+  TuneChoice chosen;
   int autotune() {
+    const std::string key = tune_key();
+    {
+      std::lock_guard<std::mutex> lock(tune_mutex());
+      auto it = tune_cache().find(key);
+      if (it != tune_cache().end()) {
+        chosen = it->second.choice;
+        tuning = it->second.record;
+        tuning.cached = 1;
+        return apply_choice(chosen);
+      }
+    }
     const V w0 = mk4<T>(T(1), T(0.5), T(0.1), T(2.5));
     const int tb = 256;
     k_fill_uniform<T><<<(int)std::min<long long>((total + tb - 1) / tb, 65535), tb, 0, stream>>>(W.p, total, w0);
@@ -437,44 +513,56 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpyAsync(dt.p, dts.data(), n_slots * sizeof(T), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemcpyAsync(active.p, on.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
     const Cases<T> cs = cases(true);
-    const int cand[3] = {64, 128, 256};
     const int64_t before = launches;
-    double best = 1e300;
-    int best_blk = block;
+    tuning = esr_tuning{};
+    double best = 1e300, ms = 0.0;
+    TuneChoice best_c;
+    auto consider = [&](const TuneChoice& c) -> int {
+      ESR_TRY(time_choice(c, cs, ms));
+      if (ms < best) { best = ms; best_c = c; }
+      return ESR_OK;
+    };
+    const int cand[3] = {64, 128, 256};
     tuning.n_candidates = 3;
     for (int i = 0; i < 3; ++i) {
-      ESR_TRY(build_blocks(cand[i]));
-      step_kernels(cs, 0);   // warm-up
-      ESR_CUDA(cudaEventRecord(ev0, stream));
-      for (int r = 0; r < 3; ++r) step_kernels(cs, 0);
-      ESR_CUDA(cudaEventRecord(ev1, stream));
-      ESR_CUDA(cudaEventSynchronize(ev1));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev0, ev1);
+      TuneChoice c;
+      c.block = cand[i];
+      ESR_TRY(consider(c));
       tuning.candidates[i] = cand[i];
-      tuning.step_ms[i] = ms / 3.0;
-      if (ms / 3.0 < best) { best = ms / 3.0; best_blk = cand[i]; }
+      tuning.step_ms[i] = ms;
     }
-    // K2 by patches, with K1 at the best block size
-    if (patch_eligible()) {
-      ESR_TRY(build_blocks(best_blk));
-      use_patch = true;
-      step_kernels(cs, 0);
-      ESR_CUDA(cudaEventRecord(ev0, stream));
-      for (int r = 0; r < 3; ++r) step_kernels(cs, 0);
-      ESR_CUDA(cudaEventRecord(ev1, stream));
-      ESR_CUDA(cudaEventSynchronize(ev1));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev0, ev1);
+    const int best_blk = best_c.block;
+    const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
+    if (fast_float() && muscl && P.flux == ESR_FLUX_HLLC) {   // K2 per cell, second budget
+      TuneChoice c;
+      c.block = best_blk;
+      c.k2 = true;
+      ESR_TRY(consider(c));
+    }
+    if (patch_eligible()) {   // K2 by patches, K1 at the best block size
+      TuneChoice c;
+      c.block = best_blk;
+      c.patches = true;
+      ESR_TRY(consider(c));
       tuning.candidates[3] = ESR_BLOCK_PATCHES;
-      tuning.step_ms[3] = ms / 3.0;
+      tuning.step_ms[3] = ms;
       tuning.n_candidates = 4;
-      use_patch = ms / 3.0 < best;
+      c.kp = true;
+      ESR_TRY(consider(c));
+    }
+    if (fast_float() && muscl) {   // K1, second budget, with the best K2
+      TuneChoice c = best_c;
+      c.k1 = true;
+      ESR_TRY(consider(c));
     }
     launches = before;
-    ESR_TRY(build_blocks(best_blk));
-    tuning.block_size = best_blk;
+    chosen = best_c;
+    ESR_TRY(apply_choice(chosen));
+    tuning.block_size = chosen.block;
     tuning.k2_patches = use_patch ? 1 : 0;
+    tuning.k1_minb = k1_minb_of(chosen);
+    tuning.k2_minb = k2_minb_of(chosen);
+    tuning.cached = 0;
     ESR_CUDA(cudaMemsetAsync(W.p, 0, total * sizeof(V), stream));
     ESR_CUDA(cudaMemsetAsync(Wa.p, 0, total * sizeof(V), stream));
     ESR_CUDA(cudaMemsetAsync(active.p, 0, n_slots * sizeof(int), stream));
@@ -482,12 +570,59 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemsetAsync(inlet.p, 0, n_slots * sizeof(V), stream));
     ESR_CUDA(cudaStreamSynchronize(stream));
     ESR_CUDA(cudaGetLastError());
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    tune_cache()[key] = TuneEntry{chosen, tuning};
+    return ESR_OK;
+  }
+  // a launch shape given by the caller (one recorded by an earlier
+  // autotuning, say); the chunk graphs are captured again at the next step
+  int set_shape(const esr_tuning_variant* v) {
+    if (v->block_size != 64 && v->block_size != 128 && v->block_size != 256)
+      return fail(ESR_ERR_ARG, "set_shape: block_size must be 64, 128 or 256");
+    if (v->k2_patches != 0 && v->k2_patches != 1) return fail(ESR_ERR_ARG, "set_shape: k2_patches must be 0 or 1");
+    if (v->k2_patches && !patch_eligible())
+      return fail(ESR_ERR_ARG, "set_shape: K2 by patches needs a float32 fast-fidelity HLLC + MUSCL solver");
+    TuneChoice c;
+    c.block = v->block_size;
+    c.patches = v->k2_patches == 1;
+    const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
+    if (v->k1_minb != 0) {
+      if (!fast_float() || !muscl || (v->k1_minb != ESR_K1_MINB && v->k1_minb != ESR_K1_MINB_ALT))
+        return fail(ESR_ERR_ARG, "set_shape: k1_minb must be 0 or one of K1's two register budgets (" +
+                                     std::to_string(ESR_K1_MINB) + ", " + std::to_string(ESR_K1_MINB_ALT) +
+                                     ") of a float32 fast-fidelity MUSCL solver");
+      c.k1 = v->k1_minb == ESR_K1_MINB_ALT;
+    }
+    if (v->k2_minb != 0) {
+      const int def = c.patches ? ESR_PATCH_MINB : ESR_K2_MINB, alt = c.patches ? ESR_PATCH_MINB_ALT : ESR_K2_MINB_ALT;
+      const bool ok = fast_float() && (c.patches || (muscl && P.flux == ESR_FLUX_HLLC)) &&
+                      (v->k2_minb == def || v->k2_minb == alt);
+      if (!ok)
+        return fail(ESR_ERR_ARG, "set_shape: k2_minb must be 0 or one of the K2 form's two register budgets (" +
+                                     std::to_string(def) + ", " + std::to_string(alt) +
+                                     ") of a float32 fast-fidelity HLLC + MUSCL solver");
+      (c.patches ? c.kp : c.k2) = v->k2_minb == alt;
+    }
+    ESR_TRY(apply_choice(c));
+    chosen = c;
+    if (g_run) cudaGraphExecDestroy(g_run);
+    if (g_plain) cudaGraphExecDestroy(g_plain);
+    g_run = g_plain = nullptr;
+    g_run_len = g_plain_len = 0;
+    tuning.block_size = c.block;
+    tuning.k2_patches = use_patch ? 1 : 0;
+    tuning.k1_minb = k1_minb_of(c);
+    tuning.k2_minb = k2_minb_of(c);
     return ESR_OK;
   }
   int get_tuning(esr_tuning* out) {
     *out = tuning;
     if (out->block_size == 0) out->block_size = block;   // given, not measured
     out->k2_patches = use_patch ? 1 : 0;
+    TuneChoice now = chosen;
+    now.patches = use_patch;
+    out->k1_minb = k1_minb_of(now);
+    out->k2_minb = k2_minb_of(now);
     return ESR_OK;
   }
 
@@ -503,10 +638,31 @@ struct SolverT : SolverBase {
   template <int FLUX, bool MUSCL, int STAGE, bool LOCALDT>
   void launch_flux(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
     tap_begin(1);
-    k_flux<T, kF, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(bmap(), win, wbase, wout, FV.p,
-                                                                            total, cs, kc, pos, dt_local.p, res.p);
+    bool done = false;
+    if constexpr (sizeof(T) == 4 && FLUX == 0 && MUSCL) {
+      if (k2_alt) {
+        k_flux<T, kF, FLUX, MUSCL, STAGE, LOCALDT, ESR_K2_MINB_ALT><<<n_blk, block, 0, stream>>>(
+            bmap(), win, wbase, wout, FV.p, total, cs, kc, pos, dt_local.p, res.p);
+        done = true;
+      }
+    }
+    if (!done)
+      k_flux<T, kF, FLUX, MUSCL, STAGE, LOCALDT><<<n_blk, block, 0, stream>>>(bmap(), win, wbase, wout, FV.p,
+                                                                              total, cs, kc, pos, dt_local.p, res.p);
     tap_end();
     ++launches;
+  }
+  template <int STAGE, bool LOCALDT>
+  void launch_patch(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
+    if constexpr (sizeof(T) == 4) {
+      if (kp_alt)
+        k_flux_patch<STAGE, LOCALDT, ESR_PATCH_MINB_ALT><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(
+            d_segs.p, d_pblk.p, win, wbase, wout, FV.p, total, cs, kc, pos, dt_local.p, res.p);
+      else
+        k_flux_patch<STAGE, LOCALDT><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, win, wbase, wout,
+                                                                              FV.p, total, cs, kc, pos, dt_local.p,
+                                                                              res.p);
+    }
   }
   template <int STAGE>
   void flux_dispatch(const V* win, const V* wbase, V* wout, const Cases<T>& cs, int pos) {
@@ -524,12 +680,8 @@ struct SolverT : SolverBase {
       }
       if (use_patch && n_pblk > 0) {   // eligible by construction: HLLC + MUSCL, fast fidelity
         tap_begin(1);
-        if (local)
-          k_flux_patch<STAGE, true><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, win, wbase, wout, FV.p,
-                                                                             total, cs, kc, pos, dt_local.p, res.p);
-        else
-          k_flux_patch<STAGE, false><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, win, wbase, wout, FV.p,
-                                                                              total, cs, kc, pos, dt_local.p, res.p);
+        if (local) launch_patch<STAGE, true>(win, wbase, wout, cs, pos);
+        else launch_patch<STAGE, false>(win, wbase, wout, cs, pos);
         tap_end();
         ++launches;
         return;
@@ -558,8 +710,14 @@ struct SolverT : SolverBase {
       return;
     }
     tap_begin(0);
-    if (write_dt) k_recon<T, kF, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
-    else k_recon<T, kF, true, false><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    if (write_dt) {   // the local-dt K1 keeps its one budget
+      k_recon<T, kF, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    } else if (sizeof(T) == 4 && k1_alt) {
+      k_recon<T, kF, true, false, (sizeof(T) == 4 ? ESR_K1_MINB_ALT : 0)><<<n_blk, block, 0, stream>>>(
+          bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    } else {
+      k_recon<T, kF, true, false><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
+    }
     tap_end();
     ++launches;
   }
@@ -1806,6 +1964,13 @@ int esr_solver_num_slots(const esr_solver* solver, int32_t* n) {
 int esr_solver_tuning(const esr_solver* solver, esr_tuning* out) {
   if (!solver || !out) return fail(ESR_ERR_ARG, "null argument");
   return dispatch_any(const_cast<esr_solver*>(solver), [&](auto& s) { return s.get_tuning(out); });
+}
+
+int esr_solver_set_shape(esr_solver* solver, const esr_tuning_variant* shape) {
+  if (!solver || !shape) return fail(ESR_ERR_ARG, "null argument");
+  ESR_GUARD_BEGIN
+  return dispatch(solver, [&](auto& s) { return s.set_shape(shape); });
+  ESR_GUARD_END
 }
 
 int esr_set_case(esr_solver* solver, int32_t slot, const esr_case* c, const double* W_init) {

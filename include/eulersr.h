@@ -306,21 +306,46 @@ typedef struct esr_kernel_times {
 int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out);
 
 /* The autotuner's record: with esr_params.block_size = 0 the solver times one
- * full step of all its slots for each candidate at creation and keeps the
- * fastest (no reference counterpart: XLA picks launch shapes). Candidates:
- * the cell kernels at 64, 128 and 256 threads per block, then, where
- * eligible (float32 fast fidelity, HLLC + MUSCL), K2 by patches with the
- * best of those for K1 (ESR_BLOCK_PATCHES). Results do not depend on the
- * choice. */
+ * full step of all its slots for each launch shape at creation and keeps the
+ * fastest (no reference counterpart: XLA picks launch shapes). Shapes: the
+ * cell kernels at 64, 128 and 256 threads per block; at the best of those,
+ * where the float32 fast kernels run, K2's second register budget, K2 by
+ * patches at both of its budgets (float32 fast fidelity, HLLC + MUSCL), and
+ * K1's second budget with the best K2. A register budget is the number of
+ * resident blocks per SM a kernel is compiled for. The choice is kept for
+ * the process per solver shape (device, precision, scheme, each mesh's cells
+ * and slots): a second solver of the same shape takes it without timing
+ * (cached = 1). Results do not depend on the choice. */
+#define ESR_TUNING_MAX_VARIANTS 12
+typedef struct esr_tuning_variant {
+    int32_t block_size;       /* threads per block of K1 (and of the per-cell K2) */
+    int32_t k2_patches;       /* 1: K2 by patches */
+    int32_t k1_minb;          /* register budget of K1 (0: not constrained; the K1 that
+                                 also writes the local time step keeps its own) */
+    int32_t k2_minb;          /* register budget of K2, per-cell or patch form */
+    double step_ms;           /* device ms of one step */
+} esr_tuning_variant;
 typedef struct esr_tuning {
     int32_t block_size;       /* threads per block of the cell kernels in use */
     int32_t n_candidates;     /* 0 when block_size was given */
-    int32_t candidates[4];
+    int32_t candidates[4];    /* 64, 128, 256 and ESR_BLOCK_PATCHES at the default budgets */
     int32_t k2_patches;       /* 1: K2 runs by patches */
-    int32_t reserved;
+    int32_t cached;           /* 1: taken from an earlier solver of the same shape */
     double step_ms[4];        /* device ms of one step per candidate */
+    int32_t k1_minb;          /* register budgets in use (0: not constrained) */
+    int32_t k2_minb;
+    int32_t n_variants;       /* every shape timed, in order */
+    int32_t reserved;
+    esr_tuning_variant variants[ESR_TUNING_MAX_VARIANTS];
 } esr_tuning;
 int esr_solver_tuning(const esr_solver* solver, esr_tuning* out);
+/* Run the solver with the given launch shape (a variant recorded by an
+ * earlier autotuning, or chosen by hand); step_ms is ignored, a budget of 0
+ * means the kernel's default. ESR_ERR_ARG for a shape this solver cannot run
+ * (K2 by patches or a second budget outside float32 fast fidelity, HLLC +
+ * MUSCL), ESR_ERR_STATE while a submitted batch owns the slots. Results do
+ * not depend on the shape. */
+int esr_solver_set_shape(esr_solver* solver, const esr_tuning_variant* shape);
 
 /* Solve n_cases cases through the solver's slots: every slot retired by the
  * stop rule is refilled in place with the next queued case. init_fields[i]

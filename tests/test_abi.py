@@ -126,7 +126,7 @@ def test_ctypes_structs_match_the_header(tmp_path):
         pytest.skip("no C compiler")
     pairs = {"esr_mesh_desc": F.MeshDesc, "esr_mesh_info": F.MeshInfo, "esr_params": F.Params,
              "esr_case": F.Case, "esr_result": F.Result, "esr_kernel_times": F.KernelTimes,
-             "esr_tuning": F.Tuning}
+             "esr_tuning": F.Tuning, "esr_tuning_variant": F.TuningVariant}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "eulersr.h"', 'int main(void) {']
     for cname, py in pairs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -240,33 +240,67 @@ def test_batch_submit_poll_results(diamond02, naca02):
 
 
 def test_autotuner_and_block_invariance(naca02):
-    """The autotuner times every candidate (cell kernels at 64, 128 and 256
-    threads, and K2 by patches) and keeps the fastest; the state after 30 steps
-    is bitwise the same whatever the choice: K2 by patches evaluates each inner
+    """The autotuner times every launch shape (cell kernels at 64, 128 and
+    256 threads, K2's second register budget, K2 by patches at both budgets,
+    K1's second budget) and keeps the fastest; a second solver of the same
+    shape takes the choice from the process cache. The state after 30 steps
+    is bitwise the same whatever the shape: K2 by patches evaluates each inner
     face once and the per-cell K2 the same canonical flux from the face's
-    owner."""
+    owner, with explicit rounding in both, so neither the kernel form nor the
+    register budget changes a bit."""
     from eulersr_b200.solver import Solver, FlowCase
-    states = []
-    for bs in (0, 64, 128, 256, "patches"):
-        s = Solver(naca02, 3, precision='f32', block_size=bs)
-        t = s.tuning()
-        if bs == 0:
-            assert sorted(t['step_ms'], key=str) == [128, 256, 64, "patches"]
-            assert all(v > 0 for v in t['step_ms'].values())
-            best = min(t['step_ms'], key=t['step_ms'].get)
-            assert t['k2_patches'] == (best == "patches")
-            if best != "patches":
-                assert t['block_size'] == best
-        elif bs == "patches":
-            assert t['k2_patches'] and t['block_size'] == 128 and t['step_ms'] == {}
-        else:
-            assert t['block_size'] == bs and not t['k2_patches'] and t['step_ms'] == {}
+
+    def run(s):
         for g, (m, a) in enumerate([(0.8, 1.0), (2.0, -3.0), (1.3, 2.5)]):
             s.set_case(g, FlowCase(mach=m, aoa_deg=a, tf=1.0, dtype=np.float32))
         s.step(30)
-        states.append([s.get_state(g) for g in range(3)])
+        return [s.get_state(g) for g in range(3)]
+
+    states = []
+    s = Solver(naca02, 3, precision='f32', block_size=0)
+    t = s.tuning()
+    assert sorted(t['step_ms'], key=str) == [128, 256, 64, "patches"]
+    assert all(v > 0 for v in t['step_ms'].values())
+    var = t['variants']
+    assert len(var) == 7 and all(v['step_ms'] > 0 for v in var)
+    assert [v['block_size'] for v in var[:3]] == [64, 128, 256]
+    assert {(v['k2_patches'], v['k2_minb']) for v in var} == {(False, 5), (False, 4), (True, 5), (True, 6)}
+    assert {v['k1_minb'] for v in var} == {8, 6}
+    best = min(var, key=lambda v: v['step_ms'])
+    assert (t['block_size'], t['k2_patches'], t['k1_minb'], t['k2_minb']) == (
+        best['block_size'], best['k2_patches'], best['k1_minb'], best['k2_minb'])
+    states.append(run(s))
+    again = Solver(naca02, 3, precision='f32', block_size=0)
+    t2 = again.tuning()
+    assert t2['cached'] and t2['variants'] == var and t2['block_size'] == t['block_size']
+    # every timed shape, set by hand
+    for v in var:
+        s.set_shape(v['block_size'], v['k2_patches'], v['k1_minb'], v['k2_minb'])
+        got = s.tuning()
+        assert (got['block_size'], got['k2_patches'], got['k1_minb'], got['k2_minb']) == (
+            v['block_size'], v['k2_patches'], v['k1_minb'], v['k2_minb'])
+        states.append(run(s))
+    for bs in (64, 128, 256, "patches"):
+        s = Solver(naca02, 3, precision='f32', block_size=bs)
+        t = s.tuning()
+        if bs == "patches":
+            assert t['k2_patches'] and t['block_size'] == 128 and t['step_ms'] == {}
+        else:
+            assert t['block_size'] == bs and not t['k2_patches'] and t['step_ms'] == {}
+        states.append(run(s))
     for other in states[1:]:
         assert all(np.array_equal(a, b) for a, b in zip(states[0], other))
+    # shapes a solver cannot run are refused
+    from eulersr_b200._ffi import EsrError
+    f64 = Solver(naca02, 1, precision='f64', block_size=64)
+    with pytest.raises(EsrError):
+        f64.set_shape(64, True)
+    with pytest.raises(EsrError):
+        f64.set_shape(64, False, 0, 4)
+    with pytest.raises(EsrError):
+        s.set_shape(96)
+    with pytest.raises(EsrError):
+        s.set_shape(64, False, 7, 0)
 
 
 def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
