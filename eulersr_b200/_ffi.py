@@ -49,7 +49,7 @@ class Params(C.Structure):
                 ("time_scheme", C.c_int32), ("dt_mode", C.c_int32), ("stop_rule", C.c_int32),
                 ("gamma", C.c_double), ("threshold", C.c_double), ("check_every", C.c_int32),
                 ("patience", C.c_int32), ("device", C.c_int32), ("use_graphs", C.c_int32),
-                ("block_size", C.c_int32), ("fidelity", C.c_int32)]
+                ("block_size", C.c_int32), ("fidelity", C.c_int32), ("stream_priority", C.c_int32)]
 
 
 class Case(C.Structure):

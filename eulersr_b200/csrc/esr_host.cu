@@ -220,7 +220,10 @@ struct SolverT : SolverBase {
     P = *p;
     device = p->device;
     ESR_CUDA(cudaSetDevice(device));
-    ESR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    int least = 0, greatest = 0;
+    ESR_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int prio = std::min(least, std::max(greatest, (int)p->stream_priority));
+    ESR_CUDA(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, prio));
     ESR_CUDA(cudaEventCreate(&ev0));
     ESR_CUDA(cudaEventCreate(&ev1));
     const double g = p->gamma;

@@ -181,7 +181,7 @@ class Solver:
 
     def __init__(self, meshes, slots, precision='f32', flux='hllc', reconstruction='muscl', time_scheme='SRK2',
                  dt_mode='global', stop_rule='reference', gamma=1.4, threshold=1e-6, check_every=25, patience=1,
-                 device=0, use_graphs=True, block_size=0, fidelity='fast'):
+                 device=0, use_graphs=True, block_size=0, fidelity='fast', stream_priority=0):
         L = F.lib()
         if isinstance(meshes, (DeviceMesh, Mesh)):
             meshes = [meshes]
@@ -213,6 +213,7 @@ class Solver:
             p.fidelity = F.FIDELITY[str(fidelity).lower()]
         except KeyError:
             raise ValueError(f"unknown fidelity '{fidelity}': expected 'fast' or 'reference'") from None
+        p.stream_priority = int(stream_priority)
         self.params = p
         self.precision = 'f64' if p.precision == 1 else 'f32'
         self.dtype = np.float64 if p.precision == 1 else np.float32

@@ -99,12 +99,15 @@ class WarmStartWorkflow:
                             stop_rule="engineering", threshold=1e-30, check_every=self.check_every,
                             patience=self.patience)
 
+    # the LR side runs at the device's highest stream priority: in a stream of
+    # batches its short launches get SMs ahead of the HR batch's chunks
     def _lr_solver(self, slots):
         return self._solver(("lr", slots), self.dm_lr, slots, precision="f32", dt_mode="local", stop_rule="reference",
-                            threshold=1e-30, check_every=self.check_every, patience=self.patience)
+                            threshold=1e-30, check_every=self.check_every, patience=self.patience,
+                            stream_priority=-100)
 
     def _grad_solver(self):
-        return self._solver(("grad",), self.dm_lr, 1, precision="f64")
+        return self._solver(("grad",), self.dm_lr, 1, precision="f64", stream_priority=-100)
 
     def _cases(self, machs, aoas, targets=None, max_steps=None, dtype=np.float32):
         out = []
@@ -237,6 +240,8 @@ class WarmStartWorkflow:
         import threading
         out = [None] * len(batches)
         s = self._hr_solver(min(self.slots, max(len(b[0]) for b in batches)))
+        lo, hi = torch.cuda.Stream.priority_range()
+        side = torch.cuda.Stream(device=self.device, priority=hi)   # the prediction's kernels, ahead of the HR chunks
 
         def hr(k, warm, box):
             try:
@@ -255,7 +260,12 @@ class WarmStartWorkflow:
                 th = threading.Thread(target=hr, args=(k, warm, box))
                 th.start()
                 t = time.perf_counter()
-                nxt = self.warm_fields(*batches[k + 1], use_mlp=use_mlp) if k + 1 < len(batches) else None
+                nxt = None
+                if k + 1 < len(batches):
+                    side.wait_stream(torch.cuda.current_stream())
+                    with torch.cuda.stream(side):
+                        nxt = self.warm_fields(*batches[k + 1], use_mlp=use_mlp)
+                    torch.cuda.current_stream().wait_stream(side)
                 lr_s = time.perf_counter() - t
                 th.join()
                 if "err" in box:

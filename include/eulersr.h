@@ -139,6 +139,9 @@ typedef struct esr_params {
     int32_t block_size;       /* threads per block for the cell kernels: 64, 128, 256, 0 = autotuned,
                                * or ESR_BLOCK_PATCHES: cell kernels at 128 with K2 formed by patches */
     int32_t fidelity;         /* ESR_FIDELITY_* (0: fast) */
+    int32_t stream_priority;  /* CUDA priority of the solver's stream (0: default; lower is
+                               * higher, clamped to the device's range): a solver whose small
+                               * launches run beside another solver's long chunks gets SMs first */
 } esr_params;
 
 /* One (Mach, alpha) case. inlet = conserved freestream (euler/main.py:39). */
