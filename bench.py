@@ -618,7 +618,8 @@ def run_warm(args, world, rank, local):
     from eulersr_b200.warmstart.workflow import WarmStartWorkflow
     torch.cuda.set_device(local)
     t_setup = time.perf_counter()
-    wf = WarmStartWorkflow(slots=args.slots, max_steps=args.max_steps, device=local)
+    wf = WarmStartWorkflow(slots=args.slots, max_steps=args.max_steps, device=local,
+                           warm_budget=args.warm_budget or None)
     info = {} if args.make_truth else wf.prepare(n_train=args.n_train, target_steps=args.target_steps,
                                                  train_steps=args.train_steps)
     idx, me, ae = warm_cases(args, world, rank)
@@ -687,8 +688,13 @@ def run_warm(args, world, rank, local):
             cls[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
     steps_warm = np.array([x["steps"] for x in passes[-1].results])
     capped = steps_warm >= args.max_steps
+    fallbacks = [x for x in passes[-1].results if x.get("fallback")]
     by_class = {"steady_cases": int(steady.sum()), "unsteady_cases": int((~steady).sum()),
                 "warm_capped_cases": int(capped.sum()),
+                "warm_fallbacks_to_freestream": len(fallbacks),
+                "warm_fallbacks_converged": int(sum(1 for x in fallbacks if x["status"] == 2)),
+                "warm_step_share_of_fallback_warm_phase": float(
+                    sum(x["warm_steps"] for x in fallbacks) / max(steps_warm.sum(), 1)),
                 "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
                 "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
                 "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
@@ -752,6 +758,9 @@ def run_warm(args, world, rank, local):
                            "cases_per_gpu": len(me), "slots": args.slots, "cd_tolerance": 0.005,
                            "rule": "CD within 0.5 % of the case's float64 reference CD for 8 checks 25 steps apart",
                            "dt": "local CFL 0.6 (0.45 transonic)", "max_steps": args.max_steps,
+                           "warm_budget": args.warm_budget or None,
+                           "fallback": "a warm start the rule has not stopped within warm_budget steps restarts "
+                                       "from freestream with the rest of max_steps (steps of both phases counted)",
                            "lr_steps": 6000, "training": info,
                            "reference_cd": f"float64 solves of the same kernels, 30,000 + 5,000 steps ({truth_s:.1f} s)",
                            "steady_cases": int(steady.sum()), "truth_check": truth_check,
@@ -798,6 +807,8 @@ def main():
     ap.add_argument("--max-steps", type=int, default=12000, help="warm workload: step cap of an HR solve")
     ap.add_argument("--target-steps", type=int, default=12000, help="warm workload: steps of a training target")
     ap.add_argument("--train-steps", type=int, default=2000, help="warm workload: MLP training steps")
+    ap.add_argument("--warm-budget", type=int, default=3000,
+                    help="warm workload: steps after which an unstopped warm start restarts from freestream (0: never)")
     ap.add_argument("--make-truth", action="store_true", help="write the held-out cases' reference CDs and exit")
     ap.add_argument("--block", default="0", help="throughput workloads: 0 (autotuned), 64, 128, 256 or patches")
     args = ap.parse_args()

@@ -6,6 +6,8 @@ converged HR field of each (Mach, alpha) case:
 * ``mlp``    LR solve of every case -> LR pressure gradients -> IDW (k=6, p=2)
              + residual MLP on the GPU -> HR solve from that prediction
              (eval/convergence_case.py:106-140: the whole pipeline is timed);
+             a case the rule has not stopped within ``warm_budget`` steps
+             restarts from freestream with the rest of the step cap;
 * ``idw``    the same without the MLP;
 * ``cold``   HR solve from freestream, ``slots`` cases at a time with
              retire/refill;
@@ -72,7 +74,8 @@ def _device_timed(fn):
 
 class WarmStartWorkflow:
     def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=6000, max_steps=12000,
-                 check_every=25, patience=8, cd_tol=0.005, device=0, schedule="lr_longest_first"):
+                 check_every=25, patience=8, cd_tol=0.005, device=0, schedule="lr_longest_first",
+                 warm_budget=3000):
         self.hr, self.lr = cached_mesh(geom, h_hr), cached_mesh(geom, h_lr)
         self.pair = MeshPair.build(self.hr, self.lr)
         self.dm_hr, self.dm_lr = DeviceMesh(self.hr), DeviceMesh(self.lr)
@@ -82,6 +85,7 @@ class WarmStartWorkflow:
         if schedule not in ("lr_longest_first", "fifo"):
             raise ValueError("schedule must be 'lr_longest_first' or 'fifo'")
         self.schedule = schedule
+        self.warm_budget = warm_budget   # None or 0: no fallback to freestream
         self.ws = WarmStart(self.pair, device=f"cuda:{device}")
         self._solvers = {}
         self.train_info = {}
@@ -159,11 +163,12 @@ class WarmStartWorkflow:
         key = np.where(np.isfinite(key), key, np.inf)
         return np.argsort(-key, kind="stable")
 
-    def _hr_batch(self, s, machs, aoas, truth, inits, order, want_states=False):
+    def _hr_batch(self, s, machs, aoas, truth, inits, order, want_states=False, max_steps=None):
         """HR batch solve with the cases queued in `order`; results (and
         states) returned in the callers' case order."""
         order = np.asarray(order)
-        cases = self._cases(np.asarray(machs)[order], np.asarray(aoas)[order], np.asarray(truth)[order])
+        cases = self._cases(np.asarray(machs)[order], np.asarray(aoas)[order], np.asarray(truth)[order],
+                            max_steps=max_steps)
         init_q = None if inits is None else [inits[i] for i in order]
         res_q, st_q = s.batch_solve(cases, init_fields=init_q, want_states=want_states)
         res, states = [None] * len(order), (None if st_q is None else [None] * len(order))
@@ -215,6 +220,37 @@ class WarmStartWorkflow:
         steady = np.abs(cd - cd_a) <= 1e-3 * np.abs(cd)
         return cd, steady
 
+    def _hr_warm(self, s, machs, aoas, truth, inits, order, want_states=False):
+        """HR solve from the warm fields. With a warm budget, a case the rule
+        has not stopped within ``warm_budget`` steps restarts from freestream
+        with the rest of the step cap (the plain start is the fallback: a
+        prediction that leaves, say, spurious entropy on the body can take far
+        longer to wash out than a freestream start takes to converge). Its
+        result carries ``fallback`` and the warm steps spent, counted in its
+        ``steps`` and ``stopping_step``."""
+        machs, aoas, truth = np.asarray(machs), np.asarray(aoas), np.asarray(truth)
+        budget = self.warm_budget if (self.warm_budget and self.warm_budget < self.max_steps) else None
+        res, states = self._hr_batch(s, machs, aoas, truth, inits, order, want_states, max_steps=budget)
+        if budget is None:
+            return res, states
+        rank = np.empty(len(order), dtype=np.int64)
+        rank[np.asarray(order)] = np.arange(len(order))
+        fb = np.array(sorted((i for i, r in enumerate(res) if r["status"] != 2), key=lambda i: rank[i]), dtype=np.int64)
+        if len(fb) == 0:
+            return res, states
+        res2, st2 = self._hr_batch(s, machs[fb], aoas[fb], truth[fb], None, np.arange(len(fb)), want_states,
+                                   max_steps=self.max_steps - budget)
+        for j, i in enumerate(fb):
+            r = dict(res2[j])
+            spent = int(res[i]["steps"])
+            r["fallback"], r["warm_steps"] = True, spent
+            r["steps"] = int(r["steps"]) + spent
+            r["stopping_step"] = int(r["stopping_step"]) + spent
+            res[i] = r
+            if states is not None:
+                states[i] = st2[j]
+        return res, states
+
     # ----------------------------------------------------------- the stream
     def warm_fields(self, machs, aoas, use_mlp=True, parts=None):
         """LR solve, LR pressure gradients and the IDW (+ MLP) prediction of
@@ -248,7 +284,7 @@ class WarmStartWorkflow:
                 torch.cuda.set_device(self.device)     # a new host thread starts on device 0
                 m, a = batches[k]
                 t = time.perf_counter()
-                box["res"], _ = self._hr_batch(s, m, a, truth_of[k], *warm)
+                box["res"], _ = self._hr_warm(s, m, a, truth_of[k], *warm)
                 box["s"] = time.perf_counter() - t
             except BaseException as e:   # re-raised in the caller's thread
                 box["err"] = e
@@ -300,7 +336,7 @@ class WarmStartWorkflow:
             inits, order = self.warm_fields(machs, aoas, use_mlp=(start == "mlp"), parts=parts)
             s = self._hr_solver(min(self.slots, len(machs)))
             t = time.perf_counter()
-            res, states = self._hr_batch(s, machs, aoas, truth, inits, order, want_states)
+            res, states = self._hr_warm(s, machs, aoas, truth, inits, order, want_states)
             parts["hr_solve_s"] = time.perf_counter() - t
             return res, states
 

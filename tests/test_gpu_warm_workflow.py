@@ -49,3 +49,24 @@ def test_queue_order_changes_no_result(wf):
         assert [r[key] for r in r_lpt.results] == [r[key] for r in r_fifo.results], key
     for x, y in zip(r_fifo.states, r_lpt_st.states):
         assert np.array_equal(x, y)
+
+
+def test_warm_budget_falls_back_to_freestream(wf):
+    """A warm start the rule has not stopped within the warm budget restarts
+    from freestream with the rest of the step cap: with a budget below the
+    rule's 8 checks x 25 steps every case falls back, and each result is the
+    freestream solve's under the remaining cap, with the warm steps added."""
+    m, a = np.array([0.55, 2.2, 0.75]), np.array([1.0, -2.0, 3.0])
+    t, s = wf.truth(m, a, ref_steps=2500, confirm_steps=500)
+    budget, cap = wf.warm_budget, wf.max_steps
+    wf.warm_budget = 100
+    try:
+        r = wf.solve(m, a, t, s, "mlp")
+        wf.max_steps = cap - 100
+        cold = wf.solve(m, a, t, s, "cold")
+    finally:
+        wf.warm_budget, wf.max_steps = budget, cap
+    for x, y in zip(r.results, cold.results):
+        assert x["fallback"] and x["warm_steps"] == 100
+        assert x["steps"] == y["steps"] + 100 and x["stopping_step"] == y["stopping_step"] + 100
+        assert (x["status"], x["cd"], x["cl"]) == (y["status"], y["cd"], y["cl"])
