@@ -321,72 +321,6 @@ __device__ __forceinline__ void geo_groups(const Seg<T>& s, int c, int g0, T out
   }
 }
 
-// Packed float32 pairs: Blackwell's two-wide FMA/add/mul (one instruction
-// for two values, each rounded to nearest as its scalar form is).
-namespace x2 {
-__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-// a - b, rounded once: fma(b, -1, a)
-__device__ __forceinline__ float2 sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
-}  // namespace x2
-
-// K1's fast float32 gradient, limiter and face states (euler_solver.py:45-98,
-// helper.py:136-153) on the primitive pairs (rho, u) and (v, p): the LSQ
-// gradient from the precomputed coefficients, Venkatakrishnan (K = 0) limited
-// by the min over the three faces, then the cell's face states.
-__device__ __forceinline__ void recon_faces_fast(const float Pc[4], const float Pk[3][4], const float gc[12],
-                                                 int nbw, const Consts<float>& kc, float4* __restrict__ FV,
-                                                 long long total, long long gi) {
-  const float2 pc[2] = {make_float2(Pc[0], Pc[1]), make_float2(Pc[2], Pc[3])};
-  const float cx[3] = {gc[G_C0X - 12], gc[G_C1X - 12], gc[G_C2X - 12]};
-  const float cy[3] = {gc[G_C0Y - 12], gc[G_C1Y - 12], gc[G_C2Y - 12]};
-  const float fx[3] = {gc[G_F0X - 12], gc[G_F1X - 12], gc[G_F2X - 12]};
-  const float fy[3] = {gc[G_F0Y - 12], gc[G_F1Y - 12], gc[G_F2Y - 12]};
-  const float2 two = x2::splat(2.0f), veps = x2::splat(kc.venk_eps);
-  float2 D[3][2], phi[2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    float2 dk[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) dk[k] = x2::sub(make_float2(Pk[k][2 * h], Pk[k][2 * h + 1]), pc[h]);
-    const float2 gx = x2::fma(x2::splat(cx[2]), dk[2], x2::fma(x2::splat(cx[1]), dk[1], x2::mul(x2::splat(cx[0]), dk[0])));
-    const float2 gy = x2::fma(x2::splat(cy[2]), dk[2], x2::fma(x2::splat(cy[1]), dk[1], x2::mul(x2::splat(cy[0]), dk[0])));
-    // neighbourhood bounds relative to the cell: max(0, dk) and min(0, dk)
-    const float2 up = make_float2(fmaxf(fmaxf(0.0f, dk[0].x), fmaxf(dk[1].x, dk[2].x)),
-                                  fmaxf(fmaxf(0.0f, dk[0].y), fmaxf(dk[1].y, dk[2].y)));
-    const float2 lo = make_float2(fminf(fminf(0.0f, dk[0].x), fminf(dk[1].x, dk[2].x)),
-                                  fminf(fminf(0.0f, dk[0].y), fminf(dk[1].y, dk[2].y)));
-    float2 ph = make_float2(1.0f, 1.0f);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float2 d = x2::fma(x2::splat(fy[k]), gy, x2::mul(x2::splat(fx[k]), gx));
-      D[k][h] = d;
-      // the bound on the side the face extrapolates to (used where |d| > eps_lim)
-      const float2 a = make_float2(d.x > 0.0f ? up.x : lo.x, d.y > 0.0f ? up.y : lo.y);
-      const float2 aa = x2::mul(a, a), ab = x2::mul(a, d);
-      const float2 num = x2::fma(two, ab, aa);
-      const float2 den = x2::add(x2::fma(two, x2::mul(d, d), x2::add(aa, ab)), veps);
-      const float px = fabsf(d.x) > kc.eps_lim ? __fdividef(num.x, den.x) : 1.0f;
-      const float py = fabsf(d.y) > kc.eps_lim ? __fdividef(num.y, den.y) : 1.0f;
-      ph = (k == 0) ? make_float2(px, py) : make_float2(fminf(ph.x, px), fminf(ph.y, py));
-    }
-    phi[h] = ph;
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float4 o;
-    if (slot_kind(nbw, k) == K_INTERIOR) {
-      const float2 o01 = x2::fma(phi[0], D[k][0], pc[0]), o23 = x2::fma(phi[1], D[k][1], pc[1]);
-      o = make_float4(o01.x, o01.y, o23.x, o23.y);
-    } else {
-      o = make_float4(Pc[0], Pc[1], Pc[2], Pc[3]);
-    }
-    FV[(long long)k * total + gi] = o;
-  }
-}
-
 // --------------------------------------------------------------- K1 recon
 // euler_solver.py:106-122 build_reconstruction for MUSCL: BC ghosts, LSQ
 // gradient (helper.py:136-153), limiter (euler_solver.py:45-67) and the cell's
@@ -437,10 +371,6 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, LOCALDT ? ESR_
   }
   T gc[12];   // LSQ coefficients and face offsets (groups 3-5)
   geo_groups<T, 3>(s, c, 3, gc);
-  if constexpr (kFastPath<T, FAST>) {
-    recon_faces_fast(Pc, Pk, gc, nb.w, kc, FV, total, gi);
-    return;
-  }
   T gx[4], gy[4];
   if constexpr (!FAST && sizeof(T) == 4) {
     // helper.py:136-153 per call, in the reference's float32 rounding:

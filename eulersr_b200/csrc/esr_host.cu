@@ -61,6 +61,13 @@ struct DevBuf {
     if (e != cudaSuccess) { p = nullptr; return fail(ESR_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
     return ESR_OK;
   }
+  // at least `count` elements, keeping the buffer when it is large enough: a
+  // call that runs often allocates once and frees nothing (cudaFree waits for
+  // every stream of the device, including other solvers' work)
+  int reserve(size_t count) {
+    if (p && n >= count) return ESR_OK;
+    return alloc(count);
+  }
 };
 
 // page-locked host memory owned by the solver (tables of the overlapped copies)
@@ -1396,11 +1403,13 @@ struct SolverT : SolverBase {
     }
     return ESR_OK;
   }
+  DevBuf<V> probe_save;      // residual probe: the state it restores
+  DevBuf<double> grad_out;   // gradient export
   int residual_probe(double* rel) {
     // one step of every running slot from the current state without keeping it
     // (euler/main.py:228-230): ||W_probe - W|| / (||W|| + 1e-16)
-    DevBuf<V> save;
-    ESR_TRY(save.alloc(total));
+    DevBuf<V>& save = probe_save;
+    ESR_TRY(save.reserve(total));
     ESR_CUDA(cudaMemcpyAsync(save.p, W.p, total * sizeof(V), cudaMemcpyDeviceToDevice, stream));
     std::vector<int> act(n_slots), st(n_slots);
     ESR_CUDA(cudaMemcpyAsync(act.data(), active.p, n_slots * sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1432,8 +1441,8 @@ struct SolverT : SolverBase {
     ESR_TRY(mesh_of_slot(slot, m, b));
     MeshDev& md = *meshes[m];
     const int N = md.hm->n_cells, tb = 128, nb = (N + tb - 1) / tb;
-    DevBuf<double> g;
-    ESR_TRY(g.alloc((size_t)8 * N));
+    DevBuf<double>& g = grad_out;
+    ESR_TRY(g.reserve((size_t)8 * N));
     k_grad_export<T><<<nb, tb, 0, stream>>>(d_segs.p, m, b, W.p, inlet.p, md.inv.p, slot, kc, g.p);
     ++launches;
     ESR_CUDA(cudaGetLastError());
@@ -1535,8 +1544,9 @@ struct SolverT : SolverBase {
   // A batch in flight: its queue and result buffers, the captured chunk graph
   // and the host's polling state, held between esr_batch_submit and
   // esr_batch_results (esr_batch_solve runs the three steps in one call).
+  BatchBufs batch_bufs;   // reused by every batch (one pending at a time)
   struct PendingBatch {
-    BatchBufs B;
+    BatchBufs* Bp = nullptr;
     Queue<T> q{};
     SlotParams<T> sp{};
     std::vector<int> case_mesh;
@@ -1581,6 +1591,7 @@ struct SolverT : SolverBase {
     }
     auto owned = std::make_unique<PendingBatch>();
     PendingBatch& pb = *owned;
+    pb.Bp = &batch_bufs;
     pb.n = n;
     pb.want_states = want_states;
     if (n == 0) {   // nothing to run: the slots are left as they are
@@ -1619,7 +1630,7 @@ struct SolverT : SolverBase {
       ESR_CUDA(cudaMemcpy(perm_ptrs.p, pp.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
       ESR_CUDA(cudaMemcpy(inv_ptrs.p, ip.data(), nm * sizeof(const int*), cudaMemcpyHostToDevice));
     }
-    BatchBufs& B = pb.B;
+    BatchBufs& B = *pb.Bp;
     // queue: cases grouped by mesh, submission order inside a mesh
     std::vector<int> qlist, qoff(nm + 1, 0);
     for (int m = 0; m < nm; ++m) {
@@ -1651,7 +1662,7 @@ struct SolverT : SolverBase {
     const bool want_states = pb.want_states;
     auto up = [&](auto& buf, const auto& v) -> int {
       using E = typename std::decay_t<decltype(v)>::value_type;
-      ESR_TRY(buf.alloc(std::max<size_t>(v.size(), 1)));
+      ESR_TRY(buf.reserve(std::max<size_t>(v.size(), 1)));
       if (!v.empty()) ESR_CUDA(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice, stream));
       return ESR_OK;
     };
@@ -1670,11 +1681,11 @@ struct SolverT : SolverBase {
     ESR_TRY(up(B.init_off, hinit_off));
     ESR_TRY(up(B.out_off, hout_off));
     for (DevBuf<int>* b : {&B.qhead, &B.n_done}) {
-      ESR_TRY(b->alloc(std::max(nm, 1)));
+      ESR_TRY(b->reserve(std::max(nm, 1)));
       ESR_CUDA(cudaMemsetAsync(b->p, 0, std::max(nm, 1) * sizeof(int), stream));
     }
-    ESR_TRY(B.slot_case.alloc(n_slots));
-    ESR_TRY(B.retiring.alloc(n_slots));
+    ESR_TRY(B.slot_case.reserve(n_slots));
+    ESR_TRY(B.retiring.reserve(n_slots));
     std::vector<int> minus(n_slots, -1);
     ESR_CUDA(cudaMemcpyAsync(B.slot_case.p, minus.data(), n_slots * sizeof(int), cudaMemcpyHostToDevice, stream));
     ESR_CUDA(cudaMemsetAsync(B.retiring.p, 0, n_slots * sizeof(int), stream));
@@ -1683,19 +1694,19 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaMemcpyAsync(d_live.p, h_live_full.data(), h_live_full.size() * sizeof(int4), cudaMemcpyHostToDevice,
                              stream));
     for (DevBuf<int>* b : {&B.r_status, &B.r_stop, &B.r_steps, &B.r_nmax, &B.r_eng_conv, &B.r_eng_stop})
-      ESR_TRY(b->alloc(n));
-    for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time, &B.r_probe}) ESR_TRY(b->alloc(n));
+      ESR_TRY(b->reserve(n));
+    for (DevBuf<double>* b : {&B.r_dt, &B.r_rel, &B.r_cd, &B.r_cl, &B.r_time, &B.r_probe}) ESR_TRY(b->reserve(n));
     if (Wp.n < (size_t)total) ESR_TRY(Wp.alloc(total));
     if (move_src.n < (size_t)n_slots) ESR_TRY(move_src.alloc(n_slots));
     if (init_rows > 0) {
-      ESR_TRY(B.init.alloc((size_t)4 * init_rows));
+      ESR_TRY(B.init.reserve((size_t)4 * init_rows));
       for (int i = 0; i < n; ++i)
         if (init && init[i])
           ESR_CUDA(cudaMemcpyAsync(B.init.p + 4 * hinit_off[i], init[i],
                                    (size_t)4 * meshes[cs[i].mesh]->hm->n_cells * sizeof(double),
                                    cudaMemcpyHostToDevice, stream));
     }
-    if (want_states) ESR_TRY(B.out.alloc((size_t)4 * out_rows));
+    if (want_states) ESR_TRY(B.out.reserve((size_t)4 * out_rows));
     ESR_CUDA(cudaStreamSynchronize(stream));   // host vectors above are the copy sources
     pb.q = Queue<T>{nm, B.qlist.p, B.qoff.p, B.qhead.p, B.slot_case.p, B.retiring.p, B.c_inlet.p, B.c_strength.p,
                B.c_cfl.p, B.c_tf.p, B.c_max_steps.p, B.c_qref.p, B.c_eng_track.p, B.c_eng_pat.p, B.c_eng_t.p, B.c_thr.p,
@@ -1741,7 +1752,7 @@ struct SolverT : SolverBase {
         }
       }
       if (rc == ESR_OK) {
-        cudaError_t e = cudaMemcpyAsync(&pb.done, pb.B.n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaMemcpyAsync(&pb.done, pb.Bp->n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch poll: ") + cudaGetErrorString(e));
       }
@@ -1765,7 +1776,7 @@ struct SolverT : SolverBase {
     const int n = pb.n;
     if (n > 0 && !out) return fail(ESR_ERR_ARG, "batch_results: null results");
     if (n == 0) return batch_cancel(false);
-    BatchBufs& B = pb.B;
+    BatchBufs& B = *pb.Bp;
     ESR_CUDA(cudaEventRecord(ev1, stream));
     std::vector<int> st(n), sstop(n), ssteps(n), snmax(n), sec(n), ses(n);
     std::vector<double> sdt(n), srel(n), scd(n), scl(n), stime(n), sprobe(n);
