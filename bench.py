@@ -418,15 +418,18 @@ def run_throughput(args, world, rank, local, report=True):
     hbm, peak_kind = peaks()
     alg_k2 = (40 + 64 / B_eff) * N * B
     k2_gbs = alg_k2 / (kt["flux_ms"] * 1e-3) / 1e9
+    # DRAM traffic per item of the K2 form in use, from its ncu summary
     traffic = None
-    pf = ROOT / "profiles" / "k_flux_naca0012_h0.025_b128.md"
+    patches = bool(tuning.get("k2_patches"))
+    k2_name = "k_flux_patch (K2 by patches)" if patches else "k_flux (K2 per cell)"
+    pf = ROOT / "profiles" / ("k_flux_patch_naca0012_h0.025_b128.md" if patches else "k_flux_naca0012_h0.025_b128.md")
     if pf.exists():
         for line in pf.read_text().splitlines():
             if line.startswith("traffic_bytes_per_item_per_launch"):
                 traffic = float(line.split("=")[1].split()[0]) * N * B
     roofline = {"bound": "hbm", "achieved": k2_gbs, "peak": hbm, "unit": "GB/s", "frac": k2_gbs / hbm,
                 "traffic": traffic, "traffic_source": f"ncu capture in profiles/{pf.name}, per item, scaled by items",
-                "kernel": "k_flux (K2)", "peak_source": peak_kind, "kernel_ms": kt["flux_ms"],
+                "kernel": k2_name, "peak_source": peak_kind, "kernel_ms": kt["flux_ms"],
                 "recon_ms": kt["recon_ms"], "alg_bytes_per_launch": alg_k2,
                 "workload": f"batched {args.workload} workload, {B} cases per GPU, one launch",
                 "note": "K2 is issue-bound; see profiles/"}
