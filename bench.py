@@ -711,6 +711,22 @@ def run_warm(args, world, rank, local):
         wf.schedule = "lr_longest_first"
     fifo = {"value": allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world),
             "converged": r.converged, "seconds": r.seconds, "parts_s": r.parts_s}
+    # the protocol variant with unsteady-flagged cases capped at --unsteady-cap
+    # steps for every start (they fail for every start whatever they do)
+    capped_proto = None
+    if args.unsteady_cap:
+        wf.unsteady_cap = args.unsteady_cap
+        try:
+            cp = {}
+            for start in ("mlp", "single"):
+                flush.add_(1.0)
+                barrier(world)
+                r = wf.solve(me, ae, truth, steady, start)
+                cp[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
+        finally:
+            wf.unsteady_cap = None
+        capped_proto = {"unsteady_cap_steps": args.unsteady_cap, "warm_mlp_batched": cp["mlp"],
+                        "plain_single_case": cp["single"], "ratio": cp["mlp"] / cp["single"] if cp["single"] else None}
     # a stream of batches, as a campaign runs them: the next batch's LR solve
     # and prediction overlap this batch's HR solve
     flush.add_(1.0)
@@ -780,7 +796,7 @@ def run_warm(args, world, rank, local):
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
                     "by_case_class": by_class, "warm_mlp_streamed": streamed,
-                    "warm_mlp_fifo_queue": fifo},
+                    "warm_mlp_fifo_queue": fifo, "unsteady_capped_protocol": capped_proto},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",
@@ -812,6 +828,9 @@ def main():
     ap.add_argument("--train-steps", type=int, default=2000, help="warm workload: MLP training steps")
     ap.add_argument("--warm-budget", type=int, default=3000,
                     help="warm workload: steps after which an unstopped warm start restarts from freestream (0: never)")
+    ap.add_argument("--unsteady-cap", type=int, default=3000,
+                    help="warm workload: extra leg with unsteady-flagged cases capped at this many steps for every "
+                         "start (0: skip the leg)")
     ap.add_argument("--make-truth", action="store_true", help="write the held-out cases' reference CDs and exit")
     ap.add_argument("--block", default="0", help="throughput workloads: 0 (autotuned), 64, 128, 256 or patches")
     args = ap.parse_args()

@@ -75,7 +75,7 @@ def _device_timed(fn):
 class WarmStartWorkflow:
     def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=6000, max_steps=12000,
                  check_every=25, patience=8, cd_tol=0.005, device=0, schedule="lr_longest_first",
-                 warm_budget=3000):
+                 warm_budget=3000, unsteady_cap=None):
         self.hr, self.lr = cached_mesh(geom, h_hr), cached_mesh(geom, h_lr)
         self.pair = MeshPair.build(self.hr, self.lr)
         self.dm_hr, self.dm_lr = DeviceMesh(self.hr), DeviceMesh(self.lr)
@@ -86,6 +86,7 @@ class WarmStartWorkflow:
             raise ValueError("schedule must be 'lr_longest_first' or 'fifo'")
         self.schedule = schedule
         self.warm_budget = warm_budget   # None or 0: no fallback to freestream
+        self.unsteady_cap = unsteady_cap   # None: unsteady-flagged cases run to max_steps too
         self.ws = WarmStart(self.pair, device=f"cuda:{device}")
         self._solvers = {}
         self.train_info = {}
@@ -114,6 +115,9 @@ class WarmStartWorkflow:
         return self._solver(("grad",), self.dm_lr, 1, precision="f64", stream_priority=-100)
 
     def _cases(self, machs, aoas, targets=None, max_steps=None, dtype=np.float32):
+        """FlowCases; max_steps: None (the workflow's cap), one cap, or one per case."""
+        caps = np.broadcast_to(np.asarray(self.max_steps if max_steps is None else max_steps, dtype=np.int64),
+                               (len(machs),))
         out = []
         for i, (m, a) in enumerate(zip(machs, aoas)):
             kw = {}
@@ -121,8 +125,18 @@ class WarmStartWorkflow:
                 kw = dict(eng_target_cd=float(targets[i]), eng_target_cl=0.0, eng_cd_tol=self.cd_tol,
                           eng_cl_tol=1e12, eng_patience=self.patience)
             out.append(FlowCase(mach=float(m), aoa_deg=float(a), cfl=0.6, tf=1e9,
-                                max_steps=int(max_steps or self.max_steps), dtype=dtype, **kw))
+                                max_steps=int(caps[i]), dtype=dtype, **kw))
         return out
+
+    def caps(self, steady):
+        """Step cap of each HR case: ``max_steps``, or ``unsteady_cap`` for a
+        case whose reference is flagged unsteady (it counts as a failure for
+        every start whatever it does, so every start stops it there)."""
+        steady = np.asarray(steady, dtype=bool)
+        c = np.full(len(steady), self.max_steps, dtype=np.int64)
+        if self.unsteady_cap:
+            c[~steady] = min(self.max_steps, int(self.unsteady_cap))
+        return c
 
     def close(self):
         for s in self._solvers.values():
@@ -167,6 +181,8 @@ class WarmStartWorkflow:
         """HR batch solve with the cases queued in `order`; results (and
         states) returned in the callers' case order."""
         order = np.asarray(order)
+        if max_steps is not None and np.ndim(max_steps) > 0:
+            max_steps = np.asarray(max_steps)[order]
         cases = self._cases(np.asarray(machs)[order], np.asarray(aoas)[order], np.asarray(truth)[order],
                             max_steps=max_steps)
         init_q = None if inits is None else [inits[i] for i in order]
@@ -220,26 +236,29 @@ class WarmStartWorkflow:
         steady = np.abs(cd - cd_a) <= 1e-3 * np.abs(cd)
         return cd, steady
 
-    def _hr_warm(self, s, machs, aoas, truth, inits, order, want_states=False):
-        """HR solve from the warm fields. With a warm budget, a case the rule
-        has not stopped within ``warm_budget`` steps restarts from freestream
-        with the rest of the step cap (the plain start is the fallback: a
-        prediction that leaves, say, spurious entropy on the body can take far
-        longer to wash out than a freestream start takes to converge). Its
-        result carries ``fallback`` and the warm steps spent, counted in its
-        ``steps`` and ``stopping_step``."""
+    def _hr_warm(self, s, machs, aoas, truth, inits, order, caps, want_states=False):
+        """HR solve from the warm fields, case i capped at caps[i] steps. With
+        a warm budget, a case the rule has not stopped within ``warm_budget``
+        steps restarts from freestream with the rest of its cap (the plain
+        start is the fallback: a prediction can leave the solve on another
+        steady state, e.g. with a bow shock held at the LR mesh's stand-off).
+        Its result carries ``fallback`` and the warm steps spent, counted in
+        its ``steps`` and ``stopping_step``."""
         machs, aoas, truth = np.asarray(machs), np.asarray(aoas), np.asarray(truth)
-        budget = self.warm_budget if (self.warm_budget and self.warm_budget < self.max_steps) else None
+        caps = np.asarray(caps, dtype=np.int64)
+        budget = np.minimum(caps, self.warm_budget) if self.warm_budget else caps
         res, states = self._hr_batch(s, machs, aoas, truth, inits, order, want_states, max_steps=budget)
-        if budget is None:
+        if not self.warm_budget:
             return res, states
         rank = np.empty(len(order), dtype=np.int64)
         rank[np.asarray(order)] = np.arange(len(order))
-        fb = np.array(sorted((i for i, r in enumerate(res) if r["status"] != 2), key=lambda i: rank[i]), dtype=np.int64)
+        fb = np.array(sorted((i for i, r in enumerate(res) if r["status"] != 2 and caps[i] > int(r["steps"])),
+                             key=lambda i: rank[i]), dtype=np.int64)
         if len(fb) == 0:
             return res, states
+        spent_fb = np.array([int(res[i]["steps"]) for i in fb], dtype=np.int64)
         res2, st2 = self._hr_batch(s, machs[fb], aoas[fb], truth[fb], None, np.arange(len(fb)), want_states,
-                                   max_steps=self.max_steps - budget)
+                                   max_steps=caps[fb] - spent_fb)
         for j, i in enumerate(fb):
             r = dict(res2[j])
             spent = int(res[i]["steps"])
@@ -284,7 +303,7 @@ class WarmStartWorkflow:
                 torch.cuda.set_device(self.device)     # a new host thread starts on device 0
                 m, a = batches[k]
                 t = time.perf_counter()
-                box["res"], _ = self._hr_warm(s, m, a, truth_of[k], *warm)
+                box["res"], _ = self._hr_warm(s, m, a, truth_of[k], *warm, self.caps(steady_of[k]))
                 box["s"] = time.perf_counter() - t
             except BaseException as e:   # re-raised in the caller's thread
                 box["err"] = e
@@ -330,13 +349,14 @@ class WarmStartWorkflow:
             if start in ("cold", "single"):
                 s = self._hr_solver(1 if start == "single" else min(self.slots, len(machs)))
                 t = time.perf_counter()
-                res, states = s.batch_solve(self._cases(machs, aoas, truth), want_states=want_states)
+                res, states = s.batch_solve(self._cases(machs, aoas, truth, max_steps=self.caps(steady)),
+                                            want_states=want_states)
                 parts["hr_solve_s"] = time.perf_counter() - t
                 return res, states
             inits, order = self.warm_fields(machs, aoas, use_mlp=(start == "mlp"), parts=parts)
             s = self._hr_solver(min(self.slots, len(machs)))
             t = time.perf_counter()
-            res, states = self._hr_warm(s, machs, aoas, truth, inits, order, want_states)
+            res, states = self._hr_warm(s, machs, aoas, truth, inits, order, self.caps(steady), want_states)
             parts["hr_solve_s"] = time.perf_counter() - t
             return res, states
 

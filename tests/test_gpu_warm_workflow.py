@@ -70,3 +70,22 @@ def test_warm_budget_falls_back_to_freestream(wf):
         assert x["fallback"] and x["warm_steps"] == 100
         assert x["steps"] == y["steps"] + 100 and x["stopping_step"] == y["stopping_step"] + 100
         assert (x["status"], x["cd"], x["cl"]) == (y["status"], y["cd"], y["cl"])
+
+
+def test_unsteady_cap_stops_flagged_cases_for_every_start(wf):
+    """With an unsteady cap, a case whose reference is flagged unsteady stops
+    there for every start, and the other cases' results do not change."""
+    m, a = np.array([0.6, 2.4, 0.7]), np.array([1.0, 2.0, -1.0])
+    t, _ = wf.truth(m, a, ref_steps=2500, confirm_steps=500)
+    flag = np.array([True, False, True])
+    base = {st: wf.solve(m, a, t, flag, st) for st in ("mlp", "cold")}
+    wf.unsteady_cap = 300
+    try:
+        capped = {st: wf.solve(m, a, t, flag, st) for st in ("mlp", "cold")}
+    finally:
+        wf.unsteady_cap = None
+    for st in ("mlp", "cold"):
+        r, b = capped[st].results, base[st].results
+        assert r[1]["steps"] <= 300 and not r[1].get("fallback")
+        for i in (0, 2):
+            assert (r[i]["steps"], r[i]["cd"], r[i]["status"]) == (b[i]["steps"], b[i]["cd"], b[i]["status"])
