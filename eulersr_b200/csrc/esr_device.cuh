@@ -722,11 +722,14 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, ESR_K2_MINB>))
 // ----------------------------------------------------- K2 by patches (float32)
 // The face-flux form of K2 for batched float32 HLLC + MUSCL solves: one block
 // per (patch of <= kPatchCells cells, group of 32 case slots), one warp per
-// cell at a time with its lanes over the 32 slots. Phase 1 evaluates every
+// cell at a time with its lanes over the 32 slots. Phase 0 copies the face
+// states of the patch's cells into shared memory (asynchronous 16-byte
+// copies, all issued before any is waited for). Phase 1 evaluates every
 // face of the patch's cells once: an inner face (both cells in the patch) by
-// its owner, the lower cell, which stores F and -F in shared memory for both
-// cells; a face to a cell outside the patch and a boundary face by the cell
-// itself (the canonical flux, from the owner's side). Phase 2 forms each
+// its owner, the lower cell, from the two face states in shared memory,
+// storing F and -F over them for both cells; a face to a cell outside the
+// patch (the neighbour's face state read from global memory) and a boundary
+// face by the cell itself (the canonical flux, from the owner's side). Phase 2 forms each
 // cell's residual sum_k s_k F_k in slot order from shared memory (a
 // deterministic cell-owned sum, no atomics), then the sponge and the stage
 // update as k_flux. The fluxes equal k_flux's bit for bit.
@@ -741,6 +744,15 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, ESR_K2_MINB>))
 #endif
 constexpr int kPatchWarps = ESR_PATCH_WARPS;
 
+// 16-byte asynchronous global -> shared copy (zero-filled when !valid; the
+// source address is read only when valid)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int STAGE, bool LOCALDT, int MINB = ESR_PATCH_MINB>
 __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg<float>* __restrict__ segs,
                                                                   const int4* __restrict__ pblk,
@@ -751,7 +763,8 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
                                                                   Cases<float> cs, Consts<float> kc, int pos,
                                                                   const float* __restrict__ dt_local,
                                                                   float* __restrict__ res_out) {
-  __shared__ float4 G[kPatchCells][3][32];   // signed face fluxes of the patch's cells (1.5 KB per cell)
+  // the patch's face states, then in place its signed face fluxes (1.5 KB per cell)
+  __shared__ float4 G[kPatchCells][3][32];
   const int4 pb = pblk[blockIdx.x];          // segment, patch, first slot
   const Seg<float> s = segs[pb.x];
   const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];
@@ -761,39 +774,52 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
   const int g = s.case0 + (in_seg ? b : 0);
   const bool live = in_seg && cs.active[g] && cs.step[g] + pos < cs.nmax[g];
   if (!__syncthreads_or(live)) return;        // every slot of the group idle
-  const bool warp_live = __any_sync(0xffffffffu, live);
   const float4 inlet = cs.inlet[g];
-  if (warp_live) {
-    for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
-      const int c = c0 + lc;
-      const long long gi = s.off + (long long)c * s.B + b;
-      const int4 nb = __ldg(s.nbr + c);
-      const int nbk[3] = {nb.x, nb.y, nb.z};
-      float gk[12];
-      geo_groups<float, 3>(s, c, 0, gk);
+  // Phase 0: every face state of the patch's cells (this block's 32 slots)
+  // into G by asynchronous copies, all in flight at once.
+  for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
+    const long long gi = s.off + (long long)(c0 + lc) * s.B + b;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const int kind = slot_kind(nb.w, k);
-        const float nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
-        const int j = nbk[k];
-        const bool inner = kind == K_INTERIOR && j >= c0 && j < c1;
-        if (inner && j < c) continue;   // the owner, inside the patch, stores this one
-        float qL[4] = {0.f, 0.f, 0.f, 0.f}, qR[4] = {0.f, 0.f, 0.f, 0.f};
-        if (in_seg) {
-          const float4 fl = FV[(long long)k * total + gi];
-          qL[0] = fl.x; qL[1] = fl.y; qL[2] = fl.z; qL[3] = fl.w;
-          if (kind == K_INTERIOR) {
-            const float4 fr = FV[(long long)slot_opp(nb.w, k) * total + s.off + (long long)j * s.B + b];
-            qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
-          } else {
-            xr::ghost_prim(kind, Win[gi], nx, ny, inlet, kc, qR);
-          }
+    for (int k = 0; k < 3; ++k) cp_async16(&G[lc][k][lane], FV + (long long)k * total + (in_seg ? gi : 0), in_seg);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  // Phase 1. Each slot G[cell][face] is read and then overwritten by exactly
+  // one evaluation, that of the face's owner (an inner face's other cell
+  // skips it), so the fluxes can replace the face states in place.
+  for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
+    const int c = c0 + lc;
+    const long long gi = s.off + (long long)c * s.B + b;
+    const int4 nb = __ldg(s.nbr + c);
+    const int nbk[3] = {nb.x, nb.y, nb.z};
+    float gk[12];
+    geo_groups<float, 3>(s, c, 0, gk);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int kind = slot_kind(nb.w, k);
+      const float nx = gk[G_N0X + 2 * k], ny = gk[G_N0Y + 2 * k];
+      const int j = nbk[k];
+      const bool inner = kind == K_INTERIOR && j >= c0 && j < c1;
+      if (inner && j < c) continue;   // the owner, inside the patch, stores this one
+      const int ko = slot_opp(nb.w, k);
+      const float4 fl = G[lc][k][lane];
+      const float qL[4] = {fl.x, fl.y, fl.z, fl.w};
+      float qR[4] = {0.f, 0.f, 0.f, 0.f};
+      if (inner) {
+        const float4 fr = G[j - c0][ko][lane];
+        qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
+      } else if (in_seg) {
+        if (kind == K_INTERIOR) {
+          const float4 fr = FV[(long long)ko * total + s.off + (long long)j * s.B + b];
+          qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
+        } else {
+          xr::ghost_prim(kind, Win[gi], nx, ny, inlet, kc, qR);
         }
-        float F[4];
-        xr::face_flux(qL, qR, nx, ny, kind == K_INTERIOR && j < c, kc, F);   // owner outside: its side, negated
-        G[lc][k][lane] = make_float4(F[0], F[1], F[2], F[3]);
-        if (inner) G[j - c0][slot_opp(nb.w, k)][lane] = make_float4(-F[0], -F[1], -F[2], -F[3]);
       }
+      float F[4];
+      xr::face_flux(qL, qR, nx, ny, kind == K_INTERIOR && j < c, kc, F);   // owner outside: its side, negated
+      G[lc][k][lane] = make_float4(F[0], F[1], F[2], F[3]);
+      if (inner) G[j - c0][ko][lane] = make_float4(-F[0], -F[1], -F[2], -F[3]);
     }
   }
   __syncthreads();

@@ -425,7 +425,12 @@ struct SolverT : SolverBase {
   int build_patch_blocks() {
     std::vector<int4> h;
     for (int m = 0; m < (int)meshes.size(); ++m) {
-      const int np = (int)meshes[m]->hm->patch_start.size() - 1;
+      const std::vector<int>& ps = meshes[m]->hm->patch_start;
+      const int np = (int)ps.size() - 1;
+      // the kernel's shared arrays hold kPatchCells cells
+      for (int p = 0; p < np; ++p)
+        if (ps[p + 1] - ps[p] < 1 || ps[p + 1] - ps[p] > kPatchCells)
+          return fail(ESR_ERR_STATE, "patch table: a patch has " + std::to_string(ps[p + 1] - ps[p]) + " cells");
       for (int p = 0; p < np; ++p)
         for (int b0 = 0; b0 < meshes[m]->B; b0 += 32) h.push_back(make_int4(m, p, b0, 0));
     }
