@@ -68,10 +68,13 @@ __device__ __forceinline__ int cell_of(const Seg<T>& s, int item) {
 // cell and slot of thread item `item` of segment s: items walk (cell, slot)
 // over the first A slots of every cell, A = live slots (B until a batch's
 // queue drains and compaction packs its running cases into slots 0..A-1),
-// so once few cases remain the work lands on few warps with full lanes
+// so once few cases remain the work lands on few warps with full lanes. A
+// one-slot segment has no live record (s.live null: nothing to pack), which
+// spares its small, latency-bound launches the dependent load.
 template <typename T>
 __device__ __forceinline__ bool item_slot(const Seg<T>& s, int item, int& c, int& b) {
-  const int4 L = *s.live;
+  int4 L = make_int4(s.B, 0, 0, 0);
+  if (s.live != nullptr) L = *s.live;
   if (L.x == s.B) {
     if (item >= s.n_cells * s.B) return false;
     c = cell_of(s, item);

@@ -339,7 +339,7 @@ struct SolverT : SolverBase {
     }
     ESR_TRY(d_live.alloc(hsegs.size()));
     ESR_CUDA(cudaMemcpy(d_live.p, h_live_full.data(), hsegs.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    for (size_t m = 0; m < hsegs.size(); ++m) hsegs[m].live = d_live.p + m;
+    for (size_t m = 0; m < hsegs.size(); ++m) hsegs[m].live = hsegs[m].B > 1 ? d_live.p + m : nullptr;
     ESR_TRY(d_segs.alloc(hsegs.size()));
     ESR_CUDA(cudaMemcpy(d_segs.p, hsegs.data(), hsegs.size() * sizeof(Seg<T>), cudaMemcpyHostToDevice));
     hseg0 = hsegs[0];
