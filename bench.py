@@ -701,16 +701,16 @@ def run_warm(args, world, rank, local):
                 "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
                 "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
                 "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
-    # the same warm pass with the HR cases queued in submission order
+    # the same warm pass with the HR cases queued longest-first by their LR solve
     flush.add_(1.0)
     barrier(world)
-    wf.schedule = "fifo"
+    wf.schedule = "lr_longest_first"
     try:
         r = wf.solve(me, ae, truth, steady, "mlp")
     finally:
-        wf.schedule = "lr_longest_first"
-    fifo = {"value": allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world),
-            "converged": r.converged, "seconds": r.seconds, "parts_s": r.parts_s}
+        wf.schedule = "fifo"
+    lpt = {"value": allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world),
+           "converged": r.converged, "seconds": r.seconds, "parts_s": r.parts_s}
     # the protocol variant with unsteady-flagged cases capped at --unsteady-cap
     # steps for every start (they fail for every start whatever they do)
     capped_proto = None
@@ -785,8 +785,8 @@ def run_warm(args, world, rank, local):
                            "steady_cases": int(steady.sum()), "truth_check": truth_check,
                            "l2": "256 MB buffer overwritten between passes", "setup_s": setup_s,
                            "sharding": "parallel.shard_cases (cost-balanced LPT)",
-                           "hr_queue": "warm starts: cases queued by the LR solve's last relative change, "
-                                       "largest first (WarmStartWorkflow.hr_order); cold starts: submission order"},
+                           "hr_queue": "submission order (the LR-informed longest-first order is reported beside "
+                                       "it: no measurable gain)"},
                 "converged_cases_per_s": {
                     "warm_mlp_batched": value, "warm_idw_batched": base["idw"], "plain_batched": base["cold"],
                     "plain_single_case": base["single"], "ratio_warm_vs_plain_single_case": ratio["single"],
@@ -796,7 +796,7 @@ def run_warm(args, world, rank, local):
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
                     "by_case_class": by_class, "warm_mlp_streamed": streamed,
-                    "warm_mlp_fifo_queue": fifo, "unsteady_capped_protocol": capped_proto},
+                    "warm_mlp_lr_longest_first_queue": lpt, "unsteady_capped_protocol": capped_proto},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",

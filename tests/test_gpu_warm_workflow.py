@@ -38,13 +38,13 @@ def test_streamed_batches_equal_one_pass_each(wf):
 def test_queue_order_changes_no_result(wf):
     m, a = np.array([0.50, 0.72, 0.60, 2.8, 0.65, 1.2]), np.array([0.0, 2.0, -1.0, 3.0, 1.0, -2.0])
     t, s = wf.truth(m, a, ref_steps=2500, confirm_steps=500)
-    r_lpt = wf.solve(m, a, t, s, "mlp")
-    wf.schedule = "fifo"
+    wf.schedule = "lr_longest_first"
     try:
-        r_fifo = wf.solve(m, a, t, s, "mlp", want_states=True)
+        r_lpt = wf.solve(m, a, t, s, "mlp")
+        r_lpt_st = wf.solve(m, a, t, s, "mlp", want_states=True)
     finally:
-        wf.schedule = "lr_longest_first"
-    r_lpt_st = wf.solve(m, a, t, s, "mlp", want_states=True)
+        wf.schedule = "fifo"
+    r_fifo = wf.solve(m, a, t, s, "mlp", want_states=True)
     for key in ("stopping_step", "steps", "cd", "cl", "status"):
         assert [r[key] for r in r_lpt.results] == [r[key] for r in r_fifo.results], key
     for x, y in zip(r_fifo.states, r_lpt_st.states):
