@@ -823,6 +823,12 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, ESR_K2_MINB>))
 #ifndef ESR_PATCH_MINB_ALT
 #define ESR_PATCH_MINB_ALT 6
 #endif
+// 1: the patch's states are staged in shared memory too (ghost states and the
+// cell update read them there; 0.5 KB more per cell)
+#ifndef ESR_PATCH_STAGE_W
+#define ESR_PATCH_STAGE_W 0
+#endif
+constexpr bool kPatchStageW = ESR_PATCH_STAGE_W != 0;
 #ifndef ESR_PATCH_WARPS
 #define ESR_PATCH_WARPS 8
 #endif
@@ -849,6 +855,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
                                                                   float* __restrict__ res_out) {
   // the patch's face states, then in place its signed face fluxes (1.5 KB per cell)
   __shared__ float4 G[kPatchCells][3][32];
+  __shared__ float4 SW[kPatchStageW ? kPatchCells : 1][32];
   const int4 pb = pblk[blockIdx.x];          // segment, patch, first slot
   const Seg<float> s = segs[pb.x];
   const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];
@@ -865,6 +872,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
     const long long gi = s.off + (long long)(c0 + lc) * s.B + b;
 #pragma unroll
     for (int k = 0; k < 3; ++k) cp_async16(&G[lc][k][lane], FV + (long long)k * total + (in_seg ? gi : 0), in_seg);
+    if constexpr (kPatchStageW) cp_async16(&SW[lc][lane], Win + (in_seg ? gi : 0), in_seg);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -897,7 +905,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
           const float4 fr = FV[(long long)ko * total + s.off + (long long)j * s.B + b];
           qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
         } else {
-          xr::ghost_prim(kind, Win[gi], nx, ny, inlet, kc, qR);
+          xr::ghost_prim(kind, kPatchStageW ? SW[lc][lane] : Win[gi], nx, ny, inlet, kc, qR);
         }
       }
       float F[4];
@@ -911,7 +919,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
   for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
     const int c = c0 + lc;
     const long long gi = s.off + (long long)c * s.B + b;
-    const float4 Wc = Win[gi];
+    const float4 Wc = kPatchStageW ? SW[lc][lane] : Win[gi];
     float gk[12];
     geo_groups<float, 3>(s, c, 0, gk);
     float acc[4];
