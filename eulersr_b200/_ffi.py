@@ -88,26 +88,24 @@ TUNING_MAX_VARIANTS = 12
 
 class TuningVariant(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("k2_patches", C.c_int32), ("k1_minb", C.c_int32),
-                ("k2_minb", C.c_int32), ("k1_patches", C.c_int32), ("step_ms", C.c_double)]
+                ("k2_minb", C.c_int32), ("step_ms", C.c_double)]
 
     def as_dict(self):
         return {"block_size": int(self.block_size), "k2_patches": bool(self.k2_patches),
-                "k1_minb": int(self.k1_minb), "k2_minb": int(self.k2_minb), "k1_patches": bool(self.k1_patches),
-                "step_ms": float(self.step_ms)}
+                "k1_minb": int(self.k1_minb), "k2_minb": int(self.k2_minb), "step_ms": float(self.step_ms)}
 
 
 class Tuning(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("n_candidates", C.c_int32), ("candidates", C.c_int32 * 4),
                 ("k2_patches", C.c_int32), ("cached", C.c_int32), ("step_ms", C.c_double * 4),
                 ("k1_minb", C.c_int32), ("k2_minb", C.c_int32), ("n_variants", C.c_int32),
-                ("k1_patches", C.c_int32), ("variants", TuningVariant * TUNING_MAX_VARIANTS)]
+                ("reserved", C.c_int32), ("variants", TuningVariant * TUNING_MAX_VARIANTS)]
 
     def as_dict(self):
         n = int(self.n_candidates)
         name = lambda c: "patches" if c == BLOCK_PATCHES else int(c)
         return {"block_size": int(self.block_size), "k2_patches": bool(self.k2_patches),
                 "k1_minb": int(self.k1_minb), "k2_minb": int(self.k2_minb), "cached": bool(self.cached),
-                "k1_patches": bool(self.k1_patches),
                 "step_ms": {name(self.candidates[i]): float(self.step_ms[i]) for i in range(n)},
                 "variants": [self.variants[i].as_dict() for i in range(int(self.n_variants))]}
 

@@ -324,181 +324,6 @@ __device__ __forceinline__ void geo_groups(const Seg<T>& s, int c, int g0, T out
   }
 }
 
-enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
-
-// ---- the fast float32 face flux and cell update with every rounding written
-// out (__fmul_rn / __fadd_rn / __fsub_rn / __fmaf_rn are never fused or
-// split by the compiler), so the per-cell K2 and K2 by patches, which reach
-// the same faces from different code, round every face flux and every cell
-// update identically: a case's result does not depend on which K2 ran.
-namespace xr {
-__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-
-// helper.py:37-46 (M = 1)
-__device__ __forceinline__ void prim(const float4& W, float gm1, float half, float P[4]) {
-  const float r = W.x, ri = __fdividef(1.0f, r);
-  const float u = mul(W.y, ri), v = mul(W.z, ri);
-  P[0] = r; P[1] = u; P[2] = v;
-  P[3] = mul(sub(W.w, mul(mul(half, r), fma(u, u, mul(v, v)))), gm1);
-}
-// helper.py:25-35 (M = 1)
-__device__ __forceinline__ float4 cons(const float P[4], float inv_gm1, float half) {
-  const float r = P[0], u = P[1], v = P[2];
-  return make_float4(r, mul(r, u), mul(r, v), fma(mul(half, r), fma(u, u, mul(v, v)), mul(P[3], inv_gm1)));
-}
-// helper.py:233-256 boundary states, as primitives of the ghost (gamma 1.4)
-__device__ __forceinline__ void ghost_prim(int kind, const float4& Wc, float nx, float ny, const float4& inlet,
-                                           const Consts<float>& k, float Q[4]) {
-  float P[4];
-  if (kind == K_INLET) { prim(inlet, k.gm1, k.half, Q); return; }
-  if (kind != K_WALL && kind != K_SUBSONIC) { prim(Wc, k.gm1, k.half, Q); return; }   // outlet
-  prim(Wc, k.gm1_14, k.half, P);
-  float G[4];
-  if (kind == K_WALL) {       // helper.py:196-204
-    const float t = mul(2.0f, fma(P[1], nx, mul(P[2], ny)));
-    G[0] = P[0]; G[1] = sub(P[1], mul(t, nx)); G[2] = sub(P[2], mul(t, ny)); G[3] = P[3];
-  } else {                    // helper.py:179-194
-    G[0] = k.sub_rho; G[1] = k.sub_u; G[2] = k.sub_v; G[3] = P[3];
-  }
-  prim(cons(G, k.inv_gm1_14, k.half), k.gm1, k.half, Q);
-}
-// euler_solver.py:273-374 HLLC flux from the face primitives, the conserved
-// variables formed only for the side the wave fan selects
-__device__ __forceinline__ void hllc(const float PL[4], const float PR[4], float nx, float ny,
-                                     const Consts<float>& k, float F[4]) {
-  const float rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
-  const float rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
-  const float unL = fma(uL, nx, mul(vL, ny)), unR = fma(uR, nx, mul(vR, ny));
-  const float tx = -ny, ty = nx;
-  const float aL = sqrtf(fabsf(__fdividef(mul(k.gamma, pL), rL)));
-  const float aR = sqrtf(fabsf(__fdividef(mul(k.gamma, pR), rR)));
-  float SL = fminf(sub(unL, aL), sub(unR, aR));
-  float SR = fmaxf(add(unL, aL), add(unR, aR));
-  if (SL == SR) SL = sub(SL, k.ss_eps);
-  if (SL == SR) SR = add(SR, k.ss_eps);
-  const float dL = sub(SL, unL), dR = sub(SR, unR);
-  float den = sub(mul(rL, dL), mul(rR, dR));
-  if (den == 0.0f) den = k.den_eps;
-  const float Ss = __fdividef(sub(fma(mul(rL, unL), dL, sub(pR, pL)), mul(mul(rR, unR), dR)), den);
-  const float PsL = fma(mul(rL, dL), sub(Ss, unL), pL);
-  const float PsR = fma(mul(rR, dR), sub(Ss, unR), pR);
-  const float Ps = mul(k.half, add(PsL, PsR));
-  const bool c1 = SL >= 0.0f;
-  const bool c2 = (SL <= 0.0f) && (Ss >= 0.0f);
-  const bool c3 = (Ss <= 0.0f) && (SR >= 0.0f);
-  const bool left = c1 || c2;
-  const float rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
-  const float unK = left ? unL : unR, SK = left ? SL : SR, dK = left ? dL : dR;
-  const float EK = fma(mul(k.half, rK), fma(uK, uK, mul(vK, vK)), mul(pK, k.inv_gm1));
-  const float ruK = mul(rK, uK), rvK = mul(rK, vK);
-  const float FK0 = mul(rK, unK), FK1 = fma(pK, nx, mul(ruK, unK)), FK2 = fma(pK, ny, mul(rvK, unK));
-  const float FK3 = mul(add(EK, pK), unK);
-  if (left ? !c1 : c3) {
-    const float inv = __fdividef(1.0f, sub(SK, Ss));
-    const float rs = mul(mul(rK, dK), inv);
-    const float Us3 = mul(fma(Ps, Ss, sub(mul(dK, EK), mul(pK, unK))), inv);
-    const float utK = fma(uK, tx, mul(vK, ty));
-    const float Us1 = mul(rs, fma(Ss, nx, mul(utK, tx))), Us2 = mul(rs, fma(Ss, ny, mul(utK, ty)));
-    F[0] = fma(SK, sub(rs, rK), FK0);
-    F[1] = fma(SK, sub(Us1, ruK), FK1);
-    F[2] = fma(SK, sub(Us2, rvK), FK2);
-    F[3] = fma(SK, sub(Us3, EK), FK3);
-  } else {
-    F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
-  }
-}
-// the canonical flux of a face through the cell's edge of outward normal n:
-// evaluated from the face's owner (the lower cell), negated on the other side
-__device__ __forceinline__ void face_flux(const float qOwn[4], const float qOther[4], float nx, float ny,
-                                          bool other_owns, const Consts<float>& k, float F[4]) {
-  if (other_owns) {
-    hllc(qOther, qOwn, -nx, -ny, k, F);
-    F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
-  } else {
-    hllc(qOwn, qOther, nx, ny, k, F);
-  }
-}
-// sum_k s_k F_k in slot order: face k's term added to acc
-__device__ __forceinline__ void accumulate(int k, float sk, const float F[4], float acc[4]) {
-  if (k == 0) { acc[0] = mul(sk, F[0]); acc[1] = mul(sk, F[1]); acc[2] = mul(sk, F[2]); acc[3] = mul(sk, F[3]); }
-  else { acc[0] = fma(sk, F[0], acc[0]); acc[1] = fma(sk, F[1], acc[1]); acc[2] = fma(sk, F[2], acc[2]); acc[3] = fma(sk, F[3], acc[3]); }
-}
-// euler_solver.py:602-643: residual acc / area - sponge and the stage update
-template <int STAGE>
-__device__ __forceinline__ float4 cell_update(const float acc[4], float area, float sig, const float4& inlet,
-                                              const float4& Wc, const float4& W0, float dt, float half,
-                                              float* R0_out) {
-  const float R0 = sub(__fdividef(acc[0], area), mul(sig, sub(inlet.x, Wc.x)));
-  const float R1 = sub(__fdividef(acc[1], area), mul(sig, sub(inlet.y, Wc.y)));
-  const float R2 = sub(__fdividef(acc[2], area), mul(sig, sub(inlet.z, Wc.z)));
-  const float R3 = sub(__fdividef(acc[3], area), mul(sig, sub(inlet.w, Wc.w)));
-  *R0_out = R0;
-  const float m = -dt;
-  if (STAGE == ST_FIRST) return make_float4(fma(m, R0, Wc.x), fma(m, R1, Wc.y), fma(m, R2, Wc.z), fma(m, R3, Wc.w));
-  if (STAGE == ST_SRK2_SECOND)
-    return make_float4(mul(half, fma(m, R0, add(W0.x, Wc.x))), mul(half, fma(m, R1, add(W0.y, Wc.y))),
-                       mul(half, fma(m, R2, add(W0.z, Wc.z))), mul(half, fma(m, R3, add(W0.w, Wc.w))));
-  return make_float4(mul(half, add(fma(m, R0, W0.x), Wc.x)), mul(half, add(fma(m, R1, W0.y), Wc.y)),
-                     mul(half, add(fma(m, R2, W0.z), Wc.z)), mul(half, add(fma(m, R3, W0.w), Wc.w)));
-}
-
-// ---- K1 with every rounding written out, for the same reason: the per-cell
-// K1 and K1 by patches give bitwise the same face states and local steps.
-// euler_solver.py:36-39 Venkatakrishnan (K = 0): (a^2 + 2ab) / (a^2 + 2b^2 + ab + eps)
-__device__ __forceinline__ float venkat(float a, float b, float eps) {
-  const float aa = mul(a, a);
-  return __fdividef(fma(mul(2.0f, a), b, aa), add(fma(a, b, fma(mul(2.0f, b), b, aa)), eps));
-}
-// the cell's local CFL step (helper.py get_dt per cell): area / sum_k (c + |u.n_k|) s_k x CFL
-__device__ __forceinline__ float local_dt(const float Pc[4], const float gn[12], float gamma, float cfl) {
-  const float cel = sqrtf(fabsf(__fdiv_rn(mul(gamma, Pc[3]), Pc[0])));
-  float lam = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float un = fma(Pc[1], gn[G_N0X + 2 * k], mul(Pc[2], gn[G_N0Y + 2 * k]));
-    const float term = mul(add(cel, fabsf(un)), gn[G_S0 + k]);
-    lam = (k == 0) ? term : add(lam, term);
-  }
-  return mul(__fdiv_rn(gn[G_AREA], lam), cfl);
-}
-// euler_solver.py:45-98: LSQ gradient from the precomputed coefficients
-// (helper.py:136-153), the limiter as the min over the three faces, and the
-// cell's three MUSCL face states (primitive; boundary faces keep the cell's)
-__device__ __forceinline__ void recon_faces(const float Pc[4], const float Pk[3][4], const float gc[12], int nbw,
-                                            const Consts<float>& kc, float4 out[3]) {
-  const float cx0 = gc[G_C0X - 12], cy0 = gc[G_C0Y - 12], cx1 = gc[G_C1X - 12], cy1 = gc[G_C1Y - 12];
-  const float cx2 = gc[G_C2X - 12], cy2 = gc[G_C2Y - 12];
-  const float fx[3] = {gc[G_F0X - 12], gc[G_F1X - 12], gc[G_F2X - 12]};
-  const float fy[3] = {gc[G_F0Y - 12], gc[G_F1Y - 12], gc[G_F2Y - 12]};
-  // per variable: gradient, limiter, then its value on the three faces
-  float o[3][4];
-#pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    const float d0 = sub(Pk[0][v], Pc[v]), d1 = sub(Pk[1][v], Pc[v]), d2 = sub(Pk[2][v], Pc[v]);
-    const float gx = fma(cx2, d2, fma(cx1, d1, mul(cx0, d0)));
-    const float gy = fma(cy2, d2, fma(cy1, d1, mul(cy0, d0)));
-    const float up = fmaxf(fmaxf(0.0f, d0), fmaxf(d1, d2)), lo = fminf(fminf(0.0f, d0), fminf(d1, d2));
-    float ph = 1.0f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float d = fma(fy[k], gy, mul(fx[k], gx));
-      float p = 1.0f;
-      if (d > kc.eps_lim) p = venkat(up, d, kc.venk_eps);
-      else if (d < -kc.eps_lim) p = venkat(lo, d, kc.venk_eps);
-      ph = (k == 0) ? p : fminf(ph, p);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      o[k][v] = slot_kind(nbw, k) == K_INTERIOR ? fma(ph, fma(fy[k], gy, mul(fx[k], gx)), Pc[v]) : Pc[v];
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) out[k] = make_float4(o[k][0], o[k][1], o[k][2], o[k][3]);
-}
-}  // namespace xr
-
 // --------------------------------------------------------------- K1 recon
 // euler_solver.py:106-122 build_reconstruction for MUSCL: BC ghosts, LSQ
 // gradient (helper.py:136-153), limiter (euler_solver.py:45-67) and the cell's
@@ -519,33 +344,6 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, LOCALDT ? ESR_
   if (!cs.active[g] || cs.step[g] + pos >= cs.nmax[g]) return;
   const long long gi = s.off + (long long)c * s.B + b;
   const V4<T> Wc = W[gi];
-  if constexpr (kFastPath<T, FAST>) {   // rounded as K1 by patches rounds it
-    float Pc[4];
-    xr::prim(Wc, kc.gm1, kc.half, Pc);
-    if (LOCALDT) {
-      float gn[12];
-      geo_groups<float, 3>(s, c, 0, gn);
-      dt_local[gi] = xr::local_dt(Pc, gn, kc.gamma, cs.dt[g]);   // cs.dt holds the case CFL in local mode
-    }
-    if (!MUSCL) return;
-    const int4 nb = __ldg(s.nbr + c);
-    const int nbk[3] = {nb.x, nb.y, nb.z};
-    const float4 inlet = cs.inlet[g];
-    float Pk[3][4];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int kind = slot_kind(nb.w, k);
-      if (kind == K_INTERIOR) xr::prim(W[s.off + (long long)nbk[k] * s.B + b], kc.gm1, kc.half, Pk[k]);
-      else xr::ghost_prim(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc, Pk[k]);
-    }
-    float gc[12];
-    geo_groups<float, 3>(s, c, 3, gc);
-    float4 out[3];
-    xr::recon_faces(Pc, Pk, gc, nb.w, kc, out);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) FV[(long long)k * total + gi] = out[k];
-    return;
-  }
   T Pc[4];
   prim<T, FAST>(Wc, kc.gm1, kc.half, Pc);
   if (LOCALDT) {
@@ -677,6 +475,127 @@ __global__ void k_grad_export(const Seg<T>* __restrict__ segs, int seg, int b, c
 }
 
 // ----------------------------------------------------------------- K2 flux
+enum Stage { ST_FIRST = 0, ST_SRK2_SECOND = 1, ST_RK2_SECOND = 2 };
+
+// ---- the fast float32 face flux and cell update with every rounding written
+// out (__fmul_rn / __fadd_rn / __fsub_rn / __fmaf_rn are never fused or
+// split by the compiler), so the per-cell K2 and K2 by patches, which reach
+// the same faces from different code, round every face flux and every cell
+// update identically: a case's result does not depend on which K2 ran.
+namespace xr {
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// helper.py:37-46 (M = 1)
+__device__ __forceinline__ void prim(const float4& W, float gm1, float half, float P[4]) {
+  const float r = W.x, ri = __fdividef(1.0f, r);
+  const float u = mul(W.y, ri), v = mul(W.z, ri);
+  P[0] = r; P[1] = u; P[2] = v;
+  P[3] = mul(sub(W.w, mul(mul(half, r), fma(u, u, mul(v, v)))), gm1);
+}
+// helper.py:25-35 (M = 1)
+__device__ __forceinline__ float4 cons(const float P[4], float inv_gm1, float half) {
+  const float r = P[0], u = P[1], v = P[2];
+  return make_float4(r, mul(r, u), mul(r, v), fma(mul(half, r), fma(u, u, mul(v, v)), mul(P[3], inv_gm1)));
+}
+// helper.py:233-256 boundary states, as primitives of the ghost (gamma 1.4)
+__device__ __forceinline__ void ghost_prim(int kind, const float4& Wc, float nx, float ny, const float4& inlet,
+                                           const Consts<float>& k, float Q[4]) {
+  float P[4];
+  if (kind == K_INLET) { prim(inlet, k.gm1, k.half, Q); return; }
+  if (kind != K_WALL && kind != K_SUBSONIC) { prim(Wc, k.gm1, k.half, Q); return; }   // outlet
+  prim(Wc, k.gm1_14, k.half, P);
+  float G[4];
+  if (kind == K_WALL) {       // helper.py:196-204
+    const float t = mul(2.0f, fma(P[1], nx, mul(P[2], ny)));
+    G[0] = P[0]; G[1] = sub(P[1], mul(t, nx)); G[2] = sub(P[2], mul(t, ny)); G[3] = P[3];
+  } else {                    // helper.py:179-194
+    G[0] = k.sub_rho; G[1] = k.sub_u; G[2] = k.sub_v; G[3] = P[3];
+  }
+  prim(cons(G, k.inv_gm1_14, k.half), k.gm1, k.half, Q);
+}
+// euler_solver.py:273-374 HLLC flux from the face primitives, the conserved
+// variables formed only for the side the wave fan selects
+__device__ __forceinline__ void hllc(const float PL[4], const float PR[4], float nx, float ny,
+                                     const Consts<float>& k, float F[4]) {
+  const float rL = PL[0], uL = PL[1], vL = PL[2], pL = PL[3];
+  const float rR = PR[0], uR = PR[1], vR = PR[2], pR = PR[3];
+  const float unL = fma(uL, nx, mul(vL, ny)), unR = fma(uR, nx, mul(vR, ny));
+  const float tx = -ny, ty = nx;
+  const float aL = sqrtf(fabsf(__fdividef(mul(k.gamma, pL), rL)));
+  const float aR = sqrtf(fabsf(__fdividef(mul(k.gamma, pR), rR)));
+  float SL = fminf(sub(unL, aL), sub(unR, aR));
+  float SR = fmaxf(add(unL, aL), add(unR, aR));
+  if (SL == SR) SL = sub(SL, k.ss_eps);
+  if (SL == SR) SR = add(SR, k.ss_eps);
+  const float dL = sub(SL, unL), dR = sub(SR, unR);
+  float den = sub(mul(rL, dL), mul(rR, dR));
+  if (den == 0.0f) den = k.den_eps;
+  const float Ss = __fdividef(sub(fma(mul(rL, unL), dL, sub(pR, pL)), mul(mul(rR, unR), dR)), den);
+  const float PsL = fma(mul(rL, dL), sub(Ss, unL), pL);
+  const float PsR = fma(mul(rR, dR), sub(Ss, unR), pR);
+  const float Ps = mul(k.half, add(PsL, PsR));
+  const bool c1 = SL >= 0.0f;
+  const bool c2 = (SL <= 0.0f) && (Ss >= 0.0f);
+  const bool c3 = (Ss <= 0.0f) && (SR >= 0.0f);
+  const bool left = c1 || c2;
+  const float rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
+  const float unK = left ? unL : unR, SK = left ? SL : SR, dK = left ? dL : dR;
+  const float EK = fma(mul(k.half, rK), fma(uK, uK, mul(vK, vK)), mul(pK, k.inv_gm1));
+  const float ruK = mul(rK, uK), rvK = mul(rK, vK);
+  const float FK0 = mul(rK, unK), FK1 = fma(pK, nx, mul(ruK, unK)), FK2 = fma(pK, ny, mul(rvK, unK));
+  const float FK3 = mul(add(EK, pK), unK);
+  if (left ? !c1 : c3) {
+    const float inv = __fdividef(1.0f, sub(SK, Ss));
+    const float rs = mul(mul(rK, dK), inv);
+    const float Us3 = mul(fma(Ps, Ss, sub(mul(dK, EK), mul(pK, unK))), inv);
+    const float utK = fma(uK, tx, mul(vK, ty));
+    const float Us1 = mul(rs, fma(Ss, nx, mul(utK, tx))), Us2 = mul(rs, fma(Ss, ny, mul(utK, ty)));
+    F[0] = fma(SK, sub(rs, rK), FK0);
+    F[1] = fma(SK, sub(Us1, ruK), FK1);
+    F[2] = fma(SK, sub(Us2, rvK), FK2);
+    F[3] = fma(SK, sub(Us3, EK), FK3);
+  } else {
+    F[0] = FK0; F[1] = FK1; F[2] = FK2; F[3] = FK3;
+  }
+}
+// the canonical flux of a face through the cell's edge of outward normal n:
+// evaluated from the face's owner (the lower cell), negated on the other side
+__device__ __forceinline__ void face_flux(const float qOwn[4], const float qOther[4], float nx, float ny,
+                                          bool other_owns, const Consts<float>& k, float F[4]) {
+  if (other_owns) {
+    hllc(qOther, qOwn, -nx, -ny, k, F);
+    F[0] = -F[0]; F[1] = -F[1]; F[2] = -F[2]; F[3] = -F[3];
+  } else {
+    hllc(qOwn, qOther, nx, ny, k, F);
+  }
+}
+// sum_k s_k F_k in slot order: face k's term added to acc
+__device__ __forceinline__ void accumulate(int k, float sk, const float F[4], float acc[4]) {
+  if (k == 0) { acc[0] = mul(sk, F[0]); acc[1] = mul(sk, F[1]); acc[2] = mul(sk, F[2]); acc[3] = mul(sk, F[3]); }
+  else { acc[0] = fma(sk, F[0], acc[0]); acc[1] = fma(sk, F[1], acc[1]); acc[2] = fma(sk, F[2], acc[2]); acc[3] = fma(sk, F[3], acc[3]); }
+}
+// euler_solver.py:602-643: residual acc / area - sponge and the stage update
+template <int STAGE>
+__device__ __forceinline__ float4 cell_update(const float acc[4], float area, float sig, const float4& inlet,
+                                              const float4& Wc, const float4& W0, float dt, float half,
+                                              float* R0_out) {
+  const float R0 = sub(__fdividef(acc[0], area), mul(sig, sub(inlet.x, Wc.x)));
+  const float R1 = sub(__fdividef(acc[1], area), mul(sig, sub(inlet.y, Wc.y)));
+  const float R2 = sub(__fdividef(acc[2], area), mul(sig, sub(inlet.z, Wc.z)));
+  const float R3 = sub(__fdividef(acc[3], area), mul(sig, sub(inlet.w, Wc.w)));
+  *R0_out = R0;
+  const float m = -dt;
+  if (STAGE == ST_FIRST) return make_float4(fma(m, R0, Wc.x), fma(m, R1, Wc.y), fma(m, R2, Wc.z), fma(m, R3, Wc.w));
+  if (STAGE == ST_SRK2_SECOND)
+    return make_float4(mul(half, fma(m, R0, add(W0.x, Wc.x))), mul(half, fma(m, R1, add(W0.y, Wc.y))),
+                       mul(half, fma(m, R2, add(W0.z, Wc.z))), mul(half, fma(m, R3, add(W0.w, Wc.w))));
+  return make_float4(mul(half, add(fma(m, R0, W0.x), Wc.x)), mul(half, add(fma(m, R1, W0.y), Wc.y)),
+                     mul(half, add(fma(m, R2, W0.z), Wc.z)), mul(half, add(fma(m, R3, W0.w), Wc.w)));
+}
+}  // namespace xr
 
 // euler_solver.py:602-628 residual = sum_k F_k s_k / area - sponge (helper.py:262-295),
 // then the stage update of :630-653.
@@ -823,12 +742,6 @@ __global__ void __launch_bounds__(256, (kMinBlocks<T, FAST, MINB, ESR_K2_MINB>))
 #ifndef ESR_PATCH_MINB_ALT
 #define ESR_PATCH_MINB_ALT 6
 #endif
-// 1: the patch's states are staged in shared memory too (ghost states and the
-// cell update read them there; 0.5 KB more per cell)
-#ifndef ESR_PATCH_STAGE_W
-#define ESR_PATCH_STAGE_W 0
-#endif
-constexpr bool kPatchStageW = ESR_PATCH_STAGE_W != 0;
 #ifndef ESR_PATCH_WARPS
 #define ESR_PATCH_WARPS 8
 #endif
@@ -855,7 +768,6 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
                                                                   float* __restrict__ res_out) {
   // the patch's face states, then in place its signed face fluxes (1.5 KB per cell)
   __shared__ float4 G[kPatchCells][3][32];
-  __shared__ float4 SW[kPatchStageW ? kPatchCells : 1][32];
   const int4 pb = pblk[blockIdx.x];          // segment, patch, first slot
   const Seg<float> s = segs[pb.x];
   const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];
@@ -872,7 +784,6 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
     const long long gi = s.off + (long long)(c0 + lc) * s.B + b;
 #pragma unroll
     for (int k = 0; k < 3; ++k) cp_async16(&G[lc][k][lane], FV + (long long)k * total + (in_seg ? gi : 0), in_seg);
-    if constexpr (kPatchStageW) cp_async16(&SW[lc][lane], Win + (in_seg ? gi : 0), in_seg);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -905,7 +816,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
           const float4 fr = FV[(long long)ko * total + s.off + (long long)j * s.B + b];
           qR[0] = fr.x; qR[1] = fr.y; qR[2] = fr.z; qR[3] = fr.w;
         } else {
-          xr::ghost_prim(kind, kPatchStageW ? SW[lc][lane] : Win[gi], nx, ny, inlet, kc, qR);
+          xr::ghost_prim(kind, Win[gi], nx, ny, inlet, kc, qR);
         }
       }
       float F[4];
@@ -919,7 +830,7 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
   for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
     const int c = c0 + lc;
     const long long gi = s.off + (long long)c * s.B + b;
-    const float4 Wc = kPatchStageW ? SW[lc][lane] : Win[gi];
+    const float4 Wc = Win[gi];
     float gk[12];
     geo_groups<float, 3>(s, c, 0, gk);
     float acc[4];
@@ -936,70 +847,6 @@ __global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_flux_patch(const Seg
     const float4 o = xr::cell_update<STAGE>(acc, gk[G_AREA], sig, inlet, Wc, W0, dt, kc.half, &R0);
     if (STAGE == ST_FIRST && res_out != nullptr) res_out[gi] = R0;
     Wout[gi] = o;
-  }
-}
-
-// K1 by patches (float32 fast path): the blocks of K2 by patches, one warp
-// per cell at a time with its lanes over 32 slots. The states of the patch's
-// cells are staged in shared memory by asynchronous copies (all in flight at
-// once), so a neighbour inside the patch is read from there and only a
-// neighbour in another patch from global memory; the arithmetic is K1's
-// (xr::), so the face states and local steps equal k_recon's bit for bit.
-#ifndef ESR_K1P_MINB
-#define ESR_K1P_MINB 6
-#endif
-template <bool LOCALDT, int MINB = ESR_K1P_MINB>
-__global__ void __launch_bounds__(32 * kPatchWarps, MINB) k_recon_patch(const Seg<float>* __restrict__ segs,
-                                                                  const int4* __restrict__ pblk,
-                                                                  const float4* __restrict__ W,
-                                                                  float4* __restrict__ FV, long long total,
-                                                                  Cases<float> cs, Consts<float> kc, int pos,
-                                                                  float* __restrict__ dt_local) {
-  __shared__ float4 S[kPatchCells][32];   // the patch's states, this block's slots (512 B per cell)
-  const int4 pb = pblk[blockIdx.x];
-  const Seg<float> s = segs[pb.x];
-  const int c0 = s.patch_start[pb.y], c1 = s.patch_start[pb.y + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int b = pb.z + lane;
-  const bool in_seg = b < s.B;
-  const int g = s.case0 + (in_seg ? b : 0);
-  const bool live = in_seg && cs.active[g] && cs.step[g] + pos < cs.nmax[g];
-  if (!__syncthreads_or(live)) return;
-  for (int lc = warp; lc < c1 - c0; lc += kPatchWarps)
-    cp_async16(&S[lc][lane], W + (in_seg ? s.off + (long long)(c0 + lc) * s.B + b : 0), in_seg);
-  cp_async_wait_all();
-  __syncthreads();
-  if (!live) return;
-  const float4 inlet = cs.inlet[g];
-  for (int lc = warp; lc < c1 - c0; lc += kPatchWarps) {
-    const int c = c0 + lc;
-    const long long gi = s.off + (long long)c * s.B + b;
-    const float4 Wc = S[lc][lane];
-    float Pc[4];
-    xr::prim(Wc, kc.gm1, kc.half, Pc);
-    if (LOCALDT) {
-      float gn[12];
-      geo_groups<float, 3>(s, c, 0, gn);
-      dt_local[gi] = xr::local_dt(Pc, gn, kc.gamma, cs.dt[g]);
-    }
-    const int4 nb = __ldg(s.nbr + c);
-    const int nbk[3] = {nb.x, nb.y, nb.z};
-    float Pk[3][4];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int kind = slot_kind(nb.w, k);
-      const int j = nbk[k];
-      if (kind == K_INTERIOR)
-        xr::prim((j >= c0 && j < c1) ? S[j - c0][lane] : W[s.off + (long long)j * s.B + b], kc.gm1, kc.half, Pk[k]);
-      else
-        xr::ghost_prim(kind, Wc, geo(s, G_N0X + 2 * k, c), geo(s, G_N0Y + 2 * k, c), inlet, kc, Pk[k]);
-    }
-    float gc[12];
-    geo_groups<float, 3>(s, c, 3, gc);
-    float4 out[3];
-    xr::recon_faces(Pc, Pk, gc, nb.w, kc, out);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) FV[(long long)k * total + gi] = out[k];
   }
 }
 

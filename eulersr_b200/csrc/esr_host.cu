@@ -139,7 +139,6 @@ struct SolverT : SolverBase {
   bool use_patch = false;
   // second register budget of each fast float32 kernel (autotuned)
   bool k1_alt = false, k2_alt = false, kp_alt = false;
-  bool k1_patch = false;   // K1 by patches (with K2 by patches)
   DevBuf<int> d_case_seg, d_case_slot, d_ncells;
 
   DevBuf<V> W, Wa, Wref, FV, Wp;   // Wp: probe step output (batch solves)
@@ -452,7 +451,7 @@ struct SolverT : SolverBase {
   // cells and slots), so a second solver of the same shape skips the timing.
   struct TuneChoice {
     int block = 256;
-    bool patches = false, k1 = false, k2 = false, kp = false, k1p = false;
+    bool patches = false, k1 = false, k2 = false, kp = false;
   };
   struct TuneEntry {
     TuneChoice choice;
@@ -470,7 +469,6 @@ struct SolverT : SolverBase {
   bool fast_float() const { return sizeof(T) == 4 && !faithful(); }
   int k1_minb_of(const TuneChoice& c) const {
     if (!fast_float() || P.reconstruction != ESR_RECON_MUSCL) return 0;
-    if (c.patches && c.k1p) return ESR_K1P_MINB;
     return c.k1 ? ESR_K1_MINB_ALT : ESR_K1_MINB;
   }
   int k2_minb_of(const TuneChoice& c) const {
@@ -481,7 +479,6 @@ struct SolverT : SolverBase {
   int apply_choice(const TuneChoice& c) {
     ESR_TRY(build_blocks(c.block));
     use_patch = c.patches && patch_eligible();
-    k1_patch = use_patch && c.k1p;
     k1_alt = c.k1;
     k2_alt = c.k2;
     kp_alt = c.kp;
@@ -503,7 +500,6 @@ struct SolverT : SolverBase {
       v.k2_patches = c.patches ? 1 : 0;
       v.k1_minb = k1_minb_of(c);
       v.k2_minb = k2_minb_of(c);
-      v.k1_patches = (c.patches && c.k1p) ? 1 : 0;
       v.step_ms = ms;
     }
     return ESR_OK;
@@ -574,16 +570,6 @@ struct SolverT : SolverBase {
       c.k1 = true;
       ESR_TRY(consider(c));
     }
-    if (patch_eligible()) {   // K1 by patches with the best K2 by patches
-      TuneChoice c = best_c;
-      if (!c.patches) {
-        c.patches = true;
-        c.kp = false;
-      }
-      c.k1 = false;
-      c.k1p = true;
-      ESR_TRY(consider(c));
-    }
     launches = before;
     chosen = best_c;
     ESR_TRY(apply_choice(chosen));
@@ -591,7 +577,6 @@ struct SolverT : SolverBase {
     tuning.k2_patches = use_patch ? 1 : 0;
     tuning.k1_minb = k1_minb_of(chosen);
     tuning.k2_minb = k2_minb_of(chosen);
-    tuning.k1_patches = k1_patch ? 1 : 0;
     tuning.cached = 0;
     ESR_CUDA(cudaMemsetAsync(W.p, 0, total * sizeof(V), stream));
     ESR_CUDA(cudaMemsetAsync(Wa.p, 0, total * sizeof(V), stream));
@@ -612,17 +597,11 @@ struct SolverT : SolverBase {
     if (v->k2_patches != 0 && v->k2_patches != 1) return fail(ESR_ERR_ARG, "set_shape: k2_patches must be 0 or 1");
     if (v->k2_patches && !patch_eligible())
       return fail(ESR_ERR_ARG, "set_shape: K2 by patches needs a float32 fast-fidelity HLLC + MUSCL solver");
-    if (v->k1_patches != 0 && v->k1_patches != 1) return fail(ESR_ERR_ARG, "set_shape: k1_patches must be 0 or 1");
-    if (v->k1_patches && !v->k2_patches) return fail(ESR_ERR_ARG, "set_shape: K1 by patches runs with K2 by patches");
     TuneChoice c;
     c.block = v->block_size;
     c.patches = v->k2_patches == 1;
-    c.k1p = v->k1_patches == 1;
     const bool muscl = P.reconstruction == ESR_RECON_MUSCL;
-    if (v->k1_minb != 0 && c.k1p) {
-      if (v->k1_minb != ESR_K1P_MINB)
-        return fail(ESR_ERR_ARG, "set_shape: K1 by patches has one register budget (" + std::to_string(ESR_K1P_MINB) + ")");
-    } else if (v->k1_minb != 0) {
+    if (v->k1_minb != 0) {
       if (!fast_float() || !muscl || (v->k1_minb != ESR_K1_MINB && v->k1_minb != ESR_K1_MINB_ALT))
         return fail(ESR_ERR_ARG, "set_shape: k1_minb must be 0 or one of K1's two register budgets (" +
                                      std::to_string(ESR_K1_MINB) + ", " + std::to_string(ESR_K1_MINB_ALT) +
@@ -649,7 +628,6 @@ struct SolverT : SolverBase {
     tuning.k2_patches = use_patch ? 1 : 0;
     tuning.k1_minb = k1_minb_of(c);
     tuning.k2_minb = k2_minb_of(c);
-    tuning.k1_patches = k1_patch ? 1 : 0;
     return ESR_OK;
   }
   int get_tuning(esr_tuning* out) {
@@ -658,10 +636,8 @@ struct SolverT : SolverBase {
     out->k2_patches = use_patch ? 1 : 0;
     TuneChoice now = chosen;
     now.patches = use_patch;
-    now.k1p = now.k1p && use_patch;
     out->k1_minb = k1_minb_of(now);
     out->k2_minb = k2_minb_of(now);
-    out->k1_patches = k1_patch ? 1 : 0;
     return ESR_OK;
   }
 
@@ -749,19 +725,6 @@ struct SolverT : SolverBase {
       return;
     }
     tap_begin(0);
-    if constexpr (sizeof(T) == 4) {
-      if (k1_patch && n_pblk > 0) {   // with K2 by patches: fast float32 HLLC + MUSCL
-        if (write_dt)
-          k_recon_patch<true><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, w, FV.p, total, cs, kc, pos,
-                                                                       dt_local.p);
-        else
-          k_recon_patch<false><<<n_pblk, 32 * kPatchWarps, 0, stream>>>(d_segs.p, d_pblk.p, w, FV.p, total, cs, kc,
-                                                                        pos, dt_local.p);
-        tap_end();
-        ++launches;
-        return;
-      }
-    }
     if (write_dt) {   // the local-dt K1 keeps its one budget
       k_recon<T, kF, true, true><<<n_blk, block, 0, stream>>>(bmap(), w, FV.p, total, cs, kc, pos, dt_local.p);
     } else if (sizeof(T) == 4 && k1_alt) {

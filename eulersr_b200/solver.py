@@ -435,12 +435,11 @@ class Solver:
         F.check(F.lib().esr_solver_tuning(self.handle, C.byref(t)))
         return t.as_dict()
 
-    def set_shape(self, block_size: int, k2_patches: bool = False, k1_minb: int = 0, k2_minb: int = 0,
-                  k1_patches: bool = False):
+    def set_shape(self, block_size: int, k2_patches: bool = False, k1_minb: int = 0, k2_minb: int = 0):
         """Run with this launch shape (one of ``tuning()['variants']``, say);
         a register budget of 0 is the kernel's default."""
         v = F.TuningVariant(block_size=int(block_size), k2_patches=int(bool(k2_patches)), k1_minb=int(k1_minb),
-                            k2_minb=int(k2_minb), k1_patches=int(bool(k1_patches)), step_ms=0.0)
+                            k2_minb=int(k2_minb), step_ms=0.0)
         F.check(F.lib().esr_solver_set_shape(self.handle, C.byref(v)))
 
     def profile_step(self, nsteps: int = 8) -> dict:

@@ -313,9 +313,8 @@ int esr_profile_step(esr_solver* solver, int32_t nsteps, esr_kernel_times* out);
  * fastest (no reference counterpart: XLA picks launch shapes). Shapes: the
  * cell kernels at 64, 128 and 256 threads per block; at the best of those,
  * where the float32 fast kernels run, K2's second register budget, K2 by
- * patches at both of its budgets (float32 fast fidelity, HLLC + MUSCL),
- * K1's second budget with the best K2, and K1 by patches (the patch blocks
- * of K2, states staged in shared memory) with the best K2 by patches. A register budget is the number of
+ * patches at both of its budgets (float32 fast fidelity, HLLC + MUSCL), and
+ * K1's second budget with the best K2. A register budget is the number of
  * resident blocks per SM a kernel is compiled for. The choice is kept for
  * the process per solver shape (device, precision, scheme, each mesh's cells
  * and slots): a second solver of the same shape takes it without timing
@@ -327,7 +326,6 @@ typedef struct esr_tuning_variant {
     int32_t k1_minb;          /* register budget of K1 (0: not constrained; the K1 that
                                  also writes the local time step keeps its own) */
     int32_t k2_minb;          /* register budget of K2, per-cell or patch form */
-    int32_t k1_patches;       /* 1: K1 by patches too (with K2 by patches) */
     double step_ms;           /* device ms of one step */
 } esr_tuning_variant;
 typedef struct esr_tuning {
@@ -340,7 +338,7 @@ typedef struct esr_tuning {
     int32_t k1_minb;          /* register budgets in use (0: not constrained) */
     int32_t k2_minb;
     int32_t n_variants;       /* every shape timed, in order */
-    int32_t k1_patches;       /* 1: K1 runs by patches */
+    int32_t reserved;
     esr_tuning_variant variants[ESR_TUNING_MAX_VARIANTS];
 } esr_tuning;
 int esr_solver_tuning(const esr_solver* solver, esr_tuning* out);

@@ -286,23 +286,23 @@ def test_autotuner_and_block_invariance(naca02):
     assert sorted(t['step_ms'], key=str) == [128, 256, 64, "patches"]
     assert all(v > 0 for v in t['step_ms'].values())
     var = t['variants']
-    assert len(var) == 8 and all(v['step_ms'] > 0 for v in var)
+    assert len(var) == 7 and all(v['step_ms'] > 0 for v in var)
     assert [v['block_size'] for v in var[:3]] == [64, 128, 256]
     assert {(v['k2_patches'], v['k2_minb']) for v in var} == {(False, 5), (False, 4), (True, 5), (True, 6)}
     assert {v['k1_minb'] for v in var} == {8, 6}
-    assert [v['k1_patches'] for v in var] == [False] * 7 + [True]
     best = min(var, key=lambda v: v['step_ms'])
-    key = ('block_size', 'k2_patches', 'k1_minb', 'k2_minb', 'k1_patches')
-    assert tuple(t[k] for k in key) == tuple(best[k] for k in key)
+    assert (t['block_size'], t['k2_patches'], t['k1_minb'], t['k2_minb']) == (
+        best['block_size'], best['k2_patches'], best['k1_minb'], best['k2_minb'])
     states.append(run(s))
     again = Solver(naca02, 3, precision='f32', block_size=0)
     t2 = again.tuning()
     assert t2['cached'] and t2['variants'] == var and t2['block_size'] == t['block_size']
     # every timed shape, set by hand
     for v in var:
-        s.set_shape(v['block_size'], v['k2_patches'], v['k1_minb'], v['k2_minb'], v['k1_patches'])
+        s.set_shape(v['block_size'], v['k2_patches'], v['k1_minb'], v['k2_minb'])
         got = s.tuning()
-        assert tuple(got[k] for k in key) == tuple(v[k] for k in key)
+        assert (got['block_size'], got['k2_patches'], got['k1_minb'], got['k2_minb']) == (
+            v['block_size'], v['k2_patches'], v['k1_minb'], v['k2_minb'])
         states.append(run(s))
     for bs in (64, 128, 256, "patches"):
         s = Solver(naca02, 3, precision='f32', block_size=bs)
@@ -325,8 +325,6 @@ def test_autotuner_and_block_invariance(naca02):
         s.set_shape(96)
     with pytest.raises(EsrError):
         s.set_shape(64, False, 7, 0)
-    with pytest.raises(EsrError):
-        s.set_shape(64, False, 0, 0, True)   # K1 by patches needs K2 by patches
 
 
 def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
