@@ -621,7 +621,7 @@ def run_warm(args, world, rank, local):
     from eulersr_b200.warmstart.workflow import WarmStartWorkflow
     torch.cuda.set_device(local)
     t_setup = time.perf_counter()
-    wf = WarmStartWorkflow(slots=args.slots, max_steps=args.max_steps, device=local,
+    wf = WarmStartWorkflow(slots=args.slots, max_steps=args.max_steps, device=local, lr_steps=args.lr_steps,
                            warm_budget=args.warm_budget or None)
     info = {} if args.make_truth else wf.prepare(n_train=args.n_train, target_steps=args.target_steps,
                                                  train_steps=args.train_steps)
@@ -780,7 +780,7 @@ def run_warm(args, world, rank, local):
                            "warm_budget": args.warm_budget or None,
                            "fallback": "a warm start the rule has not stopped within warm_budget steps restarts "
                                        "from freestream with the rest of max_steps (steps of both phases counted)",
-                           "lr_steps": 6000, "training": info,
+                           "lr_steps": args.lr_steps, "training": info,
                            "reference_cd": f"float64 solves of the same kernels, 30,000 + 5,000 steps ({truth_s:.1f} s)",
                            "steady_cases": int(steady.sum()), "truth_check": truth_check,
                            "l2": "256 MB buffer overwritten between passes", "setup_s": setup_s,
@@ -826,6 +826,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=12000, help="warm workload: step cap of an HR solve")
     ap.add_argument("--target-steps", type=int, default=12000, help="warm workload: steps of a training target")
     ap.add_argument("--train-steps", type=int, default=2000, help="warm workload: MLP training steps")
+    ap.add_argument("--lr-steps", type=int, default=6000, help="warm workload: steps of each LR solve")
     ap.add_argument("--warm-budget", type=int, default=3000,
                     help="warm workload: steps after which an unstopped warm start restarts from freestream (0: never)")
     ap.add_argument("--unsteady-cap", type=int, default=3000,
