@@ -826,7 +826,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=12000, help="warm workload: step cap of an HR solve")
     ap.add_argument("--target-steps", type=int, default=12000, help="warm workload: steps of a training target")
     ap.add_argument("--train-steps", type=int, default=2000, help="warm workload: MLP training steps")
-    ap.add_argument("--lr-steps", type=int, default=6000, help="warm workload: steps of each LR solve")
+    ap.add_argument("--lr-steps", type=int, default=2000, help="warm workload: steps of each LR solve")
     ap.add_argument("--warm-budget", type=int, default=3000,
                     help="warm workload: steps after which an unstopped warm start restarts from freestream (0: never)")
     ap.add_argument("--unsteady-cap", type=int, default=3000,

@@ -73,7 +73,7 @@ def _device_timed(fn):
 
 
 class WarmStartWorkflow:
-    def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=6000, max_steps=12000,
+    def __init__(self, geom="naca2412", h_hr=0.025, h_lr=0.1, slots=32, lr_steps=2000, max_steps=12000,
                  check_every=25, patience=8, cd_tol=0.005, device=0, schedule="fifo",
                  warm_budget=3000, unsteady_cap=None):
         self.hr, self.lr = cached_mesh(geom, h_hr), cached_mesh(geom, h_lr)
