@@ -1065,10 +1065,17 @@ struct SolverT : SolverBase {
     ESR_CUDA(cudaStreamWaitEvent(copy_stream, ev_in_consumed, 0));
     ESR_CUDA(cudaMemcpyAsync(st_init.p, h_init.p, n * sizeof(SlotInit<T>), cudaMemcpyHostToDevice, copy_stream));
     ESR_CUDA(cudaMemcpyAsync(st_jobs_in.p, h_jobs_in.p, n * sizeof(SlotCopy<T>), cudaMemcpyHostToDevice, copy_stream));
-    for (int i = 0; i < n; ++i)
-      ESR_CUDA(cudaMemcpyAsync(st_in.p + 4 * h_jobs_in.p[i].stage_row, W_init[i],
-                               (size_t)4 * h_jobs_in.p[i].n_cells * sizeof(float), cudaMemcpyHostToDevice,
-                               copy_stream));
+    // one copy per run of fields that lie back to back in host memory (the
+    // staging rows are consecutive), so a caller with one block for all its
+    // fields pays one copy's launch cost, not one per case
+    for (int i = 0; i < n;) {
+      int j = i + 1;
+      size_t len = (size_t)4 * h_jobs_in.p[i].n_cells;
+      while (j < n && W_init[j] == W_init[i] + len) len += (size_t)4 * h_jobs_in.p[j++].n_cells;
+      ESR_CUDA(cudaMemcpyAsync(st_in.p + 4 * h_jobs_in.p[i].stage_row, W_init[i], len * sizeof(float),
+                               cudaMemcpyHostToDevice, copy_stream));
+      i = j;
+    }
     ESR_CUDA(cudaEventRecord(ev_in_ready, copy_stream));
     staged_n = n;
     staged_max = max_n;
@@ -1127,10 +1134,14 @@ struct SolverT : SolverBase {
     }
     ESR_CUDA(cudaEventRecord(ev_out_ready, stream));
     ESR_CUDA(cudaStreamWaitEvent(copy_stream, ev_out_ready, 0));
-    for (int i = 0; i < n; ++i)
-      ESR_CUDA(cudaMemcpyAsync(out[i], st_out.p + 4 * h_jobs_out.p[i].stage_row,
-                               (size_t)4 * h_jobs_out.p[i].n_cells * sizeof(float), cudaMemcpyDeviceToHost,
-                               copy_stream));
+    for (int i = 0; i < n;) {   // one copy per run of back-to-back outputs, as in stage_in
+      int j = i + 1;
+      size_t len = (size_t)4 * h_jobs_out.p[i].n_cells;
+      while (j < n && out[j] == out[i] + len) len += (size_t)4 * h_jobs_out.p[j++].n_cells;
+      ESR_CUDA(cudaMemcpyAsync(out[i], st_out.p + 4 * h_jobs_out.p[i].stage_row, len * sizeof(float),
+                               cudaMemcpyDeviceToHost, copy_stream));
+      i = j;
+    }
     ESR_CUDA(cudaEventRecord(ev_out_done, copy_stream));
     ESR_CUDA(cudaGetLastError());
     return ESR_OK;

@@ -472,11 +472,14 @@ def test_cuda_against_reference_solver_source(tag, name, mach, aoa, prec, fideli
     assert err <= tol
 
 
-def test_overlapped_transfers_equal_synchronous(diamond02, naca02):
+@pytest.mark.parametrize("layout", ["separate", "one_block"])
+def test_overlapped_transfers_equal_synchronous(diamond02, naca02, layout):
     """The pipelined form of set_cases / step / get_states (next cases staged
     on the copy stream while the current chunk runs, final fields fetched
     while the next runs) gives bitwise the fields of the synchronous calls,
-    over three rounds of different warm fields on a two-mesh solver."""
+    over three rounds of different warm fields on a two-mesh solver; with
+    every field a view of one host block ('one_block') the library moves
+    them with one copy each way, with separate arrays one per case."""
     import torch
     from eulersr_b200.solver import Solver, FlowCase, freestream
     meshes = [diamond02, naca02]
@@ -484,16 +487,22 @@ def test_overlapped_transfers_equal_synchronous(diamond02, naca02):
     cases = [FlowCase(mach=m, aoa_deg=a, mesh=k, cfl=0.6, tf=1e9, dtype=np.float32) for k, m, a in spec]
     slots = [0, 1, 2, 3]
     rng = np.random.default_rng(5)
+    sizes = [meshes[c.mesh].n_cells for c in cases]
+
+    def host_arrays():
+        if layout == "separate":
+            return [torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy() for n in sizes]
+        big = torch.empty((sum(sizes), 4), dtype=torch.float32, pin_memory=True).numpy()
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        return [big[offs[i]:offs[i + 1]] for i in range(len(sizes))]
+
     rounds = []
     for r in range(3):
-        fields = []
-        for c in cases:
+        fields = host_arrays()
+        for c, pinned in zip(cases, fields):
             n = meshes[c.mesh].n_cells
             W = np.repeat(freestream(c.mach, c.aoa_deg, dtype=np.float32)[None, :], n, 0)
-            W = (W * (1 + 0.01 * r * rng.standard_normal((n, 1)))).astype(np.float32)
-            pinned = torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy()
-            pinned[:] = W
-            fields.append(pinned)
+            pinned[:] = (W * (1 + 0.01 * r * rng.standard_normal((n, 1)))).astype(np.float32)
         rounds.append(fields)
     sync = Solver(meshes, [2, 2], precision="f32", block_size=128)
     want = []
@@ -502,7 +511,7 @@ def test_overlapped_transfers_equal_synchronous(diamond02, naca02):
         sync.step(20)
         want.append(sync.get_states(slots, dtype=np.float32))
     pipe = Solver(meshes, [2, 2], precision="f32", block_size=128)
-    outs = [[np.empty_like(f) for f in fields] for fields in rounds]
+    outs = [host_arrays() for _ in rounds]
     pipe.stage_cases(slots, cases, rounds[0])
     pipe.apply_staged()
     for r in range(3):
