@@ -534,6 +534,62 @@ def _truth_table():
     return None
 
 
+PLAIN_TRUTH_FILE = ROOT / "tests" / "golden" / "naca0012_bench_truth.json"
+
+
+def run_plain_converged(args, world, rank, local, make_truth=False):
+    """Config 3's batch solved to the stop rule: the 256 NACA0012 h=0.025
+    cases of the throughput workload (per GPU), freestream starts, through
+    esr_batch_solve with retire/refill (the warm pipeline's 32 HR slots), each
+    stopped once its CD stayed within 0.5 % of its float64 reference for 8
+    checks 25 steps apart (12,000-step cap). The references come from
+    tests/golden/naca0012_bench_truth.json (written by --make-plain-truth
+    from float64 solves of the same kernels, 30,000 + 5,000 steps) or, for
+    cases not in it, are computed here. Returns the leg's record."""
+    from eulersr_b200.parallel import case_cost, shard_cases
+    from eulersr_b200.warmstart.workflow import WarmStartWorkflow
+    mesh = get_mesh("naca0012", args.h)
+    mach_all, aoa_all = batch_cases(args.cases * world)
+    mine = shard_cases(case_cost(mach_all, mesh.n_cells), world)[rank]
+    me, ae = mach_all[mine], aoa_all[mine]
+    wf = WarmStartWorkflow(geom="naca0012", h_hr=args.h, slots=args.slots, max_steps=args.max_steps, device=local,
+                           warm_budget=None)
+    table = {}
+    if PLAIN_TRUTH_FILE.exists() and not make_truth:
+        for r in json.loads(PLAIN_TRUTH_FILE.read_text())["cases"]:
+            table[(round(r["mach"], 12), round(r["aoa"], 12))] = (r["cd"], r["steady"])
+    keys = [(round(float(m), 12), round(float(a), 12)) for m, a in zip(me, ae)]
+    todo = [i for i, k in enumerate(keys) if k not in table]
+    t0 = time.perf_counter()
+    if todo:
+        cd, st = wf.truth(me[todo], ae[todo])
+        for j, i in enumerate(todo):
+            table[keys[i]] = (float(cd[j]), bool(st[j]))
+    truth_s = time.perf_counter() - t0
+    truth = np.array([table[k][0] for k in keys])
+    steady = np.array([table[k][1] for k in keys])
+    if make_truth:
+        if rank == 0 and world == 1:
+            rows = [{"mach": float(m), "aoa": float(a), "cd": float(c), "steady": bool(s_)}
+                    for m, a, c, s_ in zip(me, ae, truth, steady)]
+            PLAIN_TRUTH_FILE.write_text(json.dumps({
+                "about": "reference CD of the throughput workload's NACA0012 h=0.025 cases: float64 solves of the "
+                         "library's kernels (local CFL step, 30,000 steps, then 5,000 more; steady when the CD "
+                         "moved by <= 0.1 %), written by python bench.py --make-plain-truth",
+                "cases": rows}, indent=1) + "\n")
+        wf.close()
+        return {"truth_written": str(PLAIN_TRUTH_FILE), "cases": len(me), "steady": int(steady.sum())}
+    r = wf.solve(me, ae, truth, steady, "cold")
+    wf.close()
+    value = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
+    return {"value": value, "unit": WARM_UNIT, "cases_per_gpu": len(me), "steady": int(steady.sum()),
+            "converged": r.converged, "seconds": r.seconds, "slots": args.slots,
+            "median_iterations": float(np.median(r.iterations)), "references_computed_here": len(todo),
+            "references_s": truth_s,
+            "workload": "config 3's NACA0012 h=0.025 cases (Mach~U[0.7,3] seed 1, alpha on the 0.5-degree grid) "
+                        "from freestream through esr_batch_solve, 0.5 % CD rule, 12,000-step cap"}
+
+
 def cpu_converged_sample(cases, seconds_cap, mesh, cd_tol=0.005, patience=8, check_every=25, max_steps=12000):
     """The reference's method on the host: each case solved alone from
     freestream by the C/OpenMP restatement of the oracle (float32, local CFL
@@ -756,6 +812,10 @@ def run_warm(args, world, rank, local):
     wf.close()
     del flush
     torch.cuda.empty_cache()
+    # config 3's batch solved to the same CD rule from freestream
+    pargs = argparse.Namespace(**vars(args))
+    pargs.cases = 256
+    plain3 = run_plain_converged(pargs, world, rank, local)
     # the batched throughput workload: cell-updates/s and the K2 roofline
     targs = argparse.Namespace(**vars(args))
     targs.workload, targs.steps, targs.warmup = "naca", min(args.steps, 10), 3
@@ -799,7 +859,8 @@ def run_warm(args, world, rank, local):
                     "median_iterations_warm": float(np.median(passes[-1].iterations)),
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
                     "by_case_class": by_class, "warm_mlp_streamed": streamed,
-                    "warm_mlp_lr_longest_first_queue": lpt, "unsteady_capped_protocol": capped_proto},
+                    "warm_mlp_lr_longest_first_queue": lpt, "unsteady_capped_protocol": capped_proto,
+                    "plain_batched_naca0012_config3": plain3},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",
@@ -836,6 +897,8 @@ def main():
                     help="warm workload: extra leg with unsteady-flagged cases capped at this many steps for every "
                          "start (0: skip the leg)")
     ap.add_argument("--make-truth", action="store_true", help="write the held-out cases' reference CDs and exit")
+    ap.add_argument("--make-plain-truth", action="store_true",
+                    help="write the reference CDs of config 3's NACA0012 cases and exit")
     ap.add_argument("--block", default="0", help="throughput workloads: 0 (autotuned), 64, 128, 256 or patches")
     args = ap.parse_args()
     args.block = args.block if args.block == "patches" else int(args.block)
@@ -852,6 +915,11 @@ def main():
     try:
         if args.workload == "diamond":
             return run_single(args, world, rank, local)
+        if args.make_plain_truth:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(run_plain_converged(args, world, rank, local, make_truth=True)), flush=True)
+            return 0
         if args.workload == "warm":
             return run_warm(args, world, rank, local)
         run_throughput(args, world, rank, local, report=True)
