@@ -185,3 +185,19 @@ def test_warm_shards_over_two_gloo_ranks():
     assert sorted(got[0] + got[1]) == list(range(32))
     _, (me, _) = draw_cases(32, 32, seed=3)
     assert cmax - csum / 2 <= case_cost(me).max()
+
+
+def test_plain_truth_table_covers_config3_cases():
+    """The committed float64 references of config 3's NACA0012 cases (the
+    bench's converged-cases leg reads them) cover exactly the 256 cases the
+    throughput workload draws, with finite CDs and a steady flag each
+    (subsonic inviscid cases have near-zero drag, a few slightly negative
+    from the discretisation)."""
+    import json
+    import bench
+    rows = json.loads(bench.PLAIN_TRUTH_FILE.read_text())["cases"]
+    mach, aoa = bench.batch_cases(256)
+    want = {(round(float(m), 12), round(float(a), 12)) for m, a in zip(mach, aoa)}
+    got = {(round(r["mach"], 12), round(r["aoa"], 12)) for r in rows}
+    assert got == want
+    assert all(np.isfinite(r["cd"]) and abs(r["cd"]) < 1.0 and isinstance(r["steady"], bool) for r in rows)
