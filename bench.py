@@ -731,10 +731,20 @@ def run_warm(args, world, rank, local):
     value = allreduce_sum(float(conv), world) / sec_max
     # the same cases by the other starts, one pass each
     base = {}
+
+    def case_record(res):
+        ok = [bool(x["status"] == 2 and st and abs(x["cd"] - t) <= wf.cd_tol * abs(t))
+              for x, t, st in zip(res, truth, steady)]
+        return {"steps": [int(x["steps"]) for x in res], "status": [int(x["status"]) for x in res],
+                "fallback": [bool(x.get("fallback", False)) for x in res], "converged": ok}
+
+    per_case = {"mach": [float(m) for m in me], "aoa": [float(a) for a in ae], "steady": [bool(x) for x in steady],
+                "mlp": case_record(passes[-1].results)}
     for start in ("single", "cold", "idw"):
         flush.add_(1.0)
         barrier(world)
         r = wf.solve(me, ae, truth, steady, start)
+        per_case[start] = case_record(r.results)
         base[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
         base[start + "_detail"] = {"converged": r.converged, "seconds": r.seconds,
                                    "median_iterations": float(np.median(r.iterations)), "parts_s": r.parts_s}
@@ -860,7 +870,7 @@ def run_warm(args, world, rank, local):
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
                     "by_case_class": by_class, "warm_mlp_streamed": streamed,
                     "warm_mlp_lr_longest_first_queue": lpt, "unsteady_capped_protocol": capped_proto,
-                    "plain_batched_naca0012_config3": plain3},
+                    "plain_batched_naca0012_config3": plain3, "per_case": per_case},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",
