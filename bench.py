@@ -745,6 +745,18 @@ def run_warm(args, world, rank, local):
         barrier(world)
         r = wf.solve(me, ae, truth, steady, start)
         per_case[start] = case_record(r.results)
+    # converged cases and steps by Mach band, per start (this rank's cases)
+    bands = [(0.7, 0.9), (0.9, 1.2), (1.2, 1.6), (1.6, 2.2), (2.2, 3.01)]
+    by_band = []
+    for lo, hi in bands:
+        sel = [i for i, m in enumerate(me) if lo <= m < hi]
+        row = {"mach": [lo, min(hi, 3.0)], "cases": len(sel), "steady": int(sum(bool(steady[i]) for i in sel))}
+        for start in ("mlp", "idw", "cold"):
+            rec = per_case[start]
+            row[start] = {"converged": int(sum(rec["converged"][i] for i in sel)),
+                          "steps": int(sum(rec["steps"][i] for i in sel)),
+                          "fallbacks": int(sum(rec["fallback"][i] for i in sel))}
+        by_band.append(row)
         base[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
         base[start + "_detail"] = {"converged": r.converged, "seconds": r.seconds,
                                    "median_iterations": float(np.median(r.iterations)), "parts_s": r.parts_s}
@@ -769,7 +781,8 @@ def run_warm(args, world, rank, local):
                     sum(x["warm_steps"] for x in fallbacks) / max(steps_warm.sum(), 1)),
                 "warm_step_share_of_capped_cases": float(steps_warm[capped].sum() / max(steps_warm.sum(), 1)),
                 "steady_only_warm_mlp_batched": cls.get("mlp"), "steady_only_plain_single_case": cls.get("single"),
-                "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None}
+                "steady_only_ratio": (cls["mlp"] / cls["single"]) if cls.get("single") else None,
+                "by_mach_band": by_band}
     # the same warm pass with the HR cases queued longest-first by their LR solve
     flush.add_(1.0)
     barrier(world)
