@@ -33,8 +33,8 @@ the held-out cases one at a time from freestream with the same rule, on all
 host threads (reference CDs from tests/golden/warm_bench_truth.json, which
 ``--make-truth`` writes from the float64 GPU solves).
 
---workload naca / ragged / diamond: the throughput workloads alone (config 3
-batched, config 4 ragged multi-mesh batch, configs 1-2 single diamond case).
+--workload naca / ragged / diamond: the throughput workloads alone (NACA0012
+h=0.025 x 256 cases, the 12-mesh ragged batch of 1,024 cases, one diamond case).
 
 Under torchrun every rank runs its own held-out shard (weak scaling; cases
 are independent, no data-path collective); times are the max over ranks.
@@ -355,8 +355,8 @@ def run_single(args, world, rank, local):
 
 
 def run_throughput(args, world, rank, local, report=True):
-    """The batched throughput workloads (config 3 batched NACA0012, config 4
-    ragged): cell-updates/s of fixed 50-step chunks, the K2 roofline and the
+    """The batched throughput workloads (NACA0012 h=0.025 x 256 cases, the
+    12-mesh ragged batch): cell-updates/s of fixed 50-step chunks, the K2 roofline and the
     end-to-end rate with host fields. Prints its own line when `report`, and
     returns the measurements."""
     from eulersr_b200.parallel import case_cost, shard_cases
@@ -538,7 +538,7 @@ PLAIN_TRUTH_FILE = ROOT / "tests" / "golden" / "naca0012_bench_truth.json"
 
 
 def run_plain_converged(args, world, rank, local, make_truth=False):
-    """Config 3's batch solved to the stop rule: the 256 NACA0012 h=0.025
+    """The throughput workload's batch solved to the stop rule: the 256 NACA0012 h=0.025
     cases of the throughput workload (per GPU), freestream starts, through
     esr_batch_solve with retire/refill (the warm pipeline's 32 HR slots), each
     stopped once its CD stayed within 0.5 % of its float64 reference for 8
@@ -586,7 +586,7 @@ def run_plain_converged(args, world, rank, local, make_truth=False):
             "converged": r.converged, "seconds": r.seconds, "slots": args.slots,
             "median_iterations": float(np.median(r.iterations)), "references_computed_here": len(todo),
             "references_s": truth_s,
-            "workload": "config 3's NACA0012 h=0.025 cases (Mach~U[0.7,3] seed 1, alpha on the 0.5-degree grid) "
+            "workload": "the throughput workload's 256 NACA0012 h=0.025 cases (Mach~U[0.7,3] seed 1, alpha on the 0.5-degree grid) "
                         "from freestream through esr_batch_solve, 0.5 % CD rule, 12,000-step cap"}
 
 
@@ -835,7 +835,7 @@ def run_warm(args, world, rank, local):
     wf.close()
     del flush
     torch.cuda.empty_cache()
-    # config 3's batch solved to the same CD rule from freestream
+    # the throughput workload's 256 NACA0012 cases solved to the same CD rule from freestream
     pargs = argparse.Namespace(**vars(args))
     pargs.cases = 256
     plain3 = run_plain_converged(pargs, world, rank, local)
@@ -883,7 +883,7 @@ def run_warm(args, world, rank, local):
                     "details": {k: base[k + "_detail"] for k in ("single", "cold", "idw")},
                     "by_case_class": by_class, "warm_mlp_streamed": streamed,
                     "warm_mlp_lr_longest_first_queue": lpt, "unsteady_capped_protocol": capped_proto,
-                    "plain_batched_naca0012_config3": plain3, "per_case": per_case},
+                    "plain_batched_naca0012_x256": plain3, "per_case": per_case},
                 "e2e": e2e, "roofline": thr["roofline"],
                 "cell_updates": {k: thr[k] for k in ("value", "unit", "ms_per_step", "alg_gbs_per_step",
                                                       "alg_bytes_per_cell_update", "e2e", "kernel_times_ms",
@@ -921,7 +921,7 @@ def main():
                          "start (0: skip the leg)")
     ap.add_argument("--make-truth", action="store_true", help="write the held-out cases' reference CDs and exit")
     ap.add_argument("--make-plain-truth", action="store_true",
-                    help="write the reference CDs of config 3's NACA0012 cases and exit")
+                    help="write the reference CDs of the throughput workload's NACA0012 cases and exit")
     ap.add_argument("--block", default="0", help="throughput workloads: 0 (autotuned), 64, 128, 256 or patches")
     args = ap.parse_args()
     args.block = args.block if args.block == "patches" else int(args.block)

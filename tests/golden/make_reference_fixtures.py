@@ -24,7 +24,7 @@ seeded inputs and stores inputs and outputs in ``reference_utils.npz``:
   CD, CL and entropy created, plus 10 steps of the diamond with the Rusanov
   flux, constant reconstruction, explicit Euler and RK2, into
   ``reference_solver.npz``; the same 20 steps on the HR diamond of the
-  north-star workload (h = 0.025 by the package's mesher, 19,384 cells,
+  single-case HR workload (h = 0.025 by the package's mesher, 19,384 cells,
   M 2.0, alpha 0) in float32 and float64 into ``reference_solver_hr.npz``
   (``--hr-only`` writes just that one); and ``euler/main.py:43-270`` itself (the
   stepping loop with the stationarity rule, the engineering criterion and
@@ -261,8 +261,7 @@ def mesh_digest(mesh) -> str:
 
 
 def hr_fixture(ref_root: str) -> Path:
-    """The reference's own solver source on the HR diamond of the north-star
-    workload (h = 0.025, made by the package's mesher: 19,384 cells), M 2.0,
+    """The reference's own solver source on the HR diamond (h = 0.025, made by the package's mesher: 19,384 cells), M 2.0,
     alpha 0, CFL 0.6: 20 SRK2 steps in float32 and float64 with their dt,
     into ``reference_solver_hr.npz`` with the mesh's digest."""
     sys.path.insert(0, str(ROOT))

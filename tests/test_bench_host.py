@@ -187,8 +187,8 @@ def test_warm_shards_over_two_gloo_ranks():
     assert cmax - csum / 2 <= case_cost(me).max()
 
 
-def test_plain_truth_table_covers_config3_cases():
-    """The committed float64 references of config 3's NACA0012 cases (the
+def test_plain_truth_table_covers_throughput_cases():
+    """The committed float64 references of the throughput workload's NACA0012 cases (the
     bench's converged-cases leg reads them) cover exactly the 256 cases the
     throughput workload draws, with finite CDs and a steady flag each
     (subsonic inviscid cases have near-zero drag, a few slightly negative

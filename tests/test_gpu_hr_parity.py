@@ -1,4 +1,4 @@
-"""Parity at the north-star sizes, float32 rounded as the reference rounds it.
+"""Parity on the HR meshes (h = 0.025), float32 rounded as the reference rounds it.
 
 Config 2: the diamond at h = 0.025 (the package's mesher, 19,384 cells),
 M 2.0, alpha 0, CFL 0.6; and the NACA0012 h = 0.025 mesh of the batched

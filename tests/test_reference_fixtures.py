@@ -269,7 +269,7 @@ def test_oracle_run_equals_reference_main_loop(tag, name, prec):
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 def test_oracle_bitwise_equals_reference_solver_source_hr(prec):
-    """The same pin at the north-star's HR size: 20 SRK2 steps on the diamond
+    """The same pin at the HR size (h = 0.025): 20 SRK2 steps on the diamond
     h = 0.025 (19,384 cells, the package's mesher; the fixture records the
     mesh's digest), M 2.0, alpha 0, equal bit for bit to the reference's own
     source run with NumPy (tests/golden/reference_solver_hr.npz)."""
