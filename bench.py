@@ -745,21 +745,21 @@ def run_warm(args, world, rank, local):
         barrier(world)
         r = wf.solve(me, ae, truth, steady, start)
         per_case[start] = case_record(r.results)
+        base[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
+        base[start + "_detail"] = {"converged": r.converged, "seconds": r.seconds,
+                                   "median_iterations": float(np.median(r.iterations)), "parts_s": r.parts_s}
     # converged cases and steps by Mach band, per start (this rank's cases)
     bands = [(0.7, 0.9), (0.9, 1.2), (1.2, 1.6), (1.6, 2.2), (2.2, 3.01)]
     by_band = []
     for lo, hi in bands:
         sel = [i for i, m in enumerate(me) if lo <= m < hi]
         row = {"mach": [lo, min(hi, 3.0)], "cases": len(sel), "steady": int(sum(bool(steady[i]) for i in sel))}
-        for start in ("mlp", "idw", "cold"):
-            rec = per_case[start]
-            row[start] = {"converged": int(sum(rec["converged"][i] for i in sel)),
-                          "steps": int(sum(rec["steps"][i] for i in sel)),
-                          "fallbacks": int(sum(rec["fallback"][i] for i in sel))}
+        for name in ("mlp", "idw", "cold"):
+            rec = per_case[name]
+            row[name] = {"converged": int(sum(rec["converged"][i] for i in sel)),
+                         "steps": int(sum(rec["steps"][i] for i in sel)),
+                         "fallbacks": int(sum(rec["fallback"][i] for i in sel))}
         by_band.append(row)
-        base[start] = allreduce_sum(float(r.converged), world) / allreduce_max(r.seconds, world)
-        base[start + "_detail"] = {"converged": r.converged, "seconds": r.seconds,
-                                   "median_iterations": float(np.median(r.iterations)), "parts_s": r.parts_s}
     # by case class: the cases whose reference settles, alone (the cases that
     # never settle cost every start the whole step cap)
     cls = {}
