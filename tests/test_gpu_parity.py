@@ -325,6 +325,15 @@ def test_autotuner_and_block_invariance(naca02):
         s.set_shape(96)
     with pytest.raises(EsrError):
         s.set_shape(64, False, 7, 0)
+    # a submitted batch owns the slots: the shape cannot change under it
+    s.batch_submit([FlowCase(mach=1.5, aoa_deg=1.0, tf=0.2, max_steps=40, dtype=np.float32)])
+    with pytest.raises(EsrError):
+        s.set_shape(128)
+    while s.batch_poll() < 1:
+        pass
+    res, _ = s.batch_results()
+    assert len(res) == 1
+    s.set_shape(128)
 
 
 def test_set_cases_get_states_match_per_slot_calls(diamond02, naca02):
