@@ -538,3 +538,16 @@ def test_overlapped_transfers_equal_synchronous(diamond02, naca02, layout):
         pipe.apply_staged()      # nothing staged
     sync.close()
     pipe.close()
+
+
+def test_solver_refuses_cells_times_slots_beyond_2_31(diamond02):
+    """The item index of a mesh (cell x slots + slot) is 32-bit in the
+    kernels: a solver whose cells x slots reach 2^31 is refused with
+    ESR_ERR_ARG at creation, before its state arrays are allocated."""
+    from eulersr_b200._ffi import EsrError
+    from eulersr_b200.solver import Solver
+    n = diamond02.n_cells
+    slots = (2 ** 31 + n - 1) // n           # n * slots >= 2^31
+    with pytest.raises(EsrError) as e:
+        Solver(diamond02, slots, precision='f32', block_size=128)
+    assert e.value.code == 1 and "2^31" in str(e.value)
