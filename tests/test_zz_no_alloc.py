@@ -87,3 +87,25 @@ def test_rel_change_noalloc_rejects_host_and_misaligned_pointers():
         assert what in L.esr_last_error(), L.esr_last_error()
     torch.cuda.synchronize()
     assert float(out.abs().sum().item()) == 0.0      # nothing was launched
+
+
+def test_rel_change_noalloc_at_its_maximum_size():
+    """At the largest accepted size (2,097,152 rows, every block of the fixed
+    array in use) the float64 and float32 forms agree with the same statistic
+    computed by torch in float64, on two calls in a row."""
+    import torch
+    from eulersr_b200 import _ffi as F
+    L = F.lib()
+    n = 2 ** 21
+    g = torch.Generator(device='cuda').manual_seed(11)
+    out = torch.zeros(1, dtype=torch.float64, device='cuda')
+    for prec, dt in ((1, torch.float64), (0, torch.float32)):
+        A = torch.rand((n, 4), generator=g, device='cuda', dtype=torch.float64).to(dt)
+        B = torch.rand((n, 4), generator=g, device='cuda', dtype=torch.float64).to(dt)
+        want = float(torch.linalg.norm((A.double() - B.double()).flatten()) /
+                     (torch.linalg.norm(B.double().flatten()) + 1e-16))
+        for call in range(2):
+            F.check(L.esr_rel_change_noalloc(C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()), n, prec,
+                                             C.c_void_p(out.data_ptr()), None))
+            torch.cuda.synchronize()
+            assert abs(float(out.item()) - want) <= TOL * want, (prec, call)
