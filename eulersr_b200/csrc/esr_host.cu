@@ -133,12 +133,21 @@ struct SolverT : SolverBase {
   DevBuf<int2> d_blk;
   int n_blk = 0;
   DevBuf<int4> d_live;   // per mesh segment: live slots (A, divider of A)
+  std::vector<int4> h_live_poll;   // its host copy at a batch poll
   std::vector<int4> h_live_full;   // A = B for every segment
   DevBuf<int4> d_pblk;   // K2 by patches: (mesh segment, patch, first slot) per block
   int n_pblk = 0;
   bool use_patch = false;
   // second register budget of each fast float32 kernel (autotuned)
   bool k1_alt = false, k2_alt = false, kp_alt = false;
+  // K2 per cell for a batch's tail: once few cases run, a patch block's lanes
+  // (one per slot of a 32-slot group) are mostly idle while the per-cell K2
+  // maps its threads onto the live slots alone; both give the same bits
+  bool tail_cell_k2 = false;
+#ifndef ESR_TAIL_SLOTS
+#define ESR_TAIL_SLOTS 24
+#endif
+  static constexpr int kTailSlots = ESR_TAIL_SLOTS;   // live slots per mesh at or below which the tail form runs
   DevBuf<int> d_case_seg, d_case_slot, d_ncells;
 
   DevBuf<V> W, Wa, Wref, FV, Wp;   // Wp: probe step output (batch solves)
@@ -693,7 +702,7 @@ struct SolverT : SolverBase {
         ++launches;
         return;
       }
-      if (use_patch && n_pblk > 0) {   // eligible by construction: HLLC + MUSCL, fast fidelity
+      if (use_patch && !tail_cell_k2 && n_pblk > 0) {   // eligible by construction: HLLC + MUSCL, fast fidelity
         tap_begin(1);
         if (local) launch_patch<STAGE, true>(win, wbase, wout, cs, pos);
         else launch_patch<STAGE, false>(win, wbase, wout, cs, pos);
@@ -1570,12 +1579,17 @@ struct SolverT : SolverBase {
     int n = 0;
     bool want_states = false;
     cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec_tail = nullptr;   // the same chunk with K2 per cell (K2 by patches solvers)
+    bool tail = false;                      // few live slots: the tail form runs
     int len = 0;
     int64_t per_chunk = 0;
     int poll = 4;
     long long guard = 0;
     int done = 0;
-    ~PendingBatch() { if (gexec) cudaGraphExecDestroy(gexec); }
+    ~PendingBatch() {
+      if (gexec) cudaGraphExecDestroy(gexec);
+      if (gexec_tail) cudaGraphExecDestroy(gexec_tail);
+    }
   };
   std::unique_ptr<PendingBatch> pend;
 
@@ -1746,6 +1760,19 @@ struct SolverT : SolverBase {
       cudaError_t e = cudaGraphInstantiate(&pb.gexec, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) { pb.gexec = nullptr; return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)); }
+      if (use_patch && n_pblk > 0) {   // the tail form: K2 per cell
+        ESR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        tail_cell_k2 = true;
+        const int64_t b2 = launches;
+        issue_run_chunk(pb.len);
+        issue_refill(pb.q, pb.sp, want_states);
+        launches = b2;
+        tail_cell_k2 = false;
+        ESR_CUDA(cudaStreamEndCapture(stream, &graph));
+        e = cudaGraphInstantiate(&pb.gexec_tail, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { pb.gexec_tail = nullptr; return fail(ESR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)); }
+      }
     }
     return ESR_OK;
   }
@@ -1758,19 +1785,33 @@ struct SolverT : SolverBase {
     int rc = ESR_OK;
     if (pb.done < pb.n) {
       for (int i = 0; i < pb.poll && rc == ESR_OK; ++i) {
-        if (pb.gexec) {
-          cudaError_t e = cudaGraphLaunch(pb.gexec, stream);
+        cudaGraphExec_t g = (pb.tail && pb.gexec_tail) ? pb.gexec_tail : pb.gexec;
+        if (g) {
+          cudaError_t e = cudaGraphLaunch(g, stream);
           if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
           else launches += pb.per_chunk;
         } else {
+          tail_cell_k2 = pb.tail;
           issue_run_chunk(pb.len);
           issue_refill(pb.q, pb.sp, pb.want_states);
+          tail_cell_k2 = false;
         }
       }
       if (rc == ESR_OK) {
+        // the done counter and, for K2 by patches, each mesh's live slots
+        const bool watch = use_patch && n_pblk > 0;
+        h_live_poll.resize(meshes.size());
         cudaError_t e = cudaMemcpyAsync(&pb.done, pb.Bp->n_done.p, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && watch)
+          e = cudaMemcpyAsync(h_live_poll.data(), d_live.p, meshes.size() * sizeof(int4), cudaMemcpyDeviceToHost,
+                              stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) rc = fail(ESR_ERR_CUDA, std::string("batch poll: ") + cudaGetErrorString(e));
+        if (rc == ESR_OK && watch) {
+          bool few = true;
+          for (const int4& L : h_live_poll) few = few && L.x <= kTailSlots;
+          pb.tail = few;
+        }
       }
       pb.poll = std::min(pb.poll * 2, 32);
       if (rc == ESR_OK && ++pb.guard > (1LL << 40)) rc = fail(ESR_ERR_STATE, "batch: no progress");
