@@ -353,7 +353,10 @@ int esr_solver_set_shape(esr_solver* solver, const esr_tuning_variant* shape);
 /* Solve n_cases cases through the solver's slots: every slot retired by the
  * stop rule is refilled in place with the next queued case. init_fields[i]
  * is a (n_cells,4) conserved warm start or NULL; final_states[i] receives the
- * final state when non-NULL. results has n_cases entries. */
+ * final state when non-NULL. results has n_cases entries. A solver on K2 by
+ * patches runs the batch's tail (every mesh down to 24 running cases or
+ * fewer) with the per-cell K2, whose threads cover the running slots alone;
+ * the results are the same. */
 int esr_batch_solve(esr_solver* solver, const esr_case* cases, int32_t n_cases,
                     const double* const* init_fields, double* const* final_states,
                     esr_result* results);
