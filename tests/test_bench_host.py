@@ -203,76 +203,90 @@ def test_plain_truth_table_covers_throughput_cases():
     assert all(np.isfinite(r["cd"]) and abs(r["cd"]) < 1.0 and isinstance(r["steady"], bool) for r in rows)
 
 
+class _FakeWF:
+    """Stands in for the GPU warm-start workflow: fixed step counts per start,
+    every fifth case capped, every seventh a fallback."""
+
+    def __init__(self, **kw):
+        self.cd_tol, self.schedule, self.unsteady_cap, self.warm_budget = 0.005, "fifo", None, 3000
+        self.hr = types.SimpleNamespace(n_cells=100)
+        self.lr = types.SimpleNamespace(n_cells=20)
+        self.calls = []
+
+    def prepare(self, **kw):
+        return {"n_train": kw.get("n_train")}
+
+    def truth(self, me, ae):
+        return np.full(len(me), 0.05), np.arange(len(me)) % 4 != 0
+
+    def solve(self, me, ae, truth, steady, start="mlp", want_states=False):
+        from eulersr_b200.warmstart import workflow as W
+        self.calls.append(start)
+        n = len(me)
+        steps = {"mlp": 900, "idw": 1200, "cold": 2800, "single": 2800}[start]
+        res = [{"status": 2 if i % 5 else 3, "cd": float(truth[i]), "cl": 0.0, "steps": steps,
+                "stopping_step": steps, **({"fallback": True, "warm_steps": 3000} if i % 7 == 0 else {})}
+               for i in range(n)]
+        conv = sum(1 for i in range(n) if res[i]["status"] == 2 and steady[i])
+        sec = {"mlp": 1.0, "idw": 1.2, "cold": 1.5, "single": 10.0}[start]
+        return W.PassResult(start, res, conv, sec, sec, {"hr_solve_s": sec}, [steps] * n,
+                            [np.zeros((100, 4))] * n if want_states else None)
+
+    def solve_stream(self, batches, truth_of, steady_of, use_mlp=True):
+        out = [self.solve(m, a, t, s) for (m, a), t, s in zip(batches, truth_of, steady_of)]
+        return out, 0.9 * len(out), 0.9 * len(out)
+
+    def kernel_launches(self):
+        return 10 * len(self.calls)
+
+    def close(self):
+        pass
+
+
+class _FakeClock:
+    def __init__(self, *a):
+        pass
+
+    def start(self):
+        pass
+
+    def stop(self):
+        return {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 3}
+
+
+def _install_warm_fakes(put):
+    """The headline path's GPU pieces replaced by fakes (put = setattr, or
+    pytest's monkeypatch.setattr)."""
+    import torch
+    from eulersr_b200.warmstart import workflow as W
+    thr = {"value": 1e10, "unit": "cell-updates/s", "ms_per_step": 25.0, "alg_gbs_per_step": 1.0,
+           "alg_bytes_per_cell_update": 80.5, "e2e": {"value": 9e9}, "kernel_times_ms": {}, "config": {},
+           "roofline": {"frac": 0.28}, "gpu_launches": 400}
+    put(W, "WarmStartWorkflow", _FakeWF)
+    put(bench, "ClockSampler", _FakeClock)
+    put(bench, "run_throughput", lambda *a, **k: dict(thr))
+    put(bench, "run_plain_converged", lambda *a, **k: {"value": 50.0})
+    put(torch.cuda, "set_device", lambda *a: None)
+    put(torch.cuda, "synchronize", lambda *a: None)
+    put(torch.cuda, "empty_cache", lambda *a: None)
+    real_empty = torch.empty
+    put(torch, "empty", lambda *a, **k: real_empty(8, dtype=k.get("dtype")))
+
+
+def _warm_args():
+    return types.SimpleNamespace(slots=32, max_steps=12000, lr_steps=2000, warm_budget=3000, make_truth=False,
+                                 n_train=16, n_eval=12, target_steps=100, train_steps=10, steps=2, warmup=3,
+                                 unsteady_cap=3000, no_cpu=True, workload="warm", cases=256, chunk=50, h=0.025,
+                                 block=0, no_e2e=False, precision="f32", make_plain_truth=False)
+
+
 def test_warm_headline_line_on_fakes(monkeypatch, capsys):
     """The headline workload end to end on CPU with a fake workflow in place
     of the GPU one: every leg runs, and the JSON line carries the contract's
     keys, the ratios and the per-case / by-class breakdowns."""
     import json
-    import torch
-    from eulersr_b200.warmstart import workflow as W
-
-    class FakeWF:
-        def __init__(self, **kw):
-            self.cd_tol, self.schedule, self.unsteady_cap, self.warm_budget = 0.005, "fifo", None, 3000
-            self.hr = types.SimpleNamespace(n_cells=100)
-            self.lr = types.SimpleNamespace(n_cells=20)
-            self.calls = []
-
-        def prepare(self, **kw):
-            return {"n_train": kw.get("n_train")}
-
-        def truth(self, me, ae):
-            return np.full(len(me), 0.05), np.arange(len(me)) % 4 != 0
-
-        def solve(self, me, ae, truth, steady, start="mlp", want_states=False):
-            self.calls.append(start)
-            n = len(me)
-            steps = {"mlp": 900, "idw": 1200, "cold": 2800, "single": 2800}[start]
-            res = [{"status": 2 if i % 5 else 3, "cd": float(truth[i]), "cl": 0.0, "steps": steps,
-                    "stopping_step": steps, **({"fallback": True, "warm_steps": 3000} if i % 7 == 0 else {})}
-                   for i in range(n)]
-            conv = sum(1 for i in range(n) if res[i]["status"] == 2 and steady[i])
-            sec = {"mlp": 1.0, "idw": 1.2, "cold": 1.5, "single": 10.0}[start]
-            return W.PassResult(start, res, conv, sec, sec, {"hr_solve_s": sec}, [steps] * n,
-                                [np.zeros((100, 4))] * n if want_states else None)
-
-        def solve_stream(self, batches, truth_of, steady_of, use_mlp=True):
-            out = [self.solve(m, a, t, s) for (m, a), t, s in zip(batches, truth_of, steady_of)]
-            return out, 0.9 * len(out), 0.9 * len(out)
-
-        def kernel_launches(self):
-            return 10 * len(self.calls)
-
-        def close(self):
-            pass
-
-    class FakeClock:
-        def __init__(self, *a):
-            pass
-
-        def start(self):
-            pass
-
-        def stop(self):
-            return {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 3}
-
-    thr = {"value": 1e10, "unit": "cell-updates/s", "ms_per_step": 25.0, "alg_gbs_per_step": 1.0,
-           "alg_bytes_per_cell_update": 80.5, "e2e": {"value": 9e9}, "kernel_times_ms": {}, "config": {},
-           "roofline": {"frac": 0.28}, "gpu_launches": 400}
-    monkeypatch.setattr(W, "WarmStartWorkflow", FakeWF)
-    monkeypatch.setattr(bench, "ClockSampler", FakeClock)
-    monkeypatch.setattr(bench, "run_throughput", lambda *a, **k: thr)
-    monkeypatch.setattr(bench, "run_plain_converged", lambda *a, **k: {"value": 50.0})
-    monkeypatch.setattr(torch.cuda, "set_device", lambda *a: None)
-    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a: None)
-    monkeypatch.setattr(torch.cuda, "empty_cache", lambda *a: None)
-    real_empty = torch.empty
-    monkeypatch.setattr(torch, "empty", lambda *a, **k: real_empty(8, dtype=k.get("dtype")))
-    args = types.SimpleNamespace(slots=32, max_steps=12000, lr_steps=2000, warm_budget=3000, make_truth=False,
-                                 n_train=16, n_eval=12, target_steps=100, train_steps=10, steps=2, warmup=3,
-                                 unsteady_cap=3000, no_cpu=True, workload="warm", cases=256, chunk=50, h=0.025,
-                                 block=0, no_e2e=False, precision="f32", make_plain_truth=False)
-    assert bench.run_warm(args, 1, 0, 0) == 0
+    _install_warm_fakes(monkeypatch.setattr)
+    assert bench.run_warm(_warm_args(), 1, 0, 0) == 0
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
                 "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "roofline", "cpu_baseline", "clocks",
@@ -284,3 +298,49 @@ def test_warm_headline_line_on_fakes(monkeypatch, capsys):
     assert sum(b["cases"] for b in c["by_case_class"]["by_mach_band"]) == 12
     assert c["plain_batched_naca0012_x256"] == {"value": 50.0}
     assert c["warm_mlp_streamed"]["batches"] == 2 and c["unsteady_capped_protocol"]["unsteady_cap_steps"] == 3000
+
+
+def _warm_rank_main(rank, world, port, q):
+    import contextlib
+    import datetime
+    import io
+    import os
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        _install_warm_fakes(setattr)
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            rc = bench.run_warm(_warm_args(), world, rank, 0)
+        q.put((rank, rc, buf.getvalue()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_warm_headline_over_two_gloo_ranks():
+    """The headline path under two ranks (gloo here, NCCL on GPUs), on the
+    fake workflow: both ranks take the same collective steps and finish, rank
+    0 alone prints the line, whose value is the converged cases of both ranks
+    over the slower rank's time."""
+    import json
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_warm_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=180) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, rc0, text0), (r1, rc1, text1) = out
+    assert (rc0, rc1) == (0, 0) and text1.strip() == ""
+    line = json.loads(text0.strip().splitlines()[-1])
+    assert line["n_gpus"] == 2
+    passes = line["converged_cases_per_s"]["warm_passes"]
+    assert line["value"] > 0 and len(passes) == 2
