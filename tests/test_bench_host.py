@@ -344,3 +344,102 @@ def test_warm_headline_over_two_gloo_ranks():
     assert line["n_gpus"] == 2
     passes = line["converged_cases_per_s"]["warm_passes"]
     assert line["value"] > 0 and len(passes) == 2
+
+
+class _FakeSolver:
+    """Stands in for the GPU solver in the throughput workload: each chunk
+    'takes' 25 ms; transfers and tuning are no-ops."""
+
+    def __init__(self, meshes, slots, **kw):
+        self.n = int(slots) if np.isscalar(slots) else int(sum(slots))
+        self.cells = 1000
+
+    def set_cases(self, slots, cases, fields=None):
+        pass
+
+    def synchronize(self):
+        pass
+
+    def tuning(self):
+        return {"block_size": 128, "k2_patches": True, "step_ms": {}, "variants": []}
+
+    def step(self, n):
+        self.last = n
+
+    def elapsed_ms(self):
+        return 25.0
+
+    def kernel_launches(self):
+        return 0
+
+    def profile_step(self, n=8):
+        return {"recon_ms": 0.11, "flux_ms": 0.14, "other_ms": 0.0, "recon_launches": 1, "flux_launches": 1,
+                "other_launches": 0}
+
+    def _n_cells(self, b):
+        return self.cells
+
+    def stage_cases(self, slots, cases, fields):
+        pass
+
+    def apply_staged(self):
+        pass
+
+    def fetch_states(self, slots, out):
+        return out
+
+    def wait_transfers(self):
+        pass
+
+    def close(self):
+        pass
+
+
+def _throughput_rank_main(rank, world, port, q):
+    import contextlib
+    import datetime
+    import io
+    import os
+    import torch.distributed as dist
+    from eulersr_b200 import solver as S
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        setattr(S, "Solver", _FakeSolver)
+        setattr(S, "DeviceMesh", lambda m: m)
+        setattr(bench, "ClockSampler", _FakeClock)
+        setattr(bench, "get_mesh", lambda geom, h: types.SimpleNamespace(n_cells=1000, geom=geom, h=h))
+        args = types.SimpleNamespace(workload="naca", cases=64, chunk=50, h=0.025, steps=2, warmup=3, block=0,
+                                     no_e2e=False, no_cpu=True, gpus=world)
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            out = bench.run_throughput(args, world, rank, 0, report=True)
+        q.put((rank, out["value"], out["config"]["cases_this_rank"], buf.getvalue()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_throughput_over_two_gloo_ranks():
+    """The throughput workload under two ranks on a fake solver: each rank
+    takes its share of the cases by the cost-balanced scheduler, the value is
+    every rank's cell-updates over the slower rank's time, and rank 0 alone
+    prints the line."""
+    import json
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_throughput_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=180) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, v0, n0, text0), (r1, v1, n1, text1) = out
+    assert n0 + n1 == 128 and v0 == v1
+    assert v0 == 1000 * 128 * 50 * 2 / (2 * 25.0 * 1e-3)
+    assert text1.strip() == "" and json.loads(text0.strip().splitlines()[-1])["n_gpus"] == 2
